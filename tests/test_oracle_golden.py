@@ -1,0 +1,135 @@
+"""Pin the CPU oracle against the reference's own CDKLM16 golden vectors.
+
+The cases are those of gpu_ocean/tests/schemes/CDKLM16_test.py:154-421
+(nx=50, ny=70, dx=dy=200, dt=0.9, sim.step(50.0)); the expected fields are
+the reference's gpu_ocean/tests/timestep50/CDKLM16_*.dat, stored in
+tests/golden/cdklm16_timestep50.npz by tests/golden/make_golden.py.
+
+Criterion: the reference's own check (CDKLM16_test.py:114-145), the signed
+maximum of (result - ref) / max|ref| over the interior rounded to 3 places,
+plus a tighter bound on the absolute maximum (1e-4), which the FP64
+transcription meets on every case.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import cdklm16_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "cdklm16_timestep50.npz")
+
+
+def _golden():
+    return np.load(GOLD)
+
+
+def _run_case(d, name, dtype=np.float64, f_rows=None):
+    nx, ny, dx, dy, dt, g, T = d["setup"]
+    nx, ny = int(nx), int(ny)
+    f, beta = d[name + "/f_beta"]
+    eta0 = d[name + "/eta0"]
+    z = np.zeros_like(eta0)
+    sim = O.OracleSim(eta0, z, z, d[name + "/Hi"], nx, ny, dx, dy, float(dt), g, f, 0.0,
+                      coriolis_beta=beta, bc=tuple(int(b) for b in d[name + "/bc"]), dtype=dtype)
+    if f_rows is not None:
+        sim.f_rows = f_rows
+    sim.step(float(T))
+    return sim
+
+
+def _errors(sim, d, name):
+    out = []
+    for a, key in zip(sim.download(), ("eta", "hu", "hv")):
+        ref = d[name + "/" + key].astype(np.float64)
+        diff = a[2:-2, 2:-2].astype(np.float64) - ref[2:-2, 2:-2]
+        scale = np.max(np.abs(ref))
+        out.append((np.max(diff) / scale, np.max(np.abs(diff)) / scale))
+    return out
+
+
+NON_BETA = [
+    "wall_central", "wall_corner", "wall_upperCorner",
+    "periodic_central", "periodic_corner", "periodic_upperCorner",
+    "periodicNS_central", "periodicNS_corner", "periodicNS_upperCorner",
+    "periodicEW_central", "periodicEW_corner", "periodicEW_upperCorner",
+    "coriolis_central", "bathymetry_central",
+]
+
+
+@pytest.mark.parametrize("name", NON_BETA)
+def test_oracle_matches_reference_golden(name):
+    d = _golden()
+    sim = _run_case(d, name)
+    assert sim.num_iterations == 56  # 55 steps of f32(0.9) and one short step
+    for signed, absmax in _errors(sim, d, name):
+        assert round(signed, 3) == 0.0          # the reference's own criterion
+        assert absmax < 1e-4                     # and tighter
+
+
+def test_oracle_betamodel_golden_era_coriolis_table():
+    """The beta-plane golden file matches f(j) = f + beta*(j + 0.5)*dy per
+    ghost-inclusive row j (no constructor compensation).  The current host
+    code of the reference builds f(j) = f - 2*beta*dy + beta*(j - 1.5)*dy
+    (CDKLM16.py:146-148, 325-330) and misses its own golden file by ~4e-2,
+    which the second half of this test records."""
+    d = _golden()
+    name = "betamodel_central"
+    f, beta = d[name + "/f_beta"]
+    ny, dy = int(d["setup"][1]), float(d["setup"][3])
+    rows = (f + beta * (np.arange(ny + 4) + 0.5) * dy).astype(np.float32)
+    sim = _run_case(d, name, f_rows=rows)
+    for signed, absmax in _errors(sim, d, name):
+        assert round(signed, 3) == 0.0
+        assert absmax < 1e-4
+    current = _run_case(d, name)
+    worst = max(a for _, a in _errors(current, d, name))
+    assert 1e-2 < worst < 1e-1
+
+
+def test_oracle_float32_close_to_float64():
+    d = _golden()
+    a = _run_case(d, "wall_corner", dtype=np.float64).download()
+    b = _run_case(d, "wall_corner", dtype=np.float32).download()
+    for x, y in zip(a, b):
+        rel = np.max(np.abs(x[2:-2, 2:-2] - y[2:-2, 2:-2])) / np.max(np.abs(x[2:-2, 2:-2]))
+        assert rel < 2e-4
+
+
+def test_oracle_wall_mass_conservation():
+    """Known answer: the interior sum of the wall-central eta golden file is
+    pi/4 * 10 (= 7.85398), the initial bump volume; walls conserve it."""
+    d = _golden()
+    gold_sum = float(np.sum(d["wall_central/eta"][2:-2, 2:-2].astype(np.float64)))
+    assert abs(gold_sum - 7.85398) < 1e-4
+    sim = _run_case(d, "wall_central")
+    s0 = float(np.sum(d["wall_central/eta0"][2:-2, 2:-2].astype(np.float64)))
+    s1 = float(np.sum(sim.download()[0][2:-2, 2:-2]))
+    assert abs(s1 - s0) < 1e-9 * abs(s0) + 1e-10
+
+
+def test_init_bm_and_corner_fix_periodic_wrap():
+    rng = np.random.default_rng(0)
+    nx, ny = 9, 7
+    Hi = (50 + rng.random((ny + 5, nx + 5))).astype(np.float32)
+    Hi2 = O.fix_bi_ghost_corners(Hi, nx, ny, (2, 2, 2, 2))
+    # corner row/col c is identified with c +- n
+    assert np.array_equal(Hi2[0:2], Hi2[ny:ny + 2])
+    assert np.array_equal(Hi2[ny + 2:ny + 5], Hi2[2:5])
+    assert np.array_equal(Hi2[:, 0:2], Hi2[:, nx:nx + 2])
+    Bm = O.init_bm(Hi2)
+    assert np.array_equal(Bm[:, 0:2], Bm[:, nx:nx + 2])
+    Hi3 = O.fix_bi_ghost_corners(Hi, nx, ny, (1, 1, 1, 1))
+    assert np.array_equal(Hi3[0], Hi3[4]) and np.array_equal(Hi3[1], Hi3[3])
+    assert np.array_equal(Hi3[:, nx + 4], Hi3[:, nx]) and np.array_equal(Hi3[:, nx + 3], Hi3[:, nx + 1])
+
+
+def test_init_bm_land_mask():
+    Hi = np.full((6, 6), 10.0, dtype=np.float32)
+    Hi[0:3, 0:3] = O.LAND_VALUE
+    Bm = O.init_bm(Hi)
+    assert Bm[0, 0] == np.float32(O.LAND_VALUE)
+    assert Bm[1, 1] == np.float32(O.LAND_VALUE)
+    # two wet corners out of four: mean of the wet ones
+    assert abs(Bm[2, 1] - 10.0) < 1e-5
