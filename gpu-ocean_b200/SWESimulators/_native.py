@@ -1,0 +1,172 @@
+"""ctypes binding of the in-tree C ABI (include/gocean.h, lib/libgocean.so).
+
+There is no CPU fallback: if the shared library is missing, or no CUDA
+device is present when a kernel is called, the call raises.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libgocean.so")
+
+GO_OK = 0
+GO_BC_WALL = 1
+GO_BC_PERIODIC = 2
+GO_FRICTION_QUADRATIC = 0
+GO_FRICTION_LINEAR = 1
+GO_STATUS_NONFINITE = 0x1
+
+_c_float_p = ctypes.c_void_p  # device pointers travel as integers
+
+
+class GoDomainDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("dx", ctypes.c_float), ("dy", ctypes.c_float),
+        ("g", ctypes.c_float), ("r", ctypes.c_float),
+        ("theta", ctypes.c_float),
+        ("desing_eps", ctypes.c_float), ("flux_slope_eps", ctypes.c_float),
+        ("depth_cutoff", ctypes.c_float),
+        ("rk_order", ctypes.c_int),
+        ("bc_north", ctypes.c_int), ("bc_east", ctypes.c_int),
+        ("bc_south", ctypes.c_int), ("bc_west", ctypes.c_int),
+        ("friction_law", ctypes.c_int),
+        ("north_x", ctypes.c_float), ("north_y", ctypes.c_float),
+    ]
+
+
+# name -> (restype, argtypes)
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+SIGNATURES = {
+    "go_domain_create": (_I, [ctypes.POINTER(GoDomainDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "go_domain_destroy": (_I, [_P]),
+    "go_domain_set_coriolis": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I]),
+    "go_domain_set_wind_uniform": (_I, [_P, _F, _F, _F, _F]),
+    "go_domain_set_wind_field": (_I, [_P, _P, _P, _P, _P, _I]),
+    "go_domain_set_tile": (_I, [_P, _I]),
+    "go_init_bathymetry": (_I, [_P, _P, _P, _I, _P, _I, _F]),
+    "go_boundary_condition": (_I, [_P, _P, _P, _P, _P, _I]),
+    "go_cdklm_swe_2D": (_I, [_P, _P, _F, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I,
+                             _P, _I, _P, _I, _F, _F, _I]),
+    "go_cdklm_step": (_I, [_P, _P, _I, _F, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F]),
+    "go_max_dt": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _F, _P]),
+    "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
+    "go_last_error": (ctypes.c_char_p, []),
+    "go_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+def load():
+    """Load lib/libgocean.so (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise NativeError("CUDA library %s is missing; build it with gpu-ocean_b200/build.py" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != GO_OK:
+        msg = load().go_last_error().decode()
+        raise NativeError("gocean error %d: %s" % (rc, msg))
+    return rc
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise NativeError("no CUDA device: the CDKLM16 step runs on the GPU only")
+    return torch
+
+
+def ptr(t):
+    return ctypes.c_void_p(int(t.data_ptr()))
+
+
+def stream_handle(stream):
+    if stream is None:
+        return ctypes.c_void_p(0)
+    return ctypes.c_void_p(int(stream.cuda_stream))
+
+
+def pack_bc(north, east, south, west):
+    """The packed boundary code of CDKLM16.callKernel (CDKLM16.py:620-624)."""
+    return (int(north) << 24) | (int(south) << 16) | (int(east) << 8) | int(west)
+
+
+class Domain:
+    """Owner of one go_domain handle (scheme constants, Coriolis table, wind)."""
+
+    def __init__(self, nx, ny, dx, dy, g, r=0.0, theta=1.3, desing_eps=0.1,
+                 flux_slope_eps=0.1, depth_cutoff=1.0e-5, bc=(1, 1, 1, 1),
+                 friction_law=GO_FRICTION_QUADRATIC, north=(0.0, 1.0), rk_order=2):
+        lib = load()
+        d = GoDomainDesc()
+        d.nx, d.ny = int(nx), int(ny)
+        d.dx, d.dy, d.g, d.r, d.theta = float(dx), float(dy), float(g), float(r), float(theta)
+        d.desing_eps, d.flux_slope_eps, d.depth_cutoff = float(desing_eps), float(flux_slope_eps), float(depth_cutoff)
+        d.rk_order = int(rk_order)
+        d.bc_north, d.bc_east, d.bc_south, d.bc_west = (int(b) for b in bc)
+        d.friction_law = int(friction_law)
+        d.north_x, d.north_y = float(north[0]), float(north[1])
+        h = ctypes.c_void_p()
+        check(lib.go_domain_create(ctypes.byref(d), ctypes.byref(h)))
+        self.desc = d
+        self.handle = h
+        self.nx, self.ny = int(nx), int(ny)
+        self.bc = tuple(int(b) for b in bc)
+        self.bc_packed = pack_bc(*self.bc)
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            load().go_domain_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_coriolis(self, f_rows):
+        a = np.ascontiguousarray(np.asarray(f_rows, dtype=np.float32).reshape(-1))
+        check(load().go_domain_set_coriolis(self.handle, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), a.size))
+
+    def set_wind_uniform(self, x_cur, x_next, y_cur, y_next):
+        check(load().go_domain_set_wind_uniform(self.handle, float(x_cur), float(x_next), float(y_cur), float(y_next)))
+
+    def set_wind_field(self, x_cur, x_next, y_cur, y_next):
+        """Four device tensors (ny, nx) float32 with a common row stride."""
+        if x_cur is None:
+            check(load().go_domain_set_wind_field(self.handle, None, None, None, None, 0))
+            return
+        pitch = x_cur.stride(0) * 4
+        for t in (x_next, y_cur, y_next):
+            assert t.stride(0) * 4 == pitch
+        check(load().go_domain_set_wind_field(self.handle, ptr(x_cur), ptr(x_next), ptr(y_cur), ptr(y_next), pitch))
+
+    def set_tile(self, rows_per_block):
+        check(load().go_domain_set_tile(self.handle, int(rows_per_block)))
+
+    def status(self, clear=False):
+        v = ctypes.c_uint32()
+        check(load().go_domain_status(self.handle, ctypes.byref(v), int(bool(clear))))
+        return int(v.value)

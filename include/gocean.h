@@ -1,0 +1,156 @@
+/*
+ * gocean.h -- C ABI of the B200-native CDKLM16 time step.
+ *
+ * Every entry point returns GO_OK (0) on success and a negative status
+ * otherwise; go_last_error() gives the message of the last failure on the
+ * calling thread.  No exception crosses this boundary.  Device pointers are
+ * caller-owned (the library never frees them); pitches are in BYTES, as in
+ * the reference's PyCUDA calls.  Entry points that take a stream are
+ * asynchronous on that stream unless their comment says otherwise.  A
+ * go_domain handle is not thread-safe: use one handle per host thread.
+ *
+ * Reference interfaces replaced (paths inside metno/gpu-ocean):
+ *   gpu_ocean/SWESimulators/gpu_kernels/CDKLM16_kernel.cu:429   cdklm_swe_2D
+ *   gpu_ocean/SWESimulators/gpu_kernels/max_dt.cu:42,147         per_block_max_dt, max_dt_reduction
+ *   gpu_ocean/SWESimulators/gpu_kernels/boundary_kernels.cu:35,76  periodicBoundary_NS/EW
+ *   gpu_ocean/SWESimulators/gpu_kernels/boundary_kernels.cu:121-246 *_boundary_intersections_*
+ *   gpu_ocean/SWESimulators/gpu_kernels/initBm_kernel.cu:38      initBm
+ *   gpu_ocean/SWESimulators/CDKLM16.py:179-228   #defines baked into the JIT module
+ *   gpu_ocean/SWESimulators/CDKLM16.py:494-598   step() RK2 launch sequence
+ */
+#ifndef GOCEAN_H
+#define GOCEAN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GO_OK 0
+#define GO_ERR_INVALID (-1)     /* bad argument (shape, pointer, pitch, code) */
+#define GO_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define GO_ERR_UNSUPPORTED (-3) /* valid in the reference, not built here */
+#define GO_ERR_NOMEM (-4)
+
+/* Boundary codes, gpu_ocean/SWESimulators/Common.py:824-857. */
+#define GO_BC_WALL 1
+#define GO_BC_PERIODIC 2
+
+/* Bottom friction law.  QUADRATIC is what the reference kernel compiles
+ * (CDKLM16_kernel.cu:884-900 without use_linear_friction); LINEAR is the
+ * #ifdef branch at CDKLM16_kernel.cu:885. */
+#define GO_FRICTION_QUADRATIC 0
+#define GO_FRICTION_LINEAR 1
+
+/* Device status word bits (go_domain_status). */
+#define GO_STATUS_NONFINITE 0x1u /* a written cell held NaN or Inf */
+
+typedef struct go_domain go_domain;
+
+/* Scheme constants of one domain: what the reference bakes into its JIT
+ * module as #defines (CDKLM16.py:179-191) plus the boundary codes it packs
+ * per launch (CDKLM16.py:620-624). */
+typedef struct go_domain_desc {
+    int nx, ny;            /* interior cells; arrays are (ny+4) x (nx+4) */
+    float dx, dy;          /* DX, DY */
+    float g;               /* GRAV */
+    float r;               /* FRIC */
+    float theta;           /* THETA (minmod), default 1.3 */
+    float desing_eps;      /* KPSIMULATOR_DESING_EPS, default 0.1 */
+    float flux_slope_eps;  /* KPSIMULATOR_FLUX_SLOPE_EPS, default 0.1 */
+    float depth_cutoff;    /* KPSIMULATOR_DEPTH_CUTOFF, default 1e-5 */
+    int rk_order;          /* 2 (Heun); 1 = forward Euler */
+    int bc_north, bc_east, bc_south, bc_west; /* GO_BC_* */
+    int friction_law;      /* GO_FRICTION_* */
+    float north_x, north_y;/* (sin a, cos a) of a constant grid angle a */
+} go_domain_desc;
+
+/* Create / destroy a domain handle.  Allocates a small device table
+ * (Coriolis per row) and a status word. */
+int go_domain_create(const go_domain_desc* desc, go_domain** out);
+int go_domain_destroy(go_domain* d);
+
+/* Coriolis parameter per ghost-inclusive row j = 0..ny+3, as the reference
+ * samples its f texture at cell centres (CDKLM16_kernel.cu:49-58;
+ * texture built at CDKLM16.py:310-351).  n == 1 sets an f-plane.
+ * Synchronous host->device copy. */
+int go_domain_set_coriolis(go_domain* d, const float* f_rows_host, int n);
+
+/* Uniform wind stress (kinematic, N/m^2 / rho_w): current and next values
+ * of the reference's 1x1 wind textures (common.cu:601-650).  The kernel
+ * forms wind_t*next + (1-wind_t)*current as the reference does. */
+int go_domain_set_wind_uniform(go_domain* d, float x_cur, float x_next,
+                               float y_cur, float y_next);
+
+/* Per-cell wind stress: four device arrays of ny x nx interior cells
+ * (caller-owned, pitch in bytes), the reference's wind textures sampled at
+ * each cell.  Pass NULL to return to uniform wind. */
+int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_next,
+                             const float* y_cur, const float* y_next, int pitch);
+
+/* Launch shape: rows per block strip (>= 4); 0 picks the default. */
+int go_domain_set_tile(go_domain* d, int rows_per_block);
+
+/* Bathymetry set-up (Common.py:1319-1389): fixes the ghost corners of Hi
+ * in place (periodic wrap or wall mirror, boundary_kernels.cu:121-246) and
+ * writes Bm = mean of the wet corners, land_value where all four are land
+ * (initBm_kernel.cu:38-107).  Hi is (ny+5) x (nx+5), Bm (ny+4) x (nx+4). */
+int go_init_bathymetry(go_domain* d, void* stream, float* Hi, int Hi_pitch,
+                       float* Bm, int Bm_pitch, float land_value);
+
+/* Periodic ghost-cell refresh, north-south then east-west
+ * (Common.py:1219-1239 -> boundary_kernels.cu:35-110).  Walls: no-op. */
+int go_boundary_condition(go_domain* d, void* stream, float* eta, float* hu,
+                          float* hv, int pitch);
+
+/* One Runge-Kutta sub-step: the drop-in for one cdklm_swe_2D launch
+ * (CDKLM16_kernel.cu:429-1006) followed by the periodic ghost refresh of
+ * its output that CDKLM16.step() issues after it (CDKLM16.py:539-540,
+ * 585-586).  Argument meaning follows the kernel: *0 is the input state,
+ * *1 the output; rk_step 1 reads Q^n from the output buffer at each cell
+ * and writes Q^{n+1} over it.  The three input arrays must share one
+ * pitch, as must the three outputs.  Hm is accepted for ABI parity and not
+ * read: the cell bathymetry is derived from Hi in the kernel.  The packed
+ * boundary code (north<<24 | south<<16 | east<<8 | west) must match the
+ * domain's. */
+int go_cdklm_swe_2D(go_domain* d, void* stream, float dt, int rk_step,
+                    const float* eta0, int eta0_pitch, const float* hu0, int hu0_pitch,
+                    const float* hv0, int hv0_pitch,
+                    float* eta1, int eta1_pitch, float* hu1, int hu1_pitch,
+                    float* hv1, int hv1_pitch,
+                    const float* Hi, int Hi_pitch, const float* Hm, int Hm_pitch,
+                    float land_value, float wind_stress_t, int boundary_conditions);
+
+/* n_steps Heun RK2 steps of size dt (CDKLM16.py:533-544 + 585-586):
+ * stage 0 h0 -> h1, stage 1 h1 -> h0 (in place).  The state ends in h0;
+ * h1 holds the last Q*. */
+int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_stress_t,
+                  float* eta0, float* hu0, float* hv0, int pitch0,
+                  float* eta1, float* hu1, float* hv1, int pitch1,
+                  const float* Hi, int Hi_pitch, float land_value);
+
+/* Exact CFL limit min over wet interior cells of 0.25*dx/|u +- c| and
+ * 0.25*dy/|v +- c| (max_dt.cu:42-194 without its block-reduction gap).
+ * Writes one float to dt_dev (device).  Not scaled by the Courant number
+ * (CDKLM16.updateDt multiplies on the host, CDKLM16.py:739). */
+int go_max_dt(go_domain* d, void* stream, const float* eta, const float* hu,
+              const float* hv, int pitch, const float* Bm, int Bm_pitch,
+              float land_value, float* dt_dev);
+
+/* Device status word (GO_STATUS_* bits) accumulated by the step kernels;
+ * synchronous read, optionally clearing it. */
+int go_domain_status(go_domain* d, uint32_t* status, int clear);
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* go_last_error(void);
+
+/* Library version string. */
+const char* go_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GOCEAN_H */

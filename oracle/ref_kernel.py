@@ -1,0 +1,138 @@
+"""Run the reference's own CDKLM16 kernel on the GPU (test oracle only).
+
+Loads a library built by oracle/build_ref.py and replays the host side of
+gpu_ocean/SWESimulators/CDKLM16.py for the RK2 path: Coriolis texture as
+the constructor builds it (CDKLM16.py:146-148, 310-345, full resolution),
+bathymetry (Common.py:1319-1389), eta0 = max(eta0, -Hm) (CDKLM16.py:237),
+and the step() loop (CDKLM16.py:494-598).  Arrays use the reference's
+unpadded pitch ((nx+4)*4 bytes, Common.py:546).
+
+Only tests, smoke() and bench.py's reference arm import this module.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build_ref
+from .cdklm16_oracle import coriolis_rows
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+
+def available(cfg, fmad=False):
+    return os.path.exists(build_ref.lib_name(cfg, fmad))
+
+
+def _load(cfg, fmad=False):
+    path = build_ref.lib_name(cfg, fmad)
+    if not os.path.exists(path):
+        raise FileNotFoundError("reference kernel library %s not built (oracle/build_ref.py)" % path)
+    lib = ctypes.CDLL(path)
+    lib.ref_config.argtypes = [ctypes.POINTER(_I), ctypes.POINTER(_I)] + [ctypes.POINTER(_F)] * 4
+    lib.ref_setup.argtypes = [ctypes.POINTER(_F), _I, _I, _F, _F, _F, _F, _F]
+    lib.ref_bathymetry.argtypes = [_P, _I, _I, _P, _I, _F, _P, _I]
+    lib.ref_boundary.argtypes = [_P, _I, _I, _P, _P, _P, _I]
+    lib.ref_stage.argtypes = [_P, _F, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _I, _F, _F, _I]
+    lib.ref_step.argtypes = [_P, _I, _F, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _I, _F, _I]
+    lib.ref_max_dt.argtypes = [_P, _P, _P, _P, _I, _P, _I, _F, _P, _P]
+    return lib
+
+
+def _chk(rc, what):
+    if rc != 0:
+        raise RuntimeError("reference kernel call %s failed with CUDA error %d" % (what, rc))
+
+
+def _p(t):
+    return ctypes.c_void_p(int(t.data_ptr()))
+
+
+class RefKernelSim:
+    """Reference CDKLM16 RK2 simulation on the GPU (wall/periodic, f- or
+    beta-plane, uniform wind, angle 0)."""
+
+    def __init__(self, cfg, eta0, hu0, hv0, Hi, dt, f, coriolis_beta=0.0, bc=(1, 1, 1, 1),
+                 wind=(0.0, 0.0), fmad=False, f_rows=None):
+        import torch
+        self.torch = torch
+        self.lib = _load(cfg, fmad)
+        nx, ny = cfg["nx"], cfg["ny"]
+        self.nx, self.ny = nx, ny
+        self.bc = tuple(int(b) for b in bc)
+        self.bc_packed = (self.bc[0] << 24) | (self.bc[2] << 16) | (self.bc[1] << 8) | self.bc[3]
+        if f_rows is None:
+            if coriolis_beta == 0.0:
+                ftex = np.array([[np.float32(f)]], dtype=np.float32)
+            else:
+                f_rows = coriolis_rows(f, coriolis_beta, ny, cfg["dy"])
+        if f_rows is not None:
+            ftex = np.ascontiguousarray(np.repeat(np.asarray(f_rows, np.float32)[:, None], nx + 4, axis=1))
+        fh, fw = ftex.shape
+        _chk(self.lib.ref_setup(ftex.ctypes.data_as(ctypes.POINTER(_F)), fw, fh, 0.0,
+                                float(wind[0]), float(wind[0]), float(wind[1]), float(wind[1])), "setup")
+        dev = "cuda"
+        self.stream = torch.cuda.current_stream()
+        s = ctypes.c_void_p(int(self.stream.cuda_stream))
+        self.s = s
+        self.Hi = torch.from_numpy(np.ascontiguousarray(Hi, dtype=np.float32)).to(dev)
+        self.Bm = torch.zeros((ny + 4, nx + 4), dtype=torch.float32, device=dev)
+        self.land = np.float32(1e20)
+        _chk(self.lib.ref_bathymetry(s, self.bc[0], self.bc[1], _p(self.Hi), (nx + 5) * 4, float(self.land),
+                                     _p(self.Bm), (nx + 4) * 4), "bathymetry")
+        Bm = self.Bm.cpu().numpy()
+        eta0 = np.maximum(np.asarray(eta0, np.float32), -Bm)
+        self.h0 = [torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(dev) for a in (eta0, hu0, hv0)]
+        self.h1 = [a.clone() for a in self.h0]
+        self.pitch = (nx + 4) * 4
+        self.dt = dt
+        self.t = 0.0
+        self.num_iterations = 0
+        self.dt_blocks = torch.zeros(((ny + 31) // 32) * ((nx + 11) // 12) + 1, dtype=torch.float32, device=dev)
+        self.dt_out = torch.zeros(1, dtype=torch.float32, device=dev)
+
+    def boundary(self, Q):
+        _chk(self.lib.ref_boundary(self.s, self.bc[0], self.bc[1], _p(Q[0]), _p(Q[1]), _p(Q[2]), self.pitch),
+             "boundary")
+
+    def run_steps(self, n, dt, wind_t=0.0):
+        h0, h1 = self.h0, self.h1
+        _chk(self.lib.ref_step(self.s, int(n), float(dt), float(wind_t), _p(h0[0]), _p(h0[1]), _p(h0[2]),
+                               self.pitch, _p(h1[0]), _p(h1[1]), _p(h1[2]), self.pitch, _p(self.Hi),
+                               (self.nx + 5) * 4, _p(self.Bm), self.pitch, float(self.land), self.bc_packed),
+             "step")
+
+    def stage(self, rk_step, dt, Qin, Qout, wind_t=0.0):
+        _chk(self.lib.ref_stage(self.s, float(dt), int(rk_step), _p(Qin[0]), _p(Qin[1]), _p(Qin[2]), self.pitch,
+                                _p(Qout[0]), _p(Qout[1]), _p(Qout[2]), self.pitch, _p(self.Hi), (self.nx + 5) * 4,
+                                _p(self.Bm), self.pitch, float(self.land), float(wind_t), self.bc_packed), "stage")
+
+    def step(self, t_end):
+        """CDKLM16.step(t_end) (CDKLM16.py:494-598) with constant wind."""
+        if self.t == 0:
+            self.boundary(self.h0)
+        t_now = 0.0
+        while t_now < t_end:
+            local_dt = np.float32(min(self.dt, np.float32(t_end - t_now)))
+            self.run_steps(1, local_dt)
+            self.t += np.float64(local_dt)
+            t_now += np.float64(local_dt)
+            self.num_iterations += 1
+        return self.t
+
+    def max_dt(self):
+        Q = self.h0
+        _chk(self.lib.ref_max_dt(self.s, _p(Q[0]), _p(Q[1]), _p(Q[2]), self.pitch, _p(self.Bm), self.pitch,
+                                 float(self.land), _p(self.dt_blocks), _p(self.dt_out)), "max_dt")
+        return float(self.dt_out.cpu().numpy()[0])
+
+    def download(self):
+        self.torch.cuda.synchronize()
+        return tuple(a.cpu().numpy() for a in self.h0)
+
+    def download_prev(self):
+        self.torch.cuda.synchronize()
+        return tuple(a.cpu().numpy() for a in self.h1)

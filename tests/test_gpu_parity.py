@@ -1,0 +1,260 @@
+"""Parity of the sm_100a CDKLM16 path on a GPU.
+
+Three checkers, as the north star asks:
+  1. the reference's own cdklm_swe_2D (oracle/_ref, rebuilt for sm_100a):
+     max |a - b| / max |b| per field after the stated number of steps;
+  2. the FP64 restatement (oracle/cdklm16_oracle.py, run as FP64 torch on
+     the GPU for speed): the error is printed and bounded;
+  3. mass conservation under walls.
+Plus the reference's own golden files (gpu_ocean/tests/timestep50) through
+the drop-in CDKLM16 class.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from SWESimulators import CDKLM16, Common, SyntheticCases as SC, _native  # noqa: E402
+from oracle import build_ref, ref_kernel  # noqa: E402
+from oracle import cdklm16_oracle as O  # noqa: E402
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "cdklm16_timestep50.npz")
+CASES = ["wall_central", "wall_corner", "wall_upperCorner", "periodic_central", "periodic_corner",
+         "periodic_upperCorner", "periodicNS_central", "periodicNS_corner", "periodicNS_upperCorner",
+         "periodicEW_central", "periodicEW_corner", "periodicEW_upperCorner", "coriolis_central",
+         "bathymetry_central"]
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return Common.CUDAContext()
+
+
+def rel_max(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    s = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / s) if s > 0 else float(np.max(np.abs(a - b)))
+
+
+def golden_sim(ctx, d, name, f_rows=None):
+    nx, ny, dx, dy, dt, g, T = d["setup"]
+    f, beta = d[name + "/f_beta"]
+    eta0 = d[name + "/eta0"]
+    z = np.zeros_like(eta0)
+    bc = Common.BoundaryConditions(*[int(b) for b in d[name + "/bc"]])
+    sim = CDKLM16.CDKLM16(ctx, eta0, z, z.copy(), d[name + "/Hi"], int(nx), int(ny), float(dx), float(dy),
+                          float(dt), float(g), float(f), 0.0, coriolis_beta=float(beta), boundary_conditions=bc)
+    if f_rows is not None:
+        sim._domain.set_coriolis(f_rows)
+    return sim, float(T)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_golden_files_through_drop_in_class(ctx, gold, name):
+    sim, T = golden_sim(ctx, gold, name)
+    sim.step(T)
+    assert sim.num_iterations == 56
+    eta, hu, hv = sim.download()
+    for a, key in ((eta, "eta"), (hu, "hu"), (hv, "hv")):
+        ref = gold[name + "/" + key].astype(np.float64)
+        diff = a[2:-2, 2:-2].astype(np.float64) - ref[2:-2, 2:-2]
+        scale = np.max(np.abs(ref))
+        assert round(float(np.max(diff) / scale), 3) == 0.0   # CDKLM16_test.py:114-145
+        assert np.max(np.abs(diff)) / scale < 1e-4
+
+
+def test_betamodel_golden_with_golden_era_coriolis(ctx, gold):
+    name = "betamodel_central"
+    f, beta = gold[name + "/f_beta"]
+    ny, dy = int(gold["setup"][1]), float(gold["setup"][3])
+    rows = (f + beta * (np.arange(ny + 4) + 0.5) * dy).astype(np.float32)
+    sim, T = golden_sim(ctx, gold, name, f_rows=rows)
+    sim.step(T)
+    for a, key in zip(sim.download(), ("eta", "hu", "hv")):
+        assert rel_max(a[2:-2, 2:-2], gold[name + "/" + key][2:-2, 2:-2]) < 1e-4
+
+
+def _ref_for(cfg_name, eta0, hu0, hv0, Hi, dt, f, beta, bc, wind=(0.0, 0.0), fmad=False):
+    cfg = build_ref.CONFIGS[cfg_name]
+    if not ref_kernel.available(cfg, fmad):
+        pytest.skip("reference kernel library not built")
+    return ref_kernel.RefKernelSim(cfg, eta0, hu0, hv0, Hi, dt, f, beta, bc, wind=wind, fmad=fmad)
+
+
+@pytest.mark.parametrize("name", ["wall_corner", "periodic_upperCorner", "periodicNS_corner",
+                                  "periodicEW_upperCorner", "coriolis_central", "bathymetry_central"])
+def test_matches_reference_kernel_on_golden_cases(ctx, gold, name):
+    """Full arrays, ghost cells included, after sim.step(50) (56 steps)."""
+    sim, T = golden_sim(ctx, gold, name)
+    sim.step(T)
+    mine = sim.download()
+    f, beta = gold[name + "/f_beta"]
+    eta0 = gold[name + "/eta0"]
+    z = np.zeros_like(eta0)
+    ref = _ref_for("golden", eta0, z, z, O.fix_bi_ghost_corners(gold[name + "/Hi"], 50, 70,
+                                                               tuple(gold[name + "/bc"])),
+                   float(gold["setup"][4]), float(f), float(beta), tuple(int(b) for b in gold[name + "/bc"]))
+    ref.step(T)
+    theirs = ref.download()
+    errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
+    print(name, "max rel diff vs reference kernel (eta, hu, hv):", errs)
+    assert max(errs) <= 1e-5
+    # periodic ghost cells equal the reference's after its BC kernels
+    bc = tuple(int(b) for b in gold[name + "/bc"])
+    if 2 in bc:
+        for a, b in zip(mine, theirs):
+            if bc[0] == 2:
+                assert rel_max(a[[0, 1, -2, -1], 2:-2], b[[0, 1, -2, -1], 2:-2]) <= 1e-5 + 1e-30
+            if bc[1] == 2:
+                assert rel_max(a[2:-2, [0, 1, -2, -1]], b[2:-2, [0, 1, -2, -1]]) <= 1e-5 + 1e-30
+
+
+def _drop_in(ctx, case):
+    kw = case.kwargs()
+    return CDKLM16.CDKLM16(ctx, dt=case.dt, **kw)
+
+
+def test_bump256_1000_steps_vs_reference_kernel_and_fp64(ctx):
+    """The parity workload: 256x256 bump, 1000 RK2 steps at CFL 0.7."""
+    c = SC.bump256()
+    sim = _drop_in(ctx, c)
+    for _ in range(c.steps):
+        sim.step(c.dt)
+    mine = sim.download()
+    assert sim.num_iterations == c.steps
+    ref = _ref_for("bump256", c.eta0, c.hu0, c.hv0, O.fix_bi_ghost_corners(c.Hi, c.nx, c.ny, c.bc), c.dt, c.f,
+                   0.0, c.bc)
+    for _ in range(c.steps):
+        ref.step(c.dt)
+    theirs = ref.download()
+    e_ref = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
+    # noise floor: the reference kernel against itself compiled with --fmad=true
+    floor = None
+    if ref_kernel.available(build_ref.CONFIGS["bump256"], True):
+        ref2 = _ref_for("bump256", c.eta0, c.hu0, c.hv0, O.fix_bi_ghost_corners(c.Hi, c.nx, c.ny, c.bc), c.dt,
+                        c.f, 0.0, c.bc, fmad=True)
+        for _ in range(c.steps):
+            ref2.step(c.dt)
+        floor = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(ref2.download(), theirs)]
+    fp64 = O.OracleSim(c.eta0, c.hu0, c.hv0, c.Hi, c.nx, c.ny, c.dx, c.dy, c.dt, c.g, c.f, c.r, bc=c.bc,
+                       device="cuda")
+    for _ in range(c.steps):
+        fp64.step(c.dt)
+    exact = fp64.download()
+    e64 = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, exact)]
+    e64_ref = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(theirs, exact)]
+    print("bump256 1000 steps: vs reference kernel", e_ref, "| reference fmad noise floor", floor,
+          "| vs FP64", e64, "| reference vs FP64", e64_ref)
+    assert max(e_ref) <= 1e-5
+    assert max(e64) <= 1e-3
+    # wall mass conservation: FP32 rounding level
+    s0 = float(np.sum(np.maximum(c.eta0, -60.0)[2:-2, 2:-2].astype(np.float64)))
+    s1 = float(np.sum(mine[0][2:-2, 2:-2].astype(np.float64)))
+    assert abs(s1 - s0) / float(np.sum(np.abs(c.eta0[2:-2, 2:-2]))) < 1e-5
+
+
+def test_small_beta_friction_wind_periodic_vs_reference_kernel(ctx):
+    """Config-2 physics (beta plane, quadratic friction, wind, periodic E/W,
+    walls N/S) on a 96x80 grid: 200 steps against the reference kernel."""
+    cfgd = build_ref.CONFIGS["small_beta"]
+    c = SC.grf(96, dx=500.0, steps=200)
+    # crop to 96 x 80
+    ny = cfgd["ny"]
+    c.ny = ny
+    c.Hi = np.ascontiguousarray(c.Hi[: ny + 5])
+    c.eta0 = np.ascontiguousarray(c.eta0[: ny + 4])
+    c.hu0 = np.zeros_like(c.eta0)
+    c.hv0 = np.zeros_like(c.eta0)
+    c.Hi = O.fix_bi_ghost_corners(c.Hi, c.nx, c.ny, c.bc)
+    c.dt = SC.cfl_dt(c)
+    sim = _drop_in(ctx, c)
+    for _ in range(c.steps):
+        sim.step(c.dt)
+    mine = sim.download()
+    ref = _ref_for("small_beta", c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, c.bc, wind=c.wind)
+    for _ in range(c.steps):
+        ref.step(c.dt)
+    theirs = ref.download()
+    errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
+    print("small beta/friction/wind 200 steps vs reference kernel:", errs)
+    assert max(errs) <= 1e-5
+    fp64 = O.OracleSim(c.eta0, c.hu0, c.hv0, c.Hi, c.nx, c.ny, c.dx, c.dy, c.dt, c.g, c.f, c.r,
+                       coriolis_beta=c.beta, bc=c.bc, wind=c.wind, device="cuda")
+    for _ in range(c.steps):
+        fp64.step(c.dt)
+    e64 = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, fp64.download())]
+    print("  vs FP64:", e64)
+    assert max(e64) <= 1e-3
+
+
+def test_single_stage_each_rk_step_vs_reference_kernel(ctx):
+    """One call of each RK sub-step through the kernel-level ABI
+    (go_cdklm_swe_2D vs the reference cdklm_swe_2D) on a perturbed state."""
+    cfgd = build_ref.CONFIGS["small_beta"]
+    nx, ny = cfgd["nx"], cfgd["ny"]
+    rng = np.random.default_rng(7)
+    c = SC.grf(96, dx=500.0, steps=1)
+    Hi = O.fix_bi_ghost_corners(np.ascontiguousarray(c.Hi[: ny + 5]), nx, ny, c.bc)
+    eta = (0.3 * rng.standard_normal((ny + 4, nx + 4))).astype(np.float32)
+    hu = (5.0 * rng.standard_normal((ny + 4, nx + 4))).astype(np.float32)
+    hv = (5.0 * rng.standard_normal((ny + 4, nx + 4))).astype(np.float32)
+    dt = 1.0
+    ref = _ref_for("small_beta", eta, hu, hv, Hi, dt, c.f, c.beta, c.bc, wind=c.wind)
+    dom = _native.Domain(nx, ny, 500.0, 500.0, 9.81, 3e-3, bc=c.bc)
+    dom.set_coriolis(O.coriolis_rows(c.f, c.beta, ny, 500.0))
+    dom.set_wind_uniform(c.wind[0], c.wind[0], c.wind[1], c.wind[1])
+    Hi_t = torch.from_numpy(Hi).cuda()
+    for k in (0, 1):
+        qin = [a.clone() for a in ref.h0]
+        qout = [a.clone() + 1.0 for a in ref.h0]       # stage 1 reads Q^n here
+        ref.boundary(qin)
+        mine_out = [a.clone() for a in qout]
+        ref.stage(k, dt, qin, qout)
+        p = (nx + 4) * 4
+        _native.check(_native.load().go_cdklm_swe_2D(
+            dom.handle, None, dt, k, _native.ptr(qin[0]), p, _native.ptr(qin[1]), p, _native.ptr(qin[2]), p,
+            _native.ptr(mine_out[0]), p, _native.ptr(mine_out[1]), p, _native.ptr(mine_out[2]), p,
+            _native.ptr(Hi_t), (nx + 5) * 4, None, 0, 1e20, 0.0, dom.bc_packed))
+        torch.cuda.synchronize()
+        errs = [rel_max(a.cpu().numpy()[2:-2, 2:-2], b.cpu().numpy()[2:-2, 2:-2]) for a, b in zip(mine_out, qout)]
+        print("rk_step", k, "single-call max rel diff:", errs)
+        assert max(errs) <= 1e-5
+
+
+def test_max_dt_exact_minimum(ctx):
+    c = SC.grf(128, dx=1000.0, steps=1)
+    sim = _drop_in(ctx, c)
+    for _ in range(20):
+        sim.step(c.dt)
+    sim.updateDt(courant_number=1.0)
+    eta, hu, hv = sim.download()
+    Bm = sim.downloadBathymetry()[1]
+    exact = O.max_dt(eta, hu, hv, Bm, c.nx, c.ny, c.dx, c.dy, c.g)
+    assert abs(float(sim.dt) - exact) / exact < 1e-5
+    # the host reference of the reference (CDKLM16.py:741-759) agrees to FP32
+    host = sim._getMaxTimestepHost(courant_number=1.0)
+    assert abs(host - exact) / exact < 1e-4
+
+
+def test_status_word_flags_nonfinite(ctx):
+    c = SC.bump256()
+    sim = _drop_in(ctx, c)
+    eta, hu, hv = sim.download()
+    hu[100:110, 100:110] = np.nan
+    sim.upload(eta, hu, hv)
+    sim.step(c.dt)
+    assert sim.status(clear=True) & _native.GO_STATUS_NONFINITE
+    assert sim.status() == 0

@@ -32,9 +32,8 @@ def _run_case(d, name, dtype=np.float64, f_rows=None):
     eta0 = d[name + "/eta0"]
     z = np.zeros_like(eta0)
     sim = O.OracleSim(eta0, z, z, d[name + "/Hi"], nx, ny, dx, dy, float(dt), g, f, 0.0,
-                      coriolis_beta=beta, bc=tuple(int(b) for b in d[name + "/bc"]), dtype=dtype)
-    if f_rows is not None:
-        sim.f_rows = f_rows
+                      coriolis_beta=beta, bc=tuple(int(b) for b in d[name + "/bc"]), dtype=dtype,
+                      f_rows=f_rows)
     sim.step(float(T))
     return sim
 
