@@ -182,8 +182,10 @@ def run_ours(args, world, rank, local):
     cells = c.nx * c.ny
     ctx = Common.CUDAContext(local)
     sim = CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs())
-    if args.rows:
-        sim._domain.set_tile(args.rows)
+    if args.rows or args.shape:
+        sim._domain.set_launch(args.shape, args.rows)
+    if args.arith >= 0:
+        sim._domain.set_arith(args.arith)
     stream = sim.gpu_stream
     sim.step(c.dt)                     # first call applies the t == 0 boundary refresh
     for _ in range(args.warmup):
@@ -261,6 +263,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["grf4096", "bump256"], default="grf4096")
     ap.add_argument("--rows", type=int, default=0, help="rows per block strip (0: library default)")
+    ap.add_argument("--shape", type=int, default=0, help="launch shape 0..4 (include/gocean.h)")
+    ap.add_argument("--arith", type=int, default=-1,
+                    help="quotients: 0 '/' as the reference source, 1 reciprocals (library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -1,0 +1,131 @@
+"""Batched stepping of many CDKLM16 simulators.
+
+The reference's ensembles advance their members one at a time
+(gpu_ocean/SWESimulators/OceanNoiseEnsemble.py:506-531,
+OceanModelEnsemble.py:105-117, EnsembleFromFiles.py:302-324): every member
+issues its own 2 step launches (plus boundary launches) per time step from
+Python.  ``BatchedCDKLM16`` keeps the members as ordinary ``CDKLM16``
+objects (their ``gpu_data`` buffers, ``t`` and ``num_iterations`` stay valid
+for the DA code) and advances all of them with one launch per RK stage over
+a packed tile list (``go_batch_step``), optionally replayed from a captured
+CUDA graph.  Members may have different grid sizes, bathymetry and time
+steps; they must share the kernel variant (friction law, grid angle, uniform
+or per-cell wind).
+"""
+
+import numpy as np
+
+from . import _native
+
+
+class BatchedCDKLM16:
+
+    def __init__(self, sims, graph_steps=0, launch=None):
+        """sims: list of CDKLM16.  graph_steps > 0 captures that many steps
+        into a CUDA graph used by ``advance``.  launch: optional (shape,
+        rows_per_block, blocks) as chosen by Autotune.tune_batch."""
+        torch = _native.require_cuda()
+        self.sims = list(sims)
+        self.n = len(self.sims)
+        self.stream = torch.cuda.Stream()
+        self.batch = _native.Batch([s._domain for s in self.sims])
+        if launch is not None:
+            self.batch.set_launch(*launch)
+        for m, s in enumerate(self.sims):
+            self._bind(m, s)
+        self.graph_steps = 0
+        if graph_steps:
+            self.capture(graph_steps)
+
+    def _bind(self, m, s):
+        # the member's wind at its current time (Simulator.update_wind_stress)
+        wind_t = np.float32(s.update_wind_stress())
+        g = s.gpu_data
+        self.batch.set_member(m, np.float32(s.dt), (g.h0.tensor, g.hu0.tensor, g.hv0.tensor),
+                              (g.h1.tensor, g.hu1.tensor, g.hv1.tensor), s.bathymetry.Bi.tensor,
+                              float(s.bathymetry.mask_value), float(wind_t))
+
+    def _time_varying_wind(self):
+        return any(len(s.wind_stress.t) > 1 for s in self.sims)
+
+    def _sync_members(self):
+        # work queued on the members' own streams (uploads, perturbations)
+        # completes before the batched launch reads their buffers
+        for s in self.sims:
+            self.stream.wait_stream(s.gpu_stream)
+
+    def _first_step_bc(self):
+        for s in self.sims:
+            if s.t == 0:
+                s.bc_kernel.boundaryCondition(s.gpu_stream, s.gpu_data.h0, s.gpu_data.hu0, s.gpu_data.hv0)
+
+    def set_dt(self, dts):
+        """Per-member time steps (sequence of n floats)."""
+        dts = np.asarray(dts, dtype=np.float32).reshape(-1)
+        for s, d in zip(self.sims, dts):
+            s.dt = d
+        self.batch.set_dt(dts, self.stream)
+
+    def capture(self, n_steps):
+        self._sync_members()
+        self.batch.capture(int(n_steps), self.stream)
+        self.graph_steps = int(n_steps)
+
+    def advance(self, n_steps):
+        """n_steps RK2 steps of every member at its own dt (graph replays
+        for whole multiples of the captured length, plain launches for the
+        rest)."""
+        self._first_step_bc()
+        if self._time_varying_wind():
+            # wind interpolated in time: rebind every member before each step
+            for _ in range(int(n_steps)):
+                for m, s in enumerate(self.sims):
+                    self._bind(m, s)
+                self._sync_members()
+                self.batch.step(1, self.stream)
+                self._account(1)
+            return [s.t for s in self.sims]
+        self._sync_members()
+        done = 0
+        if self.graph_steps:
+            while n_steps - done >= self.graph_steps:
+                done += self.batch.replay(self.stream)
+        if n_steps - done:
+            self.batch.step(n_steps - done, self.stream)
+        self._account(n_steps)
+        return [s.t for s in self.sims]
+
+    def _account(self, n_steps):
+        for s in self.sims:
+            s.gpu_stream.wait_stream(self.stream)
+            # t accumulates float64(dt) once per step, as CDKLM16.step does
+            steps = np.full(int(n_steps), np.float64(np.float32(s.dt)))
+            s.t = float(np.cumsum(np.concatenate([[np.float64(s.t)], steps]))[-1])
+            s.num_iterations += n_steps
+
+    def step(self, t_end):
+        """Every member advances by t_end with the reference's step() loop
+        semantics (CDKLM16.py:494-598); the members must share dt."""
+        dts = {float(np.float32(s.dt)) for s in self.sims}
+        if len(dts) != 1:
+            raise ValueError("step(t_end) needs a common dt; use advance(n) for per-member dt")
+        dt = np.float32(self.sims[0].dt)
+        t_now = 0.0
+        full = 0
+        while t_now < t_end:
+            local_dt = np.float32(min(dt, np.float32(t_end - t_now)))
+            if local_dt != dt:
+                break
+            full += 1
+            t_now += np.float64(local_dt)
+        if full:
+            self.advance(full)
+        if t_now < t_end:
+            last = np.float32(min(dt, np.float32(t_end - t_now)))
+            self.set_dt([last] * self.n)
+            self.advance(1)
+            self.set_dt([dt] * self.n)
+        return self.sims[0].t
+
+    def synchronize(self):
+        self.stream.synchronize()

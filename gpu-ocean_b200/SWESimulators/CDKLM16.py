@@ -84,6 +84,9 @@ class CDKLM16(Simulator.Simulator):
 
         self.bathymetry = Common.Bathymetry(gpu_ctx, self.gpu_stream, nx, ny, ghost_cells_x, ghost_cells_y,
                                             H, boundary_conditions)
+        # land tests of the kernel only when the bathymetry holds land
+        Hh = np.ma.filled(H, self.bathymetry.mask_value) if np.ma.is_masked(H) else np.asarray(H)
+        self._domain.set_land(bool(np.any(np.abs(Hh.astype(np.float32) - self.bathymetry.mask_value) < 1e-3)))
         Hm = self.downloadBathymetry()[1]
         eta0 = np.maximum(eta0, -Hm)          # CDKLM16.py:237-238
         self.gpu_data = Common.SWEDataArakawaA(self.gpu_stream, nx, ny, ghost_cells_x, ghost_cells_y,

@@ -18,6 +18,8 @@ GO_BC_PERIODIC = 2
 GO_FRICTION_QUADRATIC = 0
 GO_FRICTION_LINEAR = 1
 GO_STATUS_NONFINITE = 0x1
+GO_ARITH_EXACT = 0
+GO_ARITH_RCP = 1
 
 _c_float_p = ctypes.c_void_p  # device pointers travel as integers
 
@@ -48,7 +50,9 @@ SIGNATURES = {
     "go_domain_set_coriolis": (_I, [_P, ctypes.POINTER(ctypes.c_float), _I]),
     "go_domain_set_wind_uniform": (_I, [_P, _F, _F, _F, _F]),
     "go_domain_set_wind_field": (_I, [_P, _P, _P, _P, _P, _I]),
-    "go_domain_set_tile": (_I, [_P, _I]),
+    "go_domain_set_launch": (_I, [_P, _I, _I]),
+    "go_domain_set_arith": (_I, [_P, _I]),
+    "go_domain_set_land": (_I, [_P, _I]),
     "go_init_bathymetry": (_I, [_P, _P, _P, _I, _P, _I, _F]),
     "go_boundary_condition": (_I, [_P, _P, _P, _P, _P, _I]),
     "go_cdklm_swe_2D": (_I, [_P, _P, _F, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I,
@@ -56,6 +60,16 @@ SIGNATURES = {
     "go_cdklm_step": (_I, [_P, _P, _I, _F, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F]),
     "go_max_dt": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _F, _P]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
+    "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),
+    "go_batch_destroy": (_I, [_P]),
+    "go_batch_set_member": (_I, [_P, _I, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F, _F]),
+    "go_batch_set_launch": (_I, [_P, _I, _I, _I]),
+    "go_batch_set_arith": (_I, [_P, _I]),
+    "go_batch_set_dt": (_I, [_P, _P, ctypes.POINTER(ctypes.c_float)]),
+    "go_batch_tiles": (_I, [_P, ctypes.POINTER(_I)]),
+    "go_batch_step": (_I, [_P, _P, _I]),
+    "go_batch_graph_capture": (_I, [_P, _P, _I]),
+    "go_batch_graph_launch": (_I, [_P, _P, ctypes.POINTER(_I)]),
     "go_last_error": (ctypes.c_char_p, []),
     "go_version": (ctypes.c_char_p, []),
 }
@@ -163,10 +177,77 @@ class Domain:
             assert t.stride(0) * 4 == pitch
         check(load().go_domain_set_wind_field(self.handle, ptr(x_cur), ptr(x_next), ptr(y_cur), ptr(y_next), pitch))
 
-    def set_tile(self, rows_per_block):
-        check(load().go_domain_set_tile(self.handle, int(rows_per_block)))
+    def set_launch(self, shape=0, rows_per_block=0):
+        check(load().go_domain_set_launch(self.handle, int(shape), int(rows_per_block)))
+
+    def set_arith(self, mode):
+        check(load().go_domain_set_arith(self.handle, int(mode)))
+
+    def set_land(self, may_have_land):
+        check(load().go_domain_set_land(self.handle, int(bool(may_have_land))))
 
     def status(self, clear=False):
         v = ctypes.c_uint32()
         check(load().go_domain_status(self.handle, ctypes.byref(v), int(bool(clear))))
         return int(v.value)
+
+
+class Batch:
+    """Owner of one go_batch handle over a list of ``Domain`` objects."""
+
+    def __init__(self, domains):
+        lib = load()
+        self.domains = list(domains)
+        arr = (ctypes.c_void_p * len(self.domains))(*[d.handle.value for d in self.domains])
+        h = ctypes.c_void_p()
+        check(lib.go_batch_create(arr, len(self.domains), ctypes.byref(h)))
+        self.handle = h
+        self.n = len(self.domains)
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            load().go_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_member(self, m, dt, h0, h1, Hi, land_value=1e20, wind_t=0.0):
+        """h0, h1: (eta, hu, hv) device tensors sharing a row stride; Hi a
+        device tensor of corners."""
+        p0 = h0[0].stride(0) * 4
+        p1 = h1[0].stride(0) * 4
+        check(load().go_batch_set_member(self.handle, int(m), float(dt), ptr(h0[0]), ptr(h0[1]), ptr(h0[2]), p0,
+                                         ptr(h1[0]), ptr(h1[1]), ptr(h1[2]), p1, ptr(Hi), Hi.stride(0) * 4,
+                                         float(land_value), float(wind_t)))
+
+    def set_launch(self, shape=0, rows_per_block=0, blocks=0):
+        check(load().go_batch_set_launch(self.handle, int(shape), int(rows_per_block), int(blocks)))
+
+    def set_arith(self, mode):
+        check(load().go_batch_set_arith(self.handle, int(mode)))
+
+    def set_dt(self, dts, stream=None):
+        a = np.ascontiguousarray(np.asarray(dts, dtype=np.float32).reshape(-1))
+        assert a.size == self.n
+        check(load().go_batch_set_dt(self.handle, stream_handle(stream),
+                                     a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def tiles(self):
+        n = ctypes.c_int()
+        check(load().go_batch_tiles(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def step(self, n_steps, stream=None):
+        check(load().go_batch_step(self.handle, stream_handle(stream), int(n_steps)))
+
+    def capture(self, n_steps, stream):
+        check(load().go_batch_graph_capture(self.handle, stream_handle(stream), int(n_steps)))
+
+    def replay(self, stream):
+        n = ctypes.c_int()
+        check(load().go_batch_graph_launch(self.handle, stream_handle(stream), ctypes.byref(n)))
+        return n.value

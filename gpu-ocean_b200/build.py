@@ -22,7 +22,7 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo",
     "--ftz=true", "--prec-div=false", "--prec-sqrt=false", "--fmad=false",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -42,15 +42,31 @@ def up_to_date():
 
 
 def build(force=False, verbose=False):
+    """Compile each csrc/*.cu to an object in parallel, then link."""
     if not force and up_to_date():
         return LIB
+    import shutil
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-I", INCLUDE, os.path.join(CSRC, "gocean.cu"), "-o", LIB + ".tmp"]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
+    units = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    work = tempfile.mkdtemp(prefix="gocean_build_")
+    try:
+        def compile_one(u):
+            obj = os.path.join(work, u + ".o")
+            cmd = [nvcc] + NVCC_FLAGS + ["-I", INCLUDE, "-c", os.path.join(CSRC, u), "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            return obj
+        with ThreadPoolExecutor(max_workers=max(1, min(len(units), os.cpu_count() or 1))) as ex:
+            objs = list(ex.map(compile_one, units))
+        cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + objs + ["-o", LIB + ".tmp"]
+        subprocess.run(cmd, check=True)
+        os.replace(LIB + ".tmp", LIB)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
     return LIB
 
 

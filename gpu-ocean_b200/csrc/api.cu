@@ -1,40 +1,17 @@
 // C ABI of the B200-native CDKLM16 step (declarations in include/gocean.h).
 //
-// Build (sm_100a only):
-//   nvcc -O3 -gencode arch=compute_100a,code=sm_100a -lineinfo \
-//        --ftz=true --prec-div=false --prec-sqrt=false --fmad=false \
-//        -Xcompiler -fPIC -shared -I include gocean.cu -o libgocean.so
-// The four floating-point flags are the reference's (CDKLM16.py:196-200).
-#include <cuda_runtime.h>
-#include <stdarg.h>
-#include <stdint.h>
-#include <stdio.h>
-#include <string.h>
-
+// Build: gpu-ocean_b200/build.py compiles every csrc/*.cu for sm_100a with
+// the reference's floating-point flags (CDKLM16.py:196-200):
+// --ftz=true --prec-div=false --prec-sqrt=false --fmad=false.
 #include <string>
 
-#include "cdklm16_stage.cuh"
-#include "gocean.h"
+#include "internal.h"
 
 using namespace go;
 
-struct go_domain {
-    go_domain_desc desc;
-    Scheme k;
-    int device;
-    float* d_frows;          // ny+4 Coriolis values
-    unsigned int* d_status;  // GO_STATUS_* bits
-    float wxc, wxn, wyc, wyn;
-    const float *wx_cur, *wx_next, *wy_cur, *wy_next;
-    int wpitch;              // floats
-    int rows_per_block;
-    int block_width;
-};
-
 static thread_local std::string g_err;
 
-static int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
-static int fail(int code, const char* fmt, ...) {
+int go_fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -44,18 +21,41 @@ static int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define GO_CUDA(call)                                                                    \
-    do {                                                                                 \
-        cudaError_t e_ = (call);                                                         \
-        if (e_ != cudaSuccess)                                                           \
-            return fail(GO_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
-    } while (0)
-
-static int check_pitch(int pitch_bytes, int min_floats, const char* what) {
+int go_check_pitch(int pitch_bytes, int min_floats, const char* what) {
     if (pitch_bytes <= 0 || (pitch_bytes % 4) != 0 || pitch_bytes / 4 < min_floats)
-        return fail(GO_ERR_INVALID, "%s pitch %d bytes is invalid (need a multiple of 4, >= %d floats)",
-                    what, pitch_bytes, min_floats);
+        return go_fail(GO_ERR_INVALID, "%s pitch %d bytes is invalid (need a multiple of 4, >= %d floats)",
+                       what, pitch_bytes, min_floats);
     return GO_OK;
+}
+
+int go_friction_mode(const go_domain* d) {
+    if (d->desc.friction_law == GO_FRICTION_LINEAR) return kFricLinear;
+    return (d->k.r > 0.0f) ? kFricQuad : kFricNone;
+}
+
+bool go_general_north(const go_domain* d) { return !(d->k.nX == 0.0f && d->k.nY == 1.0f); }
+
+
+StageArgs go_stage_args(const go_domain* d, float dt, int rk_step, const float* e0, const float* u0,
+                        const float* v0, int pin, float* e1, float* u1, float* v1, int pout,
+                        const float* Hi, int phi, float land, float wind_t) {
+    StageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.k = d->k;
+    a.k.land = land;
+    a.dt = dt;
+    a.rk_step = rk_step;
+    a.eta_in = e0; a.hu_in = u0; a.hv_in = v0; a.pin = pin;
+    a.eta_out = e1; a.hu_out = u1; a.hv_out = v1; a.pout = pout;
+    a.Hi = Hi; a.phi = phi;
+    a.f_rows = d->d_frows;
+    a.wind_t = wind_t;
+    a.wxc = d->wxc; a.wxn = d->wxn; a.wyc = d->wyc; a.wyn = d->wyn;
+    a.wx_cur = d->wx_cur; a.wx_next = d->wx_next; a.wy_cur = d->wy_cur; a.wy_next = d->wy_next;
+    a.pw = d->wpitch;
+    a.rows_per_block = d->rows_per_block;
+    a.status = d->d_status;
+    return a;
 }
 
 // ---------------------------------------------------------------------------
@@ -167,71 +167,6 @@ __global__ void k_max_dt(const float* eta, const float* hu, const float* hv, int
 __global__ void k_fill_u32(unsigned int* p, unsigned int v) { *p = v; }
 
 // ---------------------------------------------------------------------------
-// Stage dispatch
-// ---------------------------------------------------------------------------
-
-template <int BW>
-static cudaError_t launch_stage_bw(const StageArgs& a, int fric, bool gen_north, bool wind_field,
-                                   cudaStream_t s) {
-    const dim3 grid((a.k.nx + (BW - 4) - 1) / (BW - 4), (a.k.ny + a.rows_per_block - 1) / a.rows_per_block);
-    const dim3 block(BW);
-#define GO_LAUNCH(F, N, W) cdklm_stage_kernel<BW, F, N, W><<<grid, block, 0, s>>>(a)
-#define GO_LAUNCH_NW(F)                         \
-    do {                                        \
-        if (gen_north) {                        \
-            if (wind_field) GO_LAUNCH(F, true, true); \
-            else GO_LAUNCH(F, true, false);     \
-        } else {                                \
-            if (wind_field) GO_LAUNCH(F, false, true); \
-            else GO_LAUNCH(F, false, false);    \
-        }                                       \
-    } while (0)
-    if (fric == kFricNone) GO_LAUNCH_NW(kFricNone);
-    else if (fric == kFricQuad) GO_LAUNCH_NW(kFricQuad);
-    else GO_LAUNCH_NW(kFricLinear);
-#undef GO_LAUNCH_NW
-#undef GO_LAUNCH
-    return cudaGetLastError();
-}
-
-static int friction_mode(const go_domain* d) {
-    if (d->desc.friction_law == GO_FRICTION_LINEAR) return kFricLinear;
-    return (d->k.r > 0.0f) ? kFricQuad : kFricNone;
-}
-
-static int launch_stage(go_domain* d, cudaStream_t s, float dt, int rk_step,
-                        const float* e0, const float* u0, const float* v0, int pin,
-                        float* e1, float* u1, float* v1, int pout,
-                        const float* Hi, int phi, float land, float wind_t) {
-    StageArgs a;
-    a.k = d->k;
-    a.k.land = land;
-    a.dt = dt;
-    a.rk_step = rk_step;
-    a.eta_in = e0; a.hu_in = u0; a.hv_in = v0; a.pin = pin;
-    a.eta_out = e1; a.hu_out = u1; a.hv_out = v1; a.pout = pout;
-    a.Hi = Hi; a.phi = phi;
-    a.f_rows = d->d_frows;
-    a.wind_t = wind_t;
-    a.wxc = d->wxc; a.wxn = d->wxn; a.wyc = d->wyc; a.wyn = d->wyn;
-    a.wx_cur = d->wx_cur; a.wx_next = d->wx_next; a.wy_cur = d->wy_cur; a.wy_next = d->wy_next;
-    a.pw = d->wpitch;
-    a.rows_per_block = d->rows_per_block;
-    a.status = d->d_status;
-    const bool gen_north = !(d->k.nX == 0.0f && d->k.nY == 1.0f);
-    const bool wind_field = d->wx_cur != nullptr;
-    const int fric = friction_mode(d);
-    cudaError_t e;
-    switch (d->block_width) {
-        case 128: e = launch_stage_bw<128>(a, fric, gen_north, wind_field, s); break;
-        case 256: e = launch_stage_bw<256>(a, fric, gen_north, wind_field, s); break;
-        default: e = launch_stage_bw<192>(a, fric, gen_north, wind_field, s); break;
-    }
-    if (e != cudaSuccess) return fail(GO_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));
-    return GO_OK;
-}
-
-// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 
@@ -241,23 +176,23 @@ const char* go_last_error(void) { return g_err.c_str(); }
 const char* go_version(void) { return "gocean-b200 0.1 (sm_100a)"; }
 
 int go_domain_create(const go_domain_desc* desc, go_domain** out) {
-    if (!desc || !out) return fail(GO_ERR_INVALID, "null argument");
+    if (!desc || !out) return go_fail(GO_ERR_INVALID, "null argument");
     *out = nullptr;
     const go_domain_desc& s = *desc;
-    if (s.nx < 4 || s.ny < 4) return fail(GO_ERR_INVALID, "nx, ny must be >= 4 (got %d, %d)", s.nx, s.ny);
+    if (s.nx < 4 || s.ny < 4) return go_fail(GO_ERR_INVALID, "nx, ny must be >= 4 (got %d, %d)", s.nx, s.ny);
     if (!(s.dx > 0.0f) || !(s.dy > 0.0f) || !(s.g > 0.0f))
-        return fail(GO_ERR_INVALID, "dx, dy, g must be positive");
-    if (s.r < 0.0f) return fail(GO_ERR_INVALID, "friction r must be >= 0");
-    if (s.rk_order != 2) return fail(GO_ERR_UNSUPPORTED, "rk_order %d: only 2 (Heun) is built", s.rk_order);
+        return go_fail(GO_ERR_INVALID, "dx, dy, g must be positive");
+    if (s.r < 0.0f) return go_fail(GO_ERR_INVALID, "friction r must be >= 0");
+    if (s.rk_order != 2) return go_fail(GO_ERR_UNSUPPORTED, "rk_order %d: only 2 (Heun) is built", s.rk_order);
     const int bcs[4] = {s.bc_north, s.bc_east, s.bc_south, s.bc_west};
     for (int b : bcs)
         if (b != GO_BC_WALL && b != GO_BC_PERIODIC)
-            return fail(GO_ERR_UNSUPPORTED, "boundary code %d: only wall (1) and periodic (2) are built", b);
+            return go_fail(GO_ERR_UNSUPPORTED, "boundary code %d: only wall (1) and periodic (2) are built", b);
     if ((s.bc_north == GO_BC_PERIODIC) != (s.bc_south == GO_BC_PERIODIC) ||
         (s.bc_east == GO_BC_PERIODIC) != (s.bc_west == GO_BC_PERIODIC))
-        return fail(GO_ERR_INVALID, "periodic boundaries must be set on both opposite sides");
+        return go_fail(GO_ERR_INVALID, "periodic boundaries must be set on both opposite sides");
     if (s.friction_law != GO_FRICTION_QUADRATIC && s.friction_law != GO_FRICTION_LINEAR)
-        return fail(GO_ERR_INVALID, "unknown friction law %d", s.friction_law);
+        return go_fail(GO_ERR_INVALID, "unknown friction law %d", s.friction_law);
 
     go_domain* d = new go_domain();
     d->desc = s;
@@ -276,8 +211,10 @@ int go_domain_create(const go_domain_desc* desc, go_domain** out) {
     k.V = s.dx / k.two_g;
     k.U = s.dy / k.two_g;
     k.two_r = two * s.r;
-    d->rows_per_block = 64;
-    d->block_width = 192;
+    d->rows_per_block = 32;
+    d->shape = 4;
+    d->arith = GO_ARITH_RCP;
+    d->has_land = 1;
     cudaError_t e = cudaGetDevice(&d->device);
     if (e == cudaSuccess) e = cudaMalloc(&d->d_frows, sizeof(float) * (s.ny + 4));
     if (e == cudaSuccess) e = cudaMemset(d->d_frows, 0, sizeof(float) * (s.ny + 4));
@@ -287,7 +224,7 @@ int go_domain_create(const go_domain_desc* desc, go_domain** out) {
         cudaFree(d->d_frows);
         cudaFree(d->d_status);
         delete d;
-        return fail(GO_ERR_CUDA, "domain allocation failed: %s", cudaGetErrorString(e));
+        return go_fail(GO_ERR_CUDA, "domain allocation failed: %s", cudaGetErrorString(e));
     }
     *out = d;
     return GO_OK;
@@ -302,7 +239,7 @@ int go_domain_destroy(go_domain* d) {
 }
 
 int go_domain_set_coriolis(go_domain* d, const float* f_rows_host, int n) {
-    if (!d || !f_rows_host) return fail(GO_ERR_INVALID, "null argument");
+    if (!d || !f_rows_host) return go_fail(GO_ERR_INVALID, "null argument");
     const int rows = d->k.ny + 4;
     if (n == 1) {
         float* tmp = new float[rows];
@@ -312,13 +249,13 @@ int go_domain_set_coriolis(go_domain* d, const float* f_rows_host, int n) {
         GO_CUDA(e);
         return GO_OK;
     }
-    if (n != rows) return fail(GO_ERR_INVALID, "Coriolis table has %d rows, need 1 or ny+4 = %d", n, rows);
+    if (n != rows) return go_fail(GO_ERR_INVALID, "Coriolis table has %d rows, need 1 or ny+4 = %d", n, rows);
     GO_CUDA(cudaMemcpy(d->d_frows, f_rows_host, sizeof(float) * rows, cudaMemcpyHostToDevice));
     return GO_OK;
 }
 
 int go_domain_set_wind_uniform(go_domain* d, float x_cur, float x_next, float y_cur, float y_next) {
-    if (!d) return fail(GO_ERR_INVALID, "null domain");
+    if (!d) return go_fail(GO_ERR_INVALID, "null domain");
     d->wxc = x_cur; d->wxn = x_next; d->wyc = y_cur; d->wyn = y_next;
     d->wx_cur = d->wx_next = d->wy_cur = d->wy_next = nullptr;
     return GO_OK;
@@ -326,33 +263,48 @@ int go_domain_set_wind_uniform(go_domain* d, float x_cur, float x_next, float y_
 
 int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_next,
                              const float* y_cur, const float* y_next, int pitch) {
-    if (!d) return fail(GO_ERR_INVALID, "null domain");
+    if (!d) return go_fail(GO_ERR_INVALID, "null domain");
     if (!x_cur && !x_next && !y_cur && !y_next) {
         d->wx_cur = d->wx_next = d->wy_cur = d->wy_next = nullptr;
         return GO_OK;
     }
-    if (!x_cur || !x_next || !y_cur || !y_next) return fail(GO_ERR_INVALID, "wind field needs four arrays");
-    int rc = check_pitch(pitch, d->k.nx, "wind");
+    if (!x_cur || !x_next || !y_cur || !y_next) return go_fail(GO_ERR_INVALID, "wind field needs four arrays");
+    int rc = go_check_pitch(pitch, d->k.nx, "wind");
     if (rc) return rc;
     d->wx_cur = x_cur; d->wx_next = x_next; d->wy_cur = y_cur; d->wy_next = y_next;
     d->wpitch = pitch / 4;
     return GO_OK;
 }
 
-int go_domain_set_tile(go_domain* d, int rows_per_block) {
-    if (!d) return fail(GO_ERR_INVALID, "null domain");
-    if (rows_per_block == 0) rows_per_block = 64;
-    if (rows_per_block < 1) return fail(GO_ERR_INVALID, "rows_per_block must be >= 1");
+int go_domain_set_launch(go_domain* d, int shape, int rows_per_block) {
+    if (!d) return go_fail(GO_ERR_INVALID, "null domain");
+    if (shape < 0 || shape > 4) return go_fail(GO_ERR_INVALID, "launch shape %d (0..4)", shape);
+    if (rows_per_block == 0) rows_per_block = 32;
+    if (rows_per_block < 1) return go_fail(GO_ERR_INVALID, "rows_per_block must be >= 1");
+    d->shape = shape;
     d->rows_per_block = rows_per_block;
+    return GO_OK;
+}
+
+int go_domain_set_arith(go_domain* d, int mode) {
+    if (!d) return go_fail(GO_ERR_INVALID, "null domain");
+    if (mode != GO_ARITH_EXACT && mode != GO_ARITH_RCP) return go_fail(GO_ERR_INVALID, "arith mode %d", mode);
+    d->arith = mode;
+    return GO_OK;
+}
+
+int go_domain_set_land(go_domain* d, int may_have_land) {
+    if (!d) return go_fail(GO_ERR_INVALID, "null domain");
+    d->has_land = may_have_land ? 1 : 0;
     return GO_OK;
 }
 
 int go_init_bathymetry(go_domain* d, void* stream, float* Hi, int Hi_pitch, float* Bm, int Bm_pitch,
                        float land_value) {
-    if (!d || !Hi || !Bm) return fail(GO_ERR_INVALID, "null argument");
-    int rc = check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+    if (!d || !Hi || !Bm) return go_fail(GO_ERR_INVALID, "null argument");
+    int rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
     if (rc) return rc;
-    rc = check_pitch(Bm_pitch, d->k.nx + 4, "Bm");
+    rc = go_check_pitch(Bm_pitch, d->k.nx + 4, "Bm");
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     const int nx = d->k.nx, ny = d->k.ny, ph = Hi_pitch / 4, pb = Bm_pitch / 4;
@@ -365,8 +317,8 @@ int go_init_bathymetry(go_domain* d, void* stream, float* Hi, int Hi_pitch, floa
 }
 
 int go_boundary_condition(go_domain* d, void* stream, float* eta, float* hu, float* hv, int pitch) {
-    if (!d || !eta || !hu || !hv) return fail(GO_ERR_INVALID, "null argument");
-    int rc = check_pitch(pitch, d->k.nx + 4, "state");
+    if (!d || !eta || !hu || !hv) return go_fail(GO_ERR_INVALID, "null argument");
+    int rc = go_check_pitch(pitch, d->k.nx + 4, "state");
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     const int nx = d->k.nx, ny = d->k.ny, p = pitch / 4;
@@ -389,20 +341,21 @@ int go_cdklm_swe_2D(go_domain* d, void* stream, float dt, int rk_step,
                     float land_value, float wind_stress_t, int boundary_conditions) {
     (void)Hm; (void)Hm_pitch;
     if (!d || !eta0 || !hu0 || !hv0 || !eta1 || !hu1 || !hv1 || !Hi)
-        return fail(GO_ERR_INVALID, "null argument");
-    if (rk_step != 0 && rk_step != 1) return fail(GO_ERR_INVALID, "rk_step %d (RK2 has 0 and 1)", rk_step);
+        return go_fail(GO_ERR_INVALID, "null argument");
+    if (rk_step != 0 && rk_step != 1) return go_fail(GO_ERR_INVALID, "rk_step %d (RK2 has 0 and 1)", rk_step);
     if (eta0_pitch != hu0_pitch || eta0_pitch != hv0_pitch || eta1_pitch != hu1_pitch ||
         eta1_pitch != hv1_pitch)
-        return fail(GO_ERR_INVALID, "eta/hu/hv of one state must share a pitch");
+        return go_fail(GO_ERR_INVALID, "eta/hu/hv of one state must share a pitch");
     if (boundary_conditions != pack_bc(d->k))
-        return fail(GO_ERR_INVALID, "packed boundary code 0x%08x does not match the domain's 0x%08x",
+        return go_fail(GO_ERR_INVALID, "packed boundary code 0x%08x does not match the domain's 0x%08x",
                     boundary_conditions, pack_bc(d->k));
-    int rc = check_pitch(eta0_pitch, d->k.nx + 4, "input");
-    if (!rc) rc = check_pitch(eta1_pitch, d->k.nx + 4, "output");
-    if (!rc) rc = check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+    int rc = go_check_pitch(eta0_pitch, d->k.nx + 4, "input");
+    if (!rc) rc = go_check_pitch(eta1_pitch, d->k.nx + 4, "output");
+    if (!rc) rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
     if (rc) return rc;
-    return launch_stage(d, (cudaStream_t)stream, dt, rk_step, eta0, hu0, hv0, eta0_pitch / 4,
-                        eta1, hu1, hv1, eta1_pitch / 4, Hi, Hi_pitch / 4, land_value, wind_stress_t);
+    const StageArgs a = go_stage_args(d, dt, rk_step, eta0, hu0, hv0, eta0_pitch / 4, eta1, hu1, hv1,
+                                      eta1_pitch / 4, Hi, Hi_pitch / 4, land_value, wind_stress_t);
+    return go_launch_stage(d, (cudaStream_t)stream, a);
 }
 
 int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_stress_t,
@@ -410,19 +363,21 @@ int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_
                   float* eta1, float* hu1, float* hv1, int pitch1,
                   const float* Hi, int Hi_pitch, float land_value) {
     if (!d || !eta0 || !hu0 || !hv0 || !eta1 || !hu1 || !hv1 || !Hi)
-        return fail(GO_ERR_INVALID, "null argument");
-    if (n_steps < 0) return fail(GO_ERR_INVALID, "n_steps < 0");
-    int rc = check_pitch(pitch0, d->k.nx + 4, "h0");
-    if (!rc) rc = check_pitch(pitch1, d->k.nx + 4, "h1");
-    if (!rc) rc = check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+        return go_fail(GO_ERR_INVALID, "null argument");
+    if (n_steps < 0) return go_fail(GO_ERR_INVALID, "n_steps < 0");
+    int rc = go_check_pitch(pitch0, d->k.nx + 4, "h0");
+    if (!rc) rc = go_check_pitch(pitch1, d->k.nx + 4, "h1");
+    if (!rc) rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
+    const StageArgs a0 = go_stage_args(d, dt, 0, eta0, hu0, hv0, pitch0 / 4, eta1, hu1, hv1, pitch1 / 4, Hi,
+                                       Hi_pitch / 4, land_value, wind_stress_t);
+    const StageArgs a1 = go_stage_args(d, dt, 1, eta1, hu1, hv1, pitch1 / 4, eta0, hu0, hv0, pitch0 / 4, Hi,
+                                       Hi_pitch / 4, land_value, wind_stress_t);
     for (int n = 0; n < n_steps; ++n) {
-        rc = launch_stage(d, s, dt, 0, eta0, hu0, hv0, pitch0 / 4, eta1, hu1, hv1, pitch1 / 4, Hi,
-                          Hi_pitch / 4, land_value, wind_stress_t);
+        rc = go_launch_stage(d, s, a0);
         if (rc) return rc;
-        rc = launch_stage(d, s, dt, 1, eta1, hu1, hv1, pitch1 / 4, eta0, hu0, hv0, pitch0 / 4, Hi,
-                          Hi_pitch / 4, land_value, wind_stress_t);
+        rc = go_launch_stage(d, s, a1);
         if (rc) return rc;
     }
     return GO_OK;
@@ -430,9 +385,9 @@ int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_
 
 int go_max_dt(go_domain* d, void* stream, const float* eta, const float* hu, const float* hv, int pitch,
               const float* Bm, int Bm_pitch, float land_value, float* dt_dev) {
-    if (!d || !eta || !hu || !hv || !Bm || !dt_dev) return fail(GO_ERR_INVALID, "null argument");
-    int rc = check_pitch(pitch, d->k.nx + 4, "state");
-    if (!rc) rc = check_pitch(Bm_pitch, d->k.nx + 4, "Bm");
+    if (!d || !eta || !hu || !hv || !Bm || !dt_dev) return go_fail(GO_ERR_INVALID, "null argument");
+    int rc = go_check_pitch(pitch, d->k.nx + 4, "state");
+    if (!rc) rc = go_check_pitch(Bm_pitch, d->k.nx + 4, "Bm");
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     unsigned int* out = reinterpret_cast<unsigned int*>(dt_dev);
@@ -449,7 +404,7 @@ int go_max_dt(go_domain* d, void* stream, const float* eta, const float* hu, con
 }
 
 int go_domain_status(go_domain* d, uint32_t* status, int clear) {
-    if (!d || !status) return fail(GO_ERR_INVALID, "null argument");
+    if (!d || !status) return go_fail(GO_ERR_INVALID, "null argument");
     unsigned int v = 0;
     GO_CUDA(cudaMemcpy(&v, d->d_status, sizeof(v), cudaMemcpyDeviceToHost));
     *status = v;

@@ -1,0 +1,262 @@
+// Batched CDKLM16 stepping: many members (an ensemble, or independent
+// domains of uneven sizes) advanced by one launch per Runge-Kutta stage over
+// a packed tile list, optionally replayed from a captured CUDA graph.
+//
+// Replaces the member-by-member stepping of the reference's ensembles
+// (gpu_ocean/SWESimulators/OceanNoiseEnsemble.py:506-531,
+// OceanModelEnsemble.py:105-117, EnsembleFromFiles.py:302-324), which issue
+// N_members x (2 step + up to 4 boundary) launches per time step from Python.
+#include <vector>
+
+#include "dispatch.cuh"
+
+using namespace go;
+
+struct go_batch {
+    int n = 0;
+    std::vector<go_domain*> members;
+    std::vector<StageArgs> args;       // 2 per member
+    std::vector<char> member_set;
+    std::vector<float> dt;             // per member
+    StageArgs* d_args = nullptr;
+    float* d_dt = nullptr;
+    int4* d_tiles = nullptr;
+    int ntiles = 0;
+    int shape = 4, rows = 32, blocks = 0;
+    int arith = 0;
+    Variant variant;
+    bool dirty = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_steps = 0;
+};
+
+namespace {
+
+struct BatchLaunch {
+    const go_batch* b;
+    int rk_step, grid;
+    cudaStream_t s;
+    template <int BW, int MINB, int FRIC, bool GN, bool WF, bool RCP, bool LAND>
+    cudaError_t run() {
+        cdklm_batch_kernel<BW, MINB, FRIC, GN, WF, RCP, LAND><<<grid, BW, 0, s>>>(b->d_args, b->d_dt, b->d_tiles,
+                                                                              b->ntiles, rk_step);
+        return cudaGetLastError();
+    }
+};
+
+int batch_commit(go_batch* b) {
+    if (!b->dirty) return GO_OK;
+    for (int m = 0; m < b->n; ++m)
+        if (!b->member_set[m]) return go_fail(GO_ERR_INVALID, "batch member %d has no state set", m);
+    const int width = shape_block_width(b->shape) - 4;
+    std::vector<int4> tiles;
+    for (int m = 0; m < b->n; ++m) {
+        const Scheme& k = b->members[m]->k;
+        const int gx = (k.nx + width - 1) / width;
+        const int gy = (k.ny + b->rows - 1) / b->rows;
+        for (int y = 0; y < gy; ++y)
+            for (int x = 0; x < gx; ++x) tiles.push_back(make_int4(m, x, y, 0));
+        b->args[2 * m].rows_per_block = b->rows;
+        b->args[2 * m + 1].rows_per_block = b->rows;
+    }
+    cudaFree(b->d_tiles);
+    b->d_tiles = nullptr;
+    GO_CUDA(cudaMalloc(&b->d_tiles, sizeof(int4) * tiles.size()));
+    GO_CUDA(cudaMemcpy(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice));
+    GO_CUDA(cudaMemcpy(b->d_args, b->args.data(), sizeof(StageArgs) * b->args.size(), cudaMemcpyHostToDevice));
+    GO_CUDA(cudaMemcpy(b->d_dt, b->dt.data(), sizeof(float) * b->n, cudaMemcpyHostToDevice));
+    b->ntiles = (int)tiles.size();
+    b->dirty = false;
+    return GO_OK;
+}
+
+int batch_launch(go_batch* b, int rk_step, cudaStream_t s) {
+    int grid = b->ntiles;
+    if (b->blocks > 0 && b->blocks < grid) grid = b->blocks;
+    BatchLaunch L{b, rk_step, grid, s};
+    Variant v = b->variant;
+    v.shape = b->shape;
+    v.rcp = b->arith == GO_ARITH_RCP;
+    const cudaError_t e = dispatch_variant(L, v);
+    if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "batch stage launch failed: %s", cudaGetErrorString(e));
+    return GO_OK;
+}
+
+void drop_graph(go_batch* b) {
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+    b->graph_steps = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int go_batch_create(go_domain* const* members, int n, go_batch** out) {
+    if (!members || !out || n < 1) return go_fail(GO_ERR_INVALID, "need at least one member");
+    *out = nullptr;
+    go_batch* b = new go_batch();
+    b->n = n;
+    b->members.assign(members, members + n);
+    for (int m = 0; m < n; ++m) {
+        if (!members[m]) {
+            delete b;
+            return go_fail(GO_ERR_INVALID, "member %d is null", m);
+        }
+    }
+    const go_domain* d0 = members[0];
+    b->variant = go_variant(d0);
+    b->arith = d0->arith;
+    b->shape = d0->shape;
+    b->rows = d0->rows_per_block;
+    for (int m = 1; m < n; ++m) {
+        const go_domain* d = members[m];
+        b->variant.land = b->variant.land || d->has_land;
+        if (go_friction_mode(d) != b->variant.fric || go_general_north(d) != b->variant.gen_north ||
+            (d->wx_cur != nullptr) != b->variant.wind_field) {
+            delete b;
+            return go_fail(GO_ERR_INVALID,
+                           "member %d needs a different kernel variant (friction law, grid angle or wind "
+                           "field) than member 0; use one batch per variant", m);
+        }
+    }
+    b->args.resize(2 * n);
+    b->member_set.assign(n, 0);
+    b->dt.assign(n, 0.0f);
+    cudaError_t e = cudaMalloc(&b->d_args, sizeof(StageArgs) * 2 * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_dt, sizeof(float) * n);
+    if (e != cudaSuccess) {
+        cudaFree(b->d_args);
+        cudaFree(b->d_dt);
+        delete b;
+        return go_fail(GO_ERR_CUDA, "batch allocation failed: %s", cudaGetErrorString(e));
+    }
+    *out = b;
+    return GO_OK;
+}
+
+int go_batch_destroy(go_batch* b) {
+    if (!b) return GO_OK;
+    drop_graph(b);
+    cudaFree(b->d_args);
+    cudaFree(b->d_dt);
+    cudaFree(b->d_tiles);
+    delete b;
+    return GO_OK;
+}
+
+int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, float* hv0, int pitch0,
+                        float* eta1, float* hu1, float* hv1, int pitch1, const float* Hi, int Hi_pitch,
+                        float land_value, float wind_stress_t) {
+    if (!b || m < 0 || m >= b->n) return go_fail(GO_ERR_INVALID, "bad batch or member index %d", m);
+    if (!eta0 || !hu0 || !hv0 || !eta1 || !hu1 || !hv1 || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
+    const go_domain* d = b->members[m];
+    int rc = go_check_pitch(pitch0, d->k.nx + 4, "h0");
+    if (!rc) rc = go_check_pitch(pitch1, d->k.nx + 4, "h1");
+    if (!rc) rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+    if (rc) return rc;
+    b->args[2 * m] = go_stage_args(d, dt, 0, eta0, hu0, hv0, pitch0 / 4, eta1, hu1, hv1, pitch1 / 4, Hi,
+                                   Hi_pitch / 4, land_value, wind_stress_t);
+    b->args[2 * m + 1] = go_stage_args(d, dt, 1, eta1, hu1, hv1, pitch1 / 4, eta0, hu0, hv0, pitch0 / 4, Hi,
+                                       Hi_pitch / 4, land_value, wind_stress_t);
+    b->dt[m] = dt;
+    b->member_set[m] = 1;
+    b->dirty = true;
+    drop_graph(b);
+    return GO_OK;
+}
+
+int go_batch_set_launch(go_batch* b, int shape, int rows_per_block, int blocks) {
+    if (!b) return go_fail(GO_ERR_INVALID, "null batch");
+    if (shape < 0 || shape > 4) return go_fail(GO_ERR_INVALID, "launch shape %d (0..4)", shape);
+    if (rows_per_block == 0) rows_per_block = 32;
+    if (rows_per_block < 1 || blocks < 0) return go_fail(GO_ERR_INVALID, "rows_per_block >= 1, blocks >= 0");
+    b->shape = shape;
+    b->rows = rows_per_block;
+    b->blocks = blocks;
+    b->dirty = true;
+    drop_graph(b);
+    return GO_OK;
+}
+
+int go_batch_set_arith(go_batch* b, int mode) {
+    if (!b) return go_fail(GO_ERR_INVALID, "null batch");
+    if (mode != GO_ARITH_EXACT && mode != GO_ARITH_RCP) return go_fail(GO_ERR_INVALID, "arith mode %d", mode);
+    b->arith = mode;
+    drop_graph(b);
+    return GO_OK;
+}
+
+int go_batch_set_dt(go_batch* b, void* stream, const float* dt_host) {
+    if (!b || !dt_host) return go_fail(GO_ERR_INVALID, "null argument");
+    for (int m = 0; m < b->n; ++m) {
+        b->dt[m] = dt_host[m];
+        b->args[2 * m].dt = dt_host[m];
+        b->args[2 * m + 1].dt = dt_host[m];
+    }
+    if (b->dirty) return GO_OK;  // uploaded by the next commit
+    GO_CUDA(cudaMemcpyAsync(b->d_dt, b->dt.data(), sizeof(float) * b->n, cudaMemcpyHostToDevice,
+                            (cudaStream_t)stream));
+    GO_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return GO_OK;
+}
+
+int go_batch_tiles(go_batch* b, int* ntiles) {
+    if (!b || !ntiles) return go_fail(GO_ERR_INVALID, "null argument");
+    int rc = batch_commit(b);
+    if (rc) return rc;
+    *ntiles = b->ntiles;
+    return GO_OK;
+}
+
+int go_batch_step(go_batch* b, void* stream, int n_steps) {
+    if (!b || n_steps < 0) return go_fail(GO_ERR_INVALID, "bad arguments");
+    int rc = batch_commit(b);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int i = 0; i < n_steps; ++i) {
+        rc = batch_launch(b, 0, s);
+        if (rc) return rc;
+        rc = batch_launch(b, 1, s);
+        if (rc) return rc;
+    }
+    return GO_OK;
+}
+
+int go_batch_graph_capture(go_batch* b, void* stream, int n_steps) {
+    if (!b || n_steps < 1) return go_fail(GO_ERR_INVALID, "bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (s == nullptr) return go_fail(GO_ERR_INVALID, "graph capture needs a non-default stream");
+    int rc = batch_commit(b);
+    if (rc) return rc;
+    drop_graph(b);
+    GO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < n_steps && !rc; ++i) {
+        rc = batch_launch(b, 0, s);
+        if (!rc) rc = batch_launch(b, 1, s);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    b->graph = g;
+    GO_CUDA(cudaGraphInstantiate(&b->graph_exec, g, 0));
+    b->graph_steps = n_steps;
+    return GO_OK;
+}
+
+int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done) {
+    if (!b) return go_fail(GO_ERR_INVALID, "null batch");
+    if (!b->graph_exec) return go_fail(GO_ERR_INVALID, "no captured graph (go_batch_graph_capture)");
+    GO_CUDA(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream));
+    if (steps_done) *steps_done = b->graph_steps;
+    return GO_OK;
+}
+
+}  // extern "C"

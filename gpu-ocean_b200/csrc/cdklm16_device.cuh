@@ -64,7 +64,15 @@ __device__ __forceinline__ float desingularize(float h, float hu, float eps) {
     return hu / fmaxf(fminf(a, eps), fabsf(h));
 }
 
-// CDKLM16_flux, CDKLM16_kernel.cu:80-140.  Face states are (h, u, v).
+__device__ __forceinline__ float rcp_approx_f(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// CDKLM16_flux, CDKLM16_kernel.cu:80-140.  Face states are (h, u, v).  RCP:
+// the two quotients by (ap - am) share one reciprocal.
+template <bool RCP>
 __device__ __forceinline__ F3 central_upwind(float hm, float um, float vm,
                                              float hp, float up, float vp,
                                              const Scheme& k) {
@@ -88,8 +96,14 @@ __device__ __forceinline__ F3 central_upwind(float hm, float um, float vm,
     const float ap = fmaxf(fmaxf(umw + cm, upw + cp), 0.0f);
     if (fabsf(ap - am) < k.flux_slope_eps) return F3{0.0f, 0.0f, 0.0f};
     F3 F;
-    F.a = ((ap * Fm0 - am * Fp0) + ap * am * (hp - hm)) / (ap - am);
-    F.b = ((ap * Fm1 - am * Fp1) + ap * am * (Fp0 - Fm0)) / (ap - am);
+    if (RCP) {
+        const float rd = rcp_approx_f(ap - am);
+        F.a = ((ap * Fm0 - am * Fp0) + ap * am * (hp - hm)) * rd;
+        F.b = ((ap * Fm1 - am * Fp1) + ap * am * (Fp0 - Fm0)) * rd;
+    } else {
+        F.a = ((ap * Fm0 - am * Fp0) + ap * am * (hp - hm)) / (ap - am);
+        F.b = ((ap * Fm1 - am * Fp1) + ap * am * (Fp0 - Fm0)) / (ap - am);
+    }
     F.c = (um + up > 0.0f) ? Fm2 : Fp2;
     return F;
 }

@@ -4,18 +4,35 @@
 // followed by the periodic ghost refresh the host issues after it
 // (Common.py:1219-1239 -> boundary_kernels.cu:35-110).
 //
-// Layout of the work: a block of BW threads covers BW consecutive
-// ghost-inclusive columns cl = c0-2 .. c0+BW-3 and writes the BW-4 interior
-// columns c0 .. c0+BW-5.  Each thread owns one column and marches down the
-// block's strip of rows [r0, r1).  Everything along y (the slopes u_y, v_y,
-// L_y and the G fluxes) lives in registers as a sliding window of rows; the
-// x direction (slopes u_x, v_x, K_x and the F fluxes) is exchanged between
-// neighbouring threads through three shared-memory row buffers.  Each face
-// flux is evaluated once (the reference evaluates every face twice, once
-// per adjacent cell).  Ghost cells: wall sides are mirrored on load (as
-// handleWallBC, CDKLM16_kernel.cu:373-424, does in shared memory);
-// periodic sides read the ghost cells of the input, which the previous
-// stage refreshed.
+// Work layout.  A block of BW threads covers BW consecutive ghost-inclusive
+// columns cl = c0-2 .. c0+BW-3 and writes the BW-4 interior columns
+// c0 .. c0+BW-5.  Each thread owns one column and marches down the block's
+// strip of rows [r0, r1).  The y direction (slopes u_y, v_y, L_y, G fluxes)
+// lives in registers as a sliding window of rows; the x direction (slopes
+// u_x, v_x, K_x, F fluxes) is exchanged between neighbouring threads through
+// three shared-memory row buffers of float4.  Each face flux is evaluated
+// once (the reference evaluates every face twice, once per adjacent cell).
+//
+// Paired arithmetic.  At row j the x-direction work of row j and the
+// y-direction work of row j+1 have the same shape (slopes, slope
+// adjustment, central-upwind flux), so they run side by side as the two
+// lanes of float2 values; their sums and differences issue as packed
+// add/sub.rn.ftz.f32x2 (per lane the same IEEE round-to-nearest,
+// flush-to-zero result as the scalar operation, so results stay identical
+// to the scalar evaluation order of the reference).  In the
+// flux, lane x carries (u normal, v tangential) and lane y (v normal, u
+// tangential), which is how the reference swaps u and v for the G flux
+// (CDKLM16_kernel.cu:361-369).  Signs: a - b*c is written a + (-b)*c, which
+// IEEE arithmetic rounds identically.
+//
+// Ghost cells: walls are mirrored on load (as handleWallBC,
+// CDKLM16_kernel.cu:373-424, does in shared memory); periodic sides read the
+// ghost cells of the input, which the previous stage refreshed.  Blocks that
+// touch no boundary (EDGE = false) compile without any of that logic.
+//
+// RCP selects how a quotient a/b is evaluated: false keeps the '/' of the
+// reference source (div.full.f32 under --prec-div=false); true evaluates
+// a * rcp.approx.ftz(b) with reciprocals of shared denominators hoisted.
 #pragma once
 
 #include "cdklm16_device.cuh"
@@ -42,34 +59,187 @@ struct StageArgs {
 // Friction law selector.
 enum { kFricNone = 0, kFricQuad = 1, kFricLinear = 2 };
 
-template <int BW, int FRIC, bool GEN_NORTH, bool WIND_FIELD>
-__global__ void __launch_bounds__(BW) cdklm_stage_kernel(const StageArgs a) {
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+template <bool RCP>
+__device__ __forceinline__ float quot(float a, float b) {
+    if (RCP) return a * rcp_approx(b);
+    return a / b;
+}
+
+// ---- paired float2 helpers -----------------------------------------------
+// Sums and differences run as packed add/sub.rn.ftz.f32x2: per lane the IEEE
+// round-to-nearest result with subnormals flushed, i.e. what the scalar
+// add.rn.ftz of a --ftz=true --fmad=false build computes.  Products stay two
+// scalar multiplies: ptxas may contract a packed multiply feeding a packed
+// add into a fused FFMA2 (observed on sm_100a even with explicit .rn and
+// -fmad=false), which would round differently from the reference, while a
+// scalar product cannot be fused into a packed add.
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+#ifdef GO_SCALAR_PAIRS
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return f2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return f2(a.x - b.x, a.y - b.y); }
+#else
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+#endif
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return f2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 neg2(float2 a) { return f2(-a.x, -a.y); }
+__device__ __forceinline__ float2 sel2(bool cx, bool cy, float2 a, float2 b) {
+    return f2(cx ? a.x : b.x, cy ? a.y : b.y);
+}
+
+template <bool RCP>
+__device__ __forceinline__ float2 quot2(float2 a, float2 b) {
+    if (RCP) return mul2(a, f2(rcp_approx(b.x), rcp_approx(b.y)));
+    return f2(a.x / b.x, a.y / b.y);
+}
+
+// minmod of three differences per lane (common.cu:544-551; see minmod_raw).
+__device__ __forceinline__ float2 minmod2(float2 b, float2 c, float2 f) {
+    return f2(minmod_raw(b.x, c.x, f.x), minmod_raw(b.y, c.y, f.y));
+}
+
+// minmodSlope per lane (common.cu:532-542)
+__device__ __forceinline__ float2 minmod_slope2(float2 l, float2 c, float2 r, float2 theta) {
+    const float2 backward = mul2(sub2(c, l), theta);
+    const float2 central = mul2(sub2(r, l), f2(0.5f, 0.5f));
+    const float2 forward = mul2(sub2(r, c), theta);
+    return minmod2(backward, central, forward);
+}
+
+// CDKLM16_flux (CDKLM16_kernel.cu:101-140) on two faces at once.  Per lane
+// the face states are (h, un, ut) with un the velocity normal to the face;
+// returns (mass, normal momentum, tangential momentum) fluxes per lane.
+template <bool RCP>
+__device__ __forceinline__ void central_upwind2(float2 hm, float2 um, float2 vm, float2 hp, float2 up,
+                                                float2 vp, const Scheme& k, float2& F0, float2& F1,
+                                                float2& F2) {
+    const bool wpx = hp.x > k.cutoff, wpy = hp.y > k.cutoff;
+    const bool wmx = hm.x > k.cutoff, wmy = hm.y > k.cutoff;
+    const float2 hg = f2(k.half_g, k.half_g);
+    const float2 g2 = f2(k.g, k.g);
+    const float2 z = f2(0.0f, 0.0f);
+    // F = (h u, h u u + 0.5 g h h, h u v), CDKLM16_kernel.cu:80-88
+    const float2 hpu = mul2(hp, up);
+    const float2 hmu = mul2(hm, um);
+    float2 Fp0 = hpu, Fp1 = add2(mul2(hpu, up), mul2(mul2(hg, hp), hp)), Fp2 = mul2(hpu, vp), upw = up;
+    float2 Fm0 = hmu, Fm1 = add2(mul2(hmu, um), mul2(mul2(hg, hm), hm)), Fm2 = mul2(hmu, vm), umw = um;
+    const float2 gp = mul2(g2, hp), gm = mul2(g2, hm);
+    float2 cp, cm;
+    if (wpx && wpy && wmx && wmy) {   // all four face states wet: no selection needed
+        cp = f2(sqrtf(gp.x), sqrtf(gp.y));
+        cm = f2(sqrtf(gm.x), sqrtf(gm.y));
+    } else {                          // a dry side contributes nothing (:108-123)
+        Fp0 = sel2(wpx, wpy, Fp0, z); Fp1 = sel2(wpx, wpy, Fp1, z); Fp2 = sel2(wpx, wpy, Fp2, z);
+        upw = sel2(wpx, wpy, upw, z);
+        Fm0 = sel2(wmx, wmy, Fm0, z); Fm1 = sel2(wmx, wmy, Fm1, z); Fm2 = sel2(wmx, wmy, Fm2, z);
+        umw = sel2(wmx, wmy, umw, z);
+        cp = f2(wpx ? sqrtf(gp.x) : 0.0f, wpy ? sqrtf(gp.y) : 0.0f);
+        cm = f2(wmx ? sqrtf(gm.x) : 0.0f, wmy ? sqrtf(gm.y) : 0.0f);
+    }
+    const float2 a1 = sub2(umw, cm), a2 = sub2(upw, cp);
+    const float2 b1 = add2(umw, cm), b2 = add2(upw, cp);
+    const float2 am = f2(fminf(fminf(a1.x, a2.x), 0.0f), fminf(fminf(a1.y, a2.y), 0.0f));
+    const float2 ap = f2(fmaxf(fmaxf(b1.x, b2.x), 0.0f), fmaxf(fmaxf(b1.y, b2.y), 0.0f));
+    const float2 d = sub2(ap, am);
+    const float2 apam = mul2(ap, am);
+    const float2 n0 = add2(sub2(mul2(ap, Fm0), mul2(am, Fp0)), mul2(apam, sub2(hp, hm)));
+    const float2 n1 = add2(sub2(mul2(ap, Fm1), mul2(am, Fp1)), mul2(apam, sub2(Fp0, Fm0)));
+    F0 = quot2<RCP>(n0, d);
+    F1 = quot2<RCP>(n1, d);
+    const float2 s = add2(um, up);
+    F2 = f2(s.x > 0.0f ? Fm2.x : Fp2.x, s.y > 0.0f ? Fm2.y : Fp2.y);   // upwinded tangential flux
+    const bool zx = fabsf(d.x) < k.flux_slope_eps, zy = fabsf(d.y) < k.flux_slope_eps;
+    if (zx || zy) {   // symmetric Riemann fan: zero flux (:128-131)
+        F0 = sel2(zx, zy, z, F0); F1 = sel2(zx, zy, z, F1); F2 = sel2(zx, zy, z, F2);
+    }
+}
+
+struct Cell { float e, u, v; };     // reconstruction state (eta, u, v)
+
+// Shared-memory row buffers of one block.
+template <int BW>
+struct RowBufs {
+    float4 r[BW];   // (eta, u, v, f*v along north)
+    float4 s[BW];   // (u_x, v_x, K_x, -)
+    float4 f[BW];   // F flux on the face west of the column
+};
+
+// Divisor by a domain constant c: a/c, or a * (1/c) with 1/c hoisted.
+template <bool RCP>
+struct ConstDiv {
+    float c, inv;
+    __device__ __forceinline__ explicit ConstDiv(float c_) : c(c_), inv(RCP ? rcp_approx(c_) : 0.0f) {}
+    __device__ __forceinline__ float operator()(float a) const { return RCP ? a * inv : a / c; }
+    __device__ __forceinline__ float2 operator()(float2 a) const {
+        if (RCP) return mul2(a, f2(inv, inv));
+        return f2(a.x / c, a.y / c);
+    }
+};
+
+// True when the strip [r0, r1) of columns starting at c0 touches no ghost
+// cell, wall flip, or periodic image: such blocks run the EDGE = false path.
+template <int BW>
+__device__ __forceinline__ bool interior_block(const Scheme& k, int c0, int r0, int r1) {
+    return c0 >= 6 && c0 + BW - 3 <= k.nx - 1 && r0 >= 4 && r1 <= k.ny;
+}
+
+// One block strip: columns of block bx, rows of block by.
+template <int BW, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, bool EDGE>
+__device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, const int bx, const int by,
+                                            RowBufs<BW>& sb) {
     const Scheme& k = a.k;
     const int t = threadIdx.x;
-    const int c0 = 2 + blockIdx.x * (BW - 4);
+    const int c0 = 2 + bx * (BW - 4);
     const int cl = c0 - 2 + t;
-    const int r0 = 2 + blockIdx.y * a.rows_per_block;
+    const int r0 = 2 + by * a.rows_per_block;
     const int r1 = min(r0 + a.rows_per_block, k.ny + 2);
 
-    __shared__ float sE[BW], sU[BW], sV[BW], sFv[BW];
-    __shared__ float sUx[BW], sVx[BW], sKx[BW];
-    __shared__ float sF0[BW], sF1[BW], sF2[BW];
+    const ConstDiv<RCP> by2g(k.two_g);
+    const float inv_dx = RCP ? rcp_approx(k.dx) : 0.0f;
+    const float inv_dy = RCP ? rcp_approx(k.dy) : 0.0f;
+    auto bydxdy = [&](float2 v) -> float2 {
+        if (RCP) return mul2(v, f2(inv_dx, inv_dy));
+        return f2(v.x / k.dx, v.y / k.dy);
+    };
 
     // ---- column addressing ------------------------------------------------
-    // Q columns: wall ghosts mirror the interior with hu odd; columns past
-    // the array (threads of the last block) clamp and are never written.
-    int qc = min(cl, k.nx + 3);
+    int qc = cl;
     float hu_sgn = 1.0f;
-    if (k.bcW == kWall && cl < 2) { qc = 3 - cl; hu_sgn = -1.0f; }
-    if (k.bcE == kWall && cl > k.nx + 1 && cl <= k.nx + 3) { qc = 2 * k.nx + 3 - cl; hu_sgn = -1.0f; }
-    const int hca = min(cl, k.nx + 4);      // corner column of the cell's west side
-    const int hcb = min(cl + 1, k.nx + 4);  // east side
+    if (EDGE) {
+        // wall ghosts mirror the interior with hu odd; columns past the array
+        // (threads of the last block) clamp and are never written
+        qc = min(cl, k.nx + 3);
+        if (k.bcW == kWall && cl < 2) { qc = 3 - cl; hu_sgn = -1.0f; }
+        if (k.bcE == kWall && cl > k.nx + 1 && cl <= k.nx + 3) { qc = 2 * k.nx + 3 - cl; hu_sgn = -1.0f; }
+    }
+    const int hca = EDGE ? min(cl, k.nx + 4) : cl;          // corner column west of the cell
+    const int hcb = EDGE ? min(cl + 1, k.nx + 4) : cl + 1;  // east
 
     // Wall sign flips that the reference applies by global index.
-    const bool flipKx = (k.bcW == kWall && cl < 2) || (k.bcE == kWall && cl > k.nx + 1);    // :633-641
-    const bool flipAdjX = (k.bcW == kWall && cl < 2) || (k.bcE == kWall && cl > k.nx + 2);  // :172-174
-    const bool flipFm = (k.bcW == kWall && cl == 2);            // :286 (face west of cl)
-    const bool flipFp = (k.bcE == kWall && cl == k.nx + 2);     // :288
+    const bool flipKx = EDGE && ((k.bcW == kWall && cl < 2) || (k.bcE == kWall && cl > k.nx + 1));   // :633-641
+    const bool flipAdjX = EDGE && ((k.bcW == kWall && cl < 2) || (k.bcE == kWall && cl > k.nx + 2)); // :172-174
+    const bool flipFm = EDGE && (k.bcW == kWall && cl == 2);            // :286 (face west of cl)
+    const bool flipFp = EDGE && (k.bcE == kWall && cl == k.nx + 2);     // :288
+    auto flipLy = [&](int r) { return EDGE && ((k.bcS == kWall && r < 2) || (k.bcN == kWall && r > k.ny + 1)); };
+    auto flipAdjY = [&](int r) { return EDGE && ((k.bcS == kWall && r < 2) || (k.bcN == kWall && r > k.ny + 2)); };
 
     const float eX = k.nY, eY = -k.nX;      // east = (north.y, -north.x), :681
 
@@ -79,213 +249,274 @@ __global__ void __launch_bounds__(BW) cdklm_stage_kernel(const StageArgs a) {
     const float* __restrict__ Hi = a.Hi;
     const float* __restrict__ frow = a.f_rows;
 
-    auto qrow = [&](int r, float& hv_sgn) -> int {
-        hv_sgn = 1.0f;
-        if (k.bcS == kWall && r < 2) { hv_sgn = -1.0f; return 3 - r; }
-        if (k.bcN == kWall && r > k.ny + 1) { hv_sgn = -1.0f; return 2 * k.ny + 3 - r; }
-        return r;
-    };
     auto load_q = [&](int r, float& e, float& hu, float& hv) {
-        float s;
-        const int rr = qrow(r, s);
+        float hv_sgn = 1.0f;
+        int rr = r;
+        if (EDGE) {
+            if (k.bcS == kWall && r < 2) { hv_sgn = -1.0f; rr = 3 - r; }
+            else if (k.bcN == kWall && r > k.ny + 1) { hv_sgn = -1.0f; rr = 2 * k.ny + 3 - r; }
+        }
         const size_t o = (size_t)rr * a.pin + qc;
         e = __ldg(eta_in + o);
-        hu = hu_sgn * __ldg(hu_in + o);
-        hv = s * __ldg(hv_in + o);
+        hu = __ldg(hu_in + o);
+        hv = __ldg(hv_in + o);
+        if (EDGE) { hu *= hu_sgn; hv *= hv_sgn; }
     };
     auto load_h = [&](int r, float& ha, float& hb) {
         const size_t o = (size_t)r * a.phi;
-        ha = corner(__ldg(Hi + o + hca), k);
-        hb = corner(__ldg(Hi + o + hcb), k);
+        ha = __ldg(Hi + o + hca);
+        hb = __ldg(Hi + o + hcb);
+        if (LAND) { ha = corner(ha, k); hb = corner(hb, k); }
     };
-    auto bm_of = [&](float ha0, float hb0, float ha1, float hb1) {
+    auto to_cell = [&](float e, float hu, float hv, float ha0, float hb0, float ha1, float hb1) {
         const float s = ((ha0 + ha1) + hb0) + hb1;
-        return cell_bm(ha0, ha1, hb0, hb1, s, k);
+        const float Bm = LAND ? cell_bm(ha0, ha1, hb0, hb1, s, k) : s * 0.25f;
+        Cell p;
+        const float h = e + Bm;
+        if (LAND && fabsf(Bm - k.land) <= kDryEps) {
+            p.e = kDryFlag; p.u = 0.0f; p.v = 0.0f;
+        } else if (h < k.desing_eps) {
+            if (h <= k.cutoff) {
+                p.e = -Bm + k.cutoff; p.u = 0.0f; p.v = 0.0f;
+            } else {
+                p.e = e;
+                p.u = desingularize(h, hu, k.desing_eps);
+                p.v = desingularize(h, hv, k.desing_eps);
+            }
+        } else {
+            p.e = e;
+            const float2 uv = quot2<RCP>(f2(hu, hv), f2(h, h));
+            p.u = uv.x; p.v = uv.y;
+        }
+        return p;
     };
-    // v used in the Coriolis part of K_x, and u in that of L_y
-    auto fv_of = [&](const Prim& p, float f) {
-        const float vv = flipKx ? -p.v : p.v;
-        if (GEN_NORTH) return (k.nX * p.u + k.nY * vv) * f;
-        return vv * f;
-    };
-    auto fu_of = [&](const Prim& p, int r, float f) {
-        const bool fl = (k.bcS == kWall && r < 2) || (k.bcN == kWall && r > k.ny + 1);  // :738-746
-        const float uu = fl ? -p.u : p.u;
+    // Coriolis part of L_y of a cell of row r, (east . (u', v)) f with u'
+    // flipped in wall ghost rows (:738-758)
+    auto fu_of = [&](const Cell& p, int r, float f) {
+        const float uu = flipLy(r) ? -p.u : p.u;
         if (GEN_NORTH) return (eX * uu + eY * p.v) * f;
         return uu * f;
     };
-    // y slope at row r from rows r-1 (lo), r (c), r+1 (up); Hs/Hn are the
-    // y-face depths south and north of the cell.  :715-777
-    auto y_slope = [&](const Prim& lo, const Prim& c, const Prim& up, int r,
-                       float flo, float fc, float fup, float Hs, float Hn) {
-        Slp s;
-        s.du = minmod_slope(lo.u, c.u, up.u, k.theta);
-        s.dv = minmod_slope(lo.v, c.v, up.v, k.theta);
-        const float fulo = fu_of(lo, r - 1, flo);
-        const float fuc = fu_of(c, r, fc);
-        const float fuup = fu_of(up, r + 1, fup);
+    // y slope (u_y, v_y, L_y) at row r, scalar; used for the first rows only
+    auto y_slope = [&](const Cell& lo, const Cell& c, const Cell& up, int r, float fulo, float fuc,
+                       float fuup, float fc, float Hs, float Hn, float& du, float& dv) {
+        du = minmod_slope(lo.u, c.u, up.u, k.theta);
+        dv = minmod_slope(lo.v, c.v, up.v, k.theta);
         const float backward = k.theta_g * ((c.e - lo.e) + k.U * (fuc + fulo));
         const float central = k.half_g * ((up.e - lo.e) + k.U * ((fuup + 2.0f * fuc) + fulo));
         const float forward = k.theta_g * ((up.e - c.e) + k.U * (fuc + fuup));
         float L = minmod_raw(backward, central, forward);
-        // adjustSlopes_y, :198-241
-        const bool fl = (k.bcS == kWall && r < 2) || (k.bcN == kWall && r > k.ny + 2);
-        const float uu = fl ? -c.u : c.u;
+        const float uu = flipAdjY(r) ? -c.u : c.u;   // adjustSlopes_y, :198-241
         const float dyfu = (k.dy * fc) * uu;
-        const float h_s = (c.e + Hs) - (L - dyfu) / k.two_g;
-        const float h_n = (c.e + Hn) + (L - dyfu) / k.two_g;
+        const float q = by2g(L - dyfu);
+        const float h_s = (c.e + Hs) - q;
+        const float h_n = (c.e + Hn) + q;
         L = (h_s > 0.0f) ? L : dyfu + k.two_g * (c.e + Hs);
         L = (h_n > 0.0f) ? L : dyfu - k.two_g * (c.e + Hn);
-        s.K = L;
-        return s;
-    };
-    // G flux on the face between rows r (m) and r+1 (p).  :309-370
-    auto g_face = [&](const Prim& m, const Slp& sm, const Prim& p, const Slp& sp, int r,
-                      float fm, float fp, float Hface) {
-        if (p.e == kDryFlag || m.e == kDryFlag) return F3{0.0f, 0.0f, 0.0f};
-        const float Rpu = p.u - 0.5f * sp.du, Rpv = p.v - 0.5f * sp.dv;
-        const float Rmu = m.u + 0.5f * sm.du, Rmv = m.v + 0.5f * sm.dv;
-        const float um = (k.bcS == kWall && r + 1 == 2) ? -m.u : m.u;
-        const float upp = (k.bcN == kWall && r + 1 == k.ny + 2) ? -p.u : p.u;
-        float up_east, um_east;
-        if (GEN_NORTH) { up_east = upp * eX + p.v * eY; um_east = um * eX + m.v * eY; }
-        else { up_east = upp; um_east = um; }
-        const float hp = fmaxf(0.0f, (p.e + Hface) - (sp.K - (k.dy * fp) * up_east) / k.two_g);
-        const float hm = fmaxf(0.0f, (m.e + Hface) + (sm.K - (k.dy * fm) * um_east) / k.two_g);
-        const F3 F = central_upwind(hm, Rmv, Rmu, hp, Rpv, Rpu, k);
-        return F3{F.a, F.c, F.b};
+        return L;
     };
 
     // ---- prime the window for rows r0-2 .. r0+1 ---------------------------
-    float Ha[4], Hb[4];  // corner rows j..j+3 at columns cl (a) and cl+1 (b)
-    float ha_m2, hb_m2, ha_m1, hb_m1;
-    load_h(r0 - 2, ha_m2, hb_m2);
-    load_h(r0 - 1, ha_m1, hb_m1);
-    load_h(r0, Ha[0], Hb[0]);
-    load_h(r0 + 1, Ha[1], Hb[1]);
-    load_h(r0 + 2, Ha[2], Hb[2]);
-
-    Prim Pm2, Pm1, P0, P1;
+    float Ha0, Hb0, Ha1, Hb1, Ha2, Hb2;   // corner rows j, j+1, j+2 at cl (a), cl+1 (b)
+    float ham2, hbm2, ham1, hbm1;
+    load_h(r0 - 2, ham2, hbm2);
+    load_h(r0 - 1, ham1, hbm1);
+    load_h(r0, Ha0, Hb0);
+    load_h(r0 + 1, Ha1, Hb1);
+    load_h(r0 + 2, Ha2, Hb2);
+    Cell Pm2, Pm1, P0, P1;
     {
         float e, hu, hv;
-        load_q(r0 - 2, e, hu, hv); Pm2 = to_prim(e, hu, hv, bm_of(ha_m2, hb_m2, ha_m1, hb_m1), k);
-        load_q(r0 - 1, e, hu, hv); Pm1 = to_prim(e, hu, hv, bm_of(ha_m1, hb_m1, Ha[0], Hb[0]), k);
-        load_q(r0, e, hu, hv);     P0 = to_prim(e, hu, hv, bm_of(Ha[0], Hb[0], Ha[1], Hb[1]), k);
-        load_q(r0 + 1, e, hu, hv); P1 = to_prim(e, hu, hv, bm_of(Ha[1], Hb[1], Ha[2], Hb[2]), k);
+        load_q(r0 - 2, e, hu, hv); Pm2 = to_cell(e, hu, hv, ham2, hbm2, ham1, hbm1);
+        load_q(r0 - 1, e, hu, hv); Pm1 = to_cell(e, hu, hv, ham1, hbm1, Ha0, Hb0);
+        load_q(r0, e, hu, hv);     P0 = to_cell(e, hu, hv, Ha0, Hb0, Ha1, Hb1);
+        load_q(r0 + 1, e, hu, hv); P1 = to_cell(e, hu, hv, Ha1, Hb1, Ha2, Hb2);
     }
-    float f_m2 = __ldg(frow + r0 - 2), f_m1 = __ldg(frow + r0 - 1);
+    const float f_m2 = __ldg(frow + r0 - 2), f_m1 = __ldg(frow + r0 - 1);
     float f0 = __ldg(frow + r0), f1 = __ldg(frow + r0 + 1);
+    const float fu_m2 = fu_of(Pm2, r0 - 2, f_m2);
+    const float fu_m1 = fu_of(Pm1, r0 - 1, f_m1);
+    float fu0 = fu_of(P0, r0, f0);
+    float fu1 = fu_of(P1, r0 + 1, f1);
+    const float Hy_m1 = 0.5f * (ham1 + hbm1);
+    float Hy0 = 0.5f * (Ha0 + Hb0);
+    float Hy1 = 0.5f * (Ha1 + Hb1);
+    // slopes at r0-1 and r0, G flux on the face (r0-1 | r0)
+    float uy_m1, vy_m1, uy0, vy0;
+    const float Ly_m1 = y_slope(Pm2, Pm1, P0, r0 - 1, fu_m2, fu_m1, fu0, f_m1, Hy_m1, Hy0, uy_m1, vy_m1);
+    float Ly0 = y_slope(Pm1, P0, P1, r0, fu_m1, fu0, fu1, f0, Hy0, Hy1, uy0, vy0);
+    float Gs0, Gs1, Gs2;   // G on the face south of row j: (mass, hu, hv) fluxes
+    {
+        const bool dry = (P0.e == kDryFlag || Pm1.e == kDryFlag);
+        const float um = (EDGE && k.bcS == kWall && r0 == 2) ? -Pm1.u : Pm1.u;
+        const float upp = (EDGE && k.bcN == kWall && r0 == k.ny + 2) ? -P0.u : P0.u;
+        float up_east = upp, um_east = um;
+        if (GEN_NORTH) { up_east = upp * eX + P0.v * eY; um_east = um * eX + Pm1.v * eY; }
+        const float hp = fmaxf(0.0f, (P0.e + Hy0) - by2g(Ly0 - (k.dy * f0) * up_east));
+        const float hm = fmaxf(0.0f, (Pm1.e + Hy0) + by2g(Ly_m1 - (k.dy * f_m1) * um_east));
+        float2 F0, F1, F2;
+        central_upwind2<RCP>(f2(hm, hm), f2(Pm1.v + 0.5f * vy_m1, 0.0f), f2(Pm1.u + 0.5f * uy_m1, 0.0f),
+                             f2(hp, hp), f2(P0.v - 0.5f * vy0, 0.0f), f2(P0.u - 0.5f * uy0, 0.0f), k, F0, F1, F2);
+        Gs0 = dry ? 0.0f : F0.x;
+        Gs1 = dry ? 0.0f : F2.x;
+        Gs2 = dry ? 0.0f : F1.x;
+    }
 
-    const float Hy_m1 = 0.5f * (ha_m1 + hb_m1);
-    const float Hy_0 = 0.5f * (Ha[0] + Hb[0]);
-    const float Hy_1 = 0.5f * (Ha[1] + Hb[1]);
-    const Slp Sm1 = y_slope(Pm2, Pm1, P0, r0 - 1, f_m2, f_m1, f0, Hy_m1, Hy_0);
-    Slp S0 = y_slope(Pm1, P0, P1, r0, f_m1, f0, f1, Hy_0, Hy_1);
-    F3 Gs = g_face(Pm1, Sm1, P0, S0, r0 - 1, f_m1, f0, Hy_0);
-
-    // prefetch row r0+2 (Q) and corner row r0+3
+    // prefetch row r0+2 (Q), corner row r0+3, f(r0+2) and, for stage 1, Q^n(r0)
     float nq_e, nq_hu, nq_hv, nha, nhb, nf;
     load_q(r0 + 2, nq_e, nq_hu, nq_hv);
     load_h(r0 + 3, nha, nhb);
     nf = __ldg(frow + r0 + 2);
 
     const int tl = max(t - 1, 0), tr = min(t + 1, BW - 1);
-    const bool writer = (t >= 2) && (t < BW - 2) && (cl <= k.nx + 1);
+    const bool writer = (t >= 2) && (t < BW - 2) && (!EDGE || cl <= k.nx + 1);
+    const bool stage1 = (a.rk_step == 1);
+    float nqn_e = 0.0f, nqn_hu = 0.0f, nqn_hv = 0.0f;
+    if (stage1 && writer) {
+        const size_t o = (size_t)r0 * a.pout + cl;
+        nqn_e = a.eta_out[o]; nqn_hu = a.hu_out[o]; nqn_hv = a.hv_out[o];
+    }
+    const bool col_img = EDGE && (k.bcE == kPeriodic) && (cl < 4 || cl >= k.nx);
+    const float2 theta2 = f2(k.theta, k.theta);
+    const float2 thg2 = f2(k.theta_g, k.theta_g);
+    const float2 hg2 = f2(k.half_g, k.half_g);
+    const float2 VU2 = f2(-k.V, k.U);          // K_x subtracts V*(.), L_y adds U*(.)
+    const float2 two_g2 = f2(k.two_g, k.two_g);
 
+#pragma unroll 1
     for (int j = r0; j < r1; ++j) {
         // ---- row j+2 arrives; prefetch j+3 --------------------------------
-        Ha[3] = nha; Hb[3] = nhb;
-        const float f2 = nf;
-        float q_e = nq_e, q_hu = nq_hu, q_hv = nq_hv;
+        const float Ha3 = nha, Hb3 = nhb, f2r = nf;
+        const float q_e = nq_e, q_hu = nq_hu, q_hv = nq_hv;
+        const float qn_e = nqn_e, qn_hu = nqn_hu, qn_hv = nqn_hv;
         {
-            const int rn = min(j + 3, r1 + 1);
-            load_q(rn, nq_e, nq_hu, nq_hv);
-            const int hn = min(j + 4, r1 + 2);
-            load_h(hn, nha, nhb);
+            load_q(min(j + 3, r1 + 1), nq_e, nq_hu, nq_hv);
+            load_h(min(j + 4, r1 + 2), nha, nhb);
             nf = __ldg(frow + min(j + 3, k.ny + 3));
-        }
-        float qn_e = 0.0f, qn_hu = 0.0f, qn_hv = 0.0f;
-        if (a.rk_step == 1 && writer) {
-            const size_t o = (size_t)j * a.pout + cl;
-            qn_e = a.eta_out[o]; qn_hu = a.hu_out[o]; qn_hv = a.hv_out[o];
-        }
-        const Prim P2 = to_prim(q_e, q_hu, q_hv, bm_of(Ha[2], Hb[2], Ha[3], Hb[3]), k);
-
-        // ---- y direction: slope at j+1, G on face (j | j+1) ----------------
-        const float Hy1 = 0.5f * (Ha[1] + Hb[1]);
-        const float Hy2 = 0.5f * (Ha[2] + Hb[2]);
-        const Slp S1 = y_slope(P0, P1, P2, j + 1, f0, f1, f2, Hy1, Hy2);
-        const F3 Gn = g_face(P0, S0, P1, S1, j, f0, f1, Hy1);
-
-        // ---- x direction on row j ------------------------------------------
-        const float fv = fv_of(P0, f0);
-        sE[t] = P0.e; sU[t] = P0.u; sV[t] = P0.v; sFv[t] = fv;
-        __syncthreads();
-        const float eL = sE[tl], uL = sU[tl], vL = sV[tl], fvL = sFv[tl];
-        const float eR = sE[tr], uR = sU[tr], fvR = sFv[tr];
-        const float vR = sV[tr];
-        const float ux = minmod_slope(uL, P0.u, uR, k.theta);
-        const float vx = minmod_slope(vL, P0.v, vR, k.theta);
-        float Kx;
-        {
-            const float backward = k.theta_g * ((P0.e - eL) - k.V * (fv + fvL));
-            const float central = k.half_g * ((eR - eL) - k.V * ((fvR + 2.0f * fv) + fvL));
-            const float forward = k.theta_g * ((eR - P0.e) - k.V * (fv + fvR));
-            Kx = minmod_raw(backward, central, forward);
-        }
-        const float Hw = 0.5f * (Ha[0] + Ha[1]);  // x-face depth west of the cell
-        const float He = 0.5f * (Hb[0] + Hb[1]);  // east
-        {   // adjustSlopes_x, :148-191
-            const float vv = flipAdjX ? -P0.v : P0.v;
-            const float dxfv = (k.dx * f0) * vv;
-            const float h_w = (P0.e + Hw) - (Kx + dxfv) / k.two_g;
-            const float h_e = (P0.e + He) + (Kx + dxfv) / k.two_g;
-            Kx = (h_w > 0.0f) ? Kx : -dxfv + k.two_g * (P0.e + Hw);
-            Kx = (h_e > 0.0f) ? Kx : -dxfv - k.two_g * (P0.e + He);
-        }
-        sUx[t] = ux; sVx[t] = vx; sKx[t] = Kx;
-        __syncthreads();
-        F3 Fw;   // F on the face (cl-1 | cl), :246-304
-        {
-            const float uxm = sUx[tl], vxm = sVx[tl], Kxm = sKx[tl];
-            if (P0.e == kDryFlag || eL == kDryFlag) {
-                Fw = F3{0.0f, 0.0f, 0.0f};
-            } else {
-                const float Rpu = P0.u - 0.5f * ux, Rpv = P0.v - 0.5f * vx;
-                const float Rmu = uL + 0.5f * uxm, Rmv = vL + 0.5f * vxm;
-                const float vm = flipFm ? -vL : vL;
-                const float vp = flipFp ? -P0.v : P0.v;
-                float vp_n, vm_n;
-                if (GEN_NORTH) { vp_n = P0.u * k.nX + vp * k.nY; vm_n = uL * k.nX + vm * k.nY; }
-                else { vp_n = vp; vm_n = vm; }
-                const float dxf = k.dx * f0;
-                const float hp = fmaxf(0.0f, (P0.e + Hw) - (Kx + dxf * vp_n) / k.two_g);
-                const float hm = fmaxf(0.0f, (eL + Hw) + (Kxm + dxf * vm_n) / k.two_g);
-                Fw = central_upwind(hm, Rmu, Rmv, hp, Rpu, Rpv, k);
+            if (stage1 && writer && j + 1 < r1) {
+                const size_t o = (size_t)(j + 1) * a.pout + cl;
+                nqn_e = a.eta_out[o]; nqn_hu = a.hu_out[o]; nqn_hv = a.hv_out[o];
             }
         }
-        sF0[t] = Fw.a; sF1[t] = Fw.b; sF2[t] = Fw.c;
+        const Cell P2 = to_cell(q_e, q_hu, q_hv, Ha2, Hb2, Ha3, Hb3);
+        const float fu2 = fu_of(P2, j + 2, f2r);
+        const float Hy2 = 0.5f * (Ha2 + Hb2);
+
+        // ---- publish row j --------------------------------------------------
+        const float vK = flipKx ? -P0.v : P0.v;
+        const float fv = GEN_NORTH ? (k.nX * P0.u + k.nY * vK) * f0 : vK * f0;
+        sb.r[t] = make_float4(P0.e, P0.u, P0.v, fv);
         __syncthreads();
-        const float Fe0 = sF0[tr], Fe1 = sF1[tr], Fe2 = sF2[tr];
+        const float4 RL = sb.r[tl], RR = sb.r[tr];
+
+        // ---- slopes: lane x = x direction at row j, lane y = y at row j+1 ---
+        //   x: l = (j, cl-1), c = (j, cl), r = (j, cl+1)
+        //   y: l = (j, cl),   c = (j+1, cl), r = (j+2, cl)
+        const float2 lu = f2(RL.y, P0.u), cu = f2(P0.u, P1.u), ru = f2(RR.y, P2.u);
+        const float2 lv = f2(RL.z, P0.v), cv = f2(P0.v, P1.v), rv = f2(RR.z, P2.v);
+        const float2 le = f2(RL.x, P0.e), ce = f2(P0.e, P1.e), re = f2(RR.x, P2.e);
+        const float2 lf = f2(RL.w, fu0), cf = f2(fv, fu1), rf = f2(RR.w, fu2);
+        const float2 du = minmod_slope2(lu, cu, ru, theta2);   // (u_x(j), u_y(j+1))
+        const float2 dv = minmod_slope2(lv, cv, rv, theta2);   // (v_x(j), v_y(j+1))
+        float2 K;                                              // (K_x(j), L_y(j+1))
+        {
+            const float2 backward = mul2(thg2, add2(sub2(ce, le), mul2(VU2, add2(cf, lf))));
+            const float2 central = mul2(hg2, add2(sub2(re, le),
+                                                  mul2(VU2, add2(add2(rf, mul2(f2(2.0f, 2.0f), cf)), lf))));
+            const float2 forward = mul2(thg2, add2(sub2(re, ce), mul2(VU2, add2(cf, rf))));
+            K = minmod2(backward, central, forward);
+        }
+        const float Hw = 0.5f * (Ha0 + Ha1);   // x-face depth west of the cell (row j)
+        const float He = 0.5f * (Hb0 + Hb1);   // east
+        const float dxf = k.dx * f0;
+        {   // adjustSlopes_x (:148-191) and adjustSlopes_y (:198-241) in one:
+            // nw = (-dx f v, dy f u); K_x + dx f v = K_x - nw.x, L_y - dy f u = L_y - nw.y;
+            // fallbacks -dx f v + 2g(..) (x) and dy f u + 2g(..) (y) are nw + 2g(..)
+            const float vv = flipAdjX ? -P0.v : P0.v;
+            const float uu = flipAdjY(j + 1) ? -P1.u : P1.u;
+            const float2 nw = f2((-dxf) * vv, (k.dy * f1) * uu);
+            const float2 q = by2g(sub2(K, nw));
+            const float2 Hlo = f2(Hw, Hy1), Hhi = f2(He, Hy2);
+            const float2 hlo = sub2(add2(ce, Hlo), q);
+            const float2 hhi = add2(add2(ce, Hhi), q);
+            if (!(hlo.x > 0.0f && hlo.y > 0.0f && hhi.x > 0.0f && hhi.y > 0.0f)) {
+                const float2 Klo = add2(nw, mul2(two_g2, add2(ce, Hlo)));
+                const float2 Khi = sub2(nw, mul2(two_g2, add2(ce, Hhi)));
+                K = sel2(hlo.x > 0.0f, hlo.y > 0.0f, K, Klo);
+                K = sel2(hhi.x > 0.0f, hhi.y > 0.0f, K, Khi);
+            }
+        }
+        sb.s[t] = make_float4(du.x, dv.x, K.x, 0.0f);
+        __syncthreads();
+        const float4 SL = sb.s[tl];
+
+        // ---- fluxes: lane x = F on face (cl-1 | cl), lane y = G on (j | j+1)
+        float2 F0, F1, F2;
+        {
+            // minus / plus sides; lane x: m = (j, cl-1), p = (j, cl)
+            //                      lane y: m = (j, cl),   p = (j+1, cl)
+            const float2 em = f2(RL.x, P0.e), ep = f2(P0.e, P1.e);
+            // normal velocity and its slope per lane: x -> u, y -> v
+            const float2 unm = f2(RL.y, P0.v), unp = f2(P0.u, P1.v);
+            const float2 utm = f2(RL.z, P0.u), utp = f2(P0.v, P1.u);
+            const float2 dnm = f2(SL.x, vy0), dnp = f2(du.x, dv.y);
+            const float2 dtm = f2(SL.y, uy0), dtp = f2(dv.x, du.y);
+            const float2 Km = f2(SL.z, Ly0), Kp = K;
+            const float2 half = f2(0.5f, 0.5f);
+            const float2 Rpn = sub2(unp, mul2(half, dnp)), Rpt = sub2(utp, mul2(half, dtp));
+            const float2 Rmn = add2(unm, mul2(half, dnm)), Rmt = add2(utm, mul2(half, dtm));
+            // velocity used in the Coriolis part of the face depth:
+            //   x: v along north (flipped at walls), coefficient +dx f
+            //   y: u along east (flipped at walls), coefficient -dy f
+            float vmx = flipFm ? -RL.z : RL.z;
+            float vpx = flipFp ? -P0.v : P0.v;
+            float umy = (EDGE && k.bcS == kWall && j + 1 == 2) ? -P0.u : P0.u;
+            float upy = (EDGE && k.bcN == kWall && j + 1 == k.ny + 2) ? -P1.u : P1.u;
+            if (GEN_NORTH) {
+                vmx = RL.y * k.nX + vmx * k.nY; vpx = P0.u * k.nX + vpx * k.nY;
+                umy = umy * eX + P0.v * eY; upy = upy * eX + P1.v * eY;
+            }
+            const float2 cm = f2(dxf, -(k.dy * f0)), cp = f2(dxf, -(k.dy * f1));
+            const float2 Hf = f2(Hw, Hy1);
+            const float2 hp = sub2(add2(ep, Hf), by2g(add2(Kp, mul2(cp, f2(vpx, upy)))));
+            const float2 hm = add2(add2(em, Hf), by2g(add2(Km, mul2(cm, f2(vmx, umy)))));
+            const float2 hp0 = f2(fmaxf(0.0f, hp.x), fmaxf(0.0f, hp.y));
+            const float2 hm0 = f2(fmaxf(0.0f, hm.x), fmaxf(0.0f, hm.y));
+            central_upwind2<RCP>(hm0, Rmn, Rmt, hp0, Rpn, Rpt, k, F0, F1, F2);
+            const bool dryx = (P0.e == kDryFlag || RL.x == kDryFlag);
+            const bool dryy = (P1.e == kDryFlag || P0.e == kDryFlag);
+            if (dryx || dryy) {   // a land cell on either side: zero flux (:271-273)
+                const float2 z = f2(0.0f, 0.0f);
+                F0 = sel2(dryx, dryy, z, F0);
+                F1 = sel2(dryx, dryy, z, F1);
+                F2 = sel2(dryx, dryy, z, F2);
+            }
+        }
+        // F on the west face of cl: (mass, hu, hv) = (F0.x, F1.x, F2.x)
+        // G on the north face of row j: (mass, hu, hv) = (F0.y, F2.y, F1.y)
+        sb.f[t] = make_float4(F0.x, F1.x, F2.x, 0.0f);
+        __syncthreads();
+        const float4 FE = sb.f[tr];
 
         // ---- update the cell (j, cl), :807-1004 -----------------------------
         if (writer) {
-            const float Hm = 0.25f * (((Ha[0] + Ha[1]) + Hb[0]) + Hb[1]);
-            const float fd0 = (Fe0 - Fw.a) / k.dx + (Gn.a - Gs.a) / k.dy;
-            const float fd1 = (Fe1 - Fw.b) / k.dx + (Gn.b - Gs.b) / k.dy;
-            const float fd2 = (Fe2 - Fw.c) / k.dx + (Gn.c - Gs.c) / k.dy;
-            const float tw = (Kx + (k.dx * f0) * P0.v) / k.two_g;
-            const float eta_west = P0.e - tw;
-            const float eta_east = P0.e + tw;
-            const float ts = (S0.K - (k.dy * f0) * P0.u) / k.two_g;
-            const float eta_south = P0.e - ts;
-            const float eta_north = P0.e + ts;
+            const float Hm = 0.25f * (((Ha0 + Ha1) + Hb0) + Hb1);
+            // flux differences: (F_e - F_w)/dx + (G_n - G_s)/dy per component
+            const float2 d0 = bydxdy(f2(FE.x - F0.x, F0.y - Gs0));
+            const float2 d1 = bydxdy(f2(FE.y - F1.x, F2.y - Gs1));
+            const float2 d2 = bydxdy(f2(FE.z - F2.x, F1.y - Gs2));
+            const float fd0 = d0.x + d0.y, fd1 = d1.x + d1.y, fd2 = d2.x + d2.y;
+            // face values of eta for the bathymetry source (:706-707, :803-804):
+            //   (K_x + dx f v)/2g and (L_y - dy f u)/2g of the own cell
+            const float2 tt = by2g(add2(f2(K.x, Ly0), mul2(f2(dxf, -(k.dy * f0)), f2(P0.v, P0.u))));
+            const float2 eta_lo = sub2(f2(P0.e, P0.e), tt);   // (west, south)
+            const float2 eta_hi = add2(f2(P0.e, P0.e), tt);   // (east, north)
 
             const float h = P0.e + Hm;
-            float hu = 0.0f, hv = 0.0f;
-            if (h > k.cutoff) { hu = P0.u * h; hv = P0.v * h; }
+            float2 huv = f2(0.0f, 0.0f);
+            if (h > k.cutoff) huv = mul2(f2(P0.u, P0.v), f2(h, h));
 
-            float st1 = 0.0f, st2 = 0.0f;
+            float2 st = f2(0.0f, 0.0f);
             if (h >= k.cutoff && P0.e != kDryFlag) {
                 float X, Y;
                 if (WIND_FIELD) {
@@ -296,93 +527,132 @@ __global__ void __launch_bounds__(BW) cdklm_stage_kernel(const StageArgs a) {
                     X = a.wind_t * a.wxn + (1.0f - a.wind_t) * a.wxc;
                     Y = a.wind_t * a.wyn + (1.0f - a.wind_t) * a.wyc;
                 }
-                const float H_x = He - Hw;
-                const float H_y = Hy1 - 0.5f * (Ha[0] + Hb[0]);
-                const float eta_sn = 0.5f * (eta_north + eta_south);
-                const float eta_we = 0.5f * (eta_west + eta_east);
-                const float b1 = (k.g * (eta_we + Hm)) * H_x;
-                const float b2 = (k.g * (eta_sn + Hm)) * H_y;
-                float hu_cor, hv_cor;
+                const float2 Hxy = f2(He - Hw, Hy1 - Hy0);
+                const float2 eta_mid = mul2(f2(0.5f, 0.5f), add2(eta_lo, eta_hi));   // (we, sn)
+                const float2 bb = mul2(mul2(f2(k.g, k.g), add2(eta_mid, f2(Hm, Hm))), Hxy);
+                float2 cor;
                 if (GEN_NORTH) {
-                    const float hu_east = hu * eX + hv * eY;
-                    const float hv_north = hu * k.nX + hv * k.nY;
+                    const float hu_east = huv.x * eX + huv.y * eY;
+                    const float hv_north = huv.x * k.nX + huv.y * k.nY;
                     const float hu_east_cor = f0 * hv_north;
                     const float hv_north_cor = -f0 * hu_east;
                     const float upx = -k.nX, upy = k.nY;
                     const float rx = upy, ry = -upx;
-                    hu_cor = rx * hu_east_cor + ry * hv_north_cor;
-                    hv_cor = upx * hu_east_cor + upy * hv_north_cor;
+                    cor = f2(rx * hu_east_cor + ry * hv_north_cor, upx * hu_east_cor + upy * hv_north_cor);
                 } else {
-                    hu_cor = f0 * hv;
-                    hv_cor = -f0 * hu;
+                    cor = mul2(f2(f0, -f0), f2(huv.y, huv.x));
                 }
-                st1 = (X + hu_cor) + b1 / k.dx;
-                st2 = (Y + hv_cor) + b2 / k.dy;
+                st = add2(add2(f2(X, Y), cor), bydxdy(bb));
             }
             const float L1 = -fd0;
-            const float L2 = -fd1 + st1;
-            const float L3 = -fd2 + st2;
+            const float2 L23 = sub2(st, f2(fd1, fd2));   // -fd + st
 
             float C = 0.0f;
             if (FRIC == kFricLinear) {
-                C = k.two_r * a.dt / (P0.e + Hm);
+                C = quot<RCP>(k.two_r * dt, P0.e + Hm);
             } else if (FRIC == kFricQuad) {
                 if (h < k.desing_eps) {
-                    const float u = desingularize(h, hu, k.desing_eps);
-                    const float v = desingularize(h, hv, k.desing_eps);
-                    C = a.dt * k.r * desingularize(h, sqrtf(u * u + v * v), k.desing_eps);
+                    const float u = desingularize(h, huv.x, k.desing_eps);
+                    const float v = desingularize(h, huv.y, k.desing_eps);
+                    C = dt * k.r * desingularize(h, sqrtf(u * u + v * v), k.desing_eps);
                 } else {
-                    const float u = hu / h;
-                    const float v = hv / h;
-                    C = a.dt * k.r * sqrtf(u * u + v * v) / h;
+                    const float2 uv = quot2<RCP>(huv, f2(h, h));
+                    const float2 uv2 = mul2(uv, uv);
+                    C = quot<RCP>(dt * k.r * sqrtf(uv2.x + uv2.y), h);
                 }
             }
-            float ne, nhu, nhv;
-            if (a.rk_step == 0) {
-                ne = P0.e + a.dt * L1;
-                nhu = (hu + a.dt * L2) / (1.0f + C);
-                nhv = (hv + a.dt * L3) / (1.0f + C);
+            const float2 dt2 = f2(dt, dt);
+            float ne;
+            float2 nuv;
+            if (!stage1) {
+                ne = P0.e + dt * L1;
+                const float den = 1.0f + C;
+                nuv = quot2<RCP>(add2(huv, mul2(dt2, L23)), f2(den, den));
             } else {
-                ne = 0.5f * (qn_e + (P0.e + a.dt * L1));
-                nhu = (0.5f * (qn_hu + (hu + a.dt * L2))) / (1.0f + 0.5f * C);
-                nhv = (0.5f * (qn_hv + (hv + a.dt * L3))) / (1.0f + 0.5f * C);
+                ne = 0.5f * (qn_e + (P0.e + dt * L1));
+                const float den = 1.0f + 0.5f * C;
+                const float2 b = mul2(f2(0.5f, 0.5f), add2(f2(qn_hu, qn_hv), add2(huv, mul2(dt2, L23))));
+                nuv = quot2<RCP>(b, f2(den, den));
             }
+            float nhu = nuv.x, nhv = nuv.y;
             if (ne + Hm <= k.cutoff) {
                 ne = -Hm + k.cutoff; nhu = 0.0f; nhv = 0.0f;
             }
             ne = fmaxf(-Hm + k.cutoff, ne);
-            if (!(isfinite(ne) && isfinite(nhu) && isfinite(nhv)) && a.status) atomicOr(a.status, 1u);
+            if (!isfinite(ne + nhu + nhv) && a.status) atomicOr(a.status, 1u);
 
-            // own cell plus its periodic ghost images (NS rows, EW columns)
-            int rows_img[3] = {j, -1, -1};
-            int cols_img[3] = {cl, -1, -1};
-            if (k.bcN == kPeriodic) {
-                if (j < 4) rows_img[1] = j + k.ny;
-                if (j >= k.ny) rows_img[2] = j - k.ny;
-            }
-            if (k.bcE == kPeriodic) {
-                if (cl < 4) cols_img[1] = cl + k.nx;
-                if (cl >= k.nx) cols_img[2] = cl - k.nx;
-            }
-#pragma unroll
-            for (int ri = 0; ri < 3; ++ri) {
-#pragma unroll
-                for (int ci = 0; ci < 3; ++ci) {
-                    const int rr = rows_img[ri], cc = cols_img[ci];
-                    if (rr < 0 || cc < 0) continue;
-                    const size_t o = (size_t)rr * a.pout + cc;
-                    a.eta_out[o] = ne; a.hu_out[o] = nhu; a.hv_out[o] = nhv;
+            const size_t o = (size_t)j * a.pout + cl;
+            a.eta_out[o] = ne; a.hu_out[o] = nhu; a.hv_out[o] = nhv;
+            if (EDGE) {
+                // periodic ghost images (the reference's BC kernels after the stage)
+                const bool row_img = (k.bcN == kPeriodic) && (j < 4 || j >= k.ny);
+                if (row_img || col_img) {
+                    int rows_img[2] = {-1, -1}, cols_img[2] = {-1, -1};
+                    if (k.bcN == kPeriodic) {
+                        if (j < 4) rows_img[0] = j + k.ny;
+                        if (j >= k.ny) rows_img[1] = j - k.ny;
+                    }
+                    if (k.bcE == kPeriodic) {
+                        if (cl < 4) cols_img[0] = cl + k.nx;
+                        if (cl >= k.nx) cols_img[1] = cl - k.nx;
+                    }
+                    const int rr[3] = {j, rows_img[0], rows_img[1]};
+                    const int cc[3] = {cl, cols_img[0], cols_img[1]};
+                    for (int ri = 0; ri < 3; ++ri) {
+                        for (int ci = 0; ci < 3; ++ci) {
+                            if ((ri == 0 && ci == 0) || rr[ri] < 0 || cc[ci] < 0) continue;
+                            const size_t oo = (size_t)rr[ri] * a.pout + cc[ci];
+                            a.eta_out[oo] = ne; a.hu_out[oo] = nhu; a.hv_out[oo] = nhv;
+                        }
+                    }
                 }
             }
         }
 
         // ---- slide the window -----------------------------------------------
-        P0 = P1; P1 = P2;
-        S0 = S1;
-        Gs = Gn;
-        Ha[0] = Ha[1]; Ha[1] = Ha[2]; Ha[2] = Ha[3];
-        Hb[0] = Hb[1]; Hb[1] = Hb[2]; Hb[2] = Hb[3];
-        f0 = f1; f1 = f2;
+        Pm1 = P0; P0 = P1; P1 = P2;
+        fu0 = fu1; fu1 = fu2;
+        uy0 = du.y; vy0 = dv.y; Ly0 = K.y;
+        Gs0 = F0.y; Gs1 = F2.y; Gs2 = F1.y;
+        Ha0 = Ha1; Hb0 = Hb1; Ha1 = Ha2; Hb1 = Hb2; Ha2 = Ha3; Hb2 = Hb3;
+        Hy0 = Hy1; Hy1 = Hy2;
+        f0 = f1; f1 = f2r;
+    }
+}
+
+template <int BW, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND>
+__device__ __forceinline__ void stage_block(const StageArgs& a, const float dt, const int bx, const int by,
+                                            RowBufs<BW>& sb) {
+    const int c0 = 2 + bx * (BW - 4);
+    const int r0 = 2 + by * a.rows_per_block;
+    const int r1 = min(r0 + a.rows_per_block, a.k.ny + 2);
+    if (interior_block<BW>(a.k, c0, r0, r1))
+        stage_strip<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, false>(a, dt, bx, by, sb);
+    else
+        stage_strip<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, true>(a, dt, bx, by, sb);
+}
+
+template <int BW, int MINB, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND>
+__global__ void __launch_bounds__(BW, MINB) cdklm_stage_kernel(const StageArgs a) {
+    __shared__ RowBufs<BW> sb;
+    stage_block<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND>(a, a.dt, blockIdx.x, blockIdx.y, sb);
+}
+
+// Batched stage: a packed list of (member, column block, row block) tiles
+// over every member of an ensemble or set of domains, walked by a
+// persistent grid.  args holds two entries per member (stage 0: h0 -> h1,
+// stage 1: h1 -> h0); dts holds the member's time step, read at launch so a
+// captured graph picks up new values.
+template <int BW, int MINB, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND>
+__global__ void __launch_bounds__(BW, MINB)
+    cdklm_batch_kernel(const StageArgs* __restrict__ args, const float* __restrict__ dts,
+                       const int4* __restrict__ tiles, const int ntiles, const int rk_step) {
+    __shared__ RowBufs<BW> sb;
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const int4 tile = tiles[ti];
+        const StageArgs& a = args[2 * tile.x + rk_step];
+        stage_block<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND>(a, __ldg(dts + tile.x), tile.y, tile.z, sb);
+        __syncthreads();
     }
 }
 

@@ -1,0 +1,75 @@
+// Kernel-variant selection shared by the single-domain and batched launchers.
+//
+// A variant is (launch shape, friction law, general grid angle, per-cell
+// wind, reciprocal quotients, land in the bathymetry).  Every variant gives
+// the same results; the specialised ones drop work the general one would do
+// for nothing.  Instantiated set:
+//   * general: shape 4, every friction law, angle and wind combination, land
+//     checks on, reciprocal quotients;
+//   * common fast path (north up, uniform wind): every shape and friction
+//     law, with and without land checks, reciprocal or '/' quotients.
+#pragma once
+
+#include "internal.h"
+
+namespace go {
+
+struct Variant {
+    int shape, fric;
+    bool gen_north, wind_field, rcp, land;
+};
+
+// L is a functor with
+//   template <int BW, int MINB, int FRIC, bool GN, bool WF, bool RCP, bool LAND> cudaError_t run();
+template <class L>
+cudaError_t dispatch_variant(L& launcher, Variant v) {
+#define GO_V(BW, MINB, F, GN, WF, RCP, LAND) return launcher.template run<BW, MINB, F, GN, WF, RCP, LAND>()
+    if (v.gen_north || v.wind_field) {
+        // general variants: shape 4, land checks on, reciprocal quotients
+#define GO_GEN(F)                                                     \
+    do {                                                              \
+        if (v.gen_north && v.wind_field) GO_V(128, 5, F, true, true, true, true);   \
+        if (v.gen_north) GO_V(128, 5, F, true, false, true, true);    \
+        GO_V(128, 5, F, false, true, true, true);                     \
+    } while (0)
+        if (v.fric == kFricNone) GO_GEN(kFricNone);
+        if (v.fric == kFricQuad) GO_GEN(kFricQuad);
+        GO_GEN(kFricLinear);
+#undef GO_GEN
+    }
+#define GO_SHAPES(F, RCP, LAND)                                       \
+    do {                                                              \
+        switch (v.shape) {                                            \
+            case 0: GO_V(192, 2, F, false, false, RCP, LAND);         \
+            case 1: GO_V(192, 3, F, false, false, RCP, LAND);         \
+            case 2: GO_V(128, 4, F, false, false, RCP, LAND);         \
+            case 3: GO_V(256, 2, F, false, false, RCP, LAND);         \
+            default: GO_V(128, 5, F, false, false, RCP, LAND);        \
+        }                                                             \
+    } while (0)
+#define GO_RL(F)                                                      \
+    do {                                                              \
+        if (v.rcp) {                                                  \
+            if (v.land) GO_SHAPES(F, true, true);                     \
+            GO_SHAPES(F, true, false);                                \
+        }                                                             \
+        if (v.land) GO_V(128, 5, F, false, false, false, true);       \
+        GO_V(128, 5, F, false, false, false, false);                  \
+    } while (0)
+    if (v.fric == kFricNone) GO_RL(kFricNone);
+    if (v.fric == kFricQuad) GO_RL(kFricQuad);
+    GO_RL(kFricLinear);
+#undef GO_RL
+#undef GO_SHAPES
+#undef GO_V
+}
+
+inline int shape_block_width(int shape) {
+    switch (shape) {
+        case 2: case 4: return 128;
+        case 3: return 256;
+        default: return 192;
+    }
+}
+
+}  // namespace go

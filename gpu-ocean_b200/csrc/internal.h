@@ -1,0 +1,54 @@
+// Internal declarations shared by the translation units of libgocean.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "cdklm16_stage.cuh"
+#include "gocean.h"
+
+struct go_domain {
+    go_domain_desc desc;
+    go::Scheme k;
+    int device;
+    float* d_frows;          // ny+4 Coriolis values
+    unsigned int* d_status;  // GO_STATUS_* bits
+    float wxc, wxn, wyc, wyn;
+    const float *wx_cur, *wx_next, *wy_cur, *wy_next;
+    int wpitch;              // floats
+    int rows_per_block;
+    int shape;               // launch shape, see go_shape_width()
+    int arith;               // GO_ARITH_*
+    int has_land;            // bathymetry may hold land cells (checks on)
+};
+
+// Records the message of a failed call (go_last_error) and returns code.
+int go_fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+
+#define GO_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return go_fail(GO_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+    } while (0)
+
+int go_check_pitch(int pitch_bytes, int min_floats, const char* what);
+
+// Kernel-variant selectors of a domain.
+int go_friction_mode(const go_domain* d);
+bool go_general_north(const go_domain* d);
+
+// Fills the per-stage arguments of one domain.
+go::StageArgs go_stage_args(const go_domain* d, float dt, int rk_step, const float* e0, const float* u0,
+                            const float* v0, int pin, float* e1, float* u1, float* v1, int pout,
+                            const float* Hi, int phi, float land, float wind_t);
+
+namespace go { struct Variant; }
+// Kernel variant of a domain (stage_launch.cu).
+go::Variant go_variant(const go_domain* d);
+
+// One single-domain stage launch (stage_launch.cu).
+int go_launch_stage(go_domain* d, cudaStream_t s, const go::StageArgs& a);

@@ -90,8 +90,25 @@ int go_domain_set_wind_uniform(go_domain* d, float x_cur, float x_next,
 int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_next,
                              const float* y_cur, const float* y_next, int pitch);
 
-/* Launch shape: rows per block strip (>= 4); 0 picks the default. */
-int go_domain_set_tile(go_domain* d, int rows_per_block);
+/* Launch shape of the step kernel: shape 0 = 192 threads x 2 blocks/SM,
+ * 1 = 192 x 3, 2 = 128 x 4, 3 = 256 x 2, 4 = 128 x 5 (default); each block
+ * marches down a strip of rows_per_block rows (0 = default 32).  Chosen by
+ * the autotuner; every shape computes identical results. */
+int go_domain_set_launch(go_domain* d, int shape, int rows_per_block);
+
+/* How quotients are evaluated.  EXACT keeps every '/' of the reference
+ * kernel (div.full.f32 under its --prec-div=false).  RCP (the default)
+ * multiplies by reciprocals (rcp.approx.ftz) of shared denominators; on
+ * B200 the two give bit-identical results over the tested ranges, and both
+ * reproduce the reference kernel bit for bit on the parity workloads. */
+#define GO_ARITH_EXACT 0
+#define GO_ARITH_RCP 1
+int go_domain_set_arith(go_domain* d, int mode);
+
+/* Whether the bathymetry may hold land (corners equal to the land value,
+ * Common.py:1333-1337).  1 (the default) keeps every land test of the
+ * reference kernel; 0 asserts there is none and skips them. */
+int go_domain_set_land(go_domain* d, int may_have_land);
 
 /* Bathymetry set-up (Common.py:1319-1389): fixes the ghost corners of Hi
  * in place (periodic wrap or wall mirror, boundary_kernels.cu:121-246) and
@@ -138,6 +155,48 @@ int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_
 int go_max_dt(go_domain* d, void* stream, const float* eta, const float* hu,
               const float* hv, int pitch, const float* Bm, int Bm_pitch,
               float land_value, float* dt_dev);
+
+/* ---------------------------------------------------------------------
+ * Batched stepping.  No counterpart entry point in the reference: it
+ * replaces the member-by-member loops of its ensembles
+ * (OceanNoiseEnsemble.py:506-531, OceanModelEnsemble.py:105-117,
+ * EnsembleFromFiles.py:302-324), which call CDKLM16.step once per member.
+ * One launch per RK stage covers every member through a packed list of
+ * (member, column block, row block) tiles; members may have different
+ * sizes, bathymetry and time steps but must share the kernel variant
+ * (friction law, grid angle, uniform vs per-cell wind).
+ * --------------------------------------------------------------------- */
+typedef struct go_batch go_batch;
+
+/* Batch over n existing domain handles (not owned; keep them alive). */
+int go_batch_create(go_domain* const* members, int n, go_batch** out);
+int go_batch_destroy(go_batch* b);
+
+/* State buffers, bathymetry and time step of member m (as go_cdklm_step). */
+int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, float* hv0, int pitch0,
+                        float* eta1, float* hu1, float* hv1, int pitch1, const float* Hi, int Hi_pitch,
+                        float land_value, float wind_stress_t);
+
+/* Launch shape (as go_domain_set_launch) and persistent grid size: blocks
+ * = 0 launches one block per tile, blocks > 0 that many blocks walking the
+ * tile list. */
+int go_batch_set_launch(go_batch* b, int shape, int rows_per_block, int blocks);
+int go_batch_set_arith(go_batch* b, int mode);
+
+/* New per-member time steps (n floats, host).  A captured graph reads them
+ * at its next launch; no re-capture is needed. */
+int go_batch_set_dt(go_batch* b, void* stream, const float* dt_host);
+
+/* Number of tiles of the packed list (commits pending member changes). */
+int go_batch_tiles(go_batch* b, int* ntiles);
+
+/* n_steps RK2 steps of every member: 2 launches per step. */
+int go_batch_step(go_batch* b, void* stream, int n_steps);
+
+/* Capture n_steps batched steps on stream (non-default) into a CUDA graph,
+ * and replay it; steps_done (optional) receives n_steps. */
+int go_batch_graph_capture(go_batch* b, void* stream, int n_steps);
+int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done);
 
 /* Device status word (GO_STATUS_* bits) accumulated by the step kernels;
  * synchronous read, optionally clearing it. */

@@ -1,0 +1,110 @@
+"""Batched stepping (go_batch_*, BatchedCDKLM16) and the autotuner on a GPU.
+
+The batched launch must give bit-identical states to stepping each member
+alone (the reference's member-by-member loop, OceanNoiseEnsemble.py:506-531),
+for members of different sizes, bathymetry and time steps, with and without
+CUDA-graph replay.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from SWESimulators import Autotune, BatchedEnsemble, CDKLM16, Common, SyntheticCases as SC  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return Common.CUDAContext()
+
+
+def _members(ctx, sizes, seed0=40000):
+    sims = []
+    for k, n in enumerate(sizes):
+        c = SC.grf(n, dx=1000.0, seed_bathy=seed0 + k, seed_bumps=seed0 + 500 + k, steps=1)
+        sims.append(CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs()))
+    return sims
+
+
+def _states(sims):
+    return [np.stack(s.download()) for s in sims]
+
+
+def test_mixed_batch_equals_member_by_member(ctx):
+    sizes = [128, 256, 96, 200, 160]
+    alone = _members(ctx, sizes)
+    for s in alone:
+        for _ in range(12):
+            s.step(s.dt)
+    expect = _states(alone)
+    sims = _members(ctx, sizes)
+    b = BatchedEnsemble.BatchedCDKLM16(sims)
+    b.advance(12)
+    got = _states(sims)
+    for e, g in zip(expect, got):
+        assert np.array_equal(e, g)
+    for s, a in zip(sims, alone):
+        assert s.num_iterations == a.num_iterations
+        assert s.t == a.t
+
+
+def test_graph_replay_equals_plain_launches(ctx):
+    sims_a = _members(ctx, [256] * 4, seed0=41000)
+    sims_b = _members(ctx, [256] * 4, seed0=41000)
+    a = BatchedEnsemble.BatchedCDKLM16(sims_a)
+    b = BatchedEnsemble.BatchedCDKLM16(sims_b, graph_steps=5)
+    a.advance(17)
+    b.advance(17)            # 3 graph replays + 2 plain steps
+    for x, y in zip(_states(sims_a), _states(sims_b)):
+        assert np.array_equal(x, y)
+
+
+def test_batched_step_t_end_semantics(ctx):
+    sims = _members(ctx, [128, 128], seed0=42000)
+    dt = min(s.dt for s in sims)
+    for s in sims:
+        s.dt = dt
+    alone = _members(ctx, [128, 128], seed0=42000)
+    for s in alone:
+        s.dt = dt
+        s.step(10.5 * dt)
+    b = BatchedEnsemble.BatchedCDKLM16(sims)
+    b.set_dt([dt, dt])
+    b.step(10.5 * dt)
+    for x, y in zip(_states(sims), _states(alone)):
+        assert np.array_equal(x, y)
+    assert sims[0].num_iterations == alone[0].num_iterations == 11
+
+
+def test_autotune_domain_keeps_state(ctx, tmp_path, monkeypatch):
+    monkeypatch.setenv("GOCEAN_TUNE_CACHE", str(tmp_path / "tune.json"))
+    c = SC.grf(512, dx=1000.0, steps=1)
+    sim = CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs())
+    ref = CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs())
+    before = np.stack(sim.download())
+    best, info = Autotune.tune_domain(sim, steps=3)
+    assert np.array_equal(np.stack(sim.download()), before)
+    for _ in range(5):
+        sim.step(c.dt)
+        ref.step(c.dt)
+    assert np.array_equal(np.stack(sim.download()), np.stack(ref.download()))
+    again, hit = Autotune.tune_domain(sim)           # from the cache
+    assert again == best
+
+
+def test_autotune_batch(ctx, tmp_path, monkeypatch):
+    monkeypatch.setenv("GOCEAN_TUNE_CACHE", str(tmp_path / "tune.json"))
+    sims = _members(ctx, [256] * 3, seed0=43000)
+    b = BatchedEnsemble.BatchedCDKLM16(sims)
+    before = _states(sims)
+    res = Autotune.tune_batch(b, steps=3, graph_lengths=[4])
+    for x, y in zip(before, _states(sims)):
+        assert np.array_equal(x, y)
+    assert res["graph_steps"] in (0, 4)
+    b.advance(6)
+    assert sims[0].num_iterations == 6
