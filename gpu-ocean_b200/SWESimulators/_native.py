@@ -18,6 +18,9 @@ GO_BC_PERIODIC = 2
 GO_FRICTION_QUADRATIC = 0
 GO_FRICTION_LINEAR = 1
 GO_STATUS_NONFINITE = 0x1
+GO_ERR_INVALID = -1
+GO_ERR_CUDA = -2
+GO_ERR_UNSUPPORTED = -3
 GO_ARITH_EXACT = 0
 GO_ARITH_RCP = 1
 
@@ -58,6 +61,9 @@ SIGNATURES = {
     "go_cdklm_swe_2D": (_I, [_P, _P, _F, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I,
                              _P, _I, _P, _I, _F, _F, _I]),
     "go_cdklm_step": (_I, [_P, _P, _I, _F, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F]),
+    "go_cdklm_step_static": (_I, [ctypes.POINTER(GoDomainDesc), _P, ctypes.POINTER(ctypes.c_float), _I, _F, _F,
+                                  _I, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F,
+                                  ctypes.POINTER(ctypes.c_uint32)]),
     "go_max_dt": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _F, _P]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),

@@ -198,6 +198,26 @@ int go_batch_step(go_batch* b, void* stream, int n_steps);
 int go_batch_graph_capture(go_batch* b, void* stream, int n_steps);
 int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done);
 
+/* ---------------------------------------------------------------------
+ * Allocation-free step.  No counterpart in the reference (its CDKLM16
+ * allocates through pycuda).  The go_cdklm_step of a domain described by
+ * desc, with a uniform wind (wind_x, wind_y) and no domain handle, for
+ * callers that cannot call cudaMalloc: the Coriolis table (n_rows = 1 or
+ * ny+4 floats, host) and the status word live in a static __device__
+ * array of 65,808 bytes per device, so ny + 4 <= 16388 (larger ny is
+ * rejected with GO_ERR_INVALID).  The status word is cleared at the start
+ * of each call; status_out (optional, host) receives it after a stream
+ * synchronize.  The first call on each device looks up the array's address
+ * and may load the module: make it outside stream capture.  Calls on one
+ * device share the array, so overlapping calls race: order them on one
+ * stream or one host thread.
+ * --------------------------------------------------------------------- */
+int go_cdklm_step_static(const go_domain_desc* desc, void* stream, const float* f_rows_host,
+                         int n_rows, float wind_x, float wind_y, int n_steps, float dt,
+                         float* eta0, float* hu0, float* hv0, int pitch0,
+                         float* eta1, float* hu1, float* hv1, int pitch1,
+                         const float* Hi, int Hi_pitch, float land_value, uint32_t* status_out);
+
 /* Device status word (GO_STATUS_* bits) accumulated by the step kernels;
  * synchronous read, optionally clearing it. */
 int go_domain_status(go_domain* d, uint32_t* status, int clear);
