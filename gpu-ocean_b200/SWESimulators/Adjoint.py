@@ -1,0 +1,362 @@
+"""Adjoint of the CDKLM16 time step.
+
+No counterpart in the reference: gpu-ocean has no adjoint.  This module
+returns gradients of an observation misfit
+
+    J = sum over observation times and points of
+        w_eta (eta - eta_obs)^2 + w_vel ((hu - hu_obs)^2 + (hv - hv_obs)^2)
+
+with respect to the initial state (eta0, hu0, hv0) and a wind-stress field
+(X, Y) per interior cell, constant in time.  The forward model is the
+B200 CDKLM16 step (go_cdklm_step / go_traj_step, bit-identical to the
+reference kernel); the reverse sweep runs the hand-written adjoint of each
+RK stage (go_adjoint_step).  Memory is held by checkpointing: every
+``checkpoint_every`` steps the state is kept, and each segment is
+recomputed from its checkpoint before its reverse sweep (the last segment
+is kept from the forward pass).  ``Revolve`` gives binomial schedules for
+runs whose full trajectory does not fit.
+
+``CDKLM16Misfit`` (J as a differentiable function of the initial state and
+the wind) and ``CDKLM16Step`` (one RK2 step) wrap the problem in
+``torch.autograd.Function`` objects.
+
+Scope: north-up grids, no land, no cell shallower than the
+desingularisation depth (the adjoint kernel flags GO_STATUS_ADJ_SCOPE
+otherwise and ``MisfitProblem`` raises).
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+
+
+def _round_up(n, m):
+    return (n + m - 1) // m * m
+
+
+class StateSlab:
+    """n device states, each three (ny+4) x P float32 planes (eta, hu, hv)
+    with P = nx+4 rounded up to 32 floats."""
+
+    def __init__(self, n, nx, ny):
+        torch = _native.require_cuda()
+        self.n, self.nx, self.ny = int(n), int(nx), int(ny)
+        self.P = _round_up(self.nx + 4, 32)
+        self.t = torch.zeros((self.n, 3, self.ny + 4, self.P), dtype=torch.float32, device="cuda")
+        self._gs = [self._make(i) for i in range(self.n)]
+
+    def _make(self, i):
+        s = _native.GoState()
+        s.eta = int(self.t[i, 0].data_ptr())
+        s.hu = int(self.t[i, 1].data_ptr())
+        s.hv = int(self.t[i, 2].data_ptr())
+        s.pitch = self.P * 4
+        return s
+
+    def gs(self, i):
+        return ctypes.byref(self._gs[i])
+
+    def interior(self, i):
+        return self.t[i, :, 2:self.ny + 2, 2:self.nx + 2]
+
+    def full(self, i):
+        return self.t[i, :, :, :self.nx + 4]
+
+
+def _copy_state(dst, i, src, k):
+    dst.t[i].copy_(src.t[k])
+
+
+class Observations:
+    """Observed cells and values.  ij: (n, 2) interior (i, j) indices;
+    steps: the step numbers (1..n_steps) after which J sums the misfit;
+    values: (len(steps), n, 3) observed (eta, hu, hv)."""
+
+    def __init__(self, ij, steps, values, w_eta=100.0, w_vel=1.0):
+        torch = _native.require_cuda()
+        ij = np.ascontiguousarray(np.asarray(ij, dtype=np.int32).reshape(-1, 2))
+        values = np.asarray(values, dtype=np.float32).reshape(len(steps), ij.shape[0], 3)
+        self.n = ij.shape[0]
+        self.steps = [int(s) for s in steps]
+        if sorted(set(self.steps)) != self.steps:
+            raise ValueError("observation steps must be increasing and distinct")
+        self.ij_host = ij
+        self.ij = torch.as_tensor(ij, device="cuda")
+        self.values = torch.as_tensor(np.ascontiguousarray(values), device="cuda")
+        self.index = {s: k for k, s in enumerate(self.steps)}
+        self.w_eta = float(w_eta)
+        self.w_vel = float(w_vel)
+
+    @staticmethod
+    def sample(states_by_step, ij):
+        """(len(steps), n, 3) values of host states {step: (eta, hu, hv)
+        interior arrays} at the cells ij -- for building synthetic
+        observations from a truth run."""
+        ij = np.asarray(ij, dtype=np.int64).reshape(-1, 2)
+        out = []
+        for s in sorted(states_by_step):
+            e, u, v = states_by_step[s]
+            out.append(np.stack([e[ij[:, 1], ij[:, 0]], u[ij[:, 1], ij[:, 0]], v[ij[:, 1], ij[:, 0]]], axis=1))
+        return np.asarray(out, dtype=np.float32)
+
+
+class MisfitProblem:
+    """J(eta0, hu0, hv0, X, Y) over n_steps RK2 steps of size dt on the grid,
+    bathymetry, Coriolis, friction and boundaries of ``sim`` (a CDKLM16)."""
+
+    def __init__(self, sim, n_steps, obs, dt=None, checkpoint_every=50):
+        torch = _native.require_cuda()
+        d = sim._domain.desc
+        if abs(float(d.north_x)) > 0.0 or float(d.north_y) != 1.0:
+            raise NotImplementedError("the adjoint is built for north-up grids only")
+        Bm = sim.downloadBathymetry()[1]
+        if np.any(np.abs(Bm - np.float32(sim.bathymetry.mask_value)) < 1e-3):
+            raise NotImplementedError("the adjoint is built for bathymetry without land")
+        self.sim = sim
+        self.nx, self.ny = int(sim.nx), int(sim.ny)
+        self.n_steps = int(n_steps)
+        self.dt = np.float32(sim.dt if dt is None else dt)
+        self.obs = obs
+        for s in obs.steps:
+            if s < 0 or s > self.n_steps:
+                raise ValueError("observation step %d outside 0..%d" % (s, self.n_steps))
+        ij = obs.ij_host
+        if ij.size and (ij[:, 0].min() < 0 or ij[:, 0].max() >= self.nx or ij[:, 1].min() < 0
+                        or ij[:, 1].max() >= self.ny):
+            raise ValueError("observation cells must be interior cells (0 <= i < nx, 0 <= j < ny)")
+        self.k = max(1, min(int(checkpoint_every), self.n_steps))
+        self.domain = _native.Domain(self.nx, self.ny, d.dx, d.dy, d.g, d.r, theta=d.theta,
+                                     desing_eps=d.desing_eps, flux_slope_eps=d.flux_slope_eps,
+                                     depth_cutoff=d.depth_cutoff,
+                                     bc=(d.bc_north, d.bc_east, d.bc_south, d.bc_west),
+                                     friction_law=d.friction_law, north=(d.north_x, d.north_y))
+        self.domain.set_coriolis(sim.coriolis_rows)
+        self.domain.set_land(False)
+        self.Hi = sim.bathymetry.Bi.tensor
+        self.Hi_pitch = int(sim.bathymetry.Bi.pitch)
+        self.land = float(sim.bathymetry.mask_value)
+        self.stream = torch.cuda.Stream()
+        self.sh = _native.stream_handle(self.stream)
+        Pw = _round_up(self.nx, 32)
+        self.wind = torch.zeros((2, self.ny, Pw), dtype=torch.float32, device="cuda")
+        self.lam_wind = torch.zeros((2, self.ny, Pw), dtype=torch.float32, device="cuda")
+        self.wpitch = Pw * 4
+        wx, wy = self.wind[0], self.wind[1]
+        self.domain.set_wind_field(wx, wx, wy, wy)
+        n_seg = (self.n_steps + self.k - 1) // self.k
+        self.ckpt = StateSlab(max(n_seg, 1), self.nx, self.ny)
+        self.qn = StateSlab(self.k + 1, self.nx, self.ny)
+        self.qs = StateSlab(self.k, self.nx, self.ny)
+        self.work = StateSlab(2, self.nx, self.ny)
+        self.lam = StateSlab(3, self.nx, self.ny)      # lambda, scratch Q*, scratch Q^n
+        self.J_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
+        self._ready = False
+        self.recomputed_steps = 0
+
+    # -- helpers -------------------------------------------------------------
+    def _lib(self):
+        return _native.load()
+
+    def _segments(self):
+        return [(a, min(a + self.k, self.n_steps)) for a in range(0, self.n_steps, self.k)]
+
+    def _misfit(self, slab, i, step):
+        if step not in self.obs.index:
+            return
+        o = self.obs
+        k = o.index[step]
+        _native.check(self._lib().go_obs_misfit(self.sh, slab.gs(i), self.nx, self.ny, o.n, _native.ptr(o.ij),
+                                                _native.ptr(o.values[k]), o.w_eta, o.w_vel,
+                                                _native.ptr(self.J_dev)))
+
+    def _obs_adjoint(self, slab, i, step):
+        if step not in self.obs.index:
+            return
+        o = self.obs
+        k = o.index[step]
+        _native.check(self._lib().go_obs_adjoint(self.sh, slab.gs(i), self.lam.gs(0), self.nx, self.ny, o.n,
+                                                 _native.ptr(o.ij), _native.ptr(o.values[k]), o.w_eta, o.w_vel))
+
+    def _traj_step(self, a_slab, ai, s_slab, si, b_slab, bi):
+        _native.check(self._lib().go_traj_step(self.domain.handle, self.sh, float(self.dt), 0.0, a_slab.gs(ai),
+                                               s_slab.gs(si), b_slab.gs(bi), _native.ptr(self.Hi),
+                                               self.Hi_pitch, self.land))
+
+    def _plain_steps(self, n):
+        w = self.work
+        g0, g1 = w._gs[0], w._gs[1]
+        _native.check(self._lib().go_cdklm_step(
+            self.domain.handle, self.sh, int(n), float(self.dt), 0.0,
+            ctypes.c_void_p(g0.eta), ctypes.c_void_p(g0.hu), ctypes.c_void_p(g0.hv), g0.pitch,
+            ctypes.c_void_p(g1.eta), ctypes.c_void_p(g1.hu), ctypes.c_void_p(g1.hv), g1.pitch,
+            _native.ptr(self.Hi), self.Hi_pitch, self.land))
+
+    def _load(self, eta0, hu0, hv0, wind_x, wind_y):
+        torch = _native.require_cuda()
+        w = self.work
+        with torch.cuda.stream(self.stream):
+            w.t[0].zero_()
+            for f, a in enumerate((eta0, hu0, hv0)):
+                w.interior(0)[f].copy_(torch.as_tensor(a, dtype=torch.float32, device="cuda").reshape(self.ny, self.nx))
+            for f, a in enumerate((wind_x, wind_y)):
+                self.wind[f, :, :self.nx].copy_(torch.as_tensor(a, dtype=torch.float32, device="cuda")
+                                                .reshape(self.ny, self.nx))
+        g = w._gs[0]
+        _native.check(self._lib().go_boundary_condition(self.domain.handle, self.sh, ctypes.c_void_p(g.eta),
+                                                        ctypes.c_void_p(g.hu), ctypes.c_void_p(g.hv), g.pitch))
+
+    # -- forward ---------------------------------------------------------------
+    def forward(self, eta0, hu0, hv0, wind_x, wind_y):
+        """J for the given initial interior state and wind field (device
+        tensors or host arrays of ny x nx).  Keeps the checkpoints and the
+        last segment's trajectory for ``backward``."""
+        torch = _native.require_cuda()
+        self.stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(self.stream):
+            self._load(eta0, hu0, hv0, wind_x, wind_y)
+            self.J_dev.zero_()
+            self._misfit(self.work, 0, 0)
+            segs = self._segments()
+            for s, (a, b) in enumerate(segs):
+                _copy_state(self.ckpt, s, self.work, 0)
+                if s == len(segs) - 1:
+                    # the last segment's trajectory is kept for the reverse sweep
+                    _copy_state(self.qn, 0, self.work, 0)
+                    for t in range(b - a):
+                        self._traj_step(self.qn, t, self.qs, t, self.qn, t + 1)
+                        self._misfit(self.qn, t + 1, a + t + 1)
+                    _copy_state(self.work, 0, self.qn, b - a)
+                else:
+                    n = a
+                    for event in sorted({x for x in self.obs.steps if a < x <= b} | {b}):
+                        self._plain_steps(event - n)
+                        n = event
+                        self._misfit(self.work, 0, n)
+        self._ready = True
+        self.stream.synchronize()
+        return float(self.J_dev.item())
+
+    def final_state(self):
+        """Interior (eta, hu, hv) after the last forward run (device views)."""
+        return self.work.interior(0)
+
+    # -- reverse ---------------------------------------------------------------
+    def backward(self):
+        """Gradients (d eta0, d hu0, d hv0, d X, d Y) of J from the last
+        ``forward``; device tensors of ny x nx."""
+        if not self._ready:
+            raise RuntimeError("backward() needs a forward() first")
+        torch = _native.require_cuda()
+        lib = self._lib()
+        lam = self.lam
+        lw = self.lam_wind
+        self.stream.synchronize()
+        self.domain.status(clear=True)
+        with torch.cuda.stream(self.stream):
+            lam.t.zero_()
+            lw.zero_()
+            segs = self._segments()
+            for s in range(len(segs) - 1, -1, -1):
+                a, b = segs[s]
+                if s != len(segs) - 1:
+                    _copy_state(self.qn, 0, self.ckpt, s)
+                    for t in range(b - a):
+                        self._traj_step(self.qn, t, self.qs, t, self.qn, t + 1)
+                    self.recomputed_steps += b - a
+                for n in range(b - 1, a - 1, -1):
+                    t = n - a
+                    self._obs_adjoint(self.qn, t + 1, n + 1)
+                    _native.check(lib.go_adjoint_step(
+                        self.domain.handle, self.sh, float(self.dt), self.qn.gs(t), self.qs.gs(t),
+                        self.qn.gs(t + 1), lam.gs(0), lam.gs(0), lam.gs(1), lam.gs(2), _native.ptr(lw[0]),
+                        _native.ptr(lw[1]), self.wpitch, _native.ptr(self.Hi), self.Hi_pitch))
+            if 0 in self.obs.index:
+                _copy_state(self.qn, 0, self.ckpt, 0)
+                self._obs_adjoint(self.qn, 0, 0)
+        self.stream.synchronize()
+        if self.domain.status() & _native.GO_STATUS_ADJ_SCOPE:
+            raise NotImplementedError("the adjoint met land or a cell shallower than desing_eps")
+        g = lam.interior(0).clone()
+        return g[0], g[1], g[2], lw[0, :, :self.nx].clone(), lw[1, :, :self.nx].clone()
+
+    def gradient(self, eta0, hu0, hv0, wind_x, wind_y):
+        J = self.forward(eta0, hu0, hv0, wind_x, wind_y)
+        return (J,) + tuple(self.backward())
+
+
+def _autograd():
+    torch = _native.require_cuda()
+
+    class CDKLM16Misfit(torch.autograd.Function):
+        """J = problem.forward(eta0, hu0, hv0, X, Y) as a torch scalar
+        (float64) with the adjoint as its backward."""
+
+        @staticmethod
+        def forward(ctx, problem, eta0, hu0, hv0, wind_x, wind_y):
+            J = problem.forward(eta0.detach(), hu0.detach(), hv0.detach(), wind_x.detach(), wind_y.detach())
+            ctx.problem = problem
+            return torch.tensor(J, dtype=torch.float64, device=eta0.device)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            ge, gu, gv, gx, gy = ctx.problem.backward()
+            s = gJ.to(torch.float32)
+            return None, ge * s, gu * s, gv * s, gx * s, gy * s
+
+    class CDKLM16Step(torch.autograd.Function):
+        """One RK2 step (eta, hu, hv, X, Y) -> (eta', hu', hv') of the
+        problem's domain; backward through go_adjoint_step."""
+
+        @staticmethod
+        def forward(ctx, problem, eta, hu, hv, wind_x, wind_y):
+            p = problem
+            slab = StateSlab(3, p.nx, p.ny)            # Q^n, Q*, Q^{n+1}
+            p.stream.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(p.stream):
+                for f, a in enumerate((eta, hu, hv)):
+                    slab.interior(0)[f].copy_(a.detach())
+                p.wind[0, :, :p.nx].copy_(wind_x.detach())
+                p.wind[1, :, :p.nx].copy_(wind_y.detach())
+            g = slab._gs[0]
+            lib = _native.load()
+            _native.check(lib.go_boundary_condition(p.domain.handle, p.sh, ctypes.c_void_p(g.eta),
+                                                    ctypes.c_void_p(g.hu), ctypes.c_void_p(g.hv), g.pitch))
+            p._traj_step(slab, 0, slab, 1, slab, 2)
+            torch.cuda.current_stream().wait_stream(p.stream)
+            ctx.problem = p
+            ctx.slab = slab
+            out = slab.interior(2).clone()
+            return out[0], out[1], out[2]
+
+        @staticmethod
+        def backward(ctx, le, lu, lv):
+            p, slab = ctx.problem, ctx.slab
+            lam = StateSlab(3, p.nx, p.ny)
+            lw = torch.zeros_like(p.lam_wind)
+            p.stream.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(p.stream):
+                for f, a in enumerate((le, lu, lv)):
+                    if a is not None:
+                        lam.interior(0)[f].copy_(a)
+            _native.check(_native.load().go_adjoint_step(
+                p.domain.handle, p.sh, float(p.dt), slab.gs(0), slab.gs(1), slab.gs(2), lam.gs(0), lam.gs(0),
+                lam.gs(1), lam.gs(2), _native.ptr(lw[0]), _native.ptr(lw[1]), p.wpitch, _native.ptr(p.Hi),
+                p.Hi_pitch))
+            torch.cuda.current_stream().wait_stream(p.stream)
+            g = lam.interior(0).clone()
+            return None, g[0], g[1], g[2], lw[0, :, :p.nx].clone(), lw[1, :, :p.nx].clone()
+
+    return CDKLM16Misfit, CDKLM16Step
+
+
+_FUNCS = None
+
+
+def functions():
+    """(CDKLM16Misfit, CDKLM16Step) torch.autograd.Function classes."""
+    global _FUNCS
+    if _FUNCS is None:
+        _FUNCS = _autograd()
+    return _FUNCS

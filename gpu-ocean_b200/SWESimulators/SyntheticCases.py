@@ -114,9 +114,12 @@ def bump256():
     return c
 
 
-def grf(n, dx=1000.0, seed_bathy=20241, seed_bumps=20242, steps=2000, f0=1.0e-4, beta=2.0e-11):
-    """The headline physics on an n x n grid."""
-    nx = ny = int(n)
+def grf(n, dx=1000.0, seed_bathy=20241, seed_bumps=20242, steps=2000, f0=1.0e-4, beta=2.0e-11, ny=None,
+        bc=(1, 2, 1, 2), r=3.0e-3):
+    """The headline physics on an n x n grid (n x ny if ny is given);
+    bc = (north, east, south, west) codes, r the friction coefficient."""
+    nx = int(n)
+    ny = nx if ny is None else int(ny)
     dy = dx
     G = gaussian_random_field((ny + 1, nx), 20, seed_bathy)
     Hi = np.zeros((ny + 5, nx + 5), dtype=np.float64)
@@ -137,8 +140,8 @@ def grf(n, dx=1000.0, seed_bathy=20241, seed_bumps=20242, steps=2000, f0=1.0e-4,
     eta0 = np.maximum(eta0, -Bm)
     z = np.zeros_like(eta0)
     tau = 0.1 * np.cos(np.pi / 4) / RHO_WATER
-    c = Case(name="grf%d" % n, nx=nx, ny=ny, dx=dx, dy=dy, g=9.81, f=f0 + 2 * beta * dy, beta=beta, r=3.0e-3,
-             bc=(1, 2, 1, 2), wind=(np.float32(tau), np.float32(tau)), eta0=eta0, hu0=z, hv0=z.copy(),
+    c = Case(name="grf%d" % n, nx=nx, ny=ny, dx=dx, dy=dy, g=9.81, f=f0 + 2 * beta * dy, beta=beta, r=float(r),
+             bc=tuple(int(b) for b in bc), wind=(np.float32(tau), np.float32(tau)), eta0=eta0, hu0=z, hv0=z.copy(),
              Hi=Hi, steps=steps)
     c.dt = cfl_dt(c)
     return c

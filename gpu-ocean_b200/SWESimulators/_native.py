@@ -18,6 +18,7 @@ GO_BC_PERIODIC = 2
 GO_FRICTION_QUADRATIC = 0
 GO_FRICTION_LINEAR = 1
 GO_STATUS_NONFINITE = 0x1
+GO_STATUS_ADJ_SCOPE = 0x2
 GO_ERR_INVALID = -1
 GO_ERR_CUDA = -2
 GO_ERR_UNSUPPORTED = -3
@@ -43,6 +44,14 @@ class GoDomainDesc(ctypes.Structure):
     ]
 
 
+class GoState(ctypes.Structure):
+    """go_state: three device arrays sharing a pitch in bytes."""
+    _fields_ = [("eta", ctypes.c_void_p), ("hu", ctypes.c_void_p), ("hv", ctypes.c_void_p),
+                ("pitch", ctypes.c_int)]
+
+
+_SP = ctypes.POINTER(GoState)
+
 # name -> (restype, argtypes)
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -64,6 +73,11 @@ SIGNATURES = {
     "go_cdklm_step_static": (_I, [ctypes.POINTER(GoDomainDesc), _P, ctypes.POINTER(ctypes.c_float), _I, _F, _F,
                                   _I, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F,
                                   ctypes.POINTER(ctypes.c_uint32)]),
+    "go_traj_step": (_I, [_P, _P, _F, _F, _SP, _SP, _SP, _P, _I, _F]),
+    "go_adjoint_stage": (_I, [_P, _P, _I, _F, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),
+    "go_adjoint_step": (_I, [_P, _P, _F, _SP, _SP, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),
+    "go_obs_misfit": (_I, [_P, _SP, _I, _I, _I, _P, _P, _F, _F, _P]),
+    "go_obs_adjoint": (_I, [_P, _SP, _SP, _I, _I, _I, _P, _P, _F, _F]),
     "go_max_dt": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _F, _P]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),

@@ -1,0 +1,800 @@
+// Reverse mode (adjoint) of one CDKLM16 Runge-Kutta stage.
+//
+// Forward stage (cdklm_swe_2D, CDKLM16_kernel.cu:429-1006): per cell the
+// primitive state (eta, u, v); minmod slopes of u, v and of the Coriolis
+// potentials K (x) and L (y) with the positivity adjustment (adjustSlopes,
+// CDKLM16_kernel.cu:148-245); central-upwind face fluxes
+// (CDKLM16_kernel.cu:80-140, 246-370); bathymetry, Coriolis and wind sources
+// and bottom friction (CDKLM16_kernel.cu:817-904); the RK update
+// (CDKLM16_kernel.cu:905-1004).  Given lambda, the adjoint of the stage
+// output, this kernel returns the adjoint with respect to the stage input,
+// to Q^n (stage 1) and to the wind-stress field.  Non-smooth operations
+// (minmod, the max/min wave speeds, the zero-flux cut, max(h, 0), the upwind
+// choice of the transverse flux, the dry clamp) are differentiated as the
+// subgradient of the branch the forward recomputation takes.
+//
+// Scope: north-up grids (angle 0), no land and no cell shallower than the
+// desingularisation depth (0.1 m).  A tile that meets a cell outside that
+// scope sets GO_STATUS_ADJ_SCOPE in the domain's status word.
+//
+// Layout: one CTA per output tile of TX x TY cells of the ghost-inclusive
+// grid.  The forward state of the tile plus a 3-cell halo is recomputed in
+// shared memory; the adjoint then flows output -> fluxes -> slopes -> cell
+// state as in the forward, each face handled once (two passes, even and odd
+// faces, so that no two threads update one cell at the same time) and each
+// slope gathered by its three cells.  The adjoint of ghost cells is written
+// to the ghost positions and moved to the interior cells they mirror or wrap
+// (k_adj_fold) afterwards.
+#include "internal.h"
+
+using namespace go;
+
+namespace {
+
+constexpr int TX = 32, TY = 16, HALO = 3;
+constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO;   // 38 x 22 region
+constexpr int NC = RX * RY;
+constexpr int NT = 256;
+
+struct AdjArgs {
+    Scheme k;
+    float dt;
+    const float *qe, *qu, *qv; int pq;     // stage input (ghost-inclusive)
+    const float *oe, *ou, *ov; int po;     // stage output
+    const float *le, *lu, *lv; int pl;     // adjoint of the output (interior cells read)
+    float *ie, *iu, *iv; int pi;           // adjoint of the input (all cells written)
+    float *ne, *nu, *nv; int pn;           // stage 1: adjoint of Q^n (written);
+                                           // stage 0: added to the input adjoint (may be null)
+    float *wx, *wy; int pw;                // wind adjoint, accumulated (interior-indexed, may be null)
+    const float* Hi; int phi;
+    const float* f_rows;
+    unsigned int* status;
+};
+
+// Branch codes
+enum { kBrZero = 0, kBrBack = 1, kBrCent = 2, kBrFwd = 3 };
+enum { kAdjNone = 0, kAdjA = 1, kAdjB = 2 };
+
+// Which argument minmod_raw (common.cu:544-551) returns: the one of least
+// magnitude when the three signs agree, else none.  When that magnitude is
+// exactly zero (a state at rest, or the mirrored difference at a wall) the
+// slope is taken as locally constant: the zero subgradient.
+__device__ __forceinline__ int mm_branch(float b, float c, float f) {
+    const uint32_t sb = __float_as_uint(b), sc = __float_as_uint(c), sf = __float_as_uint(f);
+    if ((((sb ^ sc) | (sc ^ sf)) & 0x80000000u) != 0u) return kBrZero;
+    const float ab = fabsf(b), ac = fabsf(c), af = fabsf(f);
+    if (ab <= ac && ab <= af) return ab > 0.0f ? kBrBack : kBrZero;
+    if (ac <= af) return ac > 0.0f ? kBrCent : kBrZero;
+    return af > 0.0f ? kBrFwd : kBrZero;
+}
+
+// d slope / d value at position pos (-1 left, 0 centre, +1 right) for the
+// minmod of theta*(c-l), (r-l)/2, theta*(r-c).
+__device__ __forceinline__ float slope_coef(int br, int pos, float theta) {
+    if (br == kBrBack) return pos < 0 ? -theta : (pos == 0 ? theta : 0.0f);
+    if (br == kBrCent) return pos < 0 ? -0.5f : (pos == 0 ? 0.0f : 0.5f);
+    if (br == kBrFwd) return pos < 0 ? 0.0f : (pos == 0 ? -theta : theta);
+    return 0.0f;
+}
+
+// d (sum of the Coriolis terms inside K or L) / d f*v at position pos:
+// backward (fc + fl), central ((fr + 2 fc) + fl)/2... scaled by theta*g or g/2.
+__device__ __forceinline__ float pot_coef(int br, int pos, float theta_g, float half_g) {
+    if (br == kBrBack) return pos > 0 ? 0.0f : theta_g;
+    if (br == kBrCent) return pos == 0 ? 2.0f * half_g : half_g;
+    if (br == kBrFwd) return pos < 0 ? 0.0f : theta_g;
+    return 0.0f;
+}
+
+__device__ __forceinline__ float flip(bool f) { return f ? -1.0f : 1.0f; }
+
+struct CuGrad { float hm, um, vm, hp, up, vp; };
+
+// Vector-Jacobian product of the central-upwind flux (CDKLM16_kernel.cu:80-140)
+// for the face states (hm, um, vm | hp, up, vp) and flux adjoint (l0, l1, l2).
+__device__ __forceinline__ CuGrad cu_vjp(float hm, float um, float vm, float hp, float up, float vp,
+                                         float l0, float l1, float l2, const Scheme& k) {
+    CuGrad g{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    const bool wp = hp > k.cutoff, wm = hm > k.cutoff;
+    float Fp0 = 0.0f, Fp1 = 0.0f, upw = 0.0f, cp = 0.0f;
+    if (wp) {
+        Fp0 = hp * up;
+        Fp1 = hp * up * up + k.half_g * hp * hp;
+        upw = up;
+        cp = sqrtf(k.g * hp);
+    }
+    float Fm0 = 0.0f, Fm1 = 0.0f, umw = 0.0f, cm = 0.0f;
+    if (wm) {
+        Fm0 = hm * um;
+        Fm1 = hm * um * um + k.half_g * hm * hm;
+        umw = um;
+        cm = sqrtf(k.g * hm);
+    }
+    const float a1 = umw - cm, a2 = upw - cp;
+    const float b1 = umw + cm, b2 = upw + cp;
+    const float am = fminf(fminf(a1, a2), 0.0f);
+    const float ap = fmaxf(fmaxf(b1, b2), 0.0f);
+    if (fabsf(ap - am) < k.flux_slope_eps) return g;
+    const float id = 1.0f / (ap - am);
+    const float dh = hp - hm, dF0 = Fp0 - Fm0;
+    const float F0 = ((ap * Fm0 - am * Fp0) + ap * am * dh) * id;
+    const float F1 = ((ap * Fm1 - am * Fp1) + ap * am * dF0) * id;
+    const float lap = l0 * ((Fm0 + am * dh) - F0) * id + l1 * ((Fm1 + am * dF0) - F1) * id;
+    const float lam = l0 * ((ap * dh - Fp0) + F0) * id + l1 * ((ap * dF0 - Fp1) + F1) * id;
+    const float apam = ap * am * id;
+    const float lFm0 = l0 * ap * id - l1 * apam, lFp0 = l1 * apam - l0 * am * id;
+    const float lFm1 = l1 * ap * id, lFp1 = -l1 * am * id;
+    const bool up_side = (um + up > 0.0f);
+    const float lFm2 = up_side ? l2 : 0.0f, lFp2 = up_side ? 0.0f : l2;
+    g.hp = l0 * apam;
+    g.hm = -l0 * apam;
+    float lumw = 0.0f, lcm = 0.0f, lupw = 0.0f, lcp = 0.0f;
+    if (fmaxf(b1, b2) > 0.0f) {
+        if (b1 >= b2) { lumw += lap; lcm += lap; } else { lupw += lap; lcp += lap; }
+    }
+    if (fminf(a1, a2) < 0.0f) {
+        if (a1 <= a2) { lumw += lam; lcm -= lam; } else { lupw += lam; lcp -= lam; }
+    }
+    if (wp) {
+        g.hp += lFp0 * up + lFp1 * (up * up + k.g * hp) + lFp2 * up * vp + lcp * (0.5f * k.g / cp);
+        g.up += lupw + lFp0 * hp + lFp1 * 2.0f * hp * up + lFp2 * hp * vp;
+        g.vp += lFp2 * hp * up;
+    }
+    if (wm) {
+        g.hm += lFm0 * um + lFm1 * (um * um + k.g * hm) + lFm2 * um * vm + lcm * (0.5f * k.g / cm);
+        g.um += lumw + lFm0 * hm + lFm1 * 2.0f * hm * um + lFm2 * hm * vm;
+        g.vm += lFm2 * hm * um;
+    }
+    return g;
+}
+
+struct AdjSmem {
+    float R0[NC], R1[NC], R2[NC];           // primitive state (eta, u, v)
+    float Ux[NC], Vx[NC], Kx[NC];           // x slopes (K after adjustment)
+    float Uy[NC], Vy[NC], Ly[NC];           // y slopes
+    uint32_t br[NC];                        // branch codes
+    float LL0[NC], LL1[NC], LL2[NC];        // adjoint of the cell tendencies L
+    float Ax0[NC], Ax1[NC], Ax2[NC];        // adjoint of (eta, u, v): own terms + x faces
+    float Ay0[NC], Ay1[NC], Ay2[NC];        // adjoint of (eta, u, v): y faces
+    float AKx[NC], AUx[NC], AVx[NC];        // adjoint of the x slopes
+    float ALy[NC], AUy[NC], AVy[NC];        // adjoint of the y slopes
+    float Hi[(RY + 1) * (RX + 1)];
+    float f[RY];
+};
+
+// branch-code fields
+__device__ __forceinline__ int br_ux(uint32_t b) { return b & 3; }
+__device__ __forceinline__ int br_vx(uint32_t b) { return (b >> 2) & 3; }
+__device__ __forceinline__ int br_kx(uint32_t b) { return (b >> 4) & 3; }
+__device__ __forceinline__ int br_kxa(uint32_t b) { return (b >> 6) & 3; }
+__device__ __forceinline__ int br_uy(uint32_t b) { return (b >> 8) & 3; }
+__device__ __forceinline__ int br_vy(uint32_t b) { return (b >> 10) & 3; }
+__device__ __forceinline__ int br_ly(uint32_t b) { return (b >> 12) & 3; }
+__device__ __forceinline__ int br_lya(uint32_t b) { return (b >> 14) & 3; }
+__device__ __forceinline__ bool has_xs(uint32_t b) { return (b >> 16) & 1; }
+__device__ __forceinline__ bool has_ys(uint32_t b) { return (b >> 17) & 1; }
+
+template <int FRIC, bool STAGE1>
+__global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    AdjSmem& S = *reinterpret_cast<AdjSmem*>(smem_raw);
+    const Scheme& k = a.k;
+    const int nx = k.nx, ny = k.ny;
+    const int ox = blockIdx.x * TX - HALO, oy = blockIdx.y * TY - HALO;
+    const int tid = threadIdx.x;
+    const bool wallN = k.bcN == kWall, wallS = k.bcS == kWall, wallE = k.bcE == kWall, wallW = k.bcW == kWall;
+    const float inv2g = 1.0f / k.two_g;
+    bool scope_bad = false;
+
+    // ---- corners and Coriolis rows --------------------------------------
+    for (int c = tid; c < (RY + 1) * (RX + 1); c += NT) {
+        const int ry = c / (RX + 1), rx = c % (RX + 1);
+        const int j = min(max(oy + ry, 0), ny + 4), i = min(max(ox + rx, 0), nx + 4);
+        S.Hi[c] = a.Hi[(size_t)j * a.phi + i];
+    }
+    for (int r = tid; r < RY; r += NT) S.f[r] = a.f_rows[min(max(oy + r, 0), ny + 3)];
+    __syncthreads();
+    auto HI = [&](int ry, int rx) { return S.Hi[ry * (RX + 1) + rx]; };
+
+    // ---- P1: primitive state of every region cell -----------------------
+    for (int c = tid; c < NC; c += NT) {
+        const int ry = c / RX, rx = c % RX;
+        const int j = oy + ry, i = ox + rx;
+        float e = 0.0f, u = 0.0f, v = 0.0f;
+        if (j >= 0 && j < ny + 4 && i >= 0 && i < nx + 4) {
+            int sj = j, si = i;
+            float shu = 1.0f, shv = 1.0f;
+            if (wallS && j < 2) { sj = 3 - j; shv = -1.0f; }
+            if (wallN && j > ny + 1) { sj = 2 * ny + 3 - j; shv = -1.0f; }
+            if (wallW && i < 2) { si = 3 - i; shu = -1.0f; }
+            if (wallE && i > nx + 1) { si = 2 * nx + 3 - i; shu = -1.0f; }
+            const size_t q = (size_t)sj * a.pq + si;
+            const float eta = a.qe[q], hu = a.qu[q] * shu, hv = a.qv[q] * shv;
+            const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
+            const float Bm = s4 * 0.25f;
+            const float h = eta + Bm;
+            if (fabsf(HI(ry, rx) - k.land) < kDryEps || fabsf(HI(ry + 1, rx) - k.land) < kDryEps ||
+                fabsf(HI(ry, rx + 1) - k.land) < kDryEps || fabsf(HI(ry + 1, rx + 1) - k.land) < kDryEps ||
+                h < k.desing_eps)
+                scope_bad = true;
+            e = eta;
+            u = hu / h;
+            v = hv / h;
+        }
+        S.R0[c] = e; S.R1[c] = u; S.R2[c] = v;
+        S.br[c] = 0u;
+        S.AKx[c] = 0.0f; S.AUx[c] = 0.0f; S.AVx[c] = 0.0f;
+        S.ALy[c] = 0.0f; S.AUy[c] = 0.0f; S.AVy[c] = 0.0f;
+        S.Ay0[c] = 0.0f; S.Ay1[c] = 0.0f; S.Ay2[c] = 0.0f;
+        S.Ax0[c] = 0.0f; S.Ax1[c] = 0.0f; S.Ax2[c] = 0.0f;
+        S.LL0[c] = 0.0f; S.LL1[c] = 0.0f; S.LL2[c] = 0.0f;
+    }
+    __syncthreads();
+
+    // ---- P2: slopes (x on the tile rows, y on the tile columns) ---------
+    for (int c = tid; c < NC; c += NT) {
+        const int ry = c / RX, rx = c % RX;
+        if (rx < 1 || rx > RX - 2 || ry < 1 || ry > RY - 2) continue;
+        const int j = oy + ry, i = ox + rx;
+        const bool tile_row = ry >= HALO && ry < HALO + TY;
+        const bool tile_col = rx >= HALO && rx < HALO + TX;
+        uint32_t code = 0u;
+        if (tile_row && j >= 2 && j < ny + 2 && i >= 1 && i <= nx + 2) {
+            const float fJ = S.f[ry];
+            const float ul = S.R1[c - 1], uc = S.R1[c], ur = S.R1[c + 1];
+            const float vl = S.R2[c - 1], vc = S.R2[c], vr = S.R2[c + 1];
+            const float el = S.R0[c - 1], ec = S.R0[c], er = S.R0[c + 1];
+            S.Ux[c] = minmod_slope(ul, uc, ur, k.theta);
+            S.Vx[c] = minmod_slope(vl, vc, vr, k.theta);
+            const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
+            const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
+            const float fvl = (vl * flip((wallW && i - 1 < 2) || (wallE && i - 1 > nx + 1))) * fJ;
+            const float fvc = (vc * flip((wallW && i < 2) || (wallE && i > nx + 1))) * fJ;
+            const float fvr = (vr * flip((wallW && i + 1 < 2) || (wallE && i + 1 > nx + 1))) * fJ;
+            const float bw = k.theta_g * ((ec - el) - k.V * (fvc + fvl));
+            const float ce = k.half_g * ((er - el) - k.V * ((fvr + 2.0f * fvc) + fvl));
+            const float fw = k.theta_g * ((er - ec) - k.V * (fvc + fvr));
+            const float Kraw = minmod_raw(bw, ce, fw);
+            const int bk = mm_branch(bw, ce, fw);
+            const float dxfv = (k.dx * fJ) * (vc * flip((wallW && i < 2) || (wallE && i > nx + 2)));
+            const float Hw = 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
+            const float He = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1));
+            const float hw = (ec + Hw) - (Kraw + dxfv) / k.two_g;
+            const float he = (ec + He) + (Kraw + dxfv) / k.two_g;
+            float K = Kraw;
+            int ba = kAdjNone;
+            if (!(hw > 0.0f)) { K = -dxfv + k.two_g * (ec + Hw); ba = kAdjA; }
+            if (!(he > 0.0f)) { K = -dxfv - k.two_g * (ec + He); ba = kAdjB; }
+            S.Kx[c] = K;
+            code |= (uint32_t)bu | ((uint32_t)bv << 2) | ((uint32_t)bk << 4) | ((uint32_t)ba << 6) | (1u << 16);
+        }
+        if (tile_col && i >= 2 && i < nx + 2 && j >= 1 && j <= ny + 2) {
+            const float ul = S.R1[c - RX], uc = S.R1[c], ur = S.R1[c + RX];
+            const float vl = S.R2[c - RX], vc = S.R2[c], vr = S.R2[c + RX];
+            const float el = S.R0[c - RX], ec = S.R0[c], er = S.R0[c + RX];
+            S.Uy[c] = minmod_slope(ul, uc, ur, k.theta);
+            S.Vy[c] = minmod_slope(vl, vc, vr, k.theta);
+            const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
+            const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
+            const float ful = (ul * flip((wallS && j - 1 < 2) || (wallN && j - 1 > ny + 1))) * S.f[ry - 1];
+            const float fuc = (uc * flip((wallS && j < 2) || (wallN && j > ny + 1))) * S.f[ry];
+            const float fur = (ur * flip((wallS && j + 1 < 2) || (wallN && j + 1 > ny + 1))) * S.f[ry + 1];
+            const float bw = k.theta_g * ((ec - el) + k.U * (fuc + ful));
+            const float ce = k.half_g * ((er - el) + k.U * ((fur + 2.0f * fuc) + ful));
+            const float fw = k.theta_g * ((er - ec) + k.U * (fuc + fur));
+            const float Lraw = minmod_raw(bw, ce, fw);
+            const int bl = mm_branch(bw, ce, fw);
+            const float dyfu = (k.dy * S.f[ry]) * (uc * flip((wallS && j < 2) || (wallN && j > ny + 2)));
+            const float Hs = 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
+            const float Hn = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1));
+            const float hs = (ec + Hs) - (Lraw - dyfu) / k.two_g;
+            const float hn = (ec + Hn) + (Lraw - dyfu) / k.two_g;
+            float L = Lraw;
+            int ba = kAdjNone;
+            if (!(hs > 0.0f)) { L = dyfu + k.two_g * (ec + Hs); ba = kAdjA; }
+            if (!(hn > 0.0f)) { L = dyfu - k.two_g * (ec + Hn); ba = kAdjB; }
+            S.Ly[c] = L;
+            code |= ((uint32_t)bu << 8) | ((uint32_t)bv << 10) | ((uint32_t)bl << 12) | ((uint32_t)ba << 14) |
+                    (1u << 17);
+        }
+        S.br[c] = code;
+    }
+
+    // ---- P3: adjoint of the RK update, friction and sources -------------
+    // (interior cells of the cross tile rows x [1, RX-2] + tile columns x [1, RY-2])
+    for (int c = tid; c < NC; c += NT) {
+        const int ry = c / RX, rx = c % RX;
+        if (rx < 1 || rx > RX - 2 || ry < 1 || ry > RY - 2) continue;
+        const bool tile_row = ry >= HALO && ry < HALO + TY;
+        const bool tile_col = rx >= HALO && rx < HALO + TX;
+        if (!tile_row && !tile_col) continue;
+        const int j = oy + ry, i = ox + rx;
+        if (j < 2 || j >= ny + 2 || i < 2 || i >= nx + 2) continue;
+        const size_t lo = (size_t)j * a.pl + i, oo = (size_t)j * a.po + i;
+        float lE = a.le[lo], lU = a.lu[lo], lV = a.lv[lo];
+        const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
+        const float Hm = 0.25f * s4;
+        if (a.oe[oo] + Hm <= k.cutoff) { lE = 0.0f; lU = 0.0f; lV = 0.0f; }   // dry clamp: constant output
+        const float e = S.R0[c], u = S.R1[c], v = S.R2[c];
+        const float h = e + Hm;
+        const bool wet = h > k.cutoff;
+        const float hu = wet ? u * h : 0.0f, hv = wet ? v * h : 0.0f;
+        float Cf = 0.0f, s = 0.0f, uw = 0.0f, vw = 0.0f;
+        if (FRIC == kFricQuad) {
+            uw = hu / h; vw = hv / h;
+            s = sqrtf(uw * uw + vw * vw);
+            Cf = (a.dt * k.r * s) / h;
+        } else if (FRIC == kFricLinear) {
+            Cf = (k.two_r * a.dt) / h;
+        }
+        const float w = STAGE1 ? 0.5f : 1.0f;
+        const float iD = 1.0f / (1.0f + w * Cf);
+        const float lL1 = w * a.dt * lE, lL2 = w * a.dt * lU * iD, lL3 = w * a.dt * lV * iD;
+        float lhu = w * lU * iD, lhv = w * lV * iD, leta = w * lE, lh = 0.0f;
+        const float lCf = -w * (lU * a.ou[oo] + lV * a.ov[oo]) * iD;
+        if (FRIC == kFricQuad) {
+            const float ls = lCf * a.dt * k.r / h;
+            lh -= lCf * Cf / h;
+            if (s > 0.0f) {
+                const float luw = ls * uw / s, lvw = ls * vw / s;
+                lhu += luw / h; lhv += lvw / h;
+                lh -= (luw * uw + lvw * vw) / h;
+            }
+        } else if (FRIC == kFricLinear) {
+            lh -= lCf * Cf / h;
+        }
+        const float fc = S.f[ry];
+        if (h >= k.cutoff) {
+            const float Hx = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
+            const float Hy = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
+            lhv += fc * lL2;
+            lhu -= fc * lL3;
+            leta += lL2 * k.g * Hx / k.dx + lL3 * k.g * Hy / k.dy;
+            if (tile_row && tile_col && a.wx) {
+                const size_t wo = (size_t)(j - 2) * a.pw + (i - 2);
+                a.wx[wo] += lL2;
+                a.wy[wo] += lL3;
+            }
+        }
+        float lR1 = 0.0f, lR2 = 0.0f;
+        if (wet) {
+            lh += lhu * u + lhv * v;
+            lR1 = lhu * h;
+            lR2 = lhv * h;
+        }
+        S.LL0[c] = lL1; S.LL1[c] = lL2; S.LL2[c] = lL3;
+        S.Ax0[c] = lh + leta; S.Ax1[c] = lR1; S.Ax2[c] = lR2;
+        if (STAGE1 && tile_row && tile_col) {
+            const size_t no = (size_t)j * a.pn + i;
+            a.ne[no] = w * lE;
+            a.nu[no] = w * lU * iD;
+            a.nv[no] = w * lV * iD;
+        }
+    }
+    __syncthreads();
+
+    // ---- P4: faces, even then odd --------------------------------------
+    constexpr int NFX = RX - 3;   // x faces per tile row: m at rx = 1..RX-3
+    constexpr int NFY = RY - 3;   // y faces per tile column: m at ry = 1..RY-3
+    const float DXf = k.dx, DYf = k.dy;
+    for (int parity = 0; parity < 2; ++parity) {
+        constexpr int NXH = (NFX + 1) / 2, NYH = (NFY + 1) / 2;
+        const int nxi = TY * NXH, nyi = TX * NYH;
+        for (int it = tid; it < nxi + nyi; it += NT) {
+            if (it < nxi) {
+                const int ry = HALO + it / NXH;
+                const int rx = 1 + parity + 2 * (it % NXH);
+                if (rx > RX - 3) continue;
+                const int j = oy + ry, im = ox + rx, ip = im + 1;
+                if (j < 2 || j >= ny + 2 || im < 1 || im > nx + 1) continue;
+                const int m = ry * RX + rx, p = m + 1;
+                const float fJ = S.f[ry];
+                const float Rmu = S.R1[m] + 0.5f * S.Ux[m], Rmv = S.R2[m] + 0.5f * S.Vx[m];
+                const float Rpu = S.R1[p] - 0.5f * S.Ux[p], Rpv = S.R2[p] - 0.5f * S.Vx[p];
+                const float fm = flip(wallW && ip == 2), fp = flip(wallE && ip == nx + 2);
+                const float Hf = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1));
+                const float Ep = (S.R0[p] + Hf) - (S.Kx[p] + (k.dx * fJ) * (S.R2[p] * fp)) / k.two_g;
+                const float Em = (S.R0[m] + Hf) + (S.Kx[m] + (k.dx * fJ) * (S.R2[m] * fm)) / k.two_g;
+                const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
+                const float l0 = (S.LL0[p] - S.LL0[m]) / DXf;
+                const float l1 = (S.LL1[p] - S.LL1[m]) / DXf;
+                const float l2 = (S.LL2[p] - S.LL2[m]) / DXf;
+                const CuGrad g = cu_vjp(hm, Rmu, Rmv, hp, Rpu, Rpv, l0, l1, l2, k);
+                if (Ep > 0.0f) {
+                    S.Ax0[p] += g.hp;
+                    S.AKx[p] -= g.hp * inv2g;
+                    S.Ax2[p] -= g.hp * (k.dx * fJ) * fp * inv2g;
+                }
+                if (Em > 0.0f) {
+                    S.Ax0[m] += g.hm;
+                    S.AKx[m] += g.hm * inv2g;
+                    S.Ax2[m] += g.hm * (k.dx * fJ) * fm * inv2g;
+                }
+                S.Ax1[p] += g.up; S.AUx[p] -= 0.5f * g.up;
+                S.Ax2[p] += g.vp; S.AVx[p] -= 0.5f * g.vp;
+                S.Ax1[m] += g.um; S.AUx[m] += 0.5f * g.um;
+                S.Ax2[m] += g.vm; S.AVx[m] += 0.5f * g.vm;
+            } else {
+                const int t = it - nxi;
+                const int rx = HALO + t / NYH;
+                const int ry = 1 + parity + 2 * (t % NYH);
+                if (ry > RY - 3) continue;
+                const int i = ox + rx, jm = oy + ry, jp = jm + 1;
+                if (i < 2 || i >= nx + 2 || jm < 1 || jm > ny + 1) continue;
+                const int m = ry * RX + rx, p = m + RX;
+                const float Rmu = S.R1[m] + 0.5f * S.Uy[m], Rmv = S.R2[m] + 0.5f * S.Vy[m];
+                const float Rpu = S.R1[p] - 0.5f * S.Uy[p], Rpv = S.R2[p] - 0.5f * S.Vy[p];
+                const float fm = flip(wallS && jp == 2), fp = flip(wallN && jp == ny + 2);
+                const float fpr = S.f[ry + 1], fmr = S.f[ry];
+                const float Hf = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1));
+                const float Ep = (S.R0[p] + Hf) - (S.Ly[p] - (k.dy * fpr) * (S.R1[p] * fp)) / k.two_g;
+                const float Em = (S.R0[m] + Hf) + (S.Ly[m] - (k.dy * fmr) * (S.R1[m] * fm)) / k.two_g;
+                const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
+                // G = CU(hm, v, u | hp, v, u) with outputs (G0, G2, G1)
+                const float l0 = (S.LL0[p] - S.LL0[m]) / DYf;
+                const float l1 = (S.LL1[p] - S.LL1[m]) / DYf;
+                const float l2 = (S.LL2[p] - S.LL2[m]) / DYf;
+                const CuGrad g = cu_vjp(hm, Rmv, Rmu, hp, Rpv, Rpu, l0, l2, l1, k);
+                if (Ep > 0.0f) {
+                    S.Ay0[p] += g.hp;
+                    S.ALy[p] -= g.hp * inv2g;
+                    S.Ay1[p] += g.hp * (k.dy * fpr) * fp * inv2g;
+                }
+                if (Em > 0.0f) {
+                    S.Ay0[m] += g.hm;
+                    S.ALy[m] += g.hm * inv2g;
+                    S.Ay1[m] -= g.hm * (k.dy * fmr) * fm * inv2g;
+                }
+                S.Ay2[p] += g.up; S.AVy[p] -= 0.5f * g.up;
+                S.Ay1[p] += g.vp; S.AUy[p] -= 0.5f * g.vp;
+                S.Ay2[m] += g.um; S.AVy[m] += 0.5f * g.um;
+                S.Ay1[m] += g.vm; S.AUy[m] += 0.5f * g.vm;
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- P5: positivity adjustment of K and L ---------------------------
+    for (int c = tid; c < NC; c += NT) {
+        const int ry = c / RX, rx = c % RX;
+        if (rx < HALO - 1 || rx > HALO + TX || ry < HALO - 1 || ry > HALO + TY) continue;
+        const uint32_t b = S.br[c];
+        if (has_xs(b)) {
+            const float lK = S.AKx[c];
+            const int ba = br_kxa(b);
+            if (ba != kAdjNone) {
+                const int i = ox + rx;
+                const float fv = flip((wallW && i < 2) || (wallE && i > nx + 2));
+                S.Ax0[c] += (ba == kAdjA ? k.two_g : -k.two_g) * lK;
+                S.Ax2[c] -= lK * (k.dx * S.f[ry]) * fv;
+                S.AKx[c] = 0.0f;
+            }
+        }
+        if (has_ys(b)) {
+            const float lL = S.ALy[c];
+            const int ba = br_lya(b);
+            if (ba != kAdjNone) {
+                const int j = oy + ry;
+                const float fu = flip((wallS && j < 2) || (wallN && j > ny + 2));
+                S.Ay0[c] += (ba == kAdjA ? k.two_g : -k.two_g) * lL;
+                S.Ay1[c] += lL * (k.dy * S.f[ry]) * fu;
+                S.ALy[c] = 0.0f;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- P6: gather the slopes, cell state -> conserved variables --------
+    for (int c = tid; c < TX * TY; c += NT) {
+        const int ry = HALO + c / TX, rx = HALO + c % TX;
+        const int j = oy + ry, i = ox + rx;
+        if (j >= ny + 4 || i >= nx + 4) continue;
+        const int q = ry * RX + rx;
+        float l0 = S.Ax0[q] + S.Ay0[q];
+        float l1 = S.Ax1[q] + S.Ay1[q];
+        float l2 = S.Ax2[q] + S.Ay2[q];
+        float lfv = 0.0f, lfu = 0.0f;
+        for (int o = -1; o <= 1; ++o) {
+            const int pos = -o;       // position of this cell in the stencil of slope cell q+o
+            const uint32_t bx = S.br[q + o];
+            if (has_xs(bx)) {
+                l1 += S.AUx[q + o] * slope_coef(br_ux(bx), pos, k.theta);
+                l2 += S.AVx[q + o] * slope_coef(br_vx(bx), pos, k.theta);
+                const float lk = S.AKx[q + o];
+                const int bk = br_kx(bx);
+                l0 += lk * k.g * slope_coef(bk, pos, k.theta);
+                lfv -= lk * k.V * pot_coef(bk, pos, k.theta_g, k.half_g);
+            }
+            const uint32_t by = S.br[q + o * RX];
+            if (has_ys(by)) {
+                l1 += S.AUy[q + o * RX] * slope_coef(br_uy(by), pos, k.theta);
+                l2 += S.AVy[q + o * RX] * slope_coef(br_vy(by), pos, k.theta);
+                const float ll = S.ALy[q + o * RX];
+                const int bl = br_ly(by);
+                l0 += ll * k.g * slope_coef(bl, pos, k.theta);
+                lfu += ll * k.U * pot_coef(bl, pos, k.theta_g, k.half_g);
+            }
+        }
+        l2 += lfv * S.f[ry] * flip((wallW && i < 2) || (wallE && i > nx + 1));
+        l1 += lfu * S.f[ry] * flip((wallS && j < 2) || (wallN && j > ny + 1));
+        const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
+        const float h = S.R0[q] + s4 * 0.25f;
+        float lE = l0 - (l1 * S.R1[q] + l2 * S.R2[q]) / h;
+        float lU = l1 / h, lV = l2 / h;
+        if (!STAGE1 && a.ne && j >= 2 && j < ny + 2 && i >= 2 && i < nx + 2) {
+            const size_t no = (size_t)j * a.pn + i;
+            lE += a.ne[no]; lU += a.nu[no]; lV += a.nv[no];
+        }
+        const size_t io = (size_t)j * a.pi + i;
+        a.ie[io] = lE; a.iu[io] = lU; a.iv[io] = lV;
+    }
+    if (scope_bad && a.status) atomicOr(a.status, GO_STATUS_ADJ_SCOPE);
+}
+
+// Moves the adjoint held at ghost cells to the interior cells whose values
+// the ghosts carry: mirror (walls; hv flips at north/south walls, hu at
+// east/west) or wrap (periodic).  One thread per interior cell within two
+// cells of a side; corner ghosts are never read by the stage and carry none.
+__global__ void k_adj_fold(float* e, float* u, float* v, int p, int nx, int ny, int bcN, int bcE, int bcS,
+                           int bcW) {
+    const int nrow = 4 * nx, ncol = 4 * (ny - 4 > 0 ? ny - 4 : 0);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrow + ncol) return;
+    int j, i;
+    if (t < nrow) {
+        const int r = t / nx;
+        j = (r == 0) ? 2 : (r == 1) ? 3 : (r == 2) ? ny : ny + 1;
+        i = 2 + t % nx;
+    } else {
+        const int s = t - nrow;
+        const int cidx = s / (ny - 4);
+        i = (cidx == 0) ? 2 : (cidx == 1) ? 3 : (cidx == 2) ? nx : nx + 1;
+        j = 4 + s % (ny - 4);
+    }
+    const size_t o = (size_t)j * p + i;
+    float ae = 0.0f, au = 0.0f, av = 0.0f;
+    // source ghost row for this row, if any
+    int gj = -1;
+    float sv = 1.0f;
+    if (j == 2) { gj = (bcS == kWall) ? 1 : ny + 2; sv = (bcS == kWall) ? -1.0f : 1.0f; }
+    else if (j == 3) { gj = (bcS == kWall) ? 0 : ny + 3; sv = (bcS == kWall) ? -1.0f : 1.0f; }
+    if (j == ny + 1) { gj = (bcN == kWall) ? ny + 2 : 1; sv = (bcN == kWall) ? -1.0f : 1.0f; }
+    else if (j == ny) { gj = (bcN == kWall) ? ny + 3 : 0; sv = (bcN == kWall) ? -1.0f : 1.0f; }
+    if (gj >= 0) {
+        const size_t g = (size_t)gj * p + i;
+        ae += e[g]; au += u[g]; av += sv * v[g];
+    }
+    int gi = -1;
+    float su = 1.0f;
+    if (i == 2) { gi = (bcW == kWall) ? 1 : nx + 2; su = (bcW == kWall) ? -1.0f : 1.0f; }
+    else if (i == 3) { gi = (bcW == kWall) ? 0 : nx + 3; su = (bcW == kWall) ? -1.0f : 1.0f; }
+    if (i == nx + 1) { gi = (bcE == kWall) ? nx + 2 : 1; su = (bcE == kWall) ? -1.0f : 1.0f; }
+    else if (i == nx) { gi = (bcE == kWall) ? nx + 3 : 0; su = (bcE == kWall) ? -1.0f : 1.0f; }
+    if (gi >= 0) {
+        const size_t g = (size_t)j * p + gi;
+        ae += e[g]; au += su * u[g]; av += v[g];
+    }
+    e[o] += ae; u[o] += au; v[o] += av;
+}
+
+template <int FRIC, bool STAGE1>
+cudaError_t launch_adj(const AdjArgs& a, cudaStream_t s) {
+    // the dynamic shared-memory limit is raised once per device
+    static unsigned long long attr_set = 0ull;
+    const int bytes = (int)sizeof(AdjSmem);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 64 || !((attr_set >> dev) & 1ull)) {
+        e = cudaFuncSetAttribute(cdklm_adjoint_stage_kernel<FRIC, STAGE1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+        if (dev < 64) attr_set |= 1ull << dev;
+    }
+    const dim3 grid((a.k.nx + 4 + TX - 1) / TX, (a.k.ny + 4 + TY - 1) / TY);
+    cdklm_adjoint_stage_kernel<FRIC, STAGE1><<<grid, NT, bytes, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold(const go_domain* d, const go_state* l, cudaStream_t s) {
+    const int nx = d->k.nx, ny = d->k.ny;
+    const int n = 4 * nx + 4 * (ny - 4 > 0 ? ny - 4 : 0);
+    k_adj_fold<<<(n + 255) / 256, 256, 0, s>>>(l->eta, l->hu, l->hv, l->pitch / 4, nx, ny, d->k.bcN, d->k.bcE,
+                                               d->k.bcS, d->k.bcW);
+    return cudaGetLastError();
+}
+
+int check_state(const go_state* s, int min_floats, const char* what) {
+    if (!s || !s->eta || !s->hu || !s->hv) return go_fail(GO_ERR_INVALID, "%s: null state", what);
+    return go_check_pitch(s->pitch, min_floats, what);
+}
+
+int adjoint_stage(go_domain* d, cudaStream_t s, int rk_step, float dt, const go_state* q_in,
+                  const go_state* q_out, const go_state* lam_out, const go_state* lam_in,
+                  const go_state* lam_qn, float* lam_wx, float* lam_wy, int wind_pitch, const float* Hi,
+                  int Hi_pitch) {
+    AdjArgs a;
+    memset(&a, 0, sizeof(a));
+    a.k = d->k;
+    a.dt = dt;
+    a.qe = q_in->eta; a.qu = q_in->hu; a.qv = q_in->hv; a.pq = q_in->pitch / 4;
+    a.oe = q_out->eta; a.ou = q_out->hu; a.ov = q_out->hv; a.po = q_out->pitch / 4;
+    a.le = lam_out->eta; a.lu = lam_out->hu; a.lv = lam_out->hv; a.pl = lam_out->pitch / 4;
+    a.ie = lam_in->eta; a.iu = lam_in->hu; a.iv = lam_in->hv; a.pi = lam_in->pitch / 4;
+    if (lam_qn) { a.ne = lam_qn->eta; a.nu = lam_qn->hu; a.nv = lam_qn->hv; a.pn = lam_qn->pitch / 4; }
+    a.wx = lam_wx; a.wy = lam_wy; a.pw = wind_pitch / 4;
+    a.Hi = Hi; a.phi = Hi_pitch / 4;
+    a.f_rows = d->d_frows;
+    a.status = d->d_status;
+    const int fric = go_friction_mode(d);
+    cudaError_t e;
+    if (rk_step == 0) {
+        e = fric == kFricQuad ? launch_adj<kFricQuad, false>(a, s)
+          : fric == kFricLinear ? launch_adj<kFricLinear, false>(a, s) : launch_adj<kFricNone, false>(a, s);
+    } else {
+        e = fric == kFricQuad ? launch_adj<kFricQuad, true>(a, s)
+          : fric == kFricLinear ? launch_adj<kFricLinear, true>(a, s) : launch_adj<kFricNone, true>(a, s);
+    }
+    if (e == cudaSuccess) e = launch_fold(d, lam_in, s);
+    if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "adjoint stage launch failed: %s", cudaGetErrorString(e));
+    return GO_OK;
+}
+
+int check_adjoint_domain(const go_domain* d) {
+    if (go_general_north(d))
+        return go_fail(GO_ERR_UNSUPPORTED, "the adjoint is built for north-up grids (angle 0) only");
+    return GO_OK;
+}
+
+__global__ void k_obs_misfit(const float* e, const float* u, const float* v, int p, int nx, int ny, int n,
+                             const int* ij, const float* obs, float w_eta, float w_vel, double* J) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc = 0.0;
+    const int oi = (t < n) ? ij[2 * t] : -1, oj = (t < n) ? ij[2 * t + 1] : -1;
+    if (oi >= 0 && oi < nx && oj >= 0 && oj < ny) {      // cells outside the interior are skipped
+        const size_t o = (size_t)(oj + 2) * p + (oi + 2);
+        const double de = (double)e[o] - (double)obs[3 * t];
+        const double du = (double)u[o] - (double)obs[3 * t + 1];
+        const double dv = (double)v[o] - (double)obs[3 * t + 2];
+        acc = (double)w_eta * de * de + (double)w_vel * (du * du + dv * dv);
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(J, acc);
+}
+
+__global__ void k_obs_adjoint(const float* e, const float* u, const float* v, int p, float* le, float* lu,
+                              float* lv, int pl, int nx, int ny, int n, const int* ij, const float* obs,
+                              float w_eta, float w_vel) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = ij[2 * t] + 2, j = ij[2 * t + 1] + 2;
+    if (i < 2 || i >= nx + 2 || j < 2 || j >= ny + 2) return;   // outside the interior
+    const size_t o = (size_t)j * p + i, ol = (size_t)j * pl + i;
+    atomicAdd(le + ol, 2.0f * w_eta * (e[o] - obs[3 * t]));
+    atomicAdd(lu + ol, 2.0f * w_vel * (u[o] - obs[3 * t + 1]));
+    atomicAdd(lv + ol, 2.0f * w_vel * (v[o] - obs[3 * t + 2]));
+}
+
+}  // namespace
+
+extern "C" {
+
+int go_adjoint_stage(go_domain* d, void* stream, int rk_step, float dt, const go_state* q_in,
+                     const go_state* q_out, const go_state* lam_out, const go_state* lam_in,
+                     const go_state* lam_qn, float* lam_wx, float* lam_wy, int wind_pitch,
+                     const float* Hi, int Hi_pitch) {
+    if (!d || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
+    if (rk_step != 0 && rk_step != 1) return go_fail(GO_ERR_INVALID, "rk_step %d (RK2 has 0 and 1)", rk_step);
+    int rc = check_adjoint_domain(d);
+    const int w = d->k.nx + 4;
+    if (!rc) rc = check_state(q_in, w, "q_in");
+    if (!rc) rc = check_state(q_out, w, "q_out");
+    if (!rc) rc = check_state(lam_out, w, "lam_out");
+    if (!rc) rc = check_state(lam_in, w, "lam_in");
+    if (!rc && (lam_qn || rk_step == 1)) rc = check_state(lam_qn, w, "lam_qn");
+    if (!rc) rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+    if (!rc && (lam_wx || lam_wy)) {
+        if (!lam_wx || !lam_wy) return go_fail(GO_ERR_INVALID, "wind adjoint needs both components");
+        rc = go_check_pitch(wind_pitch, d->k.nx, "wind");
+    }
+    if (rc) return rc;
+    if (lam_in->eta == lam_out->eta || lam_in->eta == q_in->eta)
+        return go_fail(GO_ERR_INVALID, "lam_in must not alias lam_out or q_in");
+    return adjoint_stage(d, (cudaStream_t)stream, rk_step, dt, q_in, q_out, lam_out, lam_in, lam_qn, lam_wx,
+                         lam_wy, wind_pitch, Hi, Hi_pitch);
+}
+
+int go_adjoint_step(go_domain* d, void* stream, float dt, const go_state* q_n, const go_state* q_star,
+                    const go_state* q_next, const go_state* lam_next, const go_state* lam_n,
+                    const go_state* scratch_star, const go_state* scratch_qn, float* lam_wx, float* lam_wy,
+                    int wind_pitch, const float* Hi, int Hi_pitch) {
+    if (!d || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
+    int rc = check_adjoint_domain(d);
+    const int w = d->k.nx + 4;
+    if (!rc) rc = check_state(q_n, w, "q_n");
+    if (!rc) rc = check_state(q_star, w, "q_star");
+    if (!rc) rc = check_state(q_next, w, "q_next");
+    if (!rc) rc = check_state(lam_next, w, "lam_next");
+    if (!rc) rc = check_state(lam_n, w, "lam_n");
+    if (!rc) rc = check_state(scratch_star, w, "scratch_star");
+    if (!rc) rc = check_state(scratch_qn, w, "scratch_qn");
+    if (!rc) rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+    if (!rc && (lam_wx || lam_wy)) {
+        if (!lam_wx || !lam_wy) return go_fail(GO_ERR_INVALID, "wind adjoint needs both components");
+        rc = go_check_pitch(wind_pitch, d->k.nx, "wind");
+    }
+    if (rc) return rc;
+    if (scratch_star->eta == lam_next->eta || scratch_star->eta == lam_n->eta ||
+        scratch_qn->eta == lam_n->eta || scratch_qn->eta == scratch_star->eta)
+        return go_fail(GO_ERR_INVALID, "scratch buffers must not alias the adjoint states");
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = adjoint_stage(d, s, 1, dt, q_star, q_next, lam_next, scratch_star, scratch_qn, lam_wx, lam_wy,
+                       wind_pitch, Hi, Hi_pitch);
+    if (rc) return rc;
+    return adjoint_stage(d, s, 0, dt, q_n, q_star, scratch_star, lam_n, scratch_qn, lam_wx, lam_wy, wind_pitch,
+                         Hi, Hi_pitch);
+}
+
+int go_traj_step(go_domain* d, void* stream, float dt, float wind_stress_t, const go_state* q_n,
+                 const go_state* q_star, const go_state* q_next, const float* Hi, int Hi_pitch,
+                 float land_value) {
+    if (!d || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
+    const int w = d->k.nx + 4;
+    int rc = check_state(q_n, w, "q_n");
+    if (!rc) rc = check_state(q_star, w, "q_star");
+    if (!rc) rc = check_state(q_next, w, "q_next");
+    if (!rc) rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+    if (rc) return rc;
+    if (q_next->eta == q_n->eta || q_star->eta == q_n->eta || q_star->eta == q_next->eta)
+        return go_fail(GO_ERR_INVALID, "q_n, q_star and q_next must be distinct buffers");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t wb = sizeof(float) * (size_t)w;
+    const float* src[3] = {q_n->eta, q_n->hu, q_n->hv};
+    float* dst[3] = {q_next->eta, q_next->hu, q_next->hv};
+    for (int f = 0; f < 3; ++f)
+        GO_CUDA(cudaMemcpy2DAsync(dst[f], q_next->pitch, src[f], q_n->pitch, wb, d->k.ny + 4,
+                                  cudaMemcpyDeviceToDevice, s));
+    const StageArgs a0 = go_stage_args(d, dt, 0, q_n->eta, q_n->hu, q_n->hv, q_n->pitch / 4, q_star->eta,
+                                       q_star->hu, q_star->hv, q_star->pitch / 4, Hi, Hi_pitch / 4, land_value,
+                                       wind_stress_t);
+    const StageArgs a1 = go_stage_args(d, dt, 1, q_star->eta, q_star->hu, q_star->hv, q_star->pitch / 4,
+                                       q_next->eta, q_next->hu, q_next->hv, q_next->pitch / 4, Hi, Hi_pitch / 4,
+                                       land_value, wind_stress_t);
+    rc = go_launch_stage(d, s, a0);
+    if (rc) return rc;
+    return go_launch_stage(d, s, a1);
+}
+
+int go_obs_misfit(void* stream, const go_state* q, int nx, int ny, int n_obs, const int* obs_ij,
+                  const float* obs_values, float w_eta, float w_vel, double* J_dev) {
+    if (!q || !q->eta || !q->hu || !q->hv || (n_obs > 0 && (!obs_ij || !obs_values)) || !J_dev)
+        return go_fail(GO_ERR_INVALID, "null argument");
+    if (n_obs < 0) return go_fail(GO_ERR_INVALID, "n_obs < 0");
+    int rc = go_check_pitch(q->pitch, nx + 4, "q");
+    if (rc) return rc;
+    if (n_obs == 0) return GO_OK;
+    k_obs_misfit<<<(n_obs + 255) / 256, 256, 0, (cudaStream_t)stream>>>(q->eta, q->hu, q->hv, q->pitch / 4, nx, ny,
+                                                                      n_obs, obs_ij, obs_values, w_eta, w_vel,
+                                                                      J_dev);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+int go_obs_adjoint(void* stream, const go_state* q, const go_state* lam, int nx, int ny, int n_obs,
+                   const int* obs_ij, const float* obs_values, float w_eta, float w_vel) {
+    if (!q || !lam || !q->eta || !q->hu || !q->hv || !lam->eta || !lam->hu || !lam->hv ||
+        (n_obs > 0 && (!obs_ij || !obs_values)))
+        return go_fail(GO_ERR_INVALID, "null argument");
+    if (n_obs < 0) return go_fail(GO_ERR_INVALID, "n_obs < 0");
+    int rc = go_check_pitch(q->pitch, nx + 4, "q");
+    if (!rc) rc = go_check_pitch(lam->pitch, nx + 4, "lam");
+    if (rc) return rc;
+    if (n_obs == 0) return GO_OK;
+    k_obs_adjoint<<<(n_obs + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        q->eta, q->hu, q->hv, q->pitch / 4, lam->eta, lam->hu, lam->hv, lam->pitch / 4, nx, ny, n_obs, obs_ij,
+        obs_values, w_eta, w_vel);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+}  // extern "C"

@@ -46,6 +46,8 @@ extern "C" {
 
 /* Device status word bits (go_domain_status). */
 #define GO_STATUS_NONFINITE 0x1u /* a written cell held NaN or Inf */
+#define GO_STATUS_ADJ_SCOPE 0x2u /* the adjoint met land, a cell shallower than
+                                   desing_eps, or a non-north-up grid */
 
 typedef struct go_domain go_domain;
 
@@ -197,6 +199,64 @@ int go_batch_step(go_batch* b, void* stream, int n_steps);
  * and replay it; steps_done (optional) receives n_steps. */
 int go_batch_graph_capture(go_batch* b, void* stream, int n_steps);
 int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done);
+
+/* ---------------------------------------------------------------------
+ * Adjoint (reverse mode) of the RK2 step.  No counterpart in the
+ * reference, which has no adjoint.  Built for north-up grids without land
+ * or cells shallower than desing_eps (GO_STATUS_ADJ_SCOPE otherwise).
+ * A state is three device arrays of (ny+4) x (nx+4) floats sharing a pitch
+ * in bytes; adjoint states hold their values at the interior cells.
+ * --------------------------------------------------------------------- */
+typedef struct go_state {
+    float* eta;
+    float* hu;
+    float* hv;
+    int pitch;             /* bytes */
+} go_state;
+
+/* One forward step that keeps its stages: q_star = stage 0 of q_n,
+ * q_next = stage 1 (q_n copied to q_next first, since stage 1 reads Q^n
+ * from its output buffer).  Bit-identical to go_cdklm_step. */
+int go_traj_step(go_domain* d, void* stream, float dt, float wind_stress_t,
+                 const go_state* q_n, const go_state* q_star, const go_state* q_next,
+                 const float* Hi, int Hi_pitch, float land_value);
+
+/* Adjoint of one RK stage (the reverse of go_cdklm_swe_2D) given its input
+ * q_in, its stored output q_out and lam_out, the adjoint of the output.
+ * Writes lam_in, the adjoint of the input (ghost-cell adjoint moved to the
+ * interior cells the ghosts mirror or wrap).  rk_step 1 also writes lam_qn,
+ * the adjoint of Q^n; for rk_step 0 a non-NULL lam_qn is added to lam_in.
+ * lam_wx/lam_wy (optional, ny x nx, pitch in bytes) accumulate the adjoint
+ * of the per-cell wind stress. */
+int go_adjoint_stage(go_domain* d, void* stream, int rk_step, float dt,
+                     const go_state* q_in, const go_state* q_out, const go_state* lam_out,
+                     const go_state* lam_in, const go_state* lam_qn,
+                     float* lam_wx, float* lam_wy, int wind_pitch,
+                     const float* Hi, int Hi_pitch);
+
+/* Adjoint of one RK2 step: lam_n = (dQ^{n+1}/dQ^n)^T lam_next from the
+ * step's q_n, q_star, q_next (as go_traj_step stores them).  lam_n may be
+ * lam_next (in place); the two scratch states must be distinct from both. */
+int go_adjoint_step(go_domain* d, void* stream, float dt,
+                    const go_state* q_n, const go_state* q_star, const go_state* q_next,
+                    const go_state* lam_next, const go_state* lam_n,
+                    const go_state* scratch_star, const go_state* scratch_qn,
+                    float* lam_wx, float* lam_wy, int wind_pitch,
+                    const float* Hi, int Hi_pitch);
+
+/* Observation misfit J += sum w_eta (eta - eta_obs)^2 + w_vel ((hu - hu_obs)^2
+ * + (hv - hv_obs)^2) over n_obs interior cells of an nx x ny grid (device
+ * int pairs (i, j), 0-based interior indices, pairs outside the interior
+ * are skipped; device float triples of observed values), accumulated in
+ * FP64 into J_dev. */
+int go_obs_misfit(void* stream, const go_state* q, int nx, int ny, int n_obs,
+                  const int* obs_ij, const float* obs_values, float w_eta, float w_vel,
+                  double* J_dev);
+
+/* Adds dJ/dQ of that misfit to lam at the observed cells. */
+int go_obs_adjoint(void* stream, const go_state* q, const go_state* lam, int nx, int ny,
+                   int n_obs, const int* obs_ij, const float* obs_values, float w_eta,
+                   float w_vel);
 
 /* ---------------------------------------------------------------------
  * Allocation-free step.  No counterpart in the reference (its CDKLM16

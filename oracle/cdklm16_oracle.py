@@ -242,12 +242,47 @@ def namespace_for(a):
 # Kernel helpers
 # ---------------------------------------------------------------------------
 
+# ---------------------------------------------------------------------------
+# Branch recording (for finite-difference checks of the adjoint: a direction
+# is only usable when no branch of the scheme changes along it)
+# ---------------------------------------------------------------------------
+
+_REC = None
+
+
+class record_branches:
+    """Context manager: every branch decision of rk_stage inside it is
+    appended (as a boolean or small-integer array) to ``self.masks``."""
+
+    def __enter__(self):
+        global _REC
+        self.masks = []
+        self._prev = _REC
+        _REC = self.masks
+        return self
+
+    def __exit__(self, *exc):
+        global _REC
+        _REC = self._prev
+        return False
+
+
+def _rec(*arrays):
+    if _REC is not None:
+        for a in arrays:
+            _REC.append(a.detach().clone() if hasattr(a, "detach") else np.array(a, copy=True))
+
+
 def minmod_raw(xp, backward, central, forward):
     """common.cu:544-551"""
     sb = xp.sign1(backward)
     sc = xp.sign1(central)
     sf = xp.sign1(forward)
     m = xp.minimum(xp.minimum(xp.abs(backward), xp.abs(central)), xp.abs(forward))
+    if _REC is not None:
+        ab, ac, af = xp.abs(backward), xp.abs(central), xp.abs(forward)
+        same = (sb == sc) & (sc == sf)
+        _rec(same, same & (ab <= ac) & (ab <= af), same & (ac <= af))
     return 0.25 * sb * (sb + sc) * (sc + sf) * m
 
 
@@ -289,6 +324,8 @@ def central_upwind_flux(xp, hm, um, vm, hp, up_, vp, g, cutoff, slope_eps):
     am = xp.minimum(xp.minimum(umw - cm, upw - cp), 0.0)
     ap = xp.maximum(xp.maximum(umw + cm, upw + cp), 0.0)
     zero = xp.abs(ap - am) < slope_eps
+    _rec(wetp, wetm, (umw - cm) <= (upw - cp), am < 0.0, (umw + cm) >= (upw + cp), ap > 0.0, zero,
+         (um + up_) > 0)
     den = xp.where(zero, 1.0, ap - am)
     F0 = ((ap * Fm0 - am * Fp0) + ap * am * (hp - hm)) / den
     F1 = ((ap * Fm1 - am * Fp1) + ap * am * (Fp0 - Fm0)) / den
@@ -458,6 +495,7 @@ def rk_stage(p, Q_in, Q_n, S, dt, rk_step, wind=(0.0, 0.0)):
         h = eta + Bm
         shallow = h < T(des_eps)
         dry = h <= cutoff
+        _rec(shallow, dry)
         h_safe = xp.where(shallow, 1.0, h)
         u_des = desingularize(xp, h, hu, des_eps, f32)
         v_des = desingularize(xp, h, hv, des_eps, f32)
@@ -491,6 +529,7 @@ def rk_stage(p, Q_in, Q_n, S, dt, rk_step, wind=(0.0, 0.0)):
         dxfv = (DX * fJ) * vadj
         h_w = (eta_c + S.H_w) - (Kx + dxfv) / two_g
         h_e = (eta_c + S.H_e) + (Kx + dxfv) / two_g
+        _rec(h_w > 0, h_e > 0)
         Kx = xp.where(h_w > 0, Kx, -dxfv + two_g * (eta_c + S.H_w))
         Kx = xp.where(h_e > 0, Kx, -dxfv - two_g * (eta_c + S.H_e))
 
@@ -508,6 +547,7 @@ def rk_stage(p, Q_in, Q_n, S, dt, rk_step, wind=(0.0, 0.0)):
         Hfx = S.Hface_x
         hp = xp.maximum((R0[J, 2:nx + 3] + Hfx) - (Kx[:, pp] + (DX * fJ) * vp_n) / two_g, 0.0)
         hm = xp.maximum((R0[J, 1:nx + 2] + Hfx) + (Kx[:, m] + (DX * fJ) * vm_n) / two_g, 0.0)
+        _rec(hp > 0, hm > 0)
         F0, F1, F2 = central_upwind_flux(xp, hm, Rm_u, Rm_v, hp, Rp_u, Rp_v, g, cutoff, slope_eps)
         dryf = (R0[J, 2:nx + 3] == flag) | (R0[J, 1:nx + 2] == flag)
         F0 = xp.where(dryf, 0.0, F0)
@@ -544,6 +584,7 @@ def rk_stage(p, Q_in, Q_n, S, dt, rk_step, wind=(0.0, 0.0)):
         dyfu = (DY * fR) * uadj
         h_s = (e_c + S.H_s) - (Ly - dyfu) / two_g
         h_n = (e_c + S.H_n) + (Ly - dyfu) / two_g
+        _rec(h_s > 0, h_n > 0)
         Ly = xp.where(h_s > 0, Ly, dyfu + two_g * (e_c + S.H_s))
         Ly = xp.where(h_n > 0, Ly, dyfu - two_g * (e_c + S.H_n))
 
@@ -563,6 +604,7 @@ def rk_stage(p, Q_in, Q_n, S, dt, rk_step, wind=(0.0, 0.0)):
         fm = S.f[1:ny + 2][:, None]
         hp = xp.maximum((R0[2:ny + 3, I] + Hfy) - (Ly[pp] - (DY * fp) * up_e) / two_g, 0.0)
         hm = xp.maximum((R0[1:ny + 2, I] + Hfy) + (Ly[m] - (DY * fm) * um_e) / two_g, 0.0)
+        _rec(hp > 0, hm > 0)
         G0, G2, G1 = central_upwind_flux(xp, hm, Rm_v, Rm_u, hp, Rp_v, Rp_u, g, cutoff, slope_eps)
         dryg = (R0[2:ny + 3, I] == flag) | (R0[1:ny + 2, I] == flag)
         G0 = xp.where(dryg, 0.0, G0)
@@ -629,6 +671,7 @@ def rk_stage(p, Q_in, Q_n, S, dt, rk_step, wind=(0.0, 0.0)):
             new_hv = (T(0.5) * (qa[2] + (hv_own + dt * L3))) / (T(1.0) + T(0.5) * Cf)
 
         dry_new = (new_eta + Hm) <= cutoff
+        _rec(dry_new)
         floor = -Hm + cutoff
         new_eta = xp.where(dry_new, floor, new_eta)
         new_hu = xp.where(dry_new, 0.0, new_hu)
