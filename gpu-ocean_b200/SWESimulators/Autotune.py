@@ -18,8 +18,9 @@ import numpy as np
 
 from . import _native
 
-DOMAIN_CANDIDATES = [(4, 16), (4, 32), (4, 64), (2, 16), (2, 32), (1, 16), (1, 32), (3, 32), (0, 32)]
-BATCH_CANDIDATES = [(4, 16, 0), (4, 32, 0), (2, 16, 0), (2, 32, 0), (1, 32, 0), (4, 32, 148 * 5)]
+DOMAIN_CANDIDATES = [(4, 2), (4, 4), (4, 8), (4, 16), (4, 32), (2, 4), (2, 8), (2, 16), (2, 32), (1, 8),
+                     (1, 16), (1, 32), (3, 16), (0, 16)]
+BATCH_CANDIDATES = [(4, 8, 0), (4, 16, 0), (4, 32, 0), (2, 16, 0), (2, 32, 0), (1, 16, 0), (4, 16, 148 * 5)]
 GRAPH_LENGTHS = [10, 50]
 
 

@@ -4,7 +4,7 @@
 
 The floating-point flags are the reference's own (gpu_ocean/SWESimulators/
 CDKLM16.py:196-200): --ftz=true --prec-div=false --prec-sqrt=false
---fmad=false.
+--fmad=false (the adjoint unit contracts FMAs, see UNIT_FLAGS).
 """
 
 import os
@@ -24,6 +24,17 @@ NVCC_FLAGS = [
     "--ftz=true", "--prec-div=false", "--prec-sqrt=false", "--fmad=false",
     "-Xcompiler", "-fPIC",
 ]
+
+
+# Units whose flags differ: the adjoint is not bit-compared with the
+# reference and keeps the forward's rounding only where a branch depends on
+# it (written out with __fmul_rn in the source), so it may contract FMAs.
+UNIT_FLAGS = {"adjoint.cu": {"--fmad=false": "--fmad=true"}}
+
+
+def flags_for(unit):
+    sub = UNIT_FLAGS.get(unit, {})
+    return [sub.get(f, f) for f in NVCC_FLAGS]
 
 
 def sources():
@@ -55,7 +66,7 @@ def build(force=False, verbose=False):
     try:
         def compile_one(u):
             obj = os.path.join(work, u + ".o")
-            cmd = [nvcc] + NVCC_FLAGS + ["-I", INCLUDE, "-c", os.path.join(CSRC, u), "-o", obj]
+            cmd = [nvcc] + flags_for(u) + ["-I", INCLUDE, "-c", os.path.join(CSRC, u), "-o", obj]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

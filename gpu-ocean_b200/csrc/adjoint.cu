@@ -17,6 +17,12 @@
 // desingularisation depth (0.1 m).  A tile that meets a cell outside that
 // scope sets GO_STATUS_ADJ_SCOPE in the domain's status word.
 //
+// Arithmetic: this unit is compiled with FMA contraction (the adjoint is
+// compared with FP64 derivatives, not bit for bit), but every value a branch
+// decision reads (minmod arguments, the positivity tests, face depths and
+// velocities, wave speeds) keeps the forward kernel's rounding: products that
+// feed a sum are written with __fmul_rn so that they are never contracted.
+//
 // Layout: one CTA per output tile of TX x TY cells of the ghost-inclusive
 // grid.  The forward state of the tile plus a 3-cell halo is recomputed in
 // shared memory; the adjoint then flows output -> fluxes -> slopes -> cell
@@ -211,7 +217,7 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
             const size_t q = (size_t)sj * a.pq + si;
             const float eta = a.qe[q], hu = a.qu[q] * shu, hv = a.qv[q] * shv;
             const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
-            const float Bm = s4 * 0.25f;
+            const float Bm = __fmul_rn(s4, 0.25f);
             const float h = eta + Bm;
             if (fabsf(HI(ry, rx) - k.land) < kDryEps || fabsf(HI(ry + 1, rx) - k.land) < kDryEps ||
                 fabsf(HI(ry, rx + 1) - k.land) < kDryEps || fabsf(HI(ry + 1, rx + 1) - k.land) < kDryEps ||
@@ -251,20 +257,20 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
             const float fvl = (vl * flip((wallW && i - 1 < 2) || (wallE && i - 1 > nx + 1))) * fJ;
             const float fvc = (vc * flip((wallW && i < 2) || (wallE && i > nx + 1))) * fJ;
             const float fvr = (vr * flip((wallW && i + 1 < 2) || (wallE && i + 1 > nx + 1))) * fJ;
-            const float bw = k.theta_g * ((ec - el) - k.V * (fvc + fvl));
-            const float ce = k.half_g * ((er - el) - k.V * ((fvr + 2.0f * fvc) + fvl));
-            const float fw = k.theta_g * ((er - ec) - k.V * (fvc + fvr));
+            const float bw = k.theta_g * ((ec - el) - __fmul_rn(k.V, fvc + fvl));
+            const float ce = k.half_g * ((er - el) - __fmul_rn(k.V, (fvr + __fmul_rn(2.0f, fvc)) + fvl));
+            const float fw = k.theta_g * ((er - ec) - __fmul_rn(k.V, fvc + fvr));
             const float Kraw = minmod_raw(bw, ce, fw);
             const int bk = mm_branch(bw, ce, fw);
-            const float dxfv = (k.dx * fJ) * (vc * flip((wallW && i < 2) || (wallE && i > nx + 2)));
+            const float dxfv = __fmul_rn(k.dx * fJ, vc * flip((wallW && i < 2) || (wallE && i > nx + 2)));
             const float Hw = 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
             const float He = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1));
             const float hw = (ec + Hw) - (Kraw + dxfv) / k.two_g;
             const float he = (ec + He) + (Kraw + dxfv) / k.two_g;
             float K = Kraw;
             int ba = kAdjNone;
-            if (!(hw > 0.0f)) { K = -dxfv + k.two_g * (ec + Hw); ba = kAdjA; }
-            if (!(he > 0.0f)) { K = -dxfv - k.two_g * (ec + He); ba = kAdjB; }
+            if (!(hw > 0.0f)) { K = -dxfv + __fmul_rn(k.two_g, ec + Hw); ba = kAdjA; }
+            if (!(he > 0.0f)) { K = -dxfv - __fmul_rn(k.two_g, ec + He); ba = kAdjB; }
             S.Kx[c] = K;
             code |= (uint32_t)bu | ((uint32_t)bv << 2) | ((uint32_t)bk << 4) | ((uint32_t)ba << 6) | (1u << 16);
         }
@@ -279,20 +285,20 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
             const float ful = (ul * flip((wallS && j - 1 < 2) || (wallN && j - 1 > ny + 1))) * S.f[ry - 1];
             const float fuc = (uc * flip((wallS && j < 2) || (wallN && j > ny + 1))) * S.f[ry];
             const float fur = (ur * flip((wallS && j + 1 < 2) || (wallN && j + 1 > ny + 1))) * S.f[ry + 1];
-            const float bw = k.theta_g * ((ec - el) + k.U * (fuc + ful));
-            const float ce = k.half_g * ((er - el) + k.U * ((fur + 2.0f * fuc) + ful));
-            const float fw = k.theta_g * ((er - ec) + k.U * (fuc + fur));
+            const float bw = k.theta_g * ((ec - el) + __fmul_rn(k.U, fuc + ful));
+            const float ce = k.half_g * ((er - el) + __fmul_rn(k.U, (fur + __fmul_rn(2.0f, fuc)) + ful));
+            const float fw = k.theta_g * ((er - ec) + __fmul_rn(k.U, fuc + fur));
             const float Lraw = minmod_raw(bw, ce, fw);
             const int bl = mm_branch(bw, ce, fw);
-            const float dyfu = (k.dy * S.f[ry]) * (uc * flip((wallS && j < 2) || (wallN && j > ny + 2)));
+            const float dyfu = __fmul_rn(k.dy * S.f[ry], uc * flip((wallS && j < 2) || (wallN && j > ny + 2)));
             const float Hs = 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
             const float Hn = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1));
             const float hs = (ec + Hs) - (Lraw - dyfu) / k.two_g;
             const float hn = (ec + Hn) + (Lraw - dyfu) / k.two_g;
             float L = Lraw;
             int ba = kAdjNone;
-            if (!(hs > 0.0f)) { L = dyfu + k.two_g * (ec + Hs); ba = kAdjA; }
-            if (!(hn > 0.0f)) { L = dyfu - k.two_g * (ec + Hn); ba = kAdjB; }
+            if (!(hs > 0.0f)) { L = dyfu + __fmul_rn(k.two_g, ec + Hs); ba = kAdjA; }
+            if (!(hn > 0.0f)) { L = dyfu - __fmul_rn(k.two_g, ec + Hn); ba = kAdjB; }
             S.Ly[c] = L;
             code |= ((uint32_t)bu << 8) | ((uint32_t)bv << 10) | ((uint32_t)bl << 12) | ((uint32_t)ba << 14) |
                     (1u << 17);
@@ -389,12 +395,12 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
                 if (j < 2 || j >= ny + 2 || im < 1 || im > nx + 1) continue;
                 const int m = ry * RX + rx, p = m + 1;
                 const float fJ = S.f[ry];
-                const float Rmu = S.R1[m] + 0.5f * S.Ux[m], Rmv = S.R2[m] + 0.5f * S.Vx[m];
-                const float Rpu = S.R1[p] - 0.5f * S.Ux[p], Rpv = S.R2[p] - 0.5f * S.Vx[p];
+                const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Ux[m]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vx[m]);
+                const float Rpu = S.R1[p] - __fmul_rn(0.5f, S.Ux[p]), Rpv = S.R2[p] - __fmul_rn(0.5f, S.Vx[p]);
                 const float fm = flip(wallW && ip == 2), fp = flip(wallE && ip == nx + 2);
                 const float Hf = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1));
-                const float Ep = (S.R0[p] + Hf) - (S.Kx[p] + (k.dx * fJ) * (S.R2[p] * fp)) / k.two_g;
-                const float Em = (S.R0[m] + Hf) + (S.Kx[m] + (k.dx * fJ) * (S.R2[m] * fm)) / k.two_g;
+                const float Ep = (S.R0[p] + Hf) - (S.Kx[p] + __fmul_rn(k.dx * fJ, S.R2[p] * fp)) / k.two_g;
+                const float Em = (S.R0[m] + Hf) + (S.Kx[m] + __fmul_rn(k.dx * fJ, S.R2[m] * fm)) / k.two_g;
                 const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
                 const float l0 = (S.LL0[p] - S.LL0[m]) / DXf;
                 const float l1 = (S.LL1[p] - S.LL1[m]) / DXf;
@@ -422,13 +428,13 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
                 const int i = ox + rx, jm = oy + ry, jp = jm + 1;
                 if (i < 2 || i >= nx + 2 || jm < 1 || jm > ny + 1) continue;
                 const int m = ry * RX + rx, p = m + RX;
-                const float Rmu = S.R1[m] + 0.5f * S.Uy[m], Rmv = S.R2[m] + 0.5f * S.Vy[m];
-                const float Rpu = S.R1[p] - 0.5f * S.Uy[p], Rpv = S.R2[p] - 0.5f * S.Vy[p];
+                const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Uy[m]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vy[m]);
+                const float Rpu = S.R1[p] - __fmul_rn(0.5f, S.Uy[p]), Rpv = S.R2[p] - __fmul_rn(0.5f, S.Vy[p]);
                 const float fm = flip(wallS && jp == 2), fp = flip(wallN && jp == ny + 2);
                 const float fpr = S.f[ry + 1], fmr = S.f[ry];
                 const float Hf = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1));
-                const float Ep = (S.R0[p] + Hf) - (S.Ly[p] - (k.dy * fpr) * (S.R1[p] * fp)) / k.two_g;
-                const float Em = (S.R0[m] + Hf) + (S.Ly[m] - (k.dy * fmr) * (S.R1[m] * fm)) / k.two_g;
+                const float Ep = (S.R0[p] + Hf) - (S.Ly[p] - __fmul_rn(k.dy * fpr, S.R1[p] * fp)) / k.two_g;
+                const float Em = (S.R0[m] + Hf) + (S.Ly[m] - __fmul_rn(k.dy * fmr, S.R1[m] * fm)) / k.two_g;
                 const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
                 // G = CU(hm, v, u | hp, v, u) with outputs (G0, G2, G1)
                 const float l0 = (S.LL0[p] - S.LL0[m]) / DYf;
@@ -748,18 +754,13 @@ int go_traj_step(go_domain* d, void* stream, float dt, float wind_stress_t, cons
     if (q_next->eta == q_n->eta || q_star->eta == q_n->eta || q_star->eta == q_next->eta)
         return go_fail(GO_ERR_INVALID, "q_n, q_star and q_next must be distinct buffers");
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t wb = sizeof(float) * (size_t)w;
-    const float* src[3] = {q_n->eta, q_n->hu, q_n->hv};
-    float* dst[3] = {q_next->eta, q_next->hu, q_next->hv};
-    for (int f = 0; f < 3; ++f)
-        GO_CUDA(cudaMemcpy2DAsync(dst[f], q_next->pitch, src[f], q_n->pitch, wb, d->k.ny + 4,
-                                  cudaMemcpyDeviceToDevice, s));
     const StageArgs a0 = go_stage_args(d, dt, 0, q_n->eta, q_n->hu, q_n->hv, q_n->pitch / 4, q_star->eta,
                                        q_star->hu, q_star->hv, q_star->pitch / 4, Hi, Hi_pitch / 4, land_value,
                                        wind_stress_t);
-    const StageArgs a1 = go_stage_args(d, dt, 1, q_star->eta, q_star->hu, q_star->hv, q_star->pitch / 4,
-                                       q_next->eta, q_next->hu, q_next->hv, q_next->pitch / 4, Hi, Hi_pitch / 4,
-                                       land_value, wind_stress_t);
+    StageArgs a1 = go_stage_args(d, dt, 1, q_star->eta, q_star->hu, q_star->hv, q_star->pitch / 4,
+                                 q_next->eta, q_next->hu, q_next->hv, q_next->pitch / 4, Hi, Hi_pitch / 4,
+                                 land_value, wind_stress_t);
+    a1.qn_eta = q_n->eta; a1.qn_hu = q_n->hu; a1.qn_hv = q_n->hv; a1.pqn = q_n->pitch / 4;
     rc = go_launch_stage(d, s, a0);
     if (rc) return rc;
     return go_launch_stage(d, s, a1);

@@ -5,7 +5,7 @@
 // --ftz=true --prec-div=false --prec-sqrt=false --fmad=false.
 #include <string>
 
-#include "internal.h"
+#include "dispatch.cuh"
 
 using namespace go;
 
@@ -28,6 +28,15 @@ int go_check_pitch(int pitch_bytes, int min_floats, const char* what) {
     return GO_OK;
 }
 
+int go_auto_rows(int nx, int ny, int shape) {
+    const int useful = go::shape_block_width(shape) - 4;
+    const long long strips = (nx + useful - 1) / useful;
+    const long long target = strips * (long long)ny / 600;
+    int rows = 2;
+    while (rows < 16 && 2 * rows <= target) rows *= 2;
+    return rows;
+}
+
 int go_friction_mode(const go_domain* d) {
     if (d->desc.friction_law == GO_FRICTION_LINEAR) return kFricLinear;
     return (d->k.r > 0.0f) ? kFricQuad : kFricNone;
@@ -47,6 +56,7 @@ StageArgs go_stage_args(const go_domain* d, float dt, int rk_step, const float* 
     a.rk_step = rk_step;
     a.eta_in = e0; a.hu_in = u0; a.hv_in = v0; a.pin = pin;
     a.eta_out = e1; a.hu_out = u1; a.hv_out = v1; a.pout = pout;
+    a.qn_eta = e1; a.qn_hu = u1; a.qn_hv = v1; a.pqn = pout;
     a.Hi = Hi; a.phi = phi;
     a.f_rows = d->d_frows;
     a.wind_t = wind_t;
@@ -211,8 +221,8 @@ int go_domain_create(const go_domain_desc* desc, go_domain** out) {
     k.V = s.dx / k.two_g;
     k.U = s.dy / k.two_g;
     k.two_r = two * s.r;
-    d->rows_per_block = 32;
     d->shape = 4;
+    d->rows_per_block = go_auto_rows(s.nx, s.ny, d->shape);
     d->arith = GO_ARITH_RCP;
     d->has_land = 1;
     cudaError_t e = cudaGetDevice(&d->device);
@@ -279,7 +289,7 @@ int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_ne
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block) {
     if (!d) return go_fail(GO_ERR_INVALID, "null domain");
     if (shape < 0 || shape > 4) return go_fail(GO_ERR_INVALID, "launch shape %d (0..4)", shape);
-    if (rows_per_block == 0) rows_per_block = 32;
+    if (rows_per_block == 0) rows_per_block = go_auto_rows(d->k.nx, d->k.ny, shape);
     if (rows_per_block < 1) return go_fail(GO_ERR_INVALID, "rows_per_block must be >= 1");
     d->shape = shape;
     d->rows_per_block = rows_per_block;

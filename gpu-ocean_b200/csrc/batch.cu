@@ -111,7 +111,7 @@ int go_batch_create(go_domain* const* members, int n, go_batch** out) {
     b->variant = go_variant(d0);
     b->arith = d0->arith;
     b->shape = d0->shape;
-    b->rows = d0->rows_per_block;
+    b->rows = 16;          // a batch launches enough blocks for long strips
     for (int m = 1; m < n; ++m) {
         const go_domain* d = members[m];
         b->variant.land = b->variant.land || d->has_land;
@@ -172,7 +172,7 @@ int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, f
 int go_batch_set_launch(go_batch* b, int shape, int rows_per_block, int blocks) {
     if (!b) return go_fail(GO_ERR_INVALID, "null batch");
     if (shape < 0 || shape > 4) return go_fail(GO_ERR_INVALID, "launch shape %d (0..4)", shape);
-    if (rows_per_block == 0) rows_per_block = 32;
+    if (rows_per_block == 0) rows_per_block = 16;
     if (rows_per_block < 1 || blocks < 0) return go_fail(GO_ERR_INVALID, "rows_per_block >= 1, blocks >= 0");
     b->shape = shape;
     b->rows = rows_per_block;

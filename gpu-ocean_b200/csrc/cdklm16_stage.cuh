@@ -47,6 +47,10 @@ struct StageArgs {
     int pin;                     // pitch of the inputs, floats
     float* eta_out; float* hu_out; float* hv_out;
     int pout;                    // pitch of the outputs, floats
+    // Q^n read by stage 1 at each cell: the output buffer itself (the
+    // reference's in-place update) unless a separate state is given
+    const float* qn_eta; const float* qn_hu; const float* qn_hv;
+    int pqn;
     const float* Hi; int phi;    // corners (ny+5) x (nx+5)
     const float* f_rows;         // Coriolis per ghost-inclusive row
     float wind_t, wxc, wxn, wyc, wyn;
@@ -373,8 +377,8 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
     const bool stage1 = (a.rk_step == 1);
     float nqn_e = 0.0f, nqn_hu = 0.0f, nqn_hv = 0.0f;
     if (stage1 && writer) {
-        const size_t o = (size_t)r0 * a.pout + cl;
-        nqn_e = a.eta_out[o]; nqn_hu = a.hu_out[o]; nqn_hv = a.hv_out[o];
+        const size_t o = (size_t)r0 * a.pqn + cl;
+        nqn_e = a.qn_eta[o]; nqn_hu = a.qn_hu[o]; nqn_hv = a.qn_hv[o];
     }
     const bool col_img = EDGE && (k.bcE == kPeriodic) && (cl < 4 || cl >= k.nx);
     const float2 theta2 = f2(k.theta, k.theta);
@@ -394,8 +398,8 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
             load_h(min(j + 4, r1 + 2), nha, nhb);
             nf = __ldg(frow + min(j + 3, k.ny + 3));
             if (stage1 && writer && j + 1 < r1) {
-                const size_t o = (size_t)(j + 1) * a.pout + cl;
-                nqn_e = a.eta_out[o]; nqn_hu = a.hu_out[o]; nqn_hv = a.hv_out[o];
+                const size_t o = (size_t)(j + 1) * a.pqn + cl;
+                nqn_e = a.qn_eta[o]; nqn_hu = a.qn_hu[o]; nqn_hv = a.qn_hv[o];
             }
         }
         const Cell P2 = to_cell(q_e, q_hu, q_hv, Ha2, Hb2, Ha3, Hb3);

@@ -37,6 +37,11 @@ int go_fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3))
 
 int go_check_pitch(int pitch_bytes, int min_floats, const char* what);
 
+// Default rows per block strip for a grid and launch shape: the power of two
+// in [2, 16] nearest below (column strips x ny) / 600, so that small grids
+// still launch enough blocks to cover the 148 SMs.
+int go_auto_rows(int nx, int ny, int shape);
+
 // Kernel-variant selectors of a domain.
 int go_friction_mode(const go_domain* d);
 bool go_general_north(const go_domain* d);

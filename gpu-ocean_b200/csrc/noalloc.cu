@@ -100,8 +100,8 @@ int fill_domain(const go_domain_desc& s, go_domain* d) {
     k.V = s.dx / k.two_g;
     k.U = s.dy / k.two_g;
     k.two_r = two * s.r;
-    d->rows_per_block = 32;
     d->shape = 4;
+    d->rows_per_block = go_auto_rows(s.nx, s.ny, d->shape);
     d->arith = GO_ARITH_RCP;
     d->has_land = 1;
     return GO_OK;

@@ -94,8 +94,9 @@ int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_ne
 
 /* Launch shape of the step kernel: shape 0 = 192 threads x 2 blocks/SM,
  * 1 = 192 x 3, 2 = 128 x 4, 3 = 256 x 2, 4 = 128 x 5 (default); each block
- * marches down a strip of rows_per_block rows (0 = default 32).  Chosen by
- * the autotuner; every shape computes identical results. */
+ * marches down a strip of rows_per_block rows (0 = automatic: a power of two
+ * in [2, 16] that gives small grids enough blocks).  Chosen by the
+ * autotuner; every shape computes identical results. */
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block);
 
 /* How quotients are evaluated.  EXACT keeps every '/' of the reference
@@ -215,8 +216,8 @@ typedef struct go_state {
 } go_state;
 
 /* One forward step that keeps its stages: q_star = stage 0 of q_n,
- * q_next = stage 1 (q_n copied to q_next first, since stage 1 reads Q^n
- * from its output buffer).  Bit-identical to go_cdklm_step. */
+ * q_next = stage 1 (reading Q^n from q_n instead of its output buffer).
+ * Bit-identical to go_cdklm_step; q_n is left unchanged. */
 int go_traj_step(go_domain* d, void* stream, float dt, float wind_stress_t,
                  const go_state* q_n, const go_state* q_star, const go_state* q_next,
                  const float* Hi, int Hi_pitch, float land_value);
