@@ -127,5 +127,25 @@ class BatchedCDKLM16:
             self.set_dt([dt] * self.n)
         return self.sims[0].t
 
+    def perturb(self, key0, event, std=0.05, corr_cells=15.0):
+        """Every member's eta += std * field(key (key0, m), event): one
+        batched pass, identical to ModelError.perturb member by member."""
+        from . import ModelError
+        lib = _native.load()
+        n = lib.go_batch_grf_scratch_floats(self.batch.handle, float(corr_cells))
+        if n == 0:
+            raise ValueError("invalid correlation length")
+        buf = ModelError._scratch_for(n)
+        self._sync_members()
+        _native.check(lib.go_batch_grf_perturb(self.batch.handle, _native.stream_handle(self.stream),
+                                               int(key0) & 0xFFFFFFFF, int(event) & 0xFFFFFFFF, float(std),
+                                               float(corr_cells), _native.ptr(buf), int(buf.numel())))
+        for s in self.sims:
+            s.gpu_stream.wait_stream(self.stream)
+
+    def model_error(self, event, std=0.05, corr_cells=15.0):
+        from . import ModelError
+        self.perturb(ModelError.MODEL_ERROR_SEED, event, std, corr_cells)
+
     def synchronize(self):
         self.stream.synchronize()

@@ -78,6 +78,11 @@ SIGNATURES = {
     "go_adjoint_step": (_I, [_P, _P, _F, _SP, _SP, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),
     "go_obs_misfit": (_I, [_P, _SP, _I, _I, _I, _P, _P, _F, _F, _P]),
     "go_obs_adjoint": (_I, [_P, _SP, _SP, _I, _I, _I, _P, _P, _F, _F]),
+    "go_grf_scratch_floats": (ctypes.c_size_t, [_I, _I, _F]),
+    "go_grf_perturb": (_I, [_P, _P, _P, _I, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _F, _F, _P,
+                            ctypes.c_size_t]),
+    "go_batch_grf_scratch_floats": (ctypes.c_size_t, [_P, _F]),
+    "go_batch_grf_perturb": (_I, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, _F, _F, _P, ctypes.c_size_t]),
     "go_max_dt": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _F, _P]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),

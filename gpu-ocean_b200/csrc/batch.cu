@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "dispatch.cuh"
+#include "grf.cuh"
 
 using namespace go;
 
@@ -29,6 +30,10 @@ struct go_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
+    GrfMember* d_grf = nullptr;        // model-error descriptors (built on first use)
+    int grf_R = -1;
+    size_t grf_scratch = 0;
+    int grf_max_nx = 0, grf_max_ny = 0;
 };
 
 namespace {
@@ -144,6 +149,7 @@ int go_batch_destroy(go_batch* b) {
     cudaFree(b->d_args);
     cudaFree(b->d_dt);
     cudaFree(b->d_tiles);
+    cudaFree(b->d_grf);
     delete b;
     return GO_OK;
 }
@@ -165,6 +171,7 @@ int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, f
     b->dt[m] = dt;
     b->member_set[m] = 1;
     b->dirty = true;
+    b->grf_R = -1;          // model-error descriptors hold the state pointers
     drop_graph(b);
     return GO_OK;
 }
@@ -257,6 +264,56 @@ int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done) {
     GO_CUDA(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream));
     if (steps_done) *steps_done = b->graph_steps;
     return GO_OK;
+}
+
+size_t go_batch_grf_scratch_floats(go_batch* b, float corr_cells) {
+    GrfWeights W;
+    if (!b || grf_weights(corr_cells, &W)) return 0;
+    size_t total = 0;
+    for (int m = 0; m < b->n; ++m) total += grf_member_scratch(b->members[m]->k.nx, b->members[m]->k.ny, W.R);
+    return total;
+}
+
+int go_batch_grf_perturb(go_batch* b, void* stream, uint32_t key0, uint32_t event, float std_dev,
+                         float corr_cells, float* scratch, size_t scratch_floats) {
+    if (!b || !scratch) return go_fail(GO_ERR_INVALID, "null argument");
+    int rc = batch_commit(b);
+    if (rc) return rc;
+    GrfWeights W;
+    rc = grf_weights(corr_cells, &W);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b->d_grf || b->grf_R != W.R) {
+        std::vector<GrfMember> h(b->n);
+        size_t off = 0;
+        int mx = 0, my = 0;
+        for (int m = 0; m < b->n; ++m) {
+            const Scheme& k = b->members[m]->k;
+            h[m].eta = const_cast<float*>(b->args[2 * m].eta_in);
+            h[m].pitch = b->args[2 * m].pin;
+            h[m].nx = k.nx;
+            h[m].ny = k.ny;
+            h[m].periodic_x = k.bcE == kPeriodic;
+            h[m].periodic_y = k.bcN == kPeriodic;
+            h[m].key1 = (uint32_t)m;
+            h[m].tmp_off = off;
+            off += grf_member_scratch(k.nx, k.ny, W.R);
+            mx = max(mx, k.nx);
+            my = max(my, k.ny);
+        }
+        if (!b->d_grf) GO_CUDA(cudaMalloc(&b->d_grf, sizeof(GrfMember) * b->n));
+        GO_CUDA(cudaMemcpy(b->d_grf, h.data(), sizeof(GrfMember) * b->n, cudaMemcpyHostToDevice));
+        b->grf_R = W.R;
+        b->grf_scratch = off;
+        b->grf_max_nx = mx;
+        b->grf_max_ny = my;
+    }
+    if (scratch_floats < b->grf_scratch)
+        return go_fail(GO_ERR_INVALID, "scratch holds %zu floats, the batch needs %zu", scratch_floats,
+                       b->grf_scratch);
+    GrfMember none;
+    memset(&none, 0, sizeof(none));
+    return grf_launch(b->d_grf, none, b->n, b->grf_max_nx, b->grf_max_ny, key0, event, std_dev, W, scratch, s);
 }
 
 }  // extern "C"

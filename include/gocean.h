@@ -279,6 +279,35 @@ int go_cdklm_step_static(const go_domain_desc* desc, void* stream, const float* 
                          float* eta1, float* hu1, float* hv1, int pitch1,
                          const float* Hi, int Hi_pitch, float land_value, uint32_t* status_out);
 
+/* ---------------------------------------------------------------------
+ * Model error: eta += std_dev * (Gaussian random field with correlation
+ * exp(-r^2 / (2 L^2)), L = corr_cells, unit variance), periodic in x (and
+ * in y when north/south are periodic).  Normals come from Philox4x32-10
+ * (Salmon et al., SC'11) keyed by (key0, key1) with counter (index / 4,
+ * event, 0, 0) and Box-Muller; a separable Gaussian filter correlates them.
+ * The same (keys, event) give the same field in the single and the batched
+ * form.  No counterpart in the reference (its OceanStateNoise draws model
+ * error by another method).
+ * --------------------------------------------------------------------- */
+
+/* Scratch floats go_grf_perturb needs for an nx x ny grid (0 if invalid). */
+size_t go_grf_scratch_floats(int nx, int ny, float corr_cells);
+
+/* Adds the field for (key0, key1, event) to the interior of eta (device,
+ * (ny+4) x (nx+4), pitch in bytes) and rewrites its periodic ghost images. */
+int go_grf_perturb(go_domain* d, void* stream, float* eta, int pitch, uint32_t key0,
+                   uint32_t key1, uint32_t event, float std_dev, float corr_cells,
+                   float* scratch, size_t scratch_floats);
+
+/* Scratch floats go_batch_grf_perturb needs for all members. */
+size_t go_batch_grf_scratch_floats(go_batch* b, float corr_cells);
+
+/* go_grf_perturb for every member m of the batch, keys (key0, m), on the
+ * members' current state (h0), in two launches. */
+int go_batch_grf_perturb(go_batch* b, void* stream, uint32_t key0, uint32_t event,
+                         float std_dev, float corr_cells, float* scratch,
+                         size_t scratch_floats);
+
 /* Device status word (GO_STATUS_* bits) accumulated by the step kernels;
  * synchronous read, optionally clearing it. */
 int go_domain_status(go_domain* d, uint32_t* status, int clear);
