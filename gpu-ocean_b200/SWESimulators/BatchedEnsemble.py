@@ -147,5 +147,44 @@ class BatchedCDKLM16:
         from . import ModelError
         self.perturb(ModelError.MODEL_ERROR_SEED, event, std, corr_cells)
 
+    def max_dt(self):
+        """Exact CFL limit of every member (one reduction launch per member
+        on the batch stream, one device-to-host read); numpy array of n."""
+        torch = _native.require_cuda()
+        if getattr(self, "_dt_all", None) is None or self._dt_all.numel() != self.n:
+            self._dt_all = torch.empty(self.n, dtype=torch.float32, device="cuda")
+        lib = _native.load()
+        sh = _native.stream_handle(self.stream)
+        self._sync_members()
+        for m, s in enumerate(self.sims):
+            g = s.gpu_data
+            _native.check(lib.go_max_dt(s._domain.handle, sh, _native.ptr(g.h0.tensor), _native.ptr(g.hu0.tensor),
+                                        _native.ptr(g.hv0.tensor), int(g.h0.pitch),
+                                        _native.ptr(s.bathymetry.Bm.tensor), int(s.bathymetry.Bm.pitch),
+                                        float(s.bathymetry.mask_value), _native.ptr(self._dt_all[m:m + 1])))
+        self.stream.synchronize()
+        return self._dt_all.cpu().numpy()
+
+    def update_dt(self, courant=0.7):
+        """Common dt = courant * min over members of the exact CFL limit."""
+        dt = np.float32(courant * float(np.min(self.max_dt())))
+        self.set_dt([dt] * self.n)
+        return dt
+
+    def run_events(self, first_event, n_events, interval=60.0, std=0.05, corr_cells=15.0, courant=0.7):
+        """The ensemble workload loop: for each event e, every member advances
+        `interval` seconds at the common dt (step(t_end) semantics), then
+        gets model error for event e, then the common dt is recomputed from
+        the members' CFL limits -- what the reference's ensembles do member
+        by member (OceanNoiseEnsemble.py:506-531).  Returns the steps taken."""
+        steps = 0
+        for e in range(int(first_event), int(first_event) + int(n_events)):
+            n0 = self.sims[0].num_iterations
+            self.step(interval)
+            steps += self.sims[0].num_iterations - n0
+            self.model_error(e, std, corr_cells)
+            self.update_dt(courant)
+        return steps
+
     def synchronize(self):
         self.stream.synchronize()

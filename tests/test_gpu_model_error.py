@@ -81,3 +81,38 @@ def test_perturbed_ensemble_steps(ctx):
     torch.cuda.synchronize()
     for a, c in zip(sims, alone):
         assert np.array_equal(np.stack(a.download()), np.stack(c.download()))
+
+
+def test_event_loop_batched_equals_plain_loop(ctx):
+    """run_events (batched, graph replays) == the member-by-member loop with
+    the same model error and common-dt updates."""
+    def members():
+        sims = [flat_sim(ctx, 96, 80) for _ in range(3)]
+        for m, s in enumerate(sims):
+            ModelError.initial_perturbation(s, m)
+        return sims
+    a = members()
+    b = BatchedEnsemble.BatchedCDKLM16(a, graph_steps=4)
+    b.update_dt(0.7)
+    steps = b.run_events(1, 3, interval=60.0)
+    p = members()
+    dts = []
+    for s in p:
+        s.updateDt(courant_number=1.0)
+        dts.append(s.dt)
+    dt = np.float32(0.7 * float(min(dts)))       # as update_dt: product in FP64, then rounded
+    for e in range(1, 4):
+        for m, s in enumerate(p):
+            s.dt = dt
+            s.step(60.0)
+            ModelError.model_error(s, m, e)
+        lims = []
+        for s in p:
+            s.updateDt(courant_number=1.0)
+            lims.append(s.dt)
+        dt = np.float32(0.7 * float(min(lims)))
+    torch.cuda.synchronize()
+    assert steps == p[0].num_iterations
+    for x, y in zip(a, p):
+        assert np.array_equal(np.stack(x.download()), np.stack(y.download()))
+        assert x.t == y.t
