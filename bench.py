@@ -368,6 +368,64 @@ def run_adjoint(ctx, n=512, n_steps=500, k=50):
     return out
 
 
+def run_adjoint_stages(ctx, n, reps=20):
+    """Device time of one forward RK2 step (go_traj_step) and of each
+    adjoint stage (go_adjoint_stage, fold included) on an n x n grid of the
+    headline physics after 3 steps; used for the stage-level comparison and
+    as the ncu target."""
+    import ctypes
+    import torch
+    from SWESimulators import Adjoint, CDKLM16, SyntheticCases as SC, _native
+
+    lib = _native.load()
+    c = SC.grf(n, dx=1000.0, steps=1)
+    sim = CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs())
+    for _ in range(3):
+        sim.step(c.dt)
+    torch.cuda.synchronize()
+    prob = Adjoint.MisfitProblem(sim, 1, Adjoint.Observations(np.zeros((0, 2)), [], np.zeros((0, 0, 3))))
+    prob.wind[0, :, :n].fill_(float(c.wind[0]))
+    prob.wind[1, :, :n].fill_(float(c.wind[1]))
+    slab = Adjoint.StateSlab(3, n, n)
+    g = sim.gpu_data
+    for f, a in enumerate((g.h0, g.hu0, g.hv0)):
+        slab.full(0)[f].copy_(a.view)
+    lam = Adjoint.StateSlab(3, n, n)
+    lam.interior(0).normal_(generator=torch.Generator(device="cuda").manual_seed(5))
+    lw = torch.zeros_like(prob.lam_wind)
+    torch.cuda.synchronize()
+    dt = float(np.float32(c.dt))
+    P = _native.ptr
+    prob._traj_step(slab, 0, slab, 1, slab, 2)
+
+    def fwd():
+        prob._traj_step(slab, 0, slab, 1, slab, 2)
+
+    def adj(k):
+        q_in, q_out, l_out, l_in = (1, 2, 0, 1) if k == 1 else (0, 1, 1, 0)
+        _native.check(lib.go_adjoint_stage(prob.domain.handle, prob.sh, k, dt, slab.gs(q_in), slab.gs(q_out),
+                                           lam.gs(l_out), lam.gs(l_in), lam.gs(2), P(lw[0]), P(lw[1]),
+                                           prob.wpitch, P(prob.Hi), prob.Hi_pitch))
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(prob.stream)
+        for _ in range(reps):
+            fn()
+        b.record(prob.stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps * 1e3
+
+    tf = timed(fwd)
+    t1 = timed(lambda: adj(1))
+    t0 = timed(lambda: adj(0))
+    return {"workload": "adjoint_stage", "grid": "%dx%d" % (n, n), "forward_step_us": tf, "adjoint_stage1_us": t1,
+            "adjoint_stage0_us": t0, "adjoint_step_over_forward_step": (t0 + t1) / tf, "reps": reps}
+
+
 def run_reference(args):
     import torch
     from oracle import build_ref, ref_kernel
@@ -402,7 +460,9 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512"], default="grf4096")
+    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage"],
+                    default="grf4096")
+    ap.add_argument("--grid", type=int, default=2048, help="grid size of the adjoint_stage workload")
     ap.add_argument("--rows", type=int, default=0, help="rows per block strip (0: library default)")
     ap.add_argument("--shape", type=int, default=0, help="launch shape 0..4 (include/gocean.h)")
     ap.add_argument("--arith", type=int, default=-1,
@@ -440,15 +500,29 @@ def main():
         print(json.dumps(line))
         return
 
-    if args.workload in ("ensemble100", "adjoint512"):
+    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage"):
         if rank != 0:
             return
         from SWESimulators import Common
         ctx = Common.CUDAContext(local)
         sampler = ClockSampler(local)
         sampler.start()
-        r = run_ensemble(ctx) if args.workload == "ensemble100" else run_adjoint(ctx)
+        if args.workload == "ensemble100":
+            r = run_ensemble(ctx)
+        elif args.workload == "adjoint512":
+            r = run_adjoint(ctx)
+        else:
+            r = run_adjoint_stages(ctx, args.grid, reps=args.steps if args.steps < 2000 else 20)
         clocks = sampler.stop()
+        if args.workload == "adjoint_stage":
+            cells = args.grid * args.grid
+            us = r["adjoint_stage0_us"] + r["adjoint_stage1_us"]
+            print(json.dumps({"metric": METRIC, "value": cells / (us * 1e-6) / 1e9, "unit": UNIT, "n_gpus": 1,
+                              "steps": r["reps"], "warmup": 3, "ms_per_step": us * 1e-3,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic", "config": {"workload": "adjoint_stage", "grid": r["grid"]},
+                              "result": r, "clocks": clocks}))
+            return
         if args.workload == "ensemble100":
             value, ms = r["batched_gcell_steps_s"], r["batched_ms"] / max(r["steps"], 1)
         else:
