@@ -310,12 +310,12 @@ def run_ensemble(ctx, n_members=100, n=512, target_steps=300, graph_steps=10):
                     "cells), dt = 0.7 CFL min over members; both paths from the same perturbed states"}
 
 
-def run_adjoint(ctx, n=512, n_steps=500, k=50):
+def run_adjoint(ctx, n=512, n_steps=500, k=50, kind=0, rows=0):
     """Gradient of the observation misfit (64 cells, steps 50..500, truth
     bumps seed 50001, background 50002) w.r.t. the initial state and the
     wind field, against the plain forward run of the same 500 steps."""
     import torch
-    from SWESimulators import Adjoint, CDKLM16, SyntheticCases as SC
+    from SWESimulators import Adjoint, CDKLM16, SyntheticCases as SC, _native
 
     c = SC.grf(n, dx=1000.0, seed_bumps=50002, steps=1)
     ct = SC.grf(n, dx=1000.0, seed_bumps=50001, steps=1)
@@ -337,6 +337,7 @@ def run_adjoint(ctx, n=512, n_steps=500, k=50):
     out = {"workload": "adjoint512", "grid": "%dx%d" % (n, n), "steps": n_steps, "observations": "64 cells x 10"}
     for kk, tag in ((k, "k%d" % k), (n_steps, "store_all")):
         prob = Adjoint.MisfitProblem(sim, n_steps, obs, dt=c.dt, checkpoint_every=kk)
+        _native.check(_native.load().go_domain_set_adjoint_launch(prob.domain.handle, int(kind), int(rows)))
         prob.gradient(*x0, X, Y)                      # warm-up
         best_g, best_p = None, None
         for _ in range(3):
@@ -368,7 +369,7 @@ def run_adjoint(ctx, n=512, n_steps=500, k=50):
     return out
 
 
-def run_adjoint_stages(ctx, n, reps=20):
+def run_adjoint_stages(ctx, n, reps=20, kind=0, rows=0):
     """Device time of one forward RK2 step (go_traj_step) and of each
     adjoint stage (go_adjoint_stage, fold included) on an n x n grid of the
     headline physics after 3 steps; used for the stage-level comparison and
@@ -384,6 +385,7 @@ def run_adjoint_stages(ctx, n, reps=20):
         sim.step(c.dt)
     torch.cuda.synchronize()
     prob = Adjoint.MisfitProblem(sim, 1, Adjoint.Observations(np.zeros((0, 2)), [], np.zeros((0, 0, 3))))
+    _native.check(lib.go_domain_set_adjoint_launch(prob.domain.handle, int(kind), int(rows)))
     prob.wind[0, :, :n].fill_(float(c.wind[0]))
     prob.wind[1, :, :n].fill_(float(c.wind[1]))
     slab = Adjoint.StateSlab(3, n, n)
@@ -422,7 +424,8 @@ def run_adjoint_stages(ctx, n, reps=20):
     tf = timed(fwd)
     t1 = timed(lambda: adj(1))
     t0 = timed(lambda: adj(0))
-    return {"workload": "adjoint_stage", "grid": "%dx%d" % (n, n), "forward_step_us": tf, "adjoint_stage1_us": t1,
+    return {"workload": "adjoint_stage", "grid": "%dx%d" % (n, n), "adjoint_launch": [int(kind), int(rows)],
+            "forward_step_us": tf, "adjoint_stage1_us": t1,
             "adjoint_stage0_us": t0, "adjoint_step_over_forward_step": (t0 + t1) / tf, "reps": reps}
 
 
@@ -463,6 +466,8 @@ def main():
     ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage"],
                     default="grf4096")
     ap.add_argument("--grid", type=int, default=2048, help="grid size of the adjoint_stage workload")
+    ap.add_argument("--adj-kind", type=int, default=0, help="adjoint launch form (include/gocean.h GO_ADJ_*)")
+    ap.add_argument("--adj-rows", type=int, default=0, help="rows per strip of the marching adjoint (0: automatic)")
     ap.add_argument("--rows", type=int, default=0, help="rows per block strip (0: library default)")
     ap.add_argument("--shape", type=int, default=0, help="launch shape 0..4 (include/gocean.h)")
     ap.add_argument("--arith", type=int, default=-1,
@@ -510,9 +515,10 @@ def main():
         if args.workload == "ensemble100":
             r = run_ensemble(ctx)
         elif args.workload == "adjoint512":
-            r = run_adjoint(ctx)
+            r = run_adjoint(ctx, kind=args.adj_kind, rows=args.adj_rows)
         else:
-            r = run_adjoint_stages(ctx, args.grid, reps=args.steps if args.steps < 2000 else 20)
+            r = run_adjoint_stages(ctx, args.grid, reps=args.steps if args.steps < 2000 else 20,
+                                   kind=args.adj_kind, rows=args.adj_rows)
         clocks = sampler.stop()
         if args.workload == "adjoint_stage":
             cells = args.grid * args.grid

@@ -24,6 +24,10 @@ GO_ERR_CUDA = -2
 GO_ERR_UNSUPPORTED = -3
 GO_ARITH_EXACT = 0
 GO_ARITH_RCP = 1
+GO_ADJ_AUTO = 0
+GO_ADJ_TILE = 1
+GO_ADJ_MARCH64 = 2
+GO_ADJ_MARCH128 = 3
 
 _c_float_p = ctypes.c_void_p  # device pointers travel as integers
 
@@ -73,6 +77,7 @@ SIGNATURES = {
     "go_cdklm_step_static": (_I, [ctypes.POINTER(GoDomainDesc), _P, ctypes.POINTER(ctypes.c_float), _I, _F, _F,
                                   _I, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F,
                                   ctypes.POINTER(ctypes.c_uint32)]),
+    "go_domain_set_adjoint_launch": (_I, [_P, _I, _I]),
     "go_traj_step": (_I, [_P, _P, _F, _F, _SP, _SP, _SP, _P, _I, _F]),
     "go_adjoint_stage": (_I, [_P, _P, _I, _F, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),
     "go_adjoint_step": (_I, [_P, _P, _F, _SP, _SP, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),

@@ -23,8 +23,8 @@
 // velocities, wave speeds) keeps the forward kernel's rounding: products that
 // feed a sum are written with __fmul_rn so that they are never contracted.
 //
-// Layout: one CTA per output tile of TX x TY cells of the ghost-inclusive
-// grid.  The forward state of the tile plus a 3-cell halo is recomputed in
+// Two launch forms compute the same adjoint.  Tile form: one CTA per output
+// tile of TX x TY cells of the ghost-inclusive grid.  The forward state of the tile plus a 3-cell halo is recomputed in
 // shared memory; the adjoint then flows output -> fluxes -> slopes -> cell
 // state as in the forward, each face handled once (two passes, even and odd
 // faces, so that no two threads update one cell at the same time) and each
@@ -55,6 +55,7 @@ struct AdjArgs {
     const float* Hi; int phi;
     const float* f_rows;
     unsigned int* status;
+    int rows;                              // rows per strip (marching form)
 };
 
 // Branch codes
@@ -537,6 +538,382 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
     if (scope_bad && a.status) atomicOr(a.status, GO_STATUS_ADJ_SCOPE);
 }
 
+// ---------------------------------------------------------------------------
+// Column-marching form of the same adjoint stage.
+//
+// One thread per column, BW columns per block of which the middle BW - 6 are
+// written (the x direction of the adjoint reaches 3 columns); a block walks a
+// strip of rows upward with the y direction in registers.  At output row j
+// the block loads row j+3, takes the y slopes of row j+2 and the own-cell
+// adjoint (lambda_L) of row j+2, the y face (j+1, j+2), which completes the
+// y-slope adjoint of row j+1, then the whole x direction of row j (x slopes,
+// x faces, x-slope adjoints: four shared-memory exchanges), and writes the
+// adjoint of row j.  Only 3 priming rows per strip are recomputed.
+// ---------------------------------------------------------------------------
+
+struct Cor { float a, b; };                 // corners Hi(r, i), Hi(r, i+1)
+struct PrimC { float e, u, v; };
+struct SlopeC { float u, v, K; uint32_t code; };
+struct Trip { float a, b, c; };
+
+__device__ __forceinline__ Trip trip0() { return Trip{0.0f, 0.0f, 0.0f}; }
+
+template <int BW>
+struct MarchBufs {
+    float e[BW], u[BW], v[BW];              // state of the row
+    float su[BW], sv[BW], sK[BW];           // x slopes of the row
+    uint32_t code[BW];                      // their branch codes
+    float l0[BW], l1[BW], l2[BW];           // lambda_L of the row
+    float pe[BW], pu[BW], pv[BW], pK[BW], pux[BW], pvx[BW];   // face (t, t+1) -> cell t+1
+    float gu[BW], gv[BW], gK[BW];           // x-slope adjoints after the adjustment
+};
+
+template <int BW, int FRIC, bool STAGE1>
+__global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_kernel(const AdjArgs a) {
+    __shared__ MarchBufs<BW> sb;
+    const Scheme& k = a.k;
+    const int nx = k.nx, ny = k.ny;
+    const int t = threadIdx.x;
+    const int i = (int)blockIdx.x * (BW - 6) - 3 + t;
+    const int r0 = (int)blockIdx.y * a.rows;
+    const int r1 = min(r0 + a.rows, ny + 4);
+    const bool wallN = k.bcN == kWall, wallS = k.bcS == kWall, wallE = k.bcE == kWall, wallW = k.bcW == kWall;
+    const bool col_ok = i >= 0 && i < nx + 4;
+    const bool col_int = i >= 2 && i < nx + 2;
+    const bool writer = t >= 3 && t < BW - 3 && col_ok;
+    const float inv2g = 1.0f / k.two_g;
+    // column mirror of the load and sign of hu
+    int si = i;
+    float shu = 1.0f;
+    if (wallW && i < 2) { si = 3 - i; shu = -1.0f; }
+    if (wallE && i > nx + 1) { si = 2 * nx + 3 - i; shu = -1.0f; }
+    const float vflip_kx = flip((wallW && i < 2) || (wallE && i > nx + 1));
+    const float vflip_adj = flip((wallW && i < 2) || (wallE && i > nx + 2));
+    bool scope_bad = false;
+
+    auto corners = [&](int r) -> Cor {
+        if (r < 0 || r > ny + 4 || i < 0 || i > nx + 3) return Cor{0.0f, 0.0f};
+        const float* row = a.Hi + (size_t)r * a.phi;
+        return Cor{row[i], row[i + 1]};
+    };
+    auto frow = [&](int r) -> float { return a.f_rows[min(max(r, 0), ny + 3)]; };
+    auto cell = [&](int r, const Cor& lo, const Cor& hi) -> PrimC {
+        if (r < 0 || r >= ny + 4 || !col_ok) return PrimC{0.0f, 0.0f, 0.0f};
+        int sj = r;
+        float shv = 1.0f;
+        if (wallS && r < 2) { sj = 3 - r; shv = -1.0f; }
+        if (wallN && r > ny + 1) { sj = 2 * ny + 3 - r; shv = -1.0f; }
+        const size_t q = (size_t)sj * a.pq + si;
+        const float eta = a.qe[q], hu = a.qu[q] * shu, hv = a.qv[q] * shv;
+        const float Bm = __fmul_rn(((lo.a + hi.a) + lo.b) + hi.b, 0.25f);
+        const float h = eta + Bm;
+        if (fabsf(lo.a - k.land) < kDryEps || fabsf(hi.a - k.land) < kDryEps || fabsf(lo.b - k.land) < kDryEps ||
+            fabsf(hi.b - k.land) < kDryEps || h < k.desing_eps)
+            scope_bad = true;
+        return PrimC{eta, hu / h, hv / h};
+    };
+    auto uflip_ly = [&](int r) -> float { return flip((wallS && r < 2) || (wallN && r > ny + 1)); };
+
+    // y slopes of row r (cells r-1, r, r+1 of this column); lo/hi corners of row r
+    auto yslope = [&](int r, const PrimC& pl, const PrimC& pc, const PrimC& pr, float fl, float fc, float fr,
+                      const Cor& clo, const Cor& chi) -> SlopeC {
+        SlopeC s{0.0f, 0.0f, 0.0f, 0u};
+        if (!(col_int && r >= 1 && r <= ny + 2)) return s;
+        s.u = minmod_slope(pl.u, pc.u, pr.u, k.theta);
+        s.v = minmod_slope(pl.v, pc.v, pr.v, k.theta);
+        const int bu = mm_branch((pc.u - pl.u) * k.theta, (pr.u - pl.u) * 0.5f, (pr.u - pc.u) * k.theta);
+        const int bv = mm_branch((pc.v - pl.v) * k.theta, (pr.v - pl.v) * 0.5f, (pr.v - pc.v) * k.theta);
+        const float ful = (pl.u * uflip_ly(r - 1)) * fl;
+        const float fuc = (pc.u * uflip_ly(r)) * fc;
+        const float fur = (pr.u * uflip_ly(r + 1)) * fr;
+        const float bw = k.theta_g * ((pc.e - pl.e) + __fmul_rn(k.U, fuc + ful));
+        const float ce = k.half_g * ((pr.e - pl.e) + __fmul_rn(k.U, (fur + __fmul_rn(2.0f, fuc)) + ful));
+        const float fw = k.theta_g * ((pr.e - pc.e) + __fmul_rn(k.U, fuc + fur));
+        const float Lraw = minmod_raw(bw, ce, fw);
+        const int bl = mm_branch(bw, ce, fw);
+        const float dyfu = __fmul_rn(k.dy * fc, pc.u * flip((wallS && r < 2) || (wallN && r > ny + 2)));
+        const float Hs = 0.5f * (clo.a + clo.b);
+        const float Hn = 0.5f * (chi.a + chi.b);
+        const float hs = (pc.e + Hs) - (Lraw - dyfu) / k.two_g;
+        const float hn = (pc.e + Hn) + (Lraw - dyfu) / k.two_g;
+        float L = Lraw;
+        int ba = kAdjNone;
+        if (!(hs > 0.0f)) { L = dyfu + __fmul_rn(k.two_g, pc.e + Hs); ba = kAdjA; }
+        if (!(hn > 0.0f)) { L = dyfu - __fmul_rn(k.two_g, pc.e + Hn); ba = kAdjB; }
+        s.K = L;
+        s.code = (uint32_t)bu | ((uint32_t)bv << 2) | ((uint32_t)bl << 4) | ((uint32_t)ba << 6) | (1u << 16);
+        return s;
+    };
+
+    // own-cell adjoint of row r: lambda_L and the cell's own (e, u, v) terms
+    auto own = [&](int r, const PrimC& p, const Cor& clo, const Cor& chi, float fc, Trip& own_out) -> Trip {
+        own_out = trip0();
+        if (!(col_int && r >= 2 && r < ny + 2)) return trip0();
+        const size_t lo = (size_t)r * a.pl + i, oo = (size_t)r * a.po + i;
+        float lE = a.le[lo], lU = a.lu[lo], lV = a.lv[lo];
+        const float s4 = ((clo.a + chi.a) + clo.b) + chi.b;
+        const float Hm = __fmul_rn(0.25f, s4);
+        if (a.oe[oo] + Hm <= k.cutoff) { lE = 0.0f; lU = 0.0f; lV = 0.0f; }
+        const float h = p.e + Hm;
+        const bool wet = h > k.cutoff;
+        const float hu = wet ? p.u * h : 0.0f, hv = wet ? p.v * h : 0.0f;
+        float Cf = 0.0f, sq = 0.0f, uw = 0.0f, vw = 0.0f;
+        if (FRIC == kFricQuad) {
+            uw = hu / h; vw = hv / h;
+            sq = sqrtf(uw * uw + vw * vw);
+            Cf = (a.dt * k.r * sq) / h;
+        } else if (FRIC == kFricLinear) {
+            Cf = (k.two_r * a.dt) / h;
+        }
+        const float w = STAGE1 ? 0.5f : 1.0f;
+        const float iD = 1.0f / (1.0f + w * Cf);
+        const Trip LL{w * a.dt * lE, w * a.dt * lU * iD, w * a.dt * lV * iD};
+        float lhu = w * lU * iD, lhv = w * lV * iD, leta = w * lE, lh = 0.0f;
+        const float lCf = -w * (lU * a.ou[oo] + lV * a.ov[oo]) * iD;
+        if (FRIC == kFricQuad) {
+            const float ls = lCf * a.dt * k.r / h;
+            lh -= lCf * Cf / h;
+            if (sq > 0.0f) {
+                const float luw = ls * uw / sq, lvw = ls * vw / sq;
+                lhu += luw / h; lhv += lvw / h;
+                lh -= (luw * uw + lvw * vw) / h;
+            }
+        } else if (FRIC == kFricLinear) {
+            lh -= lCf * Cf / h;
+        }
+        const bool out_cell = writer && r >= r0 && r < r1;
+        if (h >= k.cutoff) {
+            const float Hx = 0.5f * (clo.b + chi.b) - 0.5f * (clo.a + chi.a);
+            const float Hy = 0.5f * (chi.a + chi.b) - 0.5f * (clo.a + clo.b);
+            lhv += fc * LL.b;
+            lhu -= fc * LL.c;
+            leta += LL.b * k.g * Hx / k.dx + LL.c * k.g * Hy / k.dy;
+            if (out_cell && a.wx) {
+                const size_t wo = (size_t)(r - 2) * a.pw + (i - 2);
+                a.wx[wo] += LL.b;
+                a.wy[wo] += LL.c;
+            }
+        }
+        float lR1 = 0.0f, lR2 = 0.0f;
+        if (wet) {
+            lh += lhu * p.u + lhv * p.v;
+            lR1 = lhu * h;
+            lR2 = lhv * h;
+        }
+        own_out = Trip{lh + leta, lR1, lR2};
+        if (STAGE1 && out_cell) {
+            const size_t no = (size_t)r * a.pn + i;
+            a.ne[no] = w * lE;
+            a.nu[no] = w * lU * iD;
+            a.nv[no] = w * lV * iD;
+        }
+        return LL;
+    };
+
+    // ---- prologue: rows r0-3 .. r0-1 -------------------------------------
+    Cor C0 = corners(r0 - 3), C1 = corners(r0 - 2), C2 = corners(r0 - 1), C3 = corners(r0);
+    float F0 = frow(r0 - 3), F1 = frow(r0 - 2), F2 = frow(r0 - 1);
+    PrimC P0 = cell(r0 - 3, C0, C1), P1 = cell(r0 - 2, C1, C2), P2 = cell(r0 - 1, C2, C3);
+    SlopeC S1 = yslope(r0 - 2, P0, P1, P2, F0, F1, F2, C1, C2);
+    Trip A0 = trip0(), A1 = trip0(), A2 = trip0();      // lambda of (e, u, v), rows j, j+1, j+2
+    Trip B1 = trip0(), B2 = trip0();                    // y-slope adjoints (u, v, L), rows j+1, j+2
+    Trip ownx;
+    Trip LL0 = trip0();
+    Trip LL1 = own(r0 - 2, P1, C1, C2, F1, ownx);
+    A1 = ownx;
+
+#pragma unroll 1
+    for (int j = r0 - 3; j < r1; ++j) {
+        // (1) front row j+3
+        const Cor C4 = corners(j + 4);
+        const float F3 = frow(j + 3);
+        const PrimC P3 = cell(j + 3, C3, C4);
+        // (2) y slopes of row j+2
+        const SlopeC S2 = yslope(j + 2, P1, P2, P3, F1, F2, F3, C2, C3);
+        // (3) own-cell adjoint of row j+2
+        const Trip LL2 = own(j + 2, P2, C2, C3, F2, ownx);
+        A2.a += ownx.a; A2.b += ownx.b; A2.c += ownx.c;
+        // (4) y face (j+1, j+2)
+        {
+            const int jm = j + 1, jp = j + 2;
+            if (col_int && jm >= 1 && jm <= ny + 1) {
+                const float Rmu = P1.u + __fmul_rn(0.5f, S1.u), Rmv = P1.v + __fmul_rn(0.5f, S1.v);
+                const float Rpu = P2.u - __fmul_rn(0.5f, S2.u), Rpv = P2.v - __fmul_rn(0.5f, S2.v);
+                const float fm = flip(wallS && jp == 2), fp = flip(wallN && jp == ny + 2);
+                const float Hf = 0.5f * (C2.a + C2.b);
+                const float Ep = (P2.e + Hf) - (S2.K - __fmul_rn(k.dy * F2, P2.u * fp)) / k.two_g;
+                const float Em = (P1.e + Hf) + (S1.K - __fmul_rn(k.dy * F1, P1.u * fm)) / k.two_g;
+                const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
+                const float l0 = (LL2.a - LL1.a) / k.dy, l1 = (LL2.b - LL1.b) / k.dy, l2 = (LL2.c - LL1.c) / k.dy;
+                const CuGrad g = cu_vjp(hm, Rmv, Rmu, hp, Rpv, Rpu, l0, l2, l1, k);
+                if (Ep > 0.0f) {
+                    A2.a += g.hp;
+                    B2.c -= g.hp * inv2g;
+                    A2.b += g.hp * (k.dy * F2) * fp * inv2g;
+                }
+                if (Em > 0.0f) {
+                    A1.a += g.hm;
+                    B1.c += g.hm * inv2g;
+                    A1.b -= g.hm * (k.dy * F1) * fm * inv2g;
+                }
+                A2.c += g.up; B2.b -= 0.5f * g.up;
+                A2.b += g.vp; B2.a -= 0.5f * g.vp;
+                A1.c += g.um; B1.b += 0.5f * g.um;
+                A1.b += g.vm; B1.a += 0.5f * g.vm;
+            }
+        }
+        // (5) y-slope adjoint of row j+1 is complete
+        if (S1.code & (1u << 16)) {
+            const int r = j + 1;
+            float lL = B1.c;
+            const int ba = (int)((S1.code >> 6) & 3u);
+            if (ba != kAdjNone) {
+                A1.a += (ba == kAdjA ? k.two_g : -k.two_g) * lL;
+                A1.b += lL * (k.dy * F1) * flip((wallS && r < 2) || (wallN && r > ny + 2));
+                lL = 0.0f;
+            }
+            const int bu = (int)(S1.code & 3u), bv = (int)((S1.code >> 2) & 3u), bl = (int)((S1.code >> 4) & 3u);
+            // cells r-1 (A0, pos -1), r (A1, pos 0), r+1 (A2, pos +1)
+            A0.b += B1.a * slope_coef(bu, -1, k.theta) + lL * k.U * pot_coef(bl, -1, k.theta_g, k.half_g) * F0 * uflip_ly(r - 1);
+            A1.b += B1.a * slope_coef(bu, 0, k.theta) + lL * k.U * pot_coef(bl, 0, k.theta_g, k.half_g) * F1 * uflip_ly(r);
+            A2.b += B1.a * slope_coef(bu, 1, k.theta) + lL * k.U * pot_coef(bl, 1, k.theta_g, k.half_g) * F2 * uflip_ly(r + 1);
+            A0.c += B1.b * slope_coef(bv, -1, k.theta);
+            A1.c += B1.b * slope_coef(bv, 0, k.theta);
+            A2.c += B1.b * slope_coef(bv, 1, k.theta);
+            A0.a += lL * k.g * slope_coef(bl, -1, k.theta);
+            A1.a += lL * k.g * slope_coef(bl, 0, k.theta);
+            A2.a += lL * k.g * slope_coef(bl, 1, k.theta);
+        }
+        // (6) x direction of row j (uniform over the block)
+        const bool out_row = j >= r0 && j < r1;
+        if (out_row && j >= 2 && j < ny + 2) {
+            sb.e[t] = P0.e; sb.u[t] = P0.u; sb.v[t] = P0.v;
+            __syncthreads();
+            // x slopes of row j
+            SlopeC sx{0.0f, 0.0f, 0.0f, 0u};
+            if (t >= 1 && t < BW - 1 && i >= 1 && i <= nx + 2) {
+                const float ul = sb.u[t - 1], uc = P0.u, ur = sb.u[t + 1];
+                const float vl = sb.v[t - 1], vc = P0.v, vr = sb.v[t + 1];
+                const float el = sb.e[t - 1], ec = P0.e, er = sb.e[t + 1];
+                sx.u = minmod_slope(ul, uc, ur, k.theta);
+                sx.v = minmod_slope(vl, vc, vr, k.theta);
+                const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
+                const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
+                const float fvl = (vl * flip((wallW && i - 1 < 2) || (wallE && i - 1 > nx + 1))) * F0;
+                const float fvc = (vc * vflip_kx) * F0;
+                const float fvr = (vr * flip((wallW && i + 1 < 2) || (wallE && i + 1 > nx + 1))) * F0;
+                const float bw = k.theta_g * ((ec - el) - __fmul_rn(k.V, fvc + fvl));
+                const float ce = k.half_g * ((er - el) - __fmul_rn(k.V, (fvr + __fmul_rn(2.0f, fvc)) + fvl));
+                const float fw = k.theta_g * ((er - ec) - __fmul_rn(k.V, fvc + fvr));
+                const float Kraw = minmod_raw(bw, ce, fw);
+                const int bk = mm_branch(bw, ce, fw);
+                const float dxfv = __fmul_rn(k.dx * F0, vc * vflip_adj);
+                const float Hw = 0.5f * (C0.a + C1.a);
+                const float He = 0.5f * (C0.b + C1.b);
+                const float hw = (ec + Hw) - (Kraw + dxfv) / k.two_g;
+                const float he = (ec + He) + (Kraw + dxfv) / k.two_g;
+                float K = Kraw;
+                int ba = kAdjNone;
+                if (!(hw > 0.0f)) { K = -dxfv + __fmul_rn(k.two_g, ec + Hw); ba = kAdjA; }
+                if (!(he > 0.0f)) { K = -dxfv - __fmul_rn(k.two_g, ec + He); ba = kAdjB; }
+                sx.K = K;
+                sx.code = (uint32_t)bu | ((uint32_t)bv << 2) | ((uint32_t)bk << 4) | ((uint32_t)ba << 6) | (1u << 16);
+            }
+            sb.su[t] = sx.u; sb.sv[t] = sx.v; sb.sK[t] = sx.K; sb.code[t] = sx.code;
+            sb.l0[t] = LL0.a; sb.l1[t] = LL0.b; sb.l2[t] = LL0.c;
+            __syncthreads();
+            // x face (i, i+1)
+            float aK = 0.0f, aux = 0.0f, avx = 0.0f;
+            float pe = 0.0f, pu = 0.0f, pv = 0.0f, pK = 0.0f, pux = 0.0f, pvx = 0.0f;
+            if (t >= 1 && t < BW - 2 && i >= 1 && i <= nx + 1) {
+                const int ip = i + 1;
+                const float Rmu = P0.u + __fmul_rn(0.5f, sx.u), Rmv = P0.v + __fmul_rn(0.5f, sx.v);
+                const float Rpu = sb.u[t + 1] - __fmul_rn(0.5f, sb.su[t + 1]);
+                const float Rpv = sb.v[t + 1] - __fmul_rn(0.5f, sb.sv[t + 1]);
+                const float fm = flip(wallW && ip == 2), fp = flip(wallE && ip == nx + 2);
+                const float Hf = 0.5f * (C0.b + C1.b);
+                const float Ep = (sb.e[t + 1] + Hf) - (sb.sK[t + 1] + __fmul_rn(k.dx * F0, sb.v[t + 1] * fp)) / k.two_g;
+                const float Em = (P0.e + Hf) + (sx.K + __fmul_rn(k.dx * F0, P0.v * fm)) / k.two_g;
+                const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
+                const float l0 = (sb.l0[t + 1] - LL0.a) / k.dx;
+                const float l1 = (sb.l1[t + 1] - LL0.b) / k.dx;
+                const float l2 = (sb.l2[t + 1] - LL0.c) / k.dx;
+                const CuGrad g = cu_vjp(hm, Rmu, Rmv, hp, Rpu, Rpv, l0, l1, l2, k);
+                if (Ep > 0.0f) {
+                    pe = g.hp;
+                    pK = -g.hp * inv2g;
+                    pv = -g.hp * (k.dx * F0) * fp * inv2g;
+                }
+                if (Em > 0.0f) {
+                    A0.a += g.hm;
+                    aK += g.hm * inv2g;
+                    A0.c += g.hm * (k.dx * F0) * fm * inv2g;
+                }
+                pu = g.up; pux = -0.5f * g.up;
+                pv += g.vp; pvx = -0.5f * g.vp;
+                A0.b += g.um; aux += 0.5f * g.um;
+                A0.c += g.vm; avx += 0.5f * g.vm;
+            }
+            sb.pe[t] = pe; sb.pu[t] = pu; sb.pv[t] = pv; sb.pK[t] = pK; sb.pux[t] = pux; sb.pvx[t] = pvx;
+            __syncthreads();
+            if (t >= 1) {
+                A0.a += sb.pe[t - 1]; A0.b += sb.pu[t - 1]; A0.c += sb.pv[t - 1];
+                aK += sb.pK[t - 1]; aux += sb.pux[t - 1]; avx += sb.pvx[t - 1];
+            }
+            // x-slope adjoint of (j, i): adjustment
+            float lKraw = aK;
+            if (sx.code & (1u << 16)) {
+                const int ba = (int)((sx.code >> 6) & 3u);
+                if (ba != kAdjNone) {
+                    A0.a += (ba == kAdjA ? k.two_g : -k.two_g) * aK;
+                    A0.c -= aK * (k.dx * F0) * vflip_adj;
+                    lKraw = 0.0f;
+                }
+            } else {
+                lKraw = 0.0f; aux = 0.0f; avx = 0.0f;
+            }
+            sb.gu[t] = aux; sb.gv[t] = avx; sb.gK[t] = lKraw;
+            __syncthreads();
+            // gather the x-slope adjoints of cells i-1, i, i+1
+            if (t >= 1 && t < BW - 1) {
+                float lfv = 0.0f;
+                for (int o = -1; o <= 1; ++o) {
+                    const int pos = -o;
+                    const uint32_t c = sb.code[t + o];
+                    if (!(c & (1u << 16))) continue;
+                    A0.b += sb.gu[t + o] * slope_coef((int)(c & 3u), pos, k.theta);
+                    A0.c += sb.gv[t + o] * slope_coef((int)((c >> 2) & 3u), pos, k.theta);
+                    const int bk = (int)((c >> 4) & 3u);
+                    A0.a += sb.gK[t + o] * k.g * slope_coef(bk, pos, k.theta);
+                    lfv -= sb.gK[t + o] * k.V * pot_coef(bk, pos, k.theta_g, k.half_g);
+                }
+                A0.c += lfv * F0 * vflip_kx;
+            }
+        }
+        // (7) write the adjoint of row j
+        if (out_row && writer) {
+            const float h = P0.e + __fmul_rn(((C0.a + C1.a) + C0.b) + C1.b, 0.25f);
+            float lE = A0.a - (A0.b * P0.u + A0.c * P0.v) / h;
+            float lU = A0.b / h, lV = A0.c / h;
+            if (!STAGE1 && a.ne && j >= 2 && j < ny + 2 && col_int) {
+                const size_t no = (size_t)j * a.pn + i;
+                lE += a.ne[no]; lU += a.nu[no]; lV += a.nv[no];
+            }
+            const size_t io = (size_t)j * a.pi + i;
+            a.ie[io] = lE; a.iu[io] = lU; a.iv[io] = lV;
+        }
+        // (8) slide the window
+        P0 = P1; P1 = P2; P2 = P3;
+        C0 = C1; C1 = C2; C2 = C3; C3 = C4;
+        F0 = F1; F1 = F2; F2 = F3;
+        S1 = S2;
+        LL0 = LL1; LL1 = LL2;
+        A0 = A1; A1 = A2; A2 = trip0();
+        B1 = B2; B2 = trip0();
+    }
+    if (scope_bad && a.status) atomicOr(a.status, GO_STATUS_ADJ_SCOPE);
+}
+
 // Moves the adjoint held at ghost cells to the interior cells whose values
 // the ghosts carry: mirror (walls; hv flips at north/south walls, hu at
 // east/west) or wrap (periodic).  One thread per interior cell within two
@@ -602,6 +979,44 @@ cudaError_t launch_adj(const AdjArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int BW, int FRIC, bool STAGE1>
+cudaError_t launch_march(const AdjArgs& a, cudaStream_t s) {
+    const dim3 grid((a.k.nx + 4 + BW - 7) / (BW - 6), (a.k.ny + 4 + a.rows - 1) / a.rows);
+    cdklm_adjoint_march_kernel<BW, FRIC, STAGE1><<<grid, BW, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int FRIC, bool STAGE1>
+cudaError_t launch_any(const AdjArgs& a, int kind, cudaStream_t s) {
+    if (kind == GO_ADJ_TILE) return launch_adj<FRIC, STAGE1>(a, s);
+    if (kind == GO_ADJ_MARCH64) return launch_march<64, FRIC, STAGE1>(a, s);
+    return launch_march<128, FRIC, STAGE1>(a, s);
+}
+
+// Launch form and strip height for a grid.  A marching block walks its
+// strip sequentially, so below ~300 k cells (512^2) the grid has too few
+// column strips to fill 148 SMs and the tile form is faster (B200: 49.5 vs
+// 58 us per stage at 512^2; 116 vs 170 at 1024^2 the other way).  Marching
+// uses 64-thread blocks up to 1024 columns and 128 above, strips of the power
+// of two in [8, 32] nearest below (column strips x rows) / 600.
+void adjoint_launch(const go_domain* d, int* kind, int* rows) {
+    int kd = d->adj_kind;
+    const int nx = d->k.nx + 4, ny = d->k.ny + 4;
+    if (kd == GO_ADJ_AUTO) {
+        if ((long long)nx * ny < 300000LL) kd = GO_ADJ_TILE;
+        else kd = (nx <= 1024) ? GO_ADJ_MARCH64 : GO_ADJ_MARCH128;
+    }
+    int r = d->adj_rows;
+    if (r <= 0) {
+        const int bw = (kd == GO_ADJ_MARCH64) ? 64 : 128;
+        const long long target = (long long)((nx + bw - 7) / (bw - 6)) * ny / 600;
+        r = 8;
+        while (r < 32 && 2 * r <= target) r *= 2;
+    }
+    *kind = kd;
+    *rows = r;
+}
+
 cudaError_t launch_fold(const go_domain* d, const go_state* l, cudaStream_t s) {
     const int nx = d->k.nx, ny = d->k.ny;
     const int n = 4 * nx + 4 * (ny - 4 > 0 ? ny - 4 : 0);
@@ -632,14 +1047,18 @@ int adjoint_stage(go_domain* d, cudaStream_t s, int rk_step, float dt, const go_
     a.Hi = Hi; a.phi = Hi_pitch / 4;
     a.f_rows = d->d_frows;
     a.status = d->d_status;
+    int kind = GO_ADJ_AUTO;
+    adjoint_launch(d, &kind, &a.rows);
     const int fric = go_friction_mode(d);
     cudaError_t e;
     if (rk_step == 0) {
-        e = fric == kFricQuad ? launch_adj<kFricQuad, false>(a, s)
-          : fric == kFricLinear ? launch_adj<kFricLinear, false>(a, s) : launch_adj<kFricNone, false>(a, s);
+        e = fric == kFricQuad ? launch_any<kFricQuad, false>(a, kind, s)
+          : fric == kFricLinear ? launch_any<kFricLinear, false>(a, kind, s)
+                                : launch_any<kFricNone, false>(a, kind, s);
     } else {
-        e = fric == kFricQuad ? launch_adj<kFricQuad, true>(a, s)
-          : fric == kFricLinear ? launch_adj<kFricLinear, true>(a, s) : launch_adj<kFricNone, true>(a, s);
+        e = fric == kFricQuad ? launch_any<kFricQuad, true>(a, kind, s)
+          : fric == kFricLinear ? launch_any<kFricLinear, true>(a, kind, s)
+                                : launch_any<kFricNone, true>(a, kind, s);
     }
     if (e == cudaSuccess) e = launch_fold(d, lam_in, s);
     if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "adjoint stage launch failed: %s", cudaGetErrorString(e));
@@ -684,6 +1103,15 @@ __global__ void k_obs_adjoint(const float* e, const float* u, const float* v, in
 }  // namespace
 
 extern "C" {
+
+int go_domain_set_adjoint_launch(go_domain* d, int kind, int rows_per_strip) {
+    if (!d) return go_fail(GO_ERR_INVALID, "null domain");
+    if (kind < GO_ADJ_AUTO || kind > GO_ADJ_MARCH128) return go_fail(GO_ERR_INVALID, "adjoint launch kind %d", kind);
+    if (rows_per_strip < 0) return go_fail(GO_ERR_INVALID, "rows_per_strip must be >= 0");
+    d->adj_kind = kind;
+    d->adj_rows = rows_per_strip;
+    return GO_OK;
+}
 
 int go_adjoint_stage(go_domain* d, void* stream, int rk_step, float dt, const go_state* q_in,
                      const go_state* q_out, const go_state* lam_out, const go_state* lam_in,

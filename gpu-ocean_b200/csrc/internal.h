@@ -23,6 +23,8 @@ struct go_domain {
     int shape;               // launch shape, see go_shape_width()
     int arith;               // GO_ARITH_*
     int has_land;            // bathymetry may hold land cells (checks on)
+    int adj_kind;            // GO_ADJ_* launch form of the adjoint stage
+    int adj_rows;            // rows per strip of the marching adjoint (0: automatic)
 };
 
 // Records the message of a failed call (go_last_error) and returns code.

@@ -215,6 +215,18 @@ typedef struct go_state {
     int pitch;             /* bytes */
 } go_state;
 
+/* Launch form of the adjoint stage: GO_ADJ_TILE (one block per 32x16 tile,
+ * forward recomputed with a 3-cell halo), GO_ADJ_MARCH64 / GO_ADJ_MARCH128
+ * (one thread per column, blocks of 64 or 128 columns marching up strips of
+ * rows_per_strip rows, 0 = automatic), GO_ADJ_AUTO (the default: the tile
+ * form below ~300 k cells, where marching strips cannot fill the GPU, else
+ * marching, 64 up to 1024 columns).  The forms agree to FP32 rounding. */
+#define GO_ADJ_AUTO 0
+#define GO_ADJ_TILE 1
+#define GO_ADJ_MARCH64 2
+#define GO_ADJ_MARCH128 3
+int go_domain_set_adjoint_launch(go_domain* d, int kind, int rows_per_strip);
+
 /* One forward step that keeps its stages: q_star = stage 0 of q_n,
  * q_next = stage 1 (reading Q^n from q_n instead of its output buffer).
  * Bit-identical to go_cdklm_step; q_n is left unchanged. */

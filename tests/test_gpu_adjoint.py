@@ -418,3 +418,46 @@ def test_autograd_functions(ctx):
     g, gx, gy = vjp_step(model, qn[0], qs[0], [wi.double() for wi in w], X, Y, np.float32(c.dt))
     errs = [rel(leaves[f].grad, g[f]) for f in range(3)] + [rel(leaves[3].grad, gx), rel(leaves[4].grad, gy)]
     assert max(errs) < 1e-4, errs
+
+
+@pytest.mark.parametrize("nx, ny, bc", [(100, 70, (1, 2, 1, 2)), (140, 90, (2, 2, 2, 2)), (70, 130, (1, 1, 1, 1))])
+def test_adjoint_launch_forms_agree(ctx, nx, ny, bc):
+    """The tile form and the marching forms (64/128 columns, several strip
+    heights) give the same stage adjoints to FP32 rounding."""
+    c, sim = make_sim(ctx, nx, ny, bc=bc, seed=63000)
+    prob = Adjoint.MisfitProblem(sim, 1, empty_obs())
+    X, Y = wind_field(c, 10)
+    prob.wind[0, :, :nx].copy_(X)
+    prob.wind[1, :, :nx].copy_(Y)
+    slab = Adjoint.StateSlab(3, nx, ny)
+    load_state(slab, 0, sim)
+    torch.cuda.synchronize()
+    dt = float(np.float32(c.dt))
+    prob._traj_step(slab, 0, slab, 1, slab, 2)
+    prob.stream.synchronize()
+    lib = _native.load()
+    lam_out = torch.randn((3, ny, nx), device="cuda", generator=torch.Generator(device="cuda").manual_seed(14))
+    results = {}
+    forms = [(_native.GO_ADJ_TILE, 0), (_native.GO_ADJ_MARCH64, 0), (_native.GO_ADJ_MARCH64, 8),
+             (_native.GO_ADJ_MARCH128, 0), (_native.GO_ADJ_MARCH128, 16), (_native.GO_ADJ_MARCH128, 5)]
+    for kind, rows in forms:
+        assert lib.go_domain_set_adjoint_launch(prob.domain.handle, kind, rows) == 0
+        lam = Adjoint.StateSlab(4, nx, ny)
+        lam.interior(0).copy_(lam_out)
+        lw = torch.zeros_like(prob.lam_wind)
+        torch.cuda.synchronize()
+        out = []
+        for k in (1, 0):
+            q_in, q_out, l_out, l_in = (1, 2, 0, 1) if k == 1 else (0, 1, 1, 3)
+            assert lib.go_adjoint_stage(prob.domain.handle, prob.sh, k, dt, slab.gs(q_in), slab.gs(q_out),
+                                        lam.gs(l_out), lam.gs(l_in), lam.gs(2), _native.ptr(lw[0]),
+                                        _native.ptr(lw[1]), prob.wpitch, _native.ptr(prob.Hi), prob.Hi_pitch) == 0
+        prob.stream.synchronize()
+        results[(kind, rows)] = [lam.interior(1).clone(), lam.interior(2).clone(), lam.interior(3).clone(),
+                                 lw[:, :, :nx].clone()]
+    ref = results[forms[0]]
+    for key, res in results.items():
+        errs = [rel(a, b) for a, b in zip(res, ref)]
+        print((nx, ny, bc), key, ["%.1e" % e for e in errs])
+        assert max(errs) < 2e-5, (key, errs)
+    assert prob.domain.status() & _native.GO_STATUS_ADJ_SCOPE == 0
