@@ -286,6 +286,278 @@ class MisfitProblem:
         return (J,) + tuple(self.backward())
 
 
+class Revolve:
+    """Binomial checkpointing: the schedule that reverses n_steps model steps
+    with `snapshots` stored states (slot 0 holds step 0) and the fewest
+    forward steps (Griewank 1992; Griewank & Walther 2000, "Algorithm 799:
+    revolve").  The split points come from the recursion
+
+        F(c, t) = min_m  m + F(c - 1, t - m) + F(c, m),   F(c, 1) = 0,
+        F(0, t) = t (t - 1) / 2,
+
+    F(c, t) = forward steps to reverse t steps from a stored start with c free
+    slots; every reversed step also takes one forward step of its own (the
+    stage states of the adjoint), which F does not count.
+
+    `actions` lists ("advance", a, b), ("takeshot", slot, step),
+    ("restore", slot, step) and ("reverse", n): at "reverse", the current
+    state is Q^n; the step n -> n+1 is taken once more and reversed."""
+
+    _tables = {}
+
+    def __init__(self, n_steps, snapshots):
+        n, s = int(n_steps), int(snapshots)
+        if n < 1 or s < 1:
+            raise ValueError("need n_steps >= 1 and snapshots >= 1")
+        self.n = n
+        self.s = min(s, n)
+        self.F, self.split = self._table(n, self.s - 1)
+        self.actions = self._schedule()
+
+    @classmethod
+    def _table(cls, t_max, c_max):
+        key = (t_max, c_max)
+        if key not in cls._tables:
+            t = np.arange(t_max + 1, dtype=np.int64)
+            F = np.zeros((c_max + 1, t_max + 1), dtype=np.int64)
+            split = np.ones((c_max + 1, t_max + 1), dtype=np.int64)
+            F[0] = t * (t - 1) // 2
+            for c in range(1, c_max + 1):
+                lim = min(c + 1, t_max)
+                F[c, :lim + 1] = np.maximum(t[:lim + 1] - 1, 0)      # enough slots: one step at a time
+                for tt in range(lim + 1, t_max + 1):
+                    m = np.arange(1, tt)
+                    cost = m + F[c - 1, tt - m] + F[c, 1:tt]
+                    k = int(np.argmin(cost))
+                    F[c, tt] = cost[k]
+                    split[c, tt] = m[k]
+            cls._tables[key] = (F, split)
+        return cls._tables[key]
+
+    def forward_steps(self):
+        """Forward steps of the schedule: advances plus one per reversed step."""
+        return int(self.F[self.s - 1, self.n]) + self.n
+
+    def _schedule(self):
+        acts = [("takeshot", 0, 0)]
+        cur = 0
+        stack = [(0, self.n, 0, tuple(range(1, self.s)))]
+        while stack:
+            a, b, slot_a, free = stack.pop()
+            if b - a == 1 or not free:
+                for n in range(b - 1, a - 1, -1):
+                    if cur != a:
+                        acts.append(("restore", slot_a, a))
+                        cur = a
+                    if n > a:
+                        acts.append(("advance", a, n))
+                    acts.append(("reverse", n))
+                    cur = n + 1
+                continue
+            m = a + int(self.split[len(free), b - a])
+            if cur != a:
+                acts.append(("restore", slot_a, a))
+                cur = a
+            acts.append(("advance", a, m))
+            acts.append(("takeshot", free[0], m))
+            cur = m
+            stack.append((a, m, slot_a, free))          # after the right part, with the slot freed
+            stack.append((m, b, free[0], free[1:]))
+        return acts
+
+
+class MemberSlab:
+    """M members' states in one (M, 3, ny+4, P) float32 tensor, so that a
+    whole ensemble state is copied in one call."""
+
+    def __init__(self, M, nx, ny, tensor=None):
+        torch = _native.require_cuda()
+        self.M, self.nx, self.ny = int(M), int(nx), int(ny)
+        self.P = _round_up(self.nx + 4, 32)
+        self.t = tensor if tensor is not None else torch.zeros((self.M, 3, self.ny + 4, self.P),
+                                                               dtype=torch.float32, device="cuda")
+        self._gs = []
+        for m in range(self.M):
+            g = _native.GoState()
+            g.eta = int(self.t[m, 0].data_ptr())
+            g.hu = int(self.t[m, 1].data_ptr())
+            g.hv = int(self.t[m, 2].data_ptr())
+            g.pitch = self.P * 4
+            self._gs.append(g)
+
+    def gs(self, m):
+        return ctypes.byref(self._gs[m])
+
+    def interior(self):
+        return self.t[:, :, 2:self.ny + 2, 2:self.nx + 2]
+
+
+class BatchedMisfitProblem:
+    """The misfit problem for an ensemble: M members of one grid size, each
+    with its own initial state and wind field and the same observations;
+    J_m and its gradient for every member.  The forward steps all members in
+    one launch per RK stage (go_batch_*), the reverse sweep runs the batched
+    adjoint (go_adjoint_batch_step), and memory is held by binomial
+    checkpointing (Revolve) over whole-ensemble snapshots."""
+
+    def __init__(self, sims, n_steps, obs, dt=None, snapshots=None, memory_fraction=0.8):
+        torch = _native.require_cuda()
+        lib = _native.load()
+        self.sims = list(sims)
+        self.M = len(self.sims)
+        s0 = self.sims[0]
+        self.nx, self.ny = int(s0.nx), int(s0.ny)
+        for s in self.sims:
+            if (int(s.nx), int(s.ny)) != (self.nx, self.ny):
+                raise ValueError("batched misfit members must share the grid size")
+            d = s._domain.desc
+            if abs(float(d.north_x)) > 0.0 or float(d.north_y) != 1.0:
+                raise NotImplementedError("the adjoint is built for north-up grids only")
+        self.n_steps = int(n_steps)
+        self.dt = np.float32(s0.dt if dt is None else dt)
+        self.obs = obs
+        ij = obs.ij_host
+        if ij.size and (ij[:, 0].min() < 0 or ij[:, 0].max() >= self.nx or ij[:, 1].min() < 0
+                        or ij[:, 1].max() >= self.ny):
+            raise ValueError("observation cells must be interior cells")
+        self.stream = torch.cuda.Stream()
+        self.sh = _native.stream_handle(self.stream)
+        M, nx, ny = self.M, self.nx, self.ny
+        Pw = _round_up(nx, 32)
+        self.wind = torch.zeros((M, 2, ny, Pw), dtype=torch.float32, device="cuda")
+        self.lam_wind = torch.zeros((M, 2, ny, Pw), dtype=torch.float32, device="cuda")
+        self.wpitch = Pw * 4
+        self.h0 = MemberSlab(M, nx, ny)          # current state Q^n (stage 1 in place)
+        self.h1 = MemberSlab(M, nx, ny)          # Q*
+        self.qn = MemberSlab(M, nx, ny)          # Q^n kept for the adjoint
+        self.lam = MemberSlab(M, nx, ny)
+        self.scr_star = MemberSlab(M, nx, ny)
+        self.scr_qn = MemberSlab(M, nx, ny)
+        self.J_dev = torch.zeros(M, dtype=torch.float64, device="cuda")
+        self.domains = []
+        for m, s in enumerate(self.sims):
+            d = s._domain.desc
+            dom = _native.Domain(nx, ny, d.dx, d.dy, d.g, d.r, theta=d.theta, desing_eps=d.desing_eps,
+                                 flux_slope_eps=d.flux_slope_eps, depth_cutoff=d.depth_cutoff,
+                                 bc=(d.bc_north, d.bc_east, d.bc_south, d.bc_west), friction_law=d.friction_law,
+                                 north=(d.north_x, d.north_y))
+            dom.set_coriolis(s.coriolis_rows)
+            dom.set_land(False)
+            dom.set_wind_field(self.wind[m, 0], self.wind[m, 0], self.wind[m, 1], self.wind[m, 1])
+            self.domains.append(dom)
+        self.batch = _native.Batch(self.domains)
+        for m, s in enumerate(self.sims):
+            self.batch.set_member(m, self.dt, tuple(self.h0.t[m, f] for f in range(3)),
+                                  tuple(self.h1.t[m, f] for f in range(3)), s.bathymetry.Bi.tensor,
+                                  float(s.bathymetry.mask_value), 0.0)
+        h = ctypes.c_void_p()
+        arr = (ctypes.c_void_p * M)(*[dom.handle.value for dom in self.domains])
+        _native.check(lib.go_adjoint_batch_create(arr, M, ctypes.byref(h)))
+        self.adj = h
+        for m, s in enumerate(self.sims):
+            _native.check(lib.go_adjoint_batch_set_member(
+                self.adj, m, float(self.dt), self.qn.gs(m), self.h1.gs(m), self.h0.gs(m), self.lam.gs(m),
+                self.scr_star.gs(m), self.scr_qn.gs(m), _native.ptr(self.lam_wind[m, 0]),
+                _native.ptr(self.lam_wind[m, 1]), self.wpitch, _native.ptr(s.bathymetry.Bi.tensor),
+                int(s.bathymetry.Bi.pitch)))
+        snap_bytes = self.h0.t.numel() * 4
+        if snapshots is None:
+            free = torch.cuda.mem_get_info()[0]
+            snapshots = max(1, int(free * float(memory_fraction) // snap_bytes))
+        self.revolve = Revolve(self.n_steps, min(int(snapshots), self.n_steps))
+        self.snap = torch.empty((self.revolve.s,) + tuple(self.h0.t.shape), dtype=torch.float32, device="cuda")
+        self.snapshot_bytes = snap_bytes
+
+    def close(self):
+        if getattr(self, "adj", None) is not None and self.adj.value:
+            _native.load().go_adjoint_batch_destroy(self.adj)
+            self.adj = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _misfit(self, step):
+        if step not in self.obs.index:
+            return
+        o, lib = self.obs, _native.load()
+        k = o.index[step]
+        for m in range(self.M):
+            _native.check(lib.go_obs_misfit(self.sh, self.h0.gs(m), self.nx, self.ny, o.n, _native.ptr(o.ij),
+                                            _native.ptr(o.values[k]), o.w_eta, o.w_vel,
+                                            _native.ptr(self.J_dev[m:m + 1])))
+
+    def _obs_adjoint(self, step):
+        if step not in self.obs.index:
+            return
+        o, lib = self.obs, _native.load()
+        k = o.index[step]
+        for m in range(self.M):
+            _native.check(lib.go_obs_adjoint(self.sh, self.h0.gs(m), self.lam.gs(m), self.nx, self.ny, o.n,
+                                             _native.ptr(o.ij), _native.ptr(o.values[k]), o.w_eta, o.w_vel))
+
+    def _advance(self, a, b):
+        """h0: Q^a -> Q^b; the misfit of states reached for the first time."""
+        cur = a
+        if b > self._reached:
+            events = sorted({x for x in self.obs.steps if max(a, self._reached) < x <= b})
+            for e in events:
+                if e > cur:
+                    self.batch.step(e - cur, self.stream)
+                    cur = e
+                self._misfit(e)
+            self._reached = b
+        if b > cur:
+            self.batch.step(b - cur, self.stream)
+
+    def gradient(self, x0, wind):
+        """x0: (M, 3, ny, nx) initial interior states; wind: (M, 2, ny, nx)
+        wind stress.  Returns (J per member (numpy), dJ/dx0 (M, 3, ny, nx),
+        dJ/dwind (M, 2, ny, nx))."""
+        torch = _native.require_cuda()
+        lib = _native.load()
+        self.stream.wait_stream(torch.cuda.current_stream())
+        nx, ny = self.nx, self.ny
+        with torch.cuda.stream(self.stream):
+            self.h0.t.zero_()
+            self.h0.interior().copy_(torch.as_tensor(x0, dtype=torch.float32, device="cuda"))
+            self.wind[:, :, :, :nx].copy_(torch.as_tensor(wind, dtype=torch.float32, device="cuda"))
+            for m, dom in enumerate(self.domains):
+                g = self.h0._gs[m]
+                _native.check(lib.go_boundary_condition(dom.handle, self.sh, ctypes.c_void_p(g.eta),
+                                                        ctypes.c_void_p(g.hu), ctypes.c_void_p(g.hv), g.pitch))
+            self.lam.t.zero_()
+            self.lam_wind.zero_()
+            self.J_dev.zero_()
+            self._reached = 0
+            self._misfit(0)
+            for act in self.revolve.actions:
+                kind = act[0]
+                if kind == "takeshot":
+                    self.snap[act[1]].copy_(self.h0.t)
+                elif kind == "restore":
+                    self.h0.t.copy_(self.snap[act[1]])
+                elif kind == "advance":
+                    self._advance(act[1], act[2])
+                else:
+                    n = act[1]
+                    self.qn.t.copy_(self.h0.t)
+                    self._advance(n, n + 1)
+                    self._obs_adjoint(n + 1)
+                    _native.check(lib.go_adjoint_batch_step(self.adj, self.sh))
+            if 0 in self.obs.index:
+                self.h0.t.copy_(self.snap[0])
+                self._obs_adjoint(0)
+        self.stream.synchronize()
+        for dom in self.domains:
+            if dom.status() & _native.GO_STATUS_ADJ_SCOPE:
+                raise NotImplementedError("the adjoint met land or a cell shallower than desing_eps")
+        return (self.J_dev.cpu().numpy(), self.lam.interior().clone(),
+                self.lam_wind[:, :, :, :nx].clone())
+
+
 def _autograd():
     torch = _native.require_cuda()
 

@@ -78,6 +78,11 @@ SIGNATURES = {
                                   _I, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F,
                                   ctypes.POINTER(ctypes.c_uint32)]),
     "go_domain_set_adjoint_launch": (_I, [_P, _I, _I]),
+    "go_adjoint_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),
+    "go_adjoint_batch_destroy": (_I, [_P]),
+    "go_adjoint_batch_set_launch": (_I, [_P, _I, _I]),
+    "go_adjoint_batch_set_member": (_I, [_P, _I, _F, _SP, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),
+    "go_adjoint_batch_step": (_I, [_P, _P]),
     "go_traj_step": (_I, [_P, _P, _F, _F, _SP, _SP, _SP, _P, _I, _F]),
     "go_adjoint_stage": (_I, [_P, _P, _I, _F, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),
     "go_adjoint_step": (_I, [_P, _P, _F, _SP, _SP, _SP, _SP, _SP, _SP, _SP, _P, _P, _I, _P, _I]),

@@ -31,6 +31,8 @@
 // slope gathered by its three cells.  The adjoint of ghost cells is written
 // to the ghost positions and moved to the interior cells they mirror or wrap
 // (k_adj_fold) afterwards.
+#include <vector>
+
 #include "internal.h"
 
 using namespace go;
@@ -569,13 +571,13 @@ struct MarchBufs {
 };
 
 template <int BW, int FRIC, bool STAGE1>
-__global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_kernel(const AdjArgs a) {
-    __shared__ MarchBufs<BW> sb;
+__device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int bx, const int by,
+                                                    MarchBufs<BW>& sb) {
     const Scheme& k = a.k;
     const int nx = k.nx, ny = k.ny;
     const int t = threadIdx.x;
-    const int i = (int)blockIdx.x * (BW - 6) - 3 + t;
-    const int r0 = (int)blockIdx.y * a.rows;
+    const int i = bx * (BW - 6) - 3 + t;
+    const int r0 = by * a.rows;
     const int r1 = min(r0 + a.rows, ny + 4);
     const bool wallN = k.bcN == kWall, wallS = k.bcS == kWall, wallE = k.bcE == kWall, wallW = k.bcW == kWall;
     const bool col_ok = i >= 0 && i < nx + 4;
@@ -914,14 +916,47 @@ __global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_kernel(const
     if (scope_bad && a.status) atomicOr(a.status, GO_STATUS_ADJ_SCOPE);
 }
 
+template <int BW, int FRIC, bool STAGE1>
+__global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_kernel(const AdjArgs a) {
+    __shared__ MarchBufs<BW> sb;
+    adjoint_march_strip<BW, FRIC, STAGE1>(a, blockIdx.x, blockIdx.y, sb);
+}
+
+// Batched form: one block per (member, column block, row strip) tile; the
+// member's arguments (2 per member: stage 0 and stage 1) in device memory.
+template <int BW, int FRIC, bool STAGE1>
+__global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_batch_kernel(
+        const AdjArgs* __restrict__ args, const int4* __restrict__ tiles) {
+    __shared__ MarchBufs<BW> sb;
+    const int4 tile = tiles[blockIdx.x];
+    adjoint_march_strip<BW, FRIC, STAGE1>(args[2 * tile.x + (STAGE1 ? 1 : 0)], tile.y, tile.z, sb);
+}
+
 // Moves the adjoint held at ghost cells to the interior cells whose values
 // the ghosts carry: mirror (walls; hv flips at north/south walls, hu at
 // east/west) or wrap (periodic).  One thread per interior cell within two
 // cells of a side; corner ghosts are never read by the stage and carry none.
+struct FoldMember {
+    float *e, *u, *v;
+    int p, nx, ny, bcN, bcE, bcS, bcW;
+};
+
+__device__ __forceinline__ void adj_fold_cell(float* e, float* u, float* v, int p, int nx, int ny, int bcN,
+                                              int bcE, int bcS, int bcW, int t);
+
 __global__ void k_adj_fold(float* e, float* u, float* v, int p, int nx, int ny, int bcN, int bcE, int bcS,
                            int bcW) {
+    adj_fold_cell(e, u, v, p, nx, ny, bcN, bcE, bcS, bcW, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void k_adj_fold_batch(const FoldMember* __restrict__ members) {
+    const FoldMember M = members[blockIdx.y];
+    adj_fold_cell(M.e, M.u, M.v, M.p, M.nx, M.ny, M.bcN, M.bcE, M.bcS, M.bcW, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__device__ __forceinline__ void adj_fold_cell(float* e, float* u, float* v, int p, int nx, int ny, int bcN,
+                                              int bcE, int bcS, int bcW, int t) {
     const int nrow = 4 * nx, ncol = 4 * (ny - 4 > 0 ? ny - 4 : 0);
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nrow + ncol) return;
     int j, i;
     if (t < nrow) {
@@ -1102,7 +1137,199 @@ __global__ void k_obs_adjoint(const float* e, const float* u, const float* v, in
 
 }  // namespace
 
+struct go_adjoint_batch {
+    int n = 0;
+    std::vector<go_domain*> members;
+    std::vector<AdjArgs> args;          // 2 per member: stage 0, stage 1
+    std::vector<FoldMember> folds;      // n folds of scratch_star, then n of lam
+    std::vector<char> member_set;
+    AdjArgs* d_args = nullptr;
+    FoldMember* d_folds = nullptr;
+    int4* d_tiles = nullptr;
+    int ntiles = 0;
+    int bw = 128, rows = 32;
+    int fric = 0;
+    int max_fold = 0;
+    bool dirty = true;
+};
+
+namespace {
+
+template <int BW, int FRIC, bool STAGE1>
+cudaError_t launch_march_batch(const go_adjoint_batch* b, cudaStream_t s) {
+    cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1><<<b->ntiles, BW, 0, s>>>(b->d_args, b->d_tiles);
+    return cudaGetLastError();
+}
+
+template <bool STAGE1>
+cudaError_t batch_stage(const go_adjoint_batch* b, cudaStream_t s) {
+    if (b->bw == 64)
+        return b->fric == kFricQuad ? launch_march_batch<64, kFricQuad, STAGE1>(b, s)
+             : b->fric == kFricLinear ? launch_march_batch<64, kFricLinear, STAGE1>(b, s)
+                                      : launch_march_batch<64, kFricNone, STAGE1>(b, s);
+    return b->fric == kFricQuad ? launch_march_batch<128, kFricQuad, STAGE1>(b, s)
+         : b->fric == kFricLinear ? launch_march_batch<128, kFricLinear, STAGE1>(b, s)
+                                  : launch_march_batch<128, kFricNone, STAGE1>(b, s);
+}
+
+int adjoint_batch_commit(go_adjoint_batch* b) {
+    if (!b->dirty) return GO_OK;
+    for (int m = 0; m < b->n; ++m)
+        if (!b->member_set[m]) return go_fail(GO_ERR_INVALID, "adjoint batch member %d has no buffers set", m);
+    std::vector<int4> tiles;
+    b->max_fold = 0;
+    for (int m = 0; m < b->n; ++m) {
+        const Scheme& k = b->members[m]->k;
+        const int gx = (k.nx + 4 + b->bw - 7) / (b->bw - 6);
+        const int gy = (k.ny + 4 + b->rows - 1) / b->rows;
+        for (int y = 0; y < gy; ++y)
+            for (int x = 0; x < gx; ++x) tiles.push_back(make_int4(m, x, y, 0));
+        b->args[2 * m].rows = b->rows;
+        b->args[2 * m + 1].rows = b->rows;
+        b->max_fold = max(b->max_fold, 4 * k.nx + 4 * max(k.ny - 4, 0));
+    }
+    if (b->d_tiles && (int)tiles.size() > b->ntiles) {
+        cudaFree(b->d_tiles);
+        b->d_tiles = nullptr;
+    }
+    if (!b->d_tiles) GO_CUDA(cudaMalloc(&b->d_tiles, sizeof(int4) * tiles.size()));
+    b->ntiles = (int)tiles.size();
+    GO_CUDA(cudaMemcpy(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice));
+    GO_CUDA(cudaMemcpy(b->d_args, b->args.data(), sizeof(AdjArgs) * b->args.size(), cudaMemcpyHostToDevice));
+    GO_CUDA(cudaMemcpy(b->d_folds, b->folds.data(), sizeof(FoldMember) * b->folds.size(), cudaMemcpyHostToDevice));
+    b->dirty = false;
+    return GO_OK;
+}
+
+FoldMember fold_of(const go_domain* d, const go_state* st) {
+    FoldMember f;
+    f.e = st->eta; f.u = st->hu; f.v = st->hv;
+    f.p = st->pitch / 4;
+    f.nx = d->k.nx; f.ny = d->k.ny;
+    f.bcN = d->k.bcN; f.bcE = d->k.bcE; f.bcS = d->k.bcS; f.bcW = d->k.bcW;
+    return f;
+}
+
+}  // namespace
+
 extern "C" {
+
+int go_adjoint_batch_create(go_domain* const* members, int n, go_adjoint_batch** out) {
+    if (!members || !out || n < 1) return go_fail(GO_ERR_INVALID, "bad arguments");
+    *out = nullptr;
+    go_adjoint_batch* b = new go_adjoint_batch();
+    b->n = n;
+    b->members.assign(members, members + n);
+    for (int m = 0; m < n; ++m) {
+        if (!members[m]) { delete b; return go_fail(GO_ERR_INVALID, "member %d is null", m); }
+        int rc = check_adjoint_domain(members[m]);
+        if (rc) { delete b; return rc; }
+        if (go_friction_mode(members[m]) != go_friction_mode(members[0])) {
+            delete b;
+            return go_fail(GO_ERR_INVALID, "adjoint batch members must share the friction law");
+        }
+    }
+    b->fric = go_friction_mode(members[0]);
+    b->args.assign(2 * n, AdjArgs());
+    b->folds.assign(2 * n, FoldMember());
+    b->member_set.assign(n, 0);
+    cudaError_t e = cudaMalloc(&b->d_args, sizeof(AdjArgs) * 2 * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_folds, sizeof(FoldMember) * 2 * n);
+    if (e != cudaSuccess) {
+        cudaFree(b->d_args);
+        cudaFree(b->d_folds);
+        delete b;
+        return go_fail(GO_ERR_CUDA, "adjoint batch allocation failed: %s", cudaGetErrorString(e));
+    }
+    *out = b;
+    return GO_OK;
+}
+
+int go_adjoint_batch_destroy(go_adjoint_batch* b) {
+    if (!b) return GO_OK;
+    cudaFree(b->d_args);
+    cudaFree(b->d_folds);
+    cudaFree(b->d_tiles);
+    delete b;
+    return GO_OK;
+}
+
+int go_adjoint_batch_set_launch(go_adjoint_batch* b, int block_columns, int rows_per_strip) {
+    if (!b) return go_fail(GO_ERR_INVALID, "null batch");
+    if (block_columns != 64 && block_columns != 128)
+        return go_fail(GO_ERR_INVALID, "block_columns must be 64 or 128 (got %d)", block_columns);
+    if (rows_per_strip < 0) return go_fail(GO_ERR_INVALID, "rows_per_strip must be >= 0");
+    b->bw = block_columns;
+    b->rows = rows_per_strip ? rows_per_strip : 32;
+    b->dirty = true;
+    return GO_OK;
+}
+
+int go_adjoint_batch_set_member(go_adjoint_batch* b, int m, float dt, const go_state* q_n, const go_state* q_star,
+                                const go_state* q_next, const go_state* lam, const go_state* scratch_star,
+                                const go_state* scratch_qn, float* lam_wx, float* lam_wy, int wind_pitch,
+                                const float* Hi, int Hi_pitch) {
+    if (!b || m < 0 || m >= b->n) return go_fail(GO_ERR_INVALID, "bad batch or member index %d", m);
+    go_domain* d = b->members[m];
+    const int w = d->k.nx + 4;
+    int rc = check_state(q_n, w, "q_n");
+    if (!rc) rc = check_state(q_star, w, "q_star");
+    if (!rc) rc = check_state(q_next, w, "q_next");
+    if (!rc) rc = check_state(lam, w, "lam");
+    if (!rc) rc = check_state(scratch_star, w, "scratch_star");
+    if (!rc) rc = check_state(scratch_qn, w, "scratch_qn");
+    if (!rc) rc = go_check_pitch(Hi_pitch, d->k.nx + 5, "Hi");
+    if (!rc && !Hi) rc = go_fail(GO_ERR_INVALID, "null Hi");
+    if (!rc && (lam_wx || lam_wy)) {
+        if (!lam_wx || !lam_wy) return go_fail(GO_ERR_INVALID, "wind adjoint needs both components");
+        rc = go_check_pitch(wind_pitch, d->k.nx, "wind");
+    }
+    if (rc) return rc;
+    if (scratch_star->eta == lam->eta || scratch_qn->eta == lam->eta || scratch_qn->eta == scratch_star->eta)
+        return go_fail(GO_ERR_INVALID, "scratch buffers must not alias the adjoint state");
+    auto fill = [&](AdjArgs& a, const go_state* qi, const go_state* qo, const go_state* lo, const go_state* li) {
+        memset(&a, 0, sizeof(a));
+        a.k = d->k;
+        a.dt = dt;
+        a.qe = qi->eta; a.qu = qi->hu; a.qv = qi->hv; a.pq = qi->pitch / 4;
+        a.oe = qo->eta; a.ou = qo->hu; a.ov = qo->hv; a.po = qo->pitch / 4;
+        a.le = lo->eta; a.lu = lo->hu; a.lv = lo->hv; a.pl = lo->pitch / 4;
+        a.ie = li->eta; a.iu = li->hu; a.iv = li->hv; a.pi = li->pitch / 4;
+        a.ne = scratch_qn->eta; a.nu = scratch_qn->hu; a.nv = scratch_qn->hv; a.pn = scratch_qn->pitch / 4;
+        a.wx = lam_wx; a.wy = lam_wy; a.pw = wind_pitch / 4;
+        a.Hi = Hi; a.phi = Hi_pitch / 4;
+        a.f_rows = d->d_frows;
+        a.status = d->d_status;
+        a.rows = b->rows;
+    };
+    fill(b->args[2 * m], q_n, q_star, scratch_star, lam);           // stage 0: lam^n = S0^T lam* + lam_qn
+    fill(b->args[2 * m + 1], q_star, q_next, lam, scratch_star);    // stage 1: lam* and lam_qn from lam^{n+1}
+    b->folds[m] = fold_of(d, scratch_star);
+    b->folds[b->n + m] = fold_of(d, lam);
+    b->member_set[m] = 1;
+    b->dirty = true;
+    return GO_OK;
+}
+
+int go_adjoint_batch_step(go_adjoint_batch* b, void* stream) {
+    if (!b) return go_fail(GO_ERR_INVALID, "null batch");
+    int rc = adjoint_batch_commit(b);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const dim3 fg((b->max_fold + 255) / 256, b->n);
+    cudaError_t e = batch_stage<true>(b, s);
+    if (e == cudaSuccess) {
+        k_adj_fold_batch<<<fg, 256, 0, s>>>(b->d_folds);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = batch_stage<false>(b, s);
+    if (e == cudaSuccess) {
+        k_adj_fold_batch<<<fg, 256, 0, s>>>(b->d_folds + b->n);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "adjoint batch launch failed: %s", cudaGetErrorString(e));
+    return GO_OK;
+}
 
 int go_domain_set_adjoint_launch(go_domain* d, int kind, int rows_per_strip) {
     if (!d) return go_fail(GO_ERR_INVALID, "null domain");

@@ -257,6 +257,23 @@ int go_adjoint_step(go_domain* d, void* stream, float dt,
                     float* lam_wx, float* lam_wy, int wind_pitch,
                     const float* Hi, int Hi_pitch);
 
+/* Batched adjoint step: every member's lam <- (dQ^{n+1}/dQ^n)^T lam in four
+ * launches (stage-1 adjoint of all members over a packed tile list, ghost
+ * fold, stage-0 adjoint, fold).  Members keep fixed buffers, so a captured
+ * CUDA graph can replay the step; they must share the friction law.
+ * set_member's buffers mean what go_adjoint_step's mean (lam in place). */
+typedef struct go_adjoint_batch go_adjoint_batch;
+int go_adjoint_batch_create(go_domain* const* members, int n, go_adjoint_batch** out);
+int go_adjoint_batch_destroy(go_adjoint_batch* b);
+/* Marching blocks of 64 or 128 columns and strips of rows (0 = 32). */
+int go_adjoint_batch_set_launch(go_adjoint_batch* b, int block_columns, int rows_per_strip);
+int go_adjoint_batch_set_member(go_adjoint_batch* b, int m, float dt,
+                                const go_state* q_n, const go_state* q_star, const go_state* q_next,
+                                const go_state* lam, const go_state* scratch_star,
+                                const go_state* scratch_qn, float* lam_wx, float* lam_wy,
+                                int wind_pitch, const float* Hi, int Hi_pitch);
+int go_adjoint_batch_step(go_adjoint_batch* b, void* stream);
+
 /* Observation misfit J += sum w_eta (eta - eta_obs)^2 + w_vel ((hu - hu_obs)^2
  * + (hv - hv_obs)^2) over n_obs interior cells of an nx x ny grid (device
  * int pairs (i, j), 0-based interior indices, pairs outside the interior

@@ -461,3 +461,45 @@ def test_adjoint_launch_forms_agree(ctx, nx, ny, bc):
         print((nx, ny, bc), key, ["%.1e" % e for e in errs])
         assert max(errs) < 2e-5, (key, errs)
     assert prob.domain.status() & _native.GO_STATUS_ADJ_SCOPE == 0
+
+
+def _ensemble_setup(ctx, M, n, n_steps, obs_every, n_obs):
+    c, sim0, prob0, obs, x0, X, Y, ij, steps = misfit_setup(ctx, n, 4000.0, n_steps, obs_every, n_obs, n_steps,
+                                                            spin=2)
+    sims = [sim0] + [make_sim(ctx, n, n, dx=4000.0, spin=2, seed=20241, seed_bumps=50010 + m)[1]
+                     for m in range(1, M)]
+    xs = torch.stack([torch.stack([torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+                                   for a in s.download(interior_domain_only=True)]) for s in sims])
+    gen = torch.Generator(device="cuda").manual_seed(21)
+    winds = torch.stack([torch.stack([X, Y])] * M) * (1.0 + 0.2 * torch.rand((M, 2, n, n), device="cuda",
+                                                                               generator=gen))
+    return c, sims, obs, xs, winds, steps
+
+
+def test_batched_adjoint_equals_member_by_member(ctx):
+    M, n, n_steps = 3, 48, 12
+    c, sims, obs, xs, winds, steps = _ensemble_setup(ctx, M, n, n_steps, 4, 10)
+    bp = Adjoint.BatchedMisfitProblem(sims, n_steps, obs, dt=c.dt, snapshots=3)
+    assert bp.revolve.s == 3
+    J, g, gw = bp.gradient(xs, winds)
+    lib = _native.load()
+    for m in range(M):
+        p = Adjoint.MisfitProblem(sims[m], n_steps, obs, dt=c.dt, checkpoint_every=5)
+        assert lib.go_domain_set_adjoint_launch(p.domain.handle, _native.GO_ADJ_MARCH128, 0) == 0
+        Jm, ge, gu, gv, gx, gy = p.gradient(xs[m, 0], xs[m, 1], xs[m, 2], winds[m, 0], winds[m, 1])
+        assert abs(J[m] - Jm) <= 1e-9 * abs(Jm)
+        for a, b in zip((g[m, 0], g[m, 1], g[m, 2], gw[m, 0], gw[m, 1]), (ge, gu, gv, gx, gy)):
+            assert torch.equal(a, b)
+
+
+def test_batched_adjoint_independent_of_snapshots(ctx):
+    M, n, n_steps = 2, 40, 16
+    c, sims, obs, xs, winds, steps = _ensemble_setup(ctx, M, n, n_steps, 4, 8)
+    res = []
+    for s in (1, 2, 5, 16):
+        bp = Adjoint.BatchedMisfitProblem(sims, n_steps, obs, dt=c.dt, snapshots=s)
+        res.append(bp.gradient(xs, winds))
+        bp.close()
+    for J, g, gw in res[1:]:
+        assert np.allclose(J, res[0][0], rtol=1e-12)
+        assert torch.equal(g, res[0][1]) and torch.equal(gw, res[0][2])
