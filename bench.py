@@ -369,6 +369,76 @@ def run_adjoint(ctx, n=512, n_steps=500, k=50, kind=0, rows=0):
     return out
 
 
+def run_adjoint_batch(ctx, M=32, n=1024, n_steps=1000, obs_every=50, memory_fraction=0.8):
+    """Batched adjoint: M members of n^2 (config-2 physics at dx = 1 km,
+    initial eta perturbed by the members' GRFs), the misfit of 64 truth
+    observations every obs_every steps for every member, gradients w.r.t.
+    each member's initial state and wind field, binomial checkpointing over
+    whole-ensemble snapshots in memory_fraction of the free HBM.  Reported
+    beside the member-by-member forward loop over the same steps."""
+    import torch
+    from SWESimulators import Adjoint, Autotune, CDKLM16, ModelError, SyntheticCases as SC
+
+    c = SC.grf(n, dx=1000.0, seed_bathy=20243, steps=1)
+    ct = SC.grf(n, dx=1000.0, seed_bathy=20243, seed_bumps=50001, steps=1)
+    sims = []
+    for m in range(M):
+        s = CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs())
+        ModelError.initial_perturbation(s, m)
+        sims.append(s)
+    truth = CDKLM16.CDKLM16(ctx, dt=c.dt, **ct.kwargs())
+    rng = np.random.default_rng(50003)
+    flat = rng.choice((n - 4) * (n - 4), size=64, replace=False)
+    ij = np.stack([2 + flat % (n - 4), 2 + flat // (n - 4)], axis=1)
+    steps = list(range(obs_every, n_steps + 1, obs_every))
+    states = {}
+    for k in range(1, n_steps + 1):
+        truth.step(c.dt)
+        if k in steps:
+            states[k] = truth.download(interior_domain_only=True)
+    obs = Adjoint.Observations(ij, steps, Adjoint.Observations.sample(states, ij))
+    torch.cuda.synchronize()
+    xs = torch.stack([torch.stack([torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+                                   for a in s.download(interior_domain_only=True)]) for s in sims])
+    winds = torch.stack([torch.full((2, n, n), float(c.wind[0]), device="cuda")] * M)
+    # member-by-member forward loop over the same steps (the reference's ensemble stepping)
+    plain = [CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs()) for _ in range(M)]
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for s in plain:
+        s.step(n_steps * np.float64(np.float32(c.dt)) - 1e-6 * float(c.dt))
+    torch.cuda.synchronize()
+    t1.record()
+    t1.synchronize()
+    plain_ms = t0.elapsed_time(t1)
+    plain_steps = plain[0].num_iterations
+    del plain
+    torch.cuda.empty_cache()
+    bp = Adjoint.BatchedMisfitProblem(sims, n_steps, obs, dt=c.dt, memory_fraction=memory_fraction)
+    tune = Autotune.tune_adjoint_batch(bp)
+    torch.cuda.synchronize()
+    t_start = time.perf_counter()
+    J, g, gw = bp.gradient(xs, winds)
+    torch.cuda.synchronize()
+    grad_ms = 1e3 * (time.perf_counter() - t_start)
+    cells = M * n * n
+    out = {"workload": "adjoint_batch", "members": M, "grid": "%dx%d" % (n, n), "steps": n_steps,
+           "observations": "64 cells x %d" % len(steps), "snapshots": bp.revolve.s,
+           "snapshot_gb": bp.snapshot_bytes / 1e9, "forward_steps_in_schedule": bp.revolve.forward_steps(),
+           "forward_adjoint_ms": grad_ms, "plain_loop_forward_ms": plain_ms, "plain_loop_steps": plain_steps,
+           "ratio_vs_plain_loop": grad_ms / plain_ms * plain_steps / n_steps,
+           "forward_adjoint_gcell_steps_s": cells * n_steps / (grad_ms * 1e-3) / 1e9,
+           "adjoint_launch": tune, "J_mean": float(np.mean(J)),
+           "note": "wall clock around BatchedMisfitProblem.gradient (host-driven schedule); plain loop by "
+                   "CUDA events around CDKLM16.step over the same number of steps, member by member"}
+    bp.close()
+    del bp, sims
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_adjoint_stages(ctx, n, reps=20, kind=0, rows=0):
     """Device time of one forward RK2 step (go_traj_step) and of each
     adjoint stage (go_adjoint_stage, fold included) on an n x n grid of the
@@ -463,7 +533,8 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage"],
+    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage",
+                                           "adjoint_batch"],
                     default="grf4096")
     ap.add_argument("--grid", type=int, default=2048, help="grid size of the adjoint_stage workload")
     ap.add_argument("--adj-kind", type=int, default=0, help="adjoint launch form (include/gocean.h GO_ADJ_*)")
@@ -505,7 +576,7 @@ def main():
         print(json.dumps(line))
         return
 
-    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage"):
+    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch"):
         if rank != 0:
             return
         from SWESimulators import Common
@@ -516,6 +587,8 @@ def main():
             r = run_ensemble(ctx)
         elif args.workload == "adjoint512":
             r = run_adjoint(ctx, kind=args.adj_kind, rows=args.adj_rows)
+        elif args.workload == "adjoint_batch":
+            r = run_adjoint_batch(ctx)
         else:
             r = run_adjoint_stages(ctx, args.grid, reps=args.steps if args.steps < 2000 else 20,
                                    kind=args.adj_kind, rows=args.adj_rows)
@@ -531,6 +604,8 @@ def main():
             return
         if args.workload == "ensemble100":
             value, ms = r["batched_gcell_steps_s"], r["batched_ms"] / max(r["steps"], 1)
+        elif args.workload == "adjoint_batch":
+            value, ms = r["forward_adjoint_gcell_steps_s"], r["forward_adjoint_ms"] / r["steps"]
         else:
             cells_steps = 512 * 512 * r["steps"]
             value, ms = cells_steps / (r["forward_adjoint_ms_k50"] * 1e-3) / 1e9, r["forward_adjoint_ms_k50"] / r["steps"]
@@ -567,7 +642,8 @@ def main():
         from SWESimulators import Common
         ctx = Common.CUDAContext(local)
         secondary = {}
-        for name, fn in (("ensemble100", run_ensemble), ("adjoint512", run_adjoint)):
+        for name, fn in (("ensemble100", run_ensemble), ("adjoint512", run_adjoint),
+                         ("adjoint_batch", run_adjoint_batch)):
             try:
                 secondary[name] = fn(ctx)
             except Exception as e:      # a secondary failure must not lose the headline line

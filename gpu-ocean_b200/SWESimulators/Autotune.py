@@ -158,3 +158,30 @@ def tune_batch(batched, candidates=None, graph_lengths=None, steps=20, use_cache
               "graph_trials": {str(k): v for k, v in gtimes.items()}}
     _store_cache(key, result)
     return result
+
+
+ADJOINT_BATCH_CANDIDATES = [(128, 32), (128, 16), (64, 32), (64, 16)]
+
+
+def tune_adjoint_batch(problem, candidates=None, steps=3):
+    """Best (block columns, rows per strip) for a BatchedMisfitProblem's
+    adjoint step, timed on its current buffers; the adjoint state is saved
+    and restored around the trials.  Applies and returns the choice."""
+    torch = _native.require_cuda()
+    lib = _native.load()
+    candidates = candidates or ADJOINT_BATCH_CANDIDATES
+    lam, lw = problem.lam.t.clone(), problem.lam_wind.clone()
+    times = {}
+    for bw, rows in candidates:
+        _native.check(lib.go_adjoint_batch_set_launch(problem.adj, int(bw), int(rows)))
+        _native.check(lib.go_adjoint_batch_step(problem.adj, problem.sh))
+        times[(bw, rows)] = _time(lambda: [_native.check(lib.go_adjoint_batch_step(problem.adj, problem.sh))
+                                           for _ in range(steps)], problem.stream) / steps
+    best = min(times, key=times.get)
+    _native.check(lib.go_adjoint_batch_set_launch(problem.adj, int(best[0]), int(best[1])))
+    torch.cuda.synchronize()
+    problem.lam.t.copy_(lam)
+    problem.lam_wind.copy_(lw)
+    return {"launch": list(best), "ms_per_adjoint_step": times[best],
+            "trials": {"%d/%d" % k: v for k, v in times.items()}}
+
