@@ -599,20 +599,46 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         return Cor{row[i], row[i + 1]};
     };
     auto frow = [&](int r) -> float { return a.f_rows[min(max(r, 0), ny + 3)]; };
-    auto cell = [&](int r, const Cor& lo, const Cor& hi) -> PrimC {
-        if (r < 0 || r >= ny + 4 || !col_ok) return PrimC{0.0f, 0.0f, 0.0f};
+    // raw (mirrored) state of row r, and its primitive form
+    auto load_q = [&](int r) -> Trip {
+        if (r < 0 || r >= ny + 4 || !col_ok) return trip0();
         int sj = r;
         float shv = 1.0f;
         if (wallS && r < 2) { sj = 3 - r; shv = -1.0f; }
         if (wallN && r > ny + 1) { sj = 2 * ny + 3 - r; shv = -1.0f; }
         const size_t q = (size_t)sj * a.pq + si;
-        const float eta = a.qe[q], hu = a.qu[q] * shu, hv = a.qv[q] * shv;
+        return Trip{a.qe[q], a.qu[q] * shu, a.qv[q] * shv};
+    };
+    auto prim = [&](int r, const Trip& q, const Cor& lo, const Cor& hi) -> PrimC {
+        if (r < 0 || r >= ny + 4 || !col_ok) return PrimC{0.0f, 0.0f, 0.0f};
         const float Bm = __fmul_rn(((lo.a + hi.a) + lo.b) + hi.b, 0.25f);
-        const float h = eta + Bm;
+        const float h = q.a + Bm;
         if (fabsf(lo.a - k.land) < kDryEps || fabsf(hi.a - k.land) < kDryEps || fabsf(lo.b - k.land) < kDryEps ||
             fabsf(hi.b - k.land) < kDryEps || h < k.desing_eps)
             scope_bad = true;
-        return PrimC{eta, hu / h, hv / h};
+        return PrimC{q.a, q.b / h, q.c / h};
+    };
+    // inputs of the own-cell adjoint of row r (output adjoint, stored stage
+    // output, and for output cells the wind adjoint accumulated so far)
+    struct OwnIn { float le, lu, lv, oe, ou, ov, wx, wy; };
+    auto load_own = [&](int r) -> OwnIn {
+        OwnIn o{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (!(col_int && r >= 2 && r < ny + 2)) return o;
+        const size_t lo = (size_t)r * a.pl + i, oo = (size_t)r * a.po + i;
+        o.le = a.le[lo]; o.lu = a.lu[lo]; o.lv = a.lv[lo];
+        o.oe = a.oe[oo]; o.ou = a.ou[oo]; o.ov = a.ov[oo];
+        if (a.wx && writer && r >= r0 && r < r1) {
+            const size_t wo = (size_t)(r - 2) * a.pw + (i - 2);
+            o.wx = a.wx[wo];
+            o.wy = a.wy[wo];
+        }
+        return o;
+    };
+    // stage 0: the adjoint of Q^n to add at row r
+    auto load_qn = [&](int r) -> Trip {
+        if (STAGE1 || !a.ne || !(writer && col_int && r >= r0 && r < r1 && r >= 2 && r < ny + 2)) return trip0();
+        const size_t no = (size_t)r * a.pn + i;
+        return Trip{a.ne[no], a.nu[no], a.nv[no]};
     };
     auto uflip_ly = [&](int r) -> float { return flip((wallS && r < 2) || (wallN && r > ny + 1)); };
 
@@ -648,14 +674,14 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     };
 
     // own-cell adjoint of row r: lambda_L and the cell's own (e, u, v) terms
-    auto own = [&](int r, const PrimC& p, const Cor& clo, const Cor& chi, float fc, Trip& own_out) -> Trip {
+    auto own = [&](int r, const PrimC& p, const Cor& clo, const Cor& chi, float fc, const OwnIn& in,
+                   Trip& own_out) -> Trip {
         own_out = trip0();
         if (!(col_int && r >= 2 && r < ny + 2)) return trip0();
-        const size_t lo = (size_t)r * a.pl + i, oo = (size_t)r * a.po + i;
-        float lE = a.le[lo], lU = a.lu[lo], lV = a.lv[lo];
+        float lE = in.le, lU = in.lu, lV = in.lv;
         const float s4 = ((clo.a + chi.a) + clo.b) + chi.b;
         const float Hm = __fmul_rn(0.25f, s4);
-        if (a.oe[oo] + Hm <= k.cutoff) { lE = 0.0f; lU = 0.0f; lV = 0.0f; }
+        if (in.oe + Hm <= k.cutoff) { lE = 0.0f; lU = 0.0f; lV = 0.0f; }
         const float h = p.e + Hm;
         const bool wet = h > k.cutoff;
         const float hu = wet ? p.u * h : 0.0f, hv = wet ? p.v * h : 0.0f;
@@ -671,7 +697,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         const float iD = 1.0f / (1.0f + w * Cf);
         const Trip LL{w * a.dt * lE, w * a.dt * lU * iD, w * a.dt * lV * iD};
         float lhu = w * lU * iD, lhv = w * lV * iD, leta = w * lE, lh = 0.0f;
-        const float lCf = -w * (lU * a.ou[oo] + lV * a.ov[oo]) * iD;
+        const float lCf = -w * (lU * in.ou + lV * in.ov) * iD;
         if (FRIC == kFricQuad) {
             const float ls = lCf * a.dt * k.r / h;
             lh -= lCf * Cf / h;
@@ -692,8 +718,8 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
             leta += LL.b * k.g * Hx / k.dx + LL.c * k.g * Hy / k.dy;
             if (out_cell && a.wx) {
                 const size_t wo = (size_t)(r - 2) * a.pw + (i - 2);
-                a.wx[wo] += LL.b;
-                a.wy[wo] += LL.c;
+                a.wx[wo] = in.wx + LL.b;
+                a.wy[wo] = in.wy + LL.c;
             }
         }
         float lR1 = 0.0f, lR2 = 0.0f;
@@ -715,25 +741,40 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     // ---- prologue: rows r0-3 .. r0-1 -------------------------------------
     Cor C0 = corners(r0 - 3), C1 = corners(r0 - 2), C2 = corners(r0 - 1), C3 = corners(r0);
     float F0 = frow(r0 - 3), F1 = frow(r0 - 2), F2 = frow(r0 - 1);
-    PrimC P0 = cell(r0 - 3, C0, C1), P1 = cell(r0 - 2, C1, C2), P2 = cell(r0 - 1, C2, C3);
+    PrimC P0 = prim(r0 - 3, load_q(r0 - 3), C0, C1), P1 = prim(r0 - 2, load_q(r0 - 2), C1, C2);
+    PrimC P2 = prim(r0 - 1, load_q(r0 - 1), C2, C3);
     SlopeC S1 = yslope(r0 - 2, P0, P1, P2, F0, F1, F2, C1, C2);
     Trip A0 = trip0(), A1 = trip0(), A2 = trip0();      // lambda of (e, u, v), rows j, j+1, j+2
     Trip B1 = trip0(), B2 = trip0();                    // y-slope adjoints (u, v, L), rows j+1, j+2
     Trip ownx;
     Trip LL0 = trip0();
-    Trip LL1 = own(r0 - 2, P1, C1, C2, F1, ownx);
+    Trip LL1 = own(r0 - 2, P1, C1, C2, F1, load_own(r0 - 2), ownx);
     A1 = ownx;
+    // loads of the first iteration, then always one iteration ahead
+    Trip nq = load_q(r0);
+    Cor nC = corners(r0 + 1);
+    float nF = frow(r0);
+    OwnIn nO = load_own(r0 - 1);
+    Trip nQN = load_qn(r0 - 3);
 
 #pragma unroll 1
     for (int j = r0 - 3; j < r1; ++j) {
-        // (1) front row j+3
-        const Cor C4 = corners(j + 4);
-        const float F3 = frow(j + 3);
-        const PrimC P3 = cell(j + 3, C3, C4);
+        // (1) front row j+3 (its loads were issued one iteration ago)
+        const Cor C4 = nC;
+        const float F3 = nF;
+        const Trip q3 = nq;
+        const OwnIn o2 = nO;
+        const Trip qn0 = nQN;
+        nq = load_q(j + 4);
+        nC = corners(j + 5);
+        nF = frow(j + 4);
+        nO = load_own(j + 3);
+        nQN = load_qn(j + 1);
+        const PrimC P3 = prim(j + 3, q3, C3, C4);
         // (2) y slopes of row j+2
         const SlopeC S2 = yslope(j + 2, P1, P2, P3, F1, F2, F3, C2, C3);
         // (3) own-cell adjoint of row j+2
-        const Trip LL2 = own(j + 2, P2, C2, C3, F2, ownx);
+        const Trip LL2 = own(j + 2, P2, C2, C3, F2, o2, ownx);
         A2.a += ownx.a; A2.b += ownx.b; A2.c += ownx.c;
         // (4) y face (j+1, j+2)
         {
@@ -897,10 +938,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
             const float h = P0.e + __fmul_rn(((C0.a + C1.a) + C0.b) + C1.b, 0.25f);
             float lE = A0.a - (A0.b * P0.u + A0.c * P0.v) / h;
             float lU = A0.b / h, lV = A0.c / h;
-            if (!STAGE1 && a.ne && j >= 2 && j < ny + 2 && col_int) {
-                const size_t no = (size_t)j * a.pn + i;
-                lE += a.ne[no]; lU += a.nu[no]; lV += a.nv[no];
-            }
+            lE += qn0.a; lU += qn0.b; lV += qn0.c;       // stage 0: the adjoint of Q^n (zero otherwise)
             const size_t io = (size_t)j * a.pi + i;
             a.ie[io] = lE; a.iu[io] = lU; a.iv[io] = lV;
         }
