@@ -570,7 +570,7 @@ struct MarchBufs {
     float gu[BW], gv[BW], gK[BW];           // x-slope adjoints after the adjustment
 };
 
-template <int BW, int FRIC, bool STAGE1>
+template <int BW, int FRIC, bool STAGE1, bool EDGE>
 __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int bx, const int by,
                                                     MarchBufs<BW>& sb) {
     const Scheme& k = a.k;
@@ -580,37 +580,39 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     const int r0 = by * a.rows;
     const int r1 = min(r0 + a.rows, ny + 4);
     const bool wallN = k.bcN == kWall, wallS = k.bcS == kWall, wallE = k.bcE == kWall, wallW = k.bcW == kWall;
-    const bool col_ok = i >= 0 && i < nx + 4;
-    const bool col_int = i >= 2 && i < nx + 2;
+    // EDGE = false: the block's columns and rows (with their halos) are all
+    // interior, so no wall, ghost or range test is needed
+    const bool col_ok = !EDGE || (i >= 0 && i < nx + 4);
+    const bool col_int = !EDGE || (i >= 2 && i < nx + 2);
     const bool writer = t >= 3 && t < BW - 3 && col_ok;
     const float inv2g = 1.0f / k.two_g;
     // column mirror of the load and sign of hu
     int si = i;
     float shu = 1.0f;
-    if (wallW && i < 2) { si = 3 - i; shu = -1.0f; }
-    if (wallE && i > nx + 1) { si = 2 * nx + 3 - i; shu = -1.0f; }
-    const float vflip_kx = flip((wallW && i < 2) || (wallE && i > nx + 1));
-    const float vflip_adj = flip((wallW && i < 2) || (wallE && i > nx + 2));
+    if (EDGE && wallW && i < 2) { si = 3 - i; shu = -1.0f; }
+    if (EDGE && wallE && i > nx + 1) { si = 2 * nx + 3 - i; shu = -1.0f; }
+    const float vflip_kx = flip(EDGE && ((wallW && i < 2) || (wallE && i > nx + 1)));
+    const float vflip_adj = flip(EDGE && ((wallW && i < 2) || (wallE && i > nx + 2)));
     bool scope_bad = false;
 
     auto corners = [&](int r) -> Cor {
-        if (r < 0 || r > ny + 4 || i < 0 || i > nx + 3) return Cor{0.0f, 0.0f};
+        if (EDGE && (r < 0 || r > ny + 4 || i < 0 || i > nx + 3)) return Cor{0.0f, 0.0f};
         const float* row = a.Hi + (size_t)r * a.phi;
         return Cor{row[i], row[i + 1]};
     };
     auto frow = [&](int r) -> float { return a.f_rows[min(max(r, 0), ny + 3)]; };
     // raw (mirrored) state of row r, and its primitive form
     auto load_q = [&](int r) -> Trip {
-        if (r < 0 || r >= ny + 4 || !col_ok) return trip0();
+        if (EDGE && (r < 0 || r >= ny + 4 || !col_ok)) return trip0();
         int sj = r;
         float shv = 1.0f;
-        if (wallS && r < 2) { sj = 3 - r; shv = -1.0f; }
-        if (wallN && r > ny + 1) { sj = 2 * ny + 3 - r; shv = -1.0f; }
+        if (EDGE && wallS && r < 2) { sj = 3 - r; shv = -1.0f; }
+        if (EDGE && wallN && r > ny + 1) { sj = 2 * ny + 3 - r; shv = -1.0f; }
         const size_t q = (size_t)sj * a.pq + si;
         return Trip{a.qe[q], a.qu[q] * shu, a.qv[q] * shv};
     };
     auto prim = [&](int r, const Trip& q, const Cor& lo, const Cor& hi) -> PrimC {
-        if (r < 0 || r >= ny + 4 || !col_ok) return PrimC{0.0f, 0.0f, 0.0f};
+        if (EDGE && (r < 0 || r >= ny + 4 || !col_ok)) return PrimC{0.0f, 0.0f, 0.0f};
         const float Bm = __fmul_rn(((lo.a + hi.a) + lo.b) + hi.b, 0.25f);
         const float h = q.a + Bm;
         if (fabsf(lo.a - k.land) < kDryEps || fabsf(hi.a - k.land) < kDryEps || fabsf(lo.b - k.land) < kDryEps ||
@@ -623,7 +625,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     struct OwnIn { float le, lu, lv, oe, ou, ov, wx, wy; };
     auto load_own = [&](int r) -> OwnIn {
         OwnIn o{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-        if (!(col_int && r >= 2 && r < ny + 2)) return o;
+        if (EDGE && !(col_int && r >= 2 && r < ny + 2)) return o;
         const size_t lo = (size_t)r * a.pl + i, oo = (size_t)r * a.po + i;
         o.le = a.le[lo]; o.lu = a.lu[lo]; o.lv = a.lv[lo];
         o.oe = a.oe[oo]; o.ou = a.ou[oo]; o.ov = a.ov[oo];
@@ -636,17 +638,18 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     };
     // stage 0: the adjoint of Q^n to add at row r
     auto load_qn = [&](int r) -> Trip {
-        if (STAGE1 || !a.ne || !(writer && col_int && r >= r0 && r < r1 && r >= 2 && r < ny + 2)) return trip0();
+        if (STAGE1 || !a.ne || !(writer && r >= r0 && r < r1)) return trip0();
+        if (EDGE && !(col_int && r >= 2 && r < ny + 2)) return trip0();
         const size_t no = (size_t)r * a.pn + i;
         return Trip{a.ne[no], a.nu[no], a.nv[no]};
     };
-    auto uflip_ly = [&](int r) -> float { return flip((wallS && r < 2) || (wallN && r > ny + 1)); };
+    auto uflip_ly = [&](int r) -> float { return flip(EDGE && ((wallS && r < 2) || (wallN && r > ny + 1))); };
 
     // y slopes of row r (cells r-1, r, r+1 of this column); lo/hi corners of row r
     auto yslope = [&](int r, const PrimC& pl, const PrimC& pc, const PrimC& pr, float fl, float fc, float fr,
                       const Cor& clo, const Cor& chi) -> SlopeC {
         SlopeC s{0.0f, 0.0f, 0.0f, 0u};
-        if (!(col_int && r >= 1 && r <= ny + 2)) return s;
+        if (EDGE && !(col_int && r >= 1 && r <= ny + 2)) return s;
         s.u = minmod_slope(pl.u, pc.u, pr.u, k.theta);
         s.v = minmod_slope(pl.v, pc.v, pr.v, k.theta);
         const int bu = mm_branch((pc.u - pl.u) * k.theta, (pr.u - pl.u) * 0.5f, (pr.u - pc.u) * k.theta);
@@ -659,7 +662,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         const float fw = k.theta_g * ((pr.e - pc.e) + __fmul_rn(k.U, fuc + fur));
         const float Lraw = minmod_raw(bw, ce, fw);
         const int bl = mm_branch(bw, ce, fw);
-        const float dyfu = __fmul_rn(k.dy * fc, pc.u * flip((wallS && r < 2) || (wallN && r > ny + 2)));
+        const float dyfu = __fmul_rn(k.dy * fc, pc.u * flip(EDGE && ((wallS && r < 2) || (wallN && r > ny + 2))));
         const float Hs = 0.5f * (clo.a + clo.b);
         const float Hn = 0.5f * (chi.a + chi.b);
         const float hs = (pc.e + Hs) - (Lraw - dyfu) / k.two_g;
@@ -677,7 +680,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     auto own = [&](int r, const PrimC& p, const Cor& clo, const Cor& chi, float fc, const OwnIn& in,
                    Trip& own_out) -> Trip {
         own_out = trip0();
-        if (!(col_int && r >= 2 && r < ny + 2)) return trip0();
+        if (EDGE && !(col_int && r >= 2 && r < ny + 2)) return trip0();
         float lE = in.le, lU = in.lu, lV = in.lv;
         const float s4 = ((clo.a + chi.a) + clo.b) + chi.b;
         const float Hm = __fmul_rn(0.25f, s4);
@@ -779,10 +782,10 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         // (4) y face (j+1, j+2)
         {
             const int jm = j + 1, jp = j + 2;
-            if (col_int && jm >= 1 && jm <= ny + 1) {
+            if (!EDGE || (col_int && jm >= 1 && jm <= ny + 1)) {
                 const float Rmu = P1.u + __fmul_rn(0.5f, S1.u), Rmv = P1.v + __fmul_rn(0.5f, S1.v);
                 const float Rpu = P2.u - __fmul_rn(0.5f, S2.u), Rpv = P2.v - __fmul_rn(0.5f, S2.v);
-                const float fm = flip(wallS && jp == 2), fp = flip(wallN && jp == ny + 2);
+                const float fm = flip(EDGE && wallS && jp == 2), fp = flip(EDGE && wallN && jp == ny + 2);
                 const float Hf = 0.5f * (C2.a + C2.b);
                 const float Ep = (P2.e + Hf) - (S2.K - __fmul_rn(k.dy * F2, P2.u * fp)) / k.two_g;
                 const float Em = (P1.e + Hf) + (S1.K - __fmul_rn(k.dy * F1, P1.u * fm)) / k.two_g;
@@ -812,7 +815,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
             const int ba = (int)((S1.code >> 6) & 3u);
             if (ba != kAdjNone) {
                 A1.a += (ba == kAdjA ? k.two_g : -k.two_g) * lL;
-                A1.b += lL * (k.dy * F1) * flip((wallS && r < 2) || (wallN && r > ny + 2));
+                A1.b += lL * (k.dy * F1) * flip(EDGE && ((wallS && r < 2) || (wallN && r > ny + 2)));
                 lL = 0.0f;
             }
             const int bu = (int)(S1.code & 3u), bv = (int)((S1.code >> 2) & 3u), bl = (int)((S1.code >> 4) & 3u);
@@ -829,12 +832,12 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         }
         // (6) x direction of row j (uniform over the block)
         const bool out_row = j >= r0 && j < r1;
-        if (out_row && j >= 2 && j < ny + 2) {
+        if (out_row && (!EDGE || (j >= 2 && j < ny + 2))) {
             sb.e[t] = P0.e; sb.u[t] = P0.u; sb.v[t] = P0.v;
             __syncthreads();
             // x slopes of row j
             SlopeC sx{0.0f, 0.0f, 0.0f, 0u};
-            if (t >= 1 && t < BW - 1 && i >= 1 && i <= nx + 2) {
+            if (t >= 1 && t < BW - 1 && (!EDGE || (i >= 1 && i <= nx + 2))) {
                 const float ul = sb.u[t - 1], uc = P0.u, ur = sb.u[t + 1];
                 const float vl = sb.v[t - 1], vc = P0.v, vr = sb.v[t + 1];
                 const float el = sb.e[t - 1], ec = P0.e, er = sb.e[t + 1];
@@ -842,9 +845,9 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
                 sx.v = minmod_slope(vl, vc, vr, k.theta);
                 const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
                 const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
-                const float fvl = (vl * flip((wallW && i - 1 < 2) || (wallE && i - 1 > nx + 1))) * F0;
+                const float fvl = (vl * flip(EDGE && ((wallW && i - 1 < 2) || (wallE && i - 1 > nx + 1)))) * F0;
                 const float fvc = (vc * vflip_kx) * F0;
-                const float fvr = (vr * flip((wallW && i + 1 < 2) || (wallE && i + 1 > nx + 1))) * F0;
+                const float fvr = (vr * flip(EDGE && ((wallW && i + 1 < 2) || (wallE && i + 1 > nx + 1)))) * F0;
                 const float bw = k.theta_g * ((ec - el) - __fmul_rn(k.V, fvc + fvl));
                 const float ce = k.half_g * ((er - el) - __fmul_rn(k.V, (fvr + __fmul_rn(2.0f, fvc)) + fvl));
                 const float fw = k.theta_g * ((er - ec) - __fmul_rn(k.V, fvc + fvr));
@@ -868,12 +871,12 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
             // x face (i, i+1)
             float aK = 0.0f, aux = 0.0f, avx = 0.0f;
             float pe = 0.0f, pu = 0.0f, pv = 0.0f, pK = 0.0f, pux = 0.0f, pvx = 0.0f;
-            if (t >= 1 && t < BW - 2 && i >= 1 && i <= nx + 1) {
+            if (t >= 1 && t < BW - 2 && (!EDGE || (i >= 1 && i <= nx + 1))) {
                 const int ip = i + 1;
                 const float Rmu = P0.u + __fmul_rn(0.5f, sx.u), Rmv = P0.v + __fmul_rn(0.5f, sx.v);
                 const float Rpu = sb.u[t + 1] - __fmul_rn(0.5f, sb.su[t + 1]);
                 const float Rpv = sb.v[t + 1] - __fmul_rn(0.5f, sb.sv[t + 1]);
-                const float fm = flip(wallW && ip == 2), fp = flip(wallE && ip == nx + 2);
+                const float fm = flip(EDGE && wallW && ip == 2), fp = flip(EDGE && wallE && ip == nx + 2);
                 const float Hf = 0.5f * (C0.b + C1.b);
                 const float Ep = (sb.e[t + 1] + Hf) - (sb.sK[t + 1] + __fmul_rn(k.dx * F0, sb.v[t + 1] * fp)) / k.two_g;
                 const float Em = (P0.e + Hf) + (sx.K + __fmul_rn(k.dx * F0, P0.v * fm)) / k.two_g;
@@ -954,10 +957,27 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     if (scope_bad && a.status) atomicOr(a.status, GO_STATUS_ADJ_SCOPE);
 }
 
+// A block needs no boundary logic when all its columns and the rows it
+// touches (3 below the strip, 4 above) are interior cells.
+template <int BW>
+__device__ __forceinline__ bool march_interior(const AdjArgs& a, int bx, int by) {
+    const int c0 = bx * (BW - 6) - 3, r0 = by * a.rows;
+    const int r1 = min(r0 + a.rows, a.k.ny + 4);
+    return c0 >= 3 && c0 + BW + 1 <= a.k.nx + 1 && r0 - 3 >= 2 && r1 + 4 <= a.k.ny + 1;
+}
+
+template <int BW, int FRIC, bool STAGE1>
+__device__ __forceinline__ void adjoint_march_block(const AdjArgs& a, int bx, int by, MarchBufs<BW>& sb) {
+    if (march_interior<BW>(a, bx, by))
+        adjoint_march_strip<BW, FRIC, STAGE1, false>(a, bx, by, sb);
+    else
+        adjoint_march_strip<BW, FRIC, STAGE1, true>(a, bx, by, sb);
+}
+
 template <int BW, int FRIC, bool STAGE1>
 __global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_kernel(const AdjArgs a) {
     __shared__ MarchBufs<BW> sb;
-    adjoint_march_strip<BW, FRIC, STAGE1>(a, blockIdx.x, blockIdx.y, sb);
+    adjoint_march_block<BW, FRIC, STAGE1>(a, blockIdx.x, blockIdx.y, sb);
 }
 
 // Batched form: one block per (member, column block, row strip) tile; the
@@ -967,7 +987,7 @@ __global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_batch_kernel
         const AdjArgs* __restrict__ args, const int4* __restrict__ tiles) {
     __shared__ MarchBufs<BW> sb;
     const int4 tile = tiles[blockIdx.x];
-    adjoint_march_strip<BW, FRIC, STAGE1>(args[2 * tile.x + (STAGE1 ? 1 : 0)], tile.y, tile.z, sb);
+    adjoint_march_block<BW, FRIC, STAGE1>(args[2 * tile.x + (STAGE1 ? 1 : 0)], tile.y, tile.z, sb);
 }
 
 // Moves the adjoint held at ghost cells to the interior cells whose values
