@@ -146,28 +146,85 @@ def make_case(name):
     return SC.grf4096() if name == "grf4096" else SC.bump256()
 
 
-def cpu_baseline(workload):
-    """FP64 NumPy restatement of the reference kernel on one host core, on a
-    bounded sample of the same physics (the reference itself has no CPU
-    path)."""
+def _oracle_rate(n, budget_s, dx=500.0, max_steps=200, seed_bumps=20242, one_stage=False):
+    """Gcell-steps/s of the FP64 NumPy restatement on one core for the
+    headline physics on an n x n grid: RK2 steps until budget_s has passed
+    (at least one), after one untimed step; one_stage times a single RK
+    stage and counts it as half a step."""
     from oracle import cdklm16_oracle as O
     from SWESimulators import SyntheticCases as SC
-    c = SC.grf(512, dx=500.0, steps=1) if workload == "grf4096" else SC.bump256()
+    c = SC.grf(n, dx=dx, steps=1, seed_bumps=seed_bumps)
     sim = O.OracleSim(c.eta0, c.hu0, c.hv0, c.Hi, c.nx, c.ny, c.dx, c.dy, c.dt, c.g, c.f, c.r,
                       coriolis_beta=c.beta, bc=c.bc, wind=c.wind)
-    sim.rk2_step(np.float32(c.dt))    # warm-up
-    n = 0
+    if one_stage:
+        t0 = time.perf_counter()
+        sim._stage(sim.h0, sim.h1, float(np.float32(c.dt)), 0)
+        el = time.perf_counter() - t0
+        return c.nx * c.ny * 0.5 / el / 1e9, 0.5, el
+    if n <= 1024:
+        sim.rk2_step(np.float32(c.dt))    # warm-up
+    steps = 0
     t0 = time.perf_counter()
     while True:
         sim.rk2_step(np.float32(c.dt))
-        n += 1
+        steps += 1
         el = time.perf_counter() - t0
-        if el > 12.0 or n >= 200:
+        if el > budget_s or steps >= max_steps:
             break
-    value = c.nx * c.ny * n / el / 1e9
-    return {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "FP64 NumPy restatement, %s physics at %dx%d, %d RK2 steps, %.1f s, 1 core, host %s (%d cores)"
-            % (workload, c.nx, c.ny, n, el, os.uname().machine, os.cpu_count() or 0)}
+    return c.nx * c.ny * steps / el / 1e9, steps, el
+
+
+def _member_proc(args):
+    n, budget, m = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    return _oracle_rate(n, budget, dx=1000.0, seed_bumps=30000 + m)
+
+
+def cpu_baseline(workload):
+    """FP64 NumPy restatement of the reference kernel (the reference itself has
+    no CPU path) on the host cores, on bounded samples of the same physics:
+    one core at 512^2 (the reported value), 256^2 and 4096^2 (one RK2 step);
+    and the ensemble form, one process per core with one 512^2 member each,
+    throughput summed."""
+    if workload != "grf4096":
+        from oracle import cdklm16_oracle as O
+        from SWESimulators import SyntheticCases as SC
+        c = SC.bump256()
+        sim = O.OracleSim(c.eta0, c.hu0, c.hv0, c.Hi, c.nx, c.ny, c.dx, c.dy, c.dt, c.g, c.f, c.r,
+                          coriolis_beta=c.beta, bc=c.bc, wind=c.wind)
+        n, t0 = 0, time.perf_counter()
+        while True:
+            sim.rk2_step(np.float32(c.dt))
+            n += 1
+            el = time.perf_counter() - t0
+            if el > 12.0 or n >= 200:
+                break
+        return {"value": c.nx * c.ny * n / el / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": "FP64 NumPy restatement, bump256, %d RK2 steps, %.1f s, 1 core" % (n, el)}
+    cores = os.cpu_count() or 1
+    v512, s512, e512 = _oracle_rate(512, 10.0)
+    v256, s256, e256 = _oracle_rate(256, 4.0)
+    v4k, s4k, e4k = _oracle_rate(4096, 0.0, one_stage=True)
+    ens = None
+    try:
+        import multiprocessing as mproc
+        with mproc.get_context("spawn").Pool(cores) as pool:
+            t0 = time.perf_counter()
+            res = pool.map(_member_proc, [(512, 6.0, m) for m in range(cores)])
+            wall = time.perf_counter() - t0
+        ens = {"value": float(sum(r[0] for r in res)), "unit": UNIT, "processes": cores,
+               "sample": "%d processes, one 512^2 member each (initial state of member m), %d-%d RK2 steps each; "
+                         "wall %.1f s" % (cores, min(r[1] for r in res), max(r[1] for r in res), wall)}
+    except Exception as e:          # a pool failure must not lose the headline line
+        ens = {"error": "%s: %s" % (type(e).__name__, e)}
+    return {"value": v512, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "FP64 NumPy restatement, grf4096 physics at 512x512, %d RK2 steps, %.1f s, 1 core, "
+                      "host %s (%d cores), OMP_NUM_THREADS=%s"
+                      % (s512, e512, os.uname().machine, cores, os.environ.get("OMP_NUM_THREADS", "unset")),
+            "by_grid_1core": {"256x256": v256, "512x512": v512, "4096x4096": v4k,
+                              "samples": "256^2: %d steps %.1f s; 512^2: %d steps %.1f s; 4096^2: %g step (one stage) %.1f s"
+                                         % (s256, e256, s512, e512, s4k, e4k)},
+            "ensemble_all_cores": ens}
 
 
 def load_traffic(cells):
