@@ -157,34 +157,39 @@ __device__ __forceinline__ CuGrad cu_vjp(float hm, float um, float vm, float hp,
     return g;
 }
 
+// Tile form.  Shared arrays are kept in the shape each phase needs: the
+// state and lambda_L on the whole region (rows padded to an odd stride, so
+// that threads walking down rows hit distinct banks), x-slope data on the
+// tile rows only, y-slope data on the tile columns only (74.7 KB per CTA,
+// three CTAs per SM).
+constexpr int RXS = RX + 1;                 // padded row stride of region arrays
+constexpr int NR = RXS * RY;                // region
+constexpr int NXR = TY * RXS;               // tile rows x region columns
+constexpr int NYC = RY * TX;                // region rows x tile columns
+
 struct AdjSmem {
-    float R0[NC], R1[NC], R2[NC];           // primitive state (eta, u, v)
-    float Ux[NC], Vx[NC], Kx[NC];           // x slopes (K after adjustment)
-    float Uy[NC], Vy[NC], Ly[NC];           // y slopes
-    uint32_t br[NC];                        // branch codes
-    float LL0[NC], LL1[NC], LL2[NC];        // adjoint of the cell tendencies L
-    float Ax0[NC], Ax1[NC], Ax2[NC];        // adjoint of (eta, u, v): own terms + x faces
-    float Ay0[NC], Ay1[NC], Ay2[NC];        // adjoint of (eta, u, v): y faces
-    float AKx[NC], AUx[NC], AVx[NC];        // adjoint of the x slopes
-    float ALy[NC], AUy[NC], AVy[NC];        // adjoint of the y slopes
+    float R0[NR], R1[NR], R2[NR];           // primitive state (eta, u, v)
+    float LL0[NR], LL1[NR], LL2[NR];        // adjoint of the cell tendencies L
+    float Ux[NXR], Vx[NXR], Kx[NXR];        // x slopes (K after adjustment)
+    float Ax0[NXR], Ax1[NXR], Ax2[NXR];     // adjoint of (eta, u, v): own terms + x faces
+    float AKx[NXR], AUx[NXR], AVx[NXR];     // adjoint of the x slopes
+    float Uy[NYC], Vy[NYC], Ly[NYC];        // y slopes
+    float Ay0[NYC], Ay1[NYC], Ay2[NYC];     // adjoint of (eta, u, v): y faces
+    float ALy[NYC], AUy[NYC], AVy[NYC];     // adjoint of the y slopes
+    uint16_t bx[NXR], by[NYC];              // branch codes
     float Hi[(RY + 1) * (RX + 1)];
     float f[RY];
 };
 
-// branch-code fields
-__device__ __forceinline__ int br_ux(uint32_t b) { return b & 3; }
-__device__ __forceinline__ int br_vx(uint32_t b) { return (b >> 2) & 3; }
-__device__ __forceinline__ int br_kx(uint32_t b) { return (b >> 4) & 3; }
-__device__ __forceinline__ int br_kxa(uint32_t b) { return (b >> 6) & 3; }
-__device__ __forceinline__ int br_uy(uint32_t b) { return (b >> 8) & 3; }
-__device__ __forceinline__ int br_vy(uint32_t b) { return (b >> 10) & 3; }
-__device__ __forceinline__ int br_ly(uint32_t b) { return (b >> 12) & 3; }
-__device__ __forceinline__ int br_lya(uint32_t b) { return (b >> 14) & 3; }
-__device__ __forceinline__ bool has_xs(uint32_t b) { return (b >> 16) & 1; }
-__device__ __forceinline__ bool has_ys(uint32_t b) { return (b >> 17) & 1; }
+// branch-code fields (x codes in bx, y codes in by)
+__device__ __forceinline__ int br_u(uint32_t b) { return b & 3; }
+__device__ __forceinline__ int br_v(uint32_t b) { return (b >> 2) & 3; }
+__device__ __forceinline__ int br_k(uint32_t b) { return (b >> 4) & 3; }
+__device__ __forceinline__ int br_a(uint32_t b) { return (b >> 6) & 3; }
+__device__ __forceinline__ bool br_has(uint32_t b) { return (b >> 8) & 1; }
 
 template <int FRIC, bool STAGE1>
-__global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArgs a) {
+__global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     AdjSmem& S = *reinterpret_cast<AdjSmem*>(smem_raw);
     const Scheme& k = a.k;
@@ -194,302 +199,361 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
     const bool wallN = k.bcN == kWall, wallS = k.bcS == kWall, wallE = k.bcE == kWall, wallW = k.bcW == kWall;
     const float inv2g = 1.0f / k.two_g;
     bool scope_bad = false;
+    auto RI = [](int ry, int rx) { return ry * RXS + rx; };                 // region
+    auto XI = [](int ry, int rx) { return (ry - HALO) * RXS + rx; };        // tile rows
+    auto YI = [](int ry, int rx) { return ry * TX + (rx - HALO); };         // tile columns
 
-    // ---- corners and Coriolis rows --------------------------------------
+    // ---- corners and Coriolis rows; zero the accumulators ----------------
     for (int c = tid; c < (RY + 1) * (RX + 1); c += NT) {
         const int ry = c / (RX + 1), rx = c % (RX + 1);
         const int j = min(max(oy + ry, 0), ny + 4), i = min(max(ox + rx, 0), nx + 4);
         S.Hi[c] = a.Hi[(size_t)j * a.phi + i];
     }
     for (int r = tid; r < RY; r += NT) S.f[r] = a.f_rows[min(max(oy + r, 0), ny + 3)];
+    for (int c = tid; c < NXR; c += NT) {
+        S.Ax0[c] = 0.0f; S.Ax1[c] = 0.0f; S.Ax2[c] = 0.0f;
+        S.AKx[c] = 0.0f; S.AUx[c] = 0.0f; S.AVx[c] = 0.0f;
+        S.bx[c] = 0;
+    }
+    for (int c = tid; c < NYC; c += NT) {
+        S.Ay0[c] = 0.0f; S.Ay1[c] = 0.0f; S.Ay2[c] = 0.0f;
+        S.ALy[c] = 0.0f; S.AUy[c] = 0.0f; S.AVy[c] = 0.0f;
+        S.by[c] = 0;
+    }
     __syncthreads();
     auto HI = [&](int ry, int rx) { return S.Hi[ry * (RX + 1) + rx]; };
 
-    // ---- P1: primitive state of every region cell -----------------------
-    for (int c = tid; c < NC; c += NT) {
-        const int ry = c / RX, rx = c % RX;
-        const int j = oy + ry, i = ox + rx;
-        float e = 0.0f, u = 0.0f, v = 0.0f;
-        if (j >= 0 && j < ny + 4 && i >= 0 && i < nx + 4) {
-            int sj = j, si = i;
-            float shu = 1.0f, shv = 1.0f;
-            if (wallS && j < 2) { sj = 3 - j; shv = -1.0f; }
-            if (wallN && j > ny + 1) { sj = 2 * ny + 3 - j; shv = -1.0f; }
-            if (wallW && i < 2) { si = 3 - i; shu = -1.0f; }
-            if (wallE && i > nx + 1) { si = 2 * nx + 3 - i; shu = -1.0f; }
-            const size_t q = (size_t)sj * a.pq + si;
-            const float eta = a.qe[q], hu = a.qu[q] * shu, hv = a.qv[q] * shv;
-            const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
-            const float Bm = __fmul_rn(s4, 0.25f);
-            const float h = eta + Bm;
-            if (fabsf(HI(ry, rx) - k.land) < kDryEps || fabsf(HI(ry + 1, rx) - k.land) < kDryEps ||
-                fabsf(HI(ry, rx + 1) - k.land) < kDryEps || fabsf(HI(ry + 1, rx + 1) - k.land) < kDryEps ||
-                h < k.desing_eps)
-                scope_bad = true;
-            e = eta;
-            u = hu / h;
-            v = hv / h;
+    // ---- P1: primitive state of every region cell (loads first) ---------
+    {
+        constexpr int IT = (RX * RY + NT - 1) / NT;
+        float qe[IT], qu[IT], qv[IT];
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int c = tid + it * NT;
+            qe[it] = 0.0f; qu[it] = 0.0f; qv[it] = 0.0f;
+            if (c < RX * RY) {
+                const int ry = c / RX, rx = c % RX;
+                const int j = oy + ry, i = ox + rx;
+                if (j >= 0 && j < ny + 4 && i >= 0 && i < nx + 4) {
+                    int sj = j, si = i;
+                    float shu = 1.0f, shv = 1.0f;
+                    if (wallS && j < 2) { sj = 3 - j; shv = -1.0f; }
+                    if (wallN && j > ny + 1) { sj = 2 * ny + 3 - j; shv = -1.0f; }
+                    if (wallW && i < 2) { si = 3 - i; shu = -1.0f; }
+                    if (wallE && i > nx + 1) { si = 2 * nx + 3 - i; shu = -1.0f; }
+                    const size_t q = (size_t)sj * a.pq + si;
+                    qe[it] = a.qe[q]; qu[it] = a.qu[q] * shu; qv[it] = a.qv[q] * shv;
+                }
+            }
         }
-        S.R0[c] = e; S.R1[c] = u; S.R2[c] = v;
-        S.br[c] = 0u;
-        S.AKx[c] = 0.0f; S.AUx[c] = 0.0f; S.AVx[c] = 0.0f;
-        S.ALy[c] = 0.0f; S.AUy[c] = 0.0f; S.AVy[c] = 0.0f;
-        S.Ay0[c] = 0.0f; S.Ay1[c] = 0.0f; S.Ay2[c] = 0.0f;
-        S.Ax0[c] = 0.0f; S.Ax1[c] = 0.0f; S.Ax2[c] = 0.0f;
-        S.LL0[c] = 0.0f; S.LL1[c] = 0.0f; S.LL2[c] = 0.0f;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int c = tid + it * NT;
+            if (c >= RX * RY) continue;
+            const int ry = c / RX, rx = c % RX;
+            const int j = oy + ry, i = ox + rx;
+            float e = 0.0f, u = 0.0f, v = 0.0f;
+            if (j >= 0 && j < ny + 4 && i >= 0 && i < nx + 4) {
+                const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
+                const float h = qe[it] + __fmul_rn(s4, 0.25f);
+                if (fabsf(HI(ry, rx) - k.land) < kDryEps || fabsf(HI(ry + 1, rx) - k.land) < kDryEps ||
+                    fabsf(HI(ry, rx + 1) - k.land) < kDryEps || fabsf(HI(ry + 1, rx + 1) - k.land) < kDryEps ||
+                    h < k.desing_eps)
+                    scope_bad = true;
+                e = qe[it];
+                u = qu[it] / h;
+                v = qv[it] / h;
+            }
+            const int r = RI(ry, rx);
+            S.R0[r] = e; S.R1[r] = u; S.R2[r] = v;
+            S.LL0[r] = 0.0f; S.LL1[r] = 0.0f; S.LL2[r] = 0.0f;
+        }
     }
     __syncthreads();
 
-    // ---- P2: slopes (x on the tile rows, y on the tile columns) ---------
-    for (int c = tid; c < NC; c += NT) {
-        const int ry = c / RX, rx = c % RX;
-        if (rx < 1 || rx > RX - 2 || ry < 1 || ry > RY - 2) continue;
+    // ---- P2: x slopes on the tile rows, y slopes on the tile columns -------
+    for (int c = tid; c < TY * RX; c += NT) {
+        const int ry = HALO + c / RX, rx = c % RX;
         const int j = oy + ry, i = ox + rx;
-        const bool tile_row = ry >= HALO && ry < HALO + TY;
-        const bool tile_col = rx >= HALO && rx < HALO + TX;
-        uint32_t code = 0u;
-        if (tile_row && j >= 2 && j < ny + 2 && i >= 1 && i <= nx + 2) {
-            const float fJ = S.f[ry];
-            const float ul = S.R1[c - 1], uc = S.R1[c], ur = S.R1[c + 1];
-            const float vl = S.R2[c - 1], vc = S.R2[c], vr = S.R2[c + 1];
-            const float el = S.R0[c - 1], ec = S.R0[c], er = S.R0[c + 1];
-            S.Ux[c] = minmod_slope(ul, uc, ur, k.theta);
-            S.Vx[c] = minmod_slope(vl, vc, vr, k.theta);
-            const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
-            const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
-            const float fvl = (vl * flip((wallW && i - 1 < 2) || (wallE && i - 1 > nx + 1))) * fJ;
-            const float fvc = (vc * flip((wallW && i < 2) || (wallE && i > nx + 1))) * fJ;
-            const float fvr = (vr * flip((wallW && i + 1 < 2) || (wallE && i + 1 > nx + 1))) * fJ;
-            const float bw = k.theta_g * ((ec - el) - __fmul_rn(k.V, fvc + fvl));
-            const float ce = k.half_g * ((er - el) - __fmul_rn(k.V, (fvr + __fmul_rn(2.0f, fvc)) + fvl));
-            const float fw = k.theta_g * ((er - ec) - __fmul_rn(k.V, fvc + fvr));
-            const float Kraw = minmod_raw(bw, ce, fw);
-            const int bk = mm_branch(bw, ce, fw);
-            const float dxfv = __fmul_rn(k.dx * fJ, vc * flip((wallW && i < 2) || (wallE && i > nx + 2)));
-            const float Hw = 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
-            const float He = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1));
-            const float hw = (ec + Hw) - (Kraw + dxfv) / k.two_g;
-            const float he = (ec + He) + (Kraw + dxfv) / k.two_g;
-            float K = Kraw;
-            int ba = kAdjNone;
-            if (!(hw > 0.0f)) { K = -dxfv + __fmul_rn(k.two_g, ec + Hw); ba = kAdjA; }
-            if (!(he > 0.0f)) { K = -dxfv - __fmul_rn(k.two_g, ec + He); ba = kAdjB; }
-            S.Kx[c] = K;
-            code |= (uint32_t)bu | ((uint32_t)bv << 2) | ((uint32_t)bk << 4) | ((uint32_t)ba << 6) | (1u << 16);
-        }
-        if (tile_col && i >= 2 && i < nx + 2 && j >= 1 && j <= ny + 2) {
-            const float ul = S.R1[c - RX], uc = S.R1[c], ur = S.R1[c + RX];
-            const float vl = S.R2[c - RX], vc = S.R2[c], vr = S.R2[c + RX];
-            const float el = S.R0[c - RX], ec = S.R0[c], er = S.R0[c + RX];
-            S.Uy[c] = minmod_slope(ul, uc, ur, k.theta);
-            S.Vy[c] = minmod_slope(vl, vc, vr, k.theta);
-            const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
-            const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
-            const float ful = (ul * flip((wallS && j - 1 < 2) || (wallN && j - 1 > ny + 1))) * S.f[ry - 1];
-            const float fuc = (uc * flip((wallS && j < 2) || (wallN && j > ny + 1))) * S.f[ry];
-            const float fur = (ur * flip((wallS && j + 1 < 2) || (wallN && j + 1 > ny + 1))) * S.f[ry + 1];
-            const float bw = k.theta_g * ((ec - el) + __fmul_rn(k.U, fuc + ful));
-            const float ce = k.half_g * ((er - el) + __fmul_rn(k.U, (fur + __fmul_rn(2.0f, fuc)) + ful));
-            const float fw = k.theta_g * ((er - ec) + __fmul_rn(k.U, fuc + fur));
-            const float Lraw = minmod_raw(bw, ce, fw);
-            const int bl = mm_branch(bw, ce, fw);
-            const float dyfu = __fmul_rn(k.dy * S.f[ry], uc * flip((wallS && j < 2) || (wallN && j > ny + 2)));
-            const float Hs = 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
-            const float Hn = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1));
-            const float hs = (ec + Hs) - (Lraw - dyfu) / k.two_g;
-            const float hn = (ec + Hn) + (Lraw - dyfu) / k.two_g;
-            float L = Lraw;
-            int ba = kAdjNone;
-            if (!(hs > 0.0f)) { L = dyfu + __fmul_rn(k.two_g, ec + Hs); ba = kAdjA; }
-            if (!(hn > 0.0f)) { L = dyfu - __fmul_rn(k.two_g, ec + Hn); ba = kAdjB; }
-            S.Ly[c] = L;
-            code |= ((uint32_t)bu << 8) | ((uint32_t)bv << 10) | ((uint32_t)bl << 12) | ((uint32_t)ba << 14) |
-                    (1u << 17);
-        }
-        S.br[c] = code;
+        if (rx < 1 || rx > RX - 2 || !(j >= 2 && j < ny + 2 && i >= 1 && i <= nx + 2)) continue;
+        const int q = RI(ry, rx);
+        const float fJ = S.f[ry];
+        const float ul = S.R1[q - 1], uc = S.R1[q], ur = S.R1[q + 1];
+        const float vl = S.R2[q - 1], vc = S.R2[q], vr = S.R2[q + 1];
+        const float el = S.R0[q - 1], ec = S.R0[q], er = S.R0[q + 1];
+        const int xi = XI(ry, rx);
+        S.Ux[xi] = minmod_slope(ul, uc, ur, k.theta);
+        S.Vx[xi] = minmod_slope(vl, vc, vr, k.theta);
+        const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
+        const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
+        const float fvl = (vl * flip((wallW && i - 1 < 2) || (wallE && i - 1 > nx + 1))) * fJ;
+        const float fvc = (vc * flip((wallW && i < 2) || (wallE && i > nx + 1))) * fJ;
+        const float fvr = (vr * flip((wallW && i + 1 < 2) || (wallE && i + 1 > nx + 1))) * fJ;
+        const float bw = k.theta_g * ((ec - el) - __fmul_rn(k.V, fvc + fvl));
+        const float ce = k.half_g * ((er - el) - __fmul_rn(k.V, (fvr + __fmul_rn(2.0f, fvc)) + fvl));
+        const float fw = k.theta_g * ((er - ec) - __fmul_rn(k.V, fvc + fvr));
+        const float Kraw = minmod_raw(bw, ce, fw);
+        const int bk = mm_branch(bw, ce, fw);
+        const float dxfv = __fmul_rn(k.dx * fJ, vc * flip((wallW && i < 2) || (wallE && i > nx + 2)));
+        const float Hw = 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
+        const float He = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1));
+        const float hw = (ec + Hw) - (Kraw + dxfv) / k.two_g;
+        const float he = (ec + He) + (Kraw + dxfv) / k.two_g;
+        float K = Kraw;
+        int ba = kAdjNone;
+        if (!(hw > 0.0f)) { K = -dxfv + __fmul_rn(k.two_g, ec + Hw); ba = kAdjA; }
+        if (!(he > 0.0f)) { K = -dxfv - __fmul_rn(k.two_g, ec + He); ba = kAdjB; }
+        S.Kx[xi] = K;
+        S.bx[xi] = (uint16_t)(bu | (bv << 2) | (bk << 4) | (ba << 6) | (1 << 8));
+    }
+    for (int c = tid; c < RY * TX; c += NT) {
+        const int ry = c / TX, rx = HALO + c % TX;
+        const int j = oy + ry, i = ox + rx;
+        if (ry < 1 || ry > RY - 2 || !(i >= 2 && i < nx + 2 && j >= 1 && j <= ny + 2)) continue;
+        const int q = RI(ry, rx);
+        const float ul = S.R1[q - RXS], uc = S.R1[q], ur = S.R1[q + RXS];
+        const float vl = S.R2[q - RXS], vc = S.R2[q], vr = S.R2[q + RXS];
+        const float el = S.R0[q - RXS], ec = S.R0[q], er = S.R0[q + RXS];
+        const int yi = YI(ry, rx);
+        S.Uy[yi] = minmod_slope(ul, uc, ur, k.theta);
+        S.Vy[yi] = minmod_slope(vl, vc, vr, k.theta);
+        const int bu = mm_branch((uc - ul) * k.theta, (ur - ul) * 0.5f, (ur - uc) * k.theta);
+        const int bv = mm_branch((vc - vl) * k.theta, (vr - vl) * 0.5f, (vr - vc) * k.theta);
+        const float ful = (ul * flip((wallS && j - 1 < 2) || (wallN && j - 1 > ny + 1))) * S.f[ry - 1];
+        const float fuc = (uc * flip((wallS && j < 2) || (wallN && j > ny + 1))) * S.f[ry];
+        const float fur = (ur * flip((wallS && j + 1 < 2) || (wallN && j + 1 > ny + 1))) * S.f[ry + 1];
+        const float bw = k.theta_g * ((ec - el) + __fmul_rn(k.U, fuc + ful));
+        const float ce = k.half_g * ((er - el) + __fmul_rn(k.U, (fur + __fmul_rn(2.0f, fuc)) + ful));
+        const float fw = k.theta_g * ((er - ec) + __fmul_rn(k.U, fuc + fur));
+        const float Lraw = minmod_raw(bw, ce, fw);
+        const int bl = mm_branch(bw, ce, fw);
+        const float dyfu = __fmul_rn(k.dy * S.f[ry], uc * flip((wallS && j < 2) || (wallN && j > ny + 2)));
+        const float Hs = 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
+        const float Hn = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1));
+        const float hs = (ec + Hs) - (Lraw - dyfu) / k.two_g;
+        const float hn = (ec + Hn) + (Lraw - dyfu) / k.two_g;
+        float L = Lraw;
+        int ba = kAdjNone;
+        if (!(hs > 0.0f)) { L = dyfu + __fmul_rn(k.two_g, ec + Hs); ba = kAdjA; }
+        if (!(hn > 0.0f)) { L = dyfu - __fmul_rn(k.two_g, ec + Hn); ba = kAdjB; }
+        S.Ly[yi] = L;
+        S.by[yi] = (uint16_t)(bu | (bv << 2) | (bl << 4) | (ba << 6) | (1 << 8));
     }
 
-    // ---- P3: adjoint of the RK update, friction and sources -------------
-    // (interior cells of the cross tile rows x [1, RX-2] + tile columns x [1, RY-2])
-    for (int c = tid; c < NC; c += NT) {
-        const int ry = c / RX, rx = c % RX;
-        if (rx < 1 || rx > RX - 2 || ry < 1 || ry > RY - 2) continue;
-        const bool tile_row = ry >= HALO && ry < HALO + TY;
-        const bool tile_col = rx >= HALO && rx < HALO + TX;
-        if (!tile_row && !tile_col) continue;
-        const int j = oy + ry, i = ox + rx;
-        if (j < 2 || j >= ny + 2 || i < 2 || i >= nx + 2) continue;
-        const size_t lo = (size_t)j * a.pl + i, oo = (size_t)j * a.po + i;
-        float lE = a.le[lo], lU = a.lu[lo], lV = a.lv[lo];
-        const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
-        const float Hm = 0.25f * s4;
-        if (a.oe[oo] + Hm <= k.cutoff) { lE = 0.0f; lU = 0.0f; lV = 0.0f; }   // dry clamp: constant output
-        const float e = S.R0[c], u = S.R1[c], v = S.R2[c];
-        const float h = e + Hm;
-        const bool wet = h > k.cutoff;
-        const float hu = wet ? u * h : 0.0f, hv = wet ? v * h : 0.0f;
-        float Cf = 0.0f, s = 0.0f, uw = 0.0f, vw = 0.0f;
-        if (FRIC == kFricQuad) {
-            uw = hu / h; vw = hv / h;
-            s = sqrtf(uw * uw + vw * vw);
-            Cf = (a.dt * k.r * s) / h;
-        } else if (FRIC == kFricLinear) {
-            Cf = (k.two_r * a.dt) / h;
-        }
-        const float w = STAGE1 ? 0.5f : 1.0f;
-        const float iD = 1.0f / (1.0f + w * Cf);
-        const float lL1 = w * a.dt * lE, lL2 = w * a.dt * lU * iD, lL3 = w * a.dt * lV * iD;
-        float lhu = w * lU * iD, lhv = w * lV * iD, leta = w * lE, lh = 0.0f;
-        const float lCf = -w * (lU * a.ou[oo] + lV * a.ov[oo]) * iD;
-        if (FRIC == kFricQuad) {
-            const float ls = lCf * a.dt * k.r / h;
-            lh -= lCf * Cf / h;
-            if (s > 0.0f) {
-                const float luw = ls * uw / s, lvw = ls * vw / s;
-                lhu += luw / h; lhv += lvw / h;
-                lh -= (luw * uw + lvw * vw) / h;
+    // ---- P3: adjoint of the RK update, friction and sources on the cross --
+    // (tile rows x region columns 1..RX-2, plus tile columns x rows 1, 2 and
+    // the two rows above the tile), loads first
+    {
+        constexpr int NCROSS = TY * (RX - 2) + 4 * TX;
+        constexpr int IT = (NCROSS + NT - 1) / NT;
+        float lE[IT], lU[IT], lV[IT], oE[IT], oU[IT], oV[IT], wX[IT], wY[IT];
+        int cry[IT], crx[IT];
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int c = tid + it * NT;
+            int ry = -1, rx = -1;
+            if (c < TY * (RX - 2)) {
+                ry = HALO + c / (RX - 2);
+                rx = 1 + c % (RX - 2);
+            } else if (c < NCROSS) {
+                const int t = c - TY * (RX - 2), kk = t / TX;
+                rx = HALO + t % TX;
+                ry = (kk < 2) ? 1 + kk : HALO + TY + (kk - 2);
             }
-        } else if (FRIC == kFricLinear) {
-            lh -= lCf * Cf / h;
-        }
-        const float fc = S.f[ry];
-        if (h >= k.cutoff) {
-            const float Hx = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
-            const float Hy = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
-            lhv += fc * lL2;
-            lhu -= fc * lL3;
-            leta += lL2 * k.g * Hx / k.dx + lL3 * k.g * Hy / k.dy;
-            if (tile_row && tile_col && a.wx) {
+            cry[it] = ry; crx[it] = rx;
+            lE[it] = lU[it] = lV[it] = oE[it] = oU[it] = oV[it] = wX[it] = wY[it] = 0.0f;
+            if (ry < 0) continue;
+            const int j = oy + ry, i = ox + rx;
+            if (j < 2 || j >= ny + 2 || i < 2 || i >= nx + 2) continue;
+            const size_t lo = (size_t)j * a.pl + i, oo = (size_t)j * a.po + i;
+            lE[it] = a.le[lo]; lU[it] = a.lu[lo]; lV[it] = a.lv[lo];
+            oE[it] = a.oe[oo]; oU[it] = a.ou[oo]; oV[it] = a.ov[oo];
+            const bool tile = ry >= HALO && ry < HALO + TY && rx >= HALO && rx < HALO + TX;
+            if (tile && a.wx) {
                 const size_t wo = (size_t)(j - 2) * a.pw + (i - 2);
-                a.wx[wo] += lL2;
-                a.wy[wo] += lL3;
+                wX[it] = a.wx[wo];
+                wY[it] = a.wy[wo];
             }
         }
-        float lR1 = 0.0f, lR2 = 0.0f;
-        if (wet) {
-            lh += lhu * u + lhv * v;
-            lR1 = lhu * h;
-            lR2 = lhv * h;
-        }
-        S.LL0[c] = lL1; S.LL1[c] = lL2; S.LL2[c] = lL3;
-        S.Ax0[c] = lh + leta; S.Ax1[c] = lR1; S.Ax2[c] = lR2;
-        if (STAGE1 && tile_row && tile_col) {
-            const size_t no = (size_t)j * a.pn + i;
-            a.ne[no] = w * lE;
-            a.nu[no] = w * lU * iD;
-            a.nv[no] = w * lV * iD;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int ry = cry[it], rx = crx[it];
+            if (ry < 0) continue;
+            const int j = oy + ry, i = ox + rx;
+            if (j < 2 || j >= ny + 2 || i < 2 || i >= nx + 2) continue;
+            const bool tile = ry >= HALO && ry < HALO + TY && rx >= HALO && rx < HALO + TX;
+            const int r = RI(ry, rx);
+            float le = lE[it], lu = lU[it], lv = lV[it];
+            const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
+            const float Hm = __fmul_rn(0.25f, s4);
+            if (oE[it] + Hm <= k.cutoff) { le = 0.0f; lu = 0.0f; lv = 0.0f; }   // dry clamp: constant output
+            const float e = S.R0[r], u = S.R1[r], v = S.R2[r];
+            const float h = e + Hm;
+            const bool wet = h > k.cutoff;
+            const float hu = wet ? u * h : 0.0f, hv = wet ? v * h : 0.0f;
+            float Cf = 0.0f, sq = 0.0f, uw = 0.0f, vw = 0.0f;
+            if (FRIC == kFricQuad) {
+                uw = hu / h; vw = hv / h;
+                sq = sqrtf(uw * uw + vw * vw);
+                Cf = (a.dt * k.r * sq) / h;
+            } else if (FRIC == kFricLinear) {
+                Cf = (k.two_r * a.dt) / h;
+            }
+            const float w = STAGE1 ? 0.5f : 1.0f;
+            const float iD = 1.0f / (1.0f + w * Cf);
+            const float lL1 = w * a.dt * le, lL2 = w * a.dt * lu * iD, lL3 = w * a.dt * lv * iD;
+            S.LL0[r] = lL1; S.LL1[r] = lL2; S.LL2[r] = lL3;
+            if (!tile) continue;        // the own-cell terms are needed for the tile's cells only
+            float lhu = w * lu * iD, lhv = w * lv * iD, leta = w * le, lh = 0.0f;
+            const float lCf = -w * (lu * oU[it] + lv * oV[it]) * iD;
+            if (FRIC == kFricQuad) {
+                const float ls = lCf * a.dt * k.r / h;
+                lh -= lCf * Cf / h;
+                if (sq > 0.0f) {
+                    const float luw = ls * uw / sq, lvw = ls * vw / sq;
+                    lhu += luw / h; lhv += lvw / h;
+                    lh -= (luw * uw + lvw * vw) / h;
+                }
+            } else if (FRIC == kFricLinear) {
+                lh -= lCf * Cf / h;
+            }
+            const float fc = S.f[ry];
+            if (h >= k.cutoff) {
+                const float Hx = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
+                const float Hy = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
+                lhv += fc * lL2;
+                lhu -= fc * lL3;
+                leta += lL2 * k.g * Hx / k.dx + lL3 * k.g * Hy / k.dy;
+                if (a.wx) {
+                    const size_t wo = (size_t)(j - 2) * a.pw + (i - 2);
+                    a.wx[wo] = wX[it] + lL2;
+                    a.wy[wo] = wY[it] + lL3;
+                }
+            }
+            float lR1 = 0.0f, lR2 = 0.0f;
+            if (wet) {
+                lh += lhu * u + lhv * v;
+                lR1 = lhu * h;
+                lR2 = lhv * h;
+            }
+            const int xi = XI(ry, rx);
+            S.Ax0[xi] = lh + leta; S.Ax1[xi] = lR1; S.Ax2[xi] = lR2;
+            if (STAGE1) {
+                const size_t no = (size_t)j * a.pn + i;
+                a.ne[no] = w * le;
+                a.nu[no] = w * lu * iD;
+                a.nv[no] = w * lv * iD;
+            }
         }
     }
     __syncthreads();
 
-    // ---- P4: faces, even then odd --------------------------------------
-    constexpr int NFX = RX - 3;   // x faces per tile row: m at rx = 1..RX-3
-    constexpr int NFY = RY - 3;   // y faces per tile column: m at ry = 1..RY-3
-    const float DXf = k.dx, DYf = k.dy;
+    // ---- P4: faces, even then odd (x faces: consecutive threads on
+    // consecutive rows; y faces: on consecutive columns) -------------------
+    constexpr int NXH = (RX - 2) / 2;        // face pairs per tile row: m at 1 + parity + 2p
+    constexpr int NYH = (RY - 2) / 2;        // face pairs per tile column
     for (int parity = 0; parity < 2; ++parity) {
-        constexpr int NXH = (NFX + 1) / 2, NYH = (NFY + 1) / 2;
         const int nxi = TY * NXH, nyi = TX * NYH;
         for (int it = tid; it < nxi + nyi; it += NT) {
             if (it < nxi) {
-                const int ry = HALO + it / NXH;
-                const int rx = 1 + parity + 2 * (it % NXH);
+                const int ry = HALO + it % TY;
+                const int rx = 1 + parity + 2 * (it / TY);
                 if (rx > RX - 3) continue;
                 const int j = oy + ry, im = ox + rx, ip = im + 1;
                 if (j < 2 || j >= ny + 2 || im < 1 || im > nx + 1) continue;
-                const int m = ry * RX + rx, p = m + 1;
+                const int m = RI(ry, rx), p = m + 1;
+                const int xm = XI(ry, rx), xp = xm + 1;
                 const float fJ = S.f[ry];
-                const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Ux[m]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vx[m]);
-                const float Rpu = S.R1[p] - __fmul_rn(0.5f, S.Ux[p]), Rpv = S.R2[p] - __fmul_rn(0.5f, S.Vx[p]);
+                const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Ux[xm]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vx[xm]);
+                const float Rpu = S.R1[p] - __fmul_rn(0.5f, S.Ux[xp]), Rpv = S.R2[p] - __fmul_rn(0.5f, S.Vx[xp]);
                 const float fm = flip(wallW && ip == 2), fp = flip(wallE && ip == nx + 2);
                 const float Hf = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1));
-                const float Ep = (S.R0[p] + Hf) - (S.Kx[p] + __fmul_rn(k.dx * fJ, S.R2[p] * fp)) / k.two_g;
-                const float Em = (S.R0[m] + Hf) + (S.Kx[m] + __fmul_rn(k.dx * fJ, S.R2[m] * fm)) / k.two_g;
+                const float Ep = (S.R0[p] + Hf) - (S.Kx[xp] + __fmul_rn(k.dx * fJ, S.R2[p] * fp)) / k.two_g;
+                const float Em = (S.R0[m] + Hf) + (S.Kx[xm] + __fmul_rn(k.dx * fJ, S.R2[m] * fm)) / k.two_g;
                 const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
-                const float l0 = (S.LL0[p] - S.LL0[m]) / DXf;
-                const float l1 = (S.LL1[p] - S.LL1[m]) / DXf;
-                const float l2 = (S.LL2[p] - S.LL2[m]) / DXf;
+                const float l0 = (S.LL0[p] - S.LL0[m]) / k.dx;
+                const float l1 = (S.LL1[p] - S.LL1[m]) / k.dx;
+                const float l2 = (S.LL2[p] - S.LL2[m]) / k.dx;
                 const CuGrad g = cu_vjp(hm, Rmu, Rmv, hp, Rpu, Rpv, l0, l1, l2, k);
                 if (Ep > 0.0f) {
-                    S.Ax0[p] += g.hp;
-                    S.AKx[p] -= g.hp * inv2g;
-                    S.Ax2[p] -= g.hp * (k.dx * fJ) * fp * inv2g;
+                    S.Ax0[xp] += g.hp;
+                    S.AKx[xp] -= g.hp * inv2g;
+                    S.Ax2[xp] -= g.hp * (k.dx * fJ) * fp * inv2g;
                 }
                 if (Em > 0.0f) {
-                    S.Ax0[m] += g.hm;
-                    S.AKx[m] += g.hm * inv2g;
-                    S.Ax2[m] += g.hm * (k.dx * fJ) * fm * inv2g;
+                    S.Ax0[xm] += g.hm;
+                    S.AKx[xm] += g.hm * inv2g;
+                    S.Ax2[xm] += g.hm * (k.dx * fJ) * fm * inv2g;
                 }
-                S.Ax1[p] += g.up; S.AUx[p] -= 0.5f * g.up;
-                S.Ax2[p] += g.vp; S.AVx[p] -= 0.5f * g.vp;
-                S.Ax1[m] += g.um; S.AUx[m] += 0.5f * g.um;
-                S.Ax2[m] += g.vm; S.AVx[m] += 0.5f * g.vm;
+                S.Ax1[xp] += g.up; S.AUx[xp] -= 0.5f * g.up;
+                S.Ax2[xp] += g.vp; S.AVx[xp] -= 0.5f * g.vp;
+                S.Ax1[xm] += g.um; S.AUx[xm] += 0.5f * g.um;
+                S.Ax2[xm] += g.vm; S.AVx[xm] += 0.5f * g.vm;
             } else {
                 const int t = it - nxi;
-                const int rx = HALO + t / NYH;
-                const int ry = 1 + parity + 2 * (t % NYH);
+                const int rx = HALO + t % TX;
+                const int ry = 1 + parity + 2 * (t / TX);
                 if (ry > RY - 3) continue;
                 const int i = ox + rx, jm = oy + ry, jp = jm + 1;
                 if (i < 2 || i >= nx + 2 || jm < 1 || jm > ny + 1) continue;
-                const int m = ry * RX + rx, p = m + RX;
-                const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Uy[m]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vy[m]);
-                const float Rpu = S.R1[p] - __fmul_rn(0.5f, S.Uy[p]), Rpv = S.R2[p] - __fmul_rn(0.5f, S.Vy[p]);
+                const int m = RI(ry, rx), p = m + RXS;
+                const int ym = YI(ry, rx), yp = ym + TX;
+                const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Uy[ym]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vy[ym]);
+                const float Rpu = S.R1[p] - __fmul_rn(0.5f, S.Uy[yp]), Rpv = S.R2[p] - __fmul_rn(0.5f, S.Vy[yp]);
                 const float fm = flip(wallS && jp == 2), fp = flip(wallN && jp == ny + 2);
                 const float fpr = S.f[ry + 1], fmr = S.f[ry];
                 const float Hf = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1));
-                const float Ep = (S.R0[p] + Hf) - (S.Ly[p] - __fmul_rn(k.dy * fpr, S.R1[p] * fp)) / k.two_g;
-                const float Em = (S.R0[m] + Hf) + (S.Ly[m] - __fmul_rn(k.dy * fmr, S.R1[m] * fm)) / k.two_g;
+                const float Ep = (S.R0[p] + Hf) - (S.Ly[yp] - __fmul_rn(k.dy * fpr, S.R1[p] * fp)) / k.two_g;
+                const float Em = (S.R0[m] + Hf) + (S.Ly[ym] - __fmul_rn(k.dy * fmr, S.R1[m] * fm)) / k.two_g;
                 const float hp = fmaxf(Ep, 0.0f), hm = fmaxf(Em, 0.0f);
                 // G = CU(hm, v, u | hp, v, u) with outputs (G0, G2, G1)
-                const float l0 = (S.LL0[p] - S.LL0[m]) / DYf;
-                const float l1 = (S.LL1[p] - S.LL1[m]) / DYf;
-                const float l2 = (S.LL2[p] - S.LL2[m]) / DYf;
+                const float l0 = (S.LL0[p] - S.LL0[m]) / k.dy;
+                const float l1 = (S.LL1[p] - S.LL1[m]) / k.dy;
+                const float l2 = (S.LL2[p] - S.LL2[m]) / k.dy;
                 const CuGrad g = cu_vjp(hm, Rmv, Rmu, hp, Rpv, Rpu, l0, l2, l1, k);
                 if (Ep > 0.0f) {
-                    S.Ay0[p] += g.hp;
-                    S.ALy[p] -= g.hp * inv2g;
-                    S.Ay1[p] += g.hp * (k.dy * fpr) * fp * inv2g;
+                    S.Ay0[yp] += g.hp;
+                    S.ALy[yp] -= g.hp * inv2g;
+                    S.Ay1[yp] += g.hp * (k.dy * fpr) * fp * inv2g;
                 }
                 if (Em > 0.0f) {
-                    S.Ay0[m] += g.hm;
-                    S.ALy[m] += g.hm * inv2g;
-                    S.Ay1[m] -= g.hm * (k.dy * fmr) * fm * inv2g;
+                    S.Ay0[ym] += g.hm;
+                    S.ALy[ym] += g.hm * inv2g;
+                    S.Ay1[ym] -= g.hm * (k.dy * fmr) * fm * inv2g;
                 }
-                S.Ay2[p] += g.up; S.AVy[p] -= 0.5f * g.up;
-                S.Ay1[p] += g.vp; S.AUy[p] -= 0.5f * g.vp;
-                S.Ay2[m] += g.um; S.AVy[m] += 0.5f * g.um;
-                S.Ay1[m] += g.vm; S.AUy[m] += 0.5f * g.vm;
+                S.Ay2[yp] += g.up; S.AVy[yp] -= 0.5f * g.up;
+                S.Ay1[yp] += g.vp; S.AUy[yp] -= 0.5f * g.vp;
+                S.Ay2[ym] += g.um; S.AVy[ym] += 0.5f * g.um;
+                S.Ay1[ym] += g.vm; S.AUy[ym] += 0.5f * g.vm;
             }
         }
         __syncthreads();
     }
 
-    // ---- P5: positivity adjustment of K and L ---------------------------
-    for (int c = tid; c < NC; c += NT) {
-        const int ry = c / RX, rx = c % RX;
-        if (rx < HALO - 1 || rx > HALO + TX || ry < HALO - 1 || ry > HALO + TY) continue;
-        const uint32_t b = S.br[c];
-        if (has_xs(b)) {
-            const float lK = S.AKx[c];
-            const int ba = br_kxa(b);
-            if (ba != kAdjNone) {
-                const int i = ox + rx;
-                const float fv = flip((wallW && i < 2) || (wallE && i > nx + 2));
-                S.Ax0[c] += (ba == kAdjA ? k.two_g : -k.two_g) * lK;
-                S.Ax2[c] -= lK * (k.dx * S.f[ry]) * fv;
-                S.AKx[c] = 0.0f;
-            }
-        }
-        if (has_ys(b)) {
-            const float lL = S.ALy[c];
-            const int ba = br_lya(b);
-            if (ba != kAdjNone) {
-                const int j = oy + ry;
-                const float fu = flip((wallS && j < 2) || (wallN && j > ny + 2));
-                S.Ay0[c] += (ba == kAdjA ? k.two_g : -k.two_g) * lL;
-                S.Ay1[c] += lL * (k.dy * S.f[ry]) * fu;
-                S.ALy[c] = 0.0f;
-            }
-        }
+    // ---- P5: positivity adjustment of K (tile rows) and L (tile columns) --
+    for (int c = tid; c < TY * (TX + 2); c += NT) {
+        const int ry = HALO + c / (TX + 2), rx = HALO - 1 + c % (TX + 2);
+        const int xi = XI(ry, rx);
+        const uint32_t b = S.bx[xi];
+        if (!br_has(b) || br_a(b) == kAdjNone) continue;
+        const float lK = S.AKx[xi];
+        const int i = ox + rx;
+        const float fv = flip((wallW && i < 2) || (wallE && i > nx + 2));
+        S.Ax0[xi] += (br_a(b) == kAdjA ? k.two_g : -k.two_g) * lK;
+        S.Ax2[xi] -= lK * (k.dx * S.f[ry]) * fv;
+        S.AKx[xi] = 0.0f;
+    }
+    for (int c = tid; c < (TY + 2) * TX; c += NT) {
+        const int ry = HALO - 1 + c / TX, rx = HALO + c % TX;
+        const int yi = YI(ry, rx);
+        const uint32_t b = S.by[yi];
+        if (!br_has(b) || br_a(b) == kAdjNone) continue;
+        const float lL = S.ALy[yi];
+        const int j = oy + ry;
+        const float fu = flip((wallS && j < 2) || (wallN && j > ny + 2));
+        S.Ay0[yi] += (br_a(b) == kAdjA ? k.two_g : -k.two_g) * lL;
+        S.Ay1[yi] += lL * (k.dy * S.f[ry]) * fu;
+        S.ALy[yi] = 0.0f;
     }
     __syncthreads();
 
@@ -498,28 +562,29 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
         const int ry = HALO + c / TX, rx = HALO + c % TX;
         const int j = oy + ry, i = ox + rx;
         if (j >= ny + 4 || i >= nx + 4) continue;
-        const int q = ry * RX + rx;
-        float l0 = S.Ax0[q] + S.Ay0[q];
-        float l1 = S.Ax1[q] + S.Ay1[q];
-        float l2 = S.Ax2[q] + S.Ay2[q];
+        const int q = RI(ry, rx), xq = XI(ry, rx), yq = YI(ry, rx);
+        float l0 = S.Ax0[xq] + S.Ay0[yq];
+        float l1 = S.Ax1[xq] + S.Ay1[yq];
+        float l2 = S.Ax2[xq] + S.Ay2[yq];
         float lfv = 0.0f, lfu = 0.0f;
+#pragma unroll
         for (int o = -1; o <= 1; ++o) {
             const int pos = -o;       // position of this cell in the stencil of slope cell q+o
-            const uint32_t bx = S.br[q + o];
-            if (has_xs(bx)) {
-                l1 += S.AUx[q + o] * slope_coef(br_ux(bx), pos, k.theta);
-                l2 += S.AVx[q + o] * slope_coef(br_vx(bx), pos, k.theta);
-                const float lk = S.AKx[q + o];
-                const int bk = br_kx(bx);
+            const uint32_t bxo = S.bx[xq + o];
+            if (br_has(bxo)) {
+                l1 += S.AUx[xq + o] * slope_coef(br_u(bxo), pos, k.theta);
+                l2 += S.AVx[xq + o] * slope_coef(br_v(bxo), pos, k.theta);
+                const float lk = S.AKx[xq + o];
+                const int bk = br_k(bxo);
                 l0 += lk * k.g * slope_coef(bk, pos, k.theta);
                 lfv -= lk * k.V * pot_coef(bk, pos, k.theta_g, k.half_g);
             }
-            const uint32_t by = S.br[q + o * RX];
-            if (has_ys(by)) {
-                l1 += S.AUy[q + o * RX] * slope_coef(br_uy(by), pos, k.theta);
-                l2 += S.AVy[q + o * RX] * slope_coef(br_vy(by), pos, k.theta);
-                const float ll = S.ALy[q + o * RX];
-                const int bl = br_ly(by);
+            const uint32_t byo = S.by[yq + o * TX];
+            if (br_has(byo)) {
+                l1 += S.AUy[yq + o * TX] * slope_coef(br_u(byo), pos, k.theta);
+                l2 += S.AVy[yq + o * TX] * slope_coef(br_v(byo), pos, k.theta);
+                const float ll = S.ALy[yq + o * TX];
+                const int bl = br_k(byo);
                 l0 += ll * k.g * slope_coef(bl, pos, k.theta);
                 lfu += ll * k.U * pot_coef(bl, pos, k.theta_g, k.half_g);
             }
@@ -527,7 +592,7 @@ __global__ void __launch_bounds__(NT, 2) cdklm_adjoint_stage_kernel(const AdjArg
         l2 += lfv * S.f[ry] * flip((wallW && i < 2) || (wallE && i > nx + 1));
         l1 += lfu * S.f[ry] * flip((wallS && j < 2) || (wallN && j > ny + 1));
         const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
-        const float h = S.R0[q] + s4 * 0.25f;
+        const float h = S.R0[q] + __fmul_rn(s4, 0.25f);
         float lE = l0 - (l1 * S.R1[q] + l2 * S.R2[q]) / h;
         float lU = l1 / h, lV = l2 / h;
         if (!STAGE1 && a.ne && j >= 2 && j < ny + 2 && i >= 2 && i < nx + 2) {
