@@ -263,3 +263,35 @@ def test_status_word_flags_nonfinite(ctx):
     sim.step(c.dt)
     assert sim.status(clear=True) & _native.GO_STATUS_NONFINITE
     assert sim.status() == 0
+
+
+@pytest.mark.parametrize("nx, ny, bc, r", [
+    (4, 4, (1, 1, 1, 1), 0.0),
+    (5, 11, (2, 2, 2, 2), 3.0e-3),
+    (17, 6, (1, 2, 1, 2), 3.0e-3),
+    (33, 129, (2, 1, 2, 1), 0.0),
+    (131, 45, (1, 1, 1, 1), 3.0e-3),
+    (257, 9, (1, 2, 1, 2), 3.0e-3),
+])
+def test_small_and_ragged_grids_vs_fp64(ctx, nx, ny, bc, r):
+    """Grids down to 4x4 and sizes that fill no launch tile evenly, every
+    boundary combination: 10 steps against the FP64 restatement, and the
+    interior mass under all-wall boundaries."""
+    c = SC.grf(nx, ny=ny, dx=1000.0, bc=bc, r=r, steps=10)
+    sim = _drop_in(ctx, c)
+    for _ in range(c.steps):
+        sim.step(c.dt)
+    mine = sim.download()
+    fp64 = O.OracleSim(c.eta0, c.hu0, c.hv0, c.Hi, c.nx, c.ny, c.dx, c.dy, c.dt, c.g, c.f, c.r,
+                       coriolis_beta=c.beta, bc=c.bc, wind=c.wind)
+    for _ in range(c.steps):
+        fp64.step(c.dt)
+    ref = fp64.download()
+    errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, ref)]
+    print("%dx%d bc=%s: vs FP64 after 10 steps %s" % (nx, ny, bc, ["%.1e" % e for e in errs]))
+    assert max(errs) < 1e-3
+    assert sim.status() == 0
+    if bc == (1, 1, 1, 1):
+        e0 = np.maximum(c.eta0, -sim.downloadBathymetry()[1])[2:-2, 2:-2].astype(np.float64).sum()
+        e1 = mine[0][2:-2, 2:-2].astype(np.float64).sum()
+        assert abs(e1 - e0) <= 1e-4 * np.abs(c.eta0).sum() + 1e-6
