@@ -41,7 +41,6 @@ namespace {
 
 constexpr int TX = 32, TY = 16, HALO = 3;
 constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO;   // 38 x 22 region
-constexpr int NC = RX * RY;
 constexpr int NT = 256;
 
 struct AdjArgs {

@@ -16,10 +16,14 @@
 // Paired arithmetic.  At row j the x-direction work of row j and the
 // y-direction work of row j+1 have the same shape (slopes, slope
 // adjustment, central-upwind flux), so they run side by side as the two
-// lanes of float2 values; their sums and differences issue as packed
-// add/sub.rn.ftz.f32x2 (per lane the same IEEE round-to-nearest,
-// flush-to-zero result as the scalar operation, so results stay identical
-// to the scalar evaluation order of the reference).  In the
+// lanes of float2 values, evaluated as two scalar operations per pair.
+// (Built with GO_PACKED_PAIRS, sums and differences issue as packed
+// add/sub.rn.ftz.f32x2 instead, per lane the same IEEE round-to-nearest,
+// flush-to-zero result as the scalar operation.  Measured at 4096^2 on a
+// B200 that build executes as many instructions per cell, 601 against 600:
+// the 52 additions per cell it saves come back as register moves that
+// assemble the operand pairs, and it runs 4% slower, so it is off by
+// default.)  In the
 // flux, lane x carries (u normal, v tangential) and lane y (v normal, u
 // tangential), which is how the reference swaps u and v for the G flux
 // (CDKLM16_kernel.cu:361-369).  Signs: a - b*c is written a + (-b)*c, which
@@ -76,15 +80,16 @@ __device__ __forceinline__ float quot(float a, float b) {
 }
 
 // ---- paired float2 helpers -----------------------------------------------
-// Sums and differences run as packed add/sub.rn.ftz.f32x2: per lane the IEEE
-// round-to-nearest result with subnormals flushed, i.e. what the scalar
-// add.rn.ftz of a --ftz=true --fmad=false build computes.  Products stay two
-// scalar multiplies: ptxas may contract a packed multiply feeding a packed
-// add into a fused FFMA2 (observed on sm_100a even with explicit .rn and
-// -fmad=false), which would round differently from the reference, while a
-// scalar product cannot be fused into a packed add.
+// Default: each lane is a scalar add.rn.ftz / mul.rn.ftz, as the reference's
+// --ftz=true --fmad=false build computes it.  GO_PACKED_PAIRS: sums and
+// differences run as packed add/sub.rn.ftz.f32x2 (per lane the same IEEE
+// round-to-nearest result with subnormals flushed).  Products stay two
+// scalar multiplies in both builds: ptxas may contract a packed multiply
+// feeding a packed add into a fused FFMA2 (observed on sm_100a even with
+// explicit .rn and -fmad=false), which would round differently from the
+// reference, while a scalar product cannot be fused into a packed add.
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
-#ifdef GO_SCALAR_PAIRS
+#ifndef GO_PACKED_PAIRS
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return f2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return f2(a.x - b.x, a.y - b.y); }
 #else
@@ -178,12 +183,44 @@ __device__ __forceinline__ void central_upwind2(float2 hm, float2 um, float2 vm,
 
 struct Cell { float e, u, v; };     // reconstruction state (eta, u, v)
 
-// Shared-memory row buffers of one block.
+// Read-ahead ring (launch shape 5).  Each thread copies the inputs of its
+// own column for row j + kReadAhead (cp.async, 4 bytes per value) into a
+// private ring of kReadAhead + 1 shared-memory slots while it computes row
+// j, so the global-load latency of a row is hidden behind kReadAhead rows of
+// arithmetic without holding the values in registers; the thread reads only
+// its own slots, so no barrier is involved.  The slot refilled at row j is
+// the one read at row j - 1, whose values were consumed by then.  Measured
+// on a B200 (us per RK2 step, 128 x 5 blocks): 4096^2 720 -> 686, 2048^2
+// 207 -> 200, but 1024^2 66 -> 70 and 512^2 29 -> 32: once the grid fits in
+// one wave of blocks the plain one-row register prefetch is faster.
+constexpr int kReadAhead = 2;
+
+__device__ __forceinline__ void cp_async4(void* smem, const float* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Per thread: Q of row j+2, Q^n of row j (stage 1), corners (cl, cl+1) of
+// corner row j+3, for SLOTS rows.
+template <int BW, int SLOTS>
+struct ReadRing {
+    float4 q[SLOTS][BW];
+    float4 qn[SLOTS][BW];
+    float2 h[SLOTS][BW];
+};
 template <int BW>
+struct ReadRing<BW, 0> {};
+
+// Shared-memory row buffers of one block (DEPTH: rows read ahead, 0 = none).
+template <int BW, int DEPTH>
 struct RowBufs {
     float4 r[BW];   // (eta, u, v, f*v along north)
     float4 s[BW];   // (u_x, v_x, K_x, -)
     float4 f[BW];   // F flux on the face west of the column
+    ReadRing<BW, (DEPTH > 0 ? DEPTH + 1 : 0)> ring;
 };
 
 // Divisor by a domain constant c: a/c, or a * (1/c) with 1/c hoisted.
@@ -206,9 +243,9 @@ __device__ __forceinline__ bool interior_block(const Scheme& k, int c0, int r0, 
 }
 
 // One block strip: columns of block bx, rows of block by.
-template <int BW, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, bool EDGE>
+template <int BW, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, bool EDGE, int D>
 __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, const int bx, const int by,
-                                            RowBufs<BW>& sb) {
+                                            RowBufs<BW, D>& sb) {
     const Scheme& k = a.k;
     const int t = threadIdx.x;
     const int c0 = 2 + bx * (BW - 4);
@@ -253,13 +290,19 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
     const float* __restrict__ Hi = a.Hi;
     const float* __restrict__ frow = a.f_rows;
 
-    auto load_q = [&](int r, float& e, float& hu, float& hv) {
-        float hv_sgn = 1.0f;
+    // wall ghost rows mirror the interior with hv odd
+    auto mirror_row = [&](int r, float& hv_sgn) {
+        hv_sgn = 1.0f;
         int rr = r;
         if (EDGE) {
             if (k.bcS == kWall && r < 2) { hv_sgn = -1.0f; rr = 3 - r; }
             else if (k.bcN == kWall && r > k.ny + 1) { hv_sgn = -1.0f; rr = 2 * k.ny + 3 - r; }
         }
+        return rr;
+    };
+    auto load_q = [&](int r, float& e, float& hu, float& hv) {
+        float hv_sgn;
+        const int rr = mirror_row(r, hv_sgn);
         const size_t o = (size_t)rr * a.pin + qc;
         e = __ldg(eta_in + o);
         hu = __ldg(hu_in + o);
@@ -366,19 +409,50 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
         Gs2 = dry ? 0.0f : F1.x;
     }
 
-    // prefetch row r0+2 (Q), corner row r0+3, f(r0+2) and, for stage 1, Q^n(r0)
-    float nq_e, nq_hu, nq_hv, nha, nhb, nf;
-    load_q(r0 + 2, nq_e, nq_hu, nq_hv);
-    load_h(r0 + 3, nha, nhb);
-    nf = __ldg(frow + r0 + 2);
-
     const int tl = max(t - 1, 0), tr = min(t + 1, BW - 1);
     const bool writer = (t >= 2) && (t < BW - 2) && (!EDGE || cl <= k.nx + 1);
     const bool stage1 = (a.rk_step == 1);
+
+    // Inputs of output row jj: Q of row jj+2, corner row jj+3, Q^n of row jj.
+    // D > 0: copied into ring slot `slot`, one commit group per row (an
+    // empty group past the strip keeps the group count per row fixed).
+    auto stage_row = [&](int jj, int slot) {
+        if constexpr (D > 0) {
+            if (jj < r1) {
+                float hv_sgn;
+                const size_t o = (size_t)mirror_row(jj + 2, hv_sgn) * a.pin + qc;
+                cp_async4(&sb.ring.q[slot][t].x, eta_in + o);
+                cp_async4(&sb.ring.q[slot][t].y, hu_in + o);
+                cp_async4(&sb.ring.q[slot][t].z, hv_in + o);
+                const size_t oh = (size_t)(jj + 3) * a.phi;
+                cp_async4(&sb.ring.h[slot][t].x, Hi + oh + hca);
+                cp_async4(&sb.ring.h[slot][t].y, Hi + oh + hcb);
+                if (stage1 && writer) {
+                    const size_t on = (size_t)jj * a.pqn + cl;
+                    cp_async4(&sb.ring.qn[slot][t].x, a.qn_eta + on);
+                    cp_async4(&sb.ring.qn[slot][t].y, a.qn_hu + on);
+                    cp_async4(&sb.ring.qn[slot][t].z, a.qn_hv + on);
+                }
+            }
+            cp_async_commit();
+        }
+    };
+
+    // prefetch row r0+2 (Q), corner row r0+3, f(r0+2) and, for stage 1, Q^n(r0)
+    float nq_e = 0.0f, nq_hu = 0.0f, nq_hv = 0.0f, nha = 0.0f, nhb = 0.0f, nf;
     float nqn_e = 0.0f, nqn_hu = 0.0f, nqn_hv = 0.0f;
-    if (stage1 && writer) {
-        const size_t o = (size_t)r0 * a.pqn + cl;
-        nqn_e = a.qn_eta[o]; nqn_hu = a.qn_hu[o]; nqn_hv = a.qn_hv[o];
+    nf = __ldg(frow + r0 + 2);
+    int slot = 0;
+    if constexpr (D > 0) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) stage_row(r0 + d, d);
+    } else {
+        load_q(r0 + 2, nq_e, nq_hu, nq_hv);
+        load_h(r0 + 3, nha, nhb);
+        if (stage1 && writer) {
+            const size_t o = (size_t)r0 * a.pqn + cl;
+            nqn_e = a.qn_eta[o]; nqn_hu = a.qn_hu[o]; nqn_hv = a.qn_hv[o];
+        }
     }
     const bool col_img = EDGE && (k.bcE == kPeriodic) && (cl < 4 || cl >= k.nx);
     const float2 theta2 = f2(k.theta, k.theta);
@@ -387,13 +461,39 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
     const float2 VU2 = f2(-k.V, k.U);          // K_x subtracts V*(.), L_y adds U*(.)
     const float2 two_g2 = f2(k.two_g, k.two_g);
 
+    // not unrolled: unrolled by 2, 3 or 4 the row loop spills under the
+    // 96-register cap of 128 x 5 blocks and runs 2-16% slower at 4096^2
 #pragma unroll 1
     for (int j = r0; j < r1; ++j) {
-        // ---- row j+2 arrives; prefetch j+3 --------------------------------
-        const float Ha3 = nha, Hb3 = nhb, f2r = nf;
-        const float q_e = nq_e, q_hu = nq_hu, q_hv = nq_hv;
-        const float qn_e = nqn_e, qn_hu = nqn_hu, qn_hv = nqn_hv;
-        {
+        // ---- row j+2 arrives; prefetch what a later row reads --------------
+        float Ha3, Hb3, q_e, q_hu, q_hv, qn_e, qn_hu, qn_hv;
+        const float f2r = nf;
+        if constexpr (D > 0) {
+            // refill the slot read at row j-1 with the inputs of row j+D,
+            // then wait for this row's group (D groups may stay in flight)
+            stage_row(j + D, (slot == 0) ? D : slot - 1);
+            cp_async_wait<D>();
+            const float4 q = sb.ring.q[slot][t];
+            const float2 h = sb.ring.h[slot][t];
+            q_e = q.x; q_hu = q.y; q_hv = q.z;
+            if (EDGE) {
+                float hv_sgn;
+                mirror_row(j + 2, hv_sgn);
+                q_hu *= hu_sgn; q_hv *= hv_sgn;
+            }
+            Ha3 = h.x; Hb3 = h.y;
+            if (LAND) { Ha3 = corner(Ha3, k); Hb3 = corner(Hb3, k); }
+            qn_e = qn_hu = qn_hv = 0.0f;
+            if (stage1 && writer) {
+                const float4 qn = sb.ring.qn[slot][t];
+                qn_e = qn.x; qn_hu = qn.y; qn_hv = qn.z;
+            }
+            slot = (slot == D) ? 0 : slot + 1;
+            nf = __ldg(frow + min(j + 3, k.ny + 3));
+        } else {
+            Ha3 = nha; Hb3 = nhb;
+            q_e = nq_e; q_hu = nq_hu; q_hv = nq_hv;
+            qn_e = nqn_e; qn_hu = nqn_hu; qn_hv = nqn_hv;
             load_q(min(j + 3, r1 + 1), nq_e, nq_hu, nq_hv);
             load_h(min(j + 4, r1 + 2), nha, nhb);
             nf = __ldg(frow + min(j + 3, k.ny + 3));
@@ -624,22 +724,22 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
     }
 }
 
-template <int BW, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND>
+template <int BW, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, int D>
 __device__ __forceinline__ void stage_block(const StageArgs& a, const float dt, const int bx, const int by,
-                                            RowBufs<BW>& sb) {
+                                            RowBufs<BW, D>& sb) {
     const int c0 = 2 + bx * (BW - 4);
     const int r0 = 2 + by * a.rows_per_block;
     const int r1 = min(r0 + a.rows_per_block, a.k.ny + 2);
     if (interior_block<BW>(a.k, c0, r0, r1))
-        stage_strip<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, false>(a, dt, bx, by, sb);
+        stage_strip<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, false, D>(a, dt, bx, by, sb);
     else
-        stage_strip<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, true>(a, dt, bx, by, sb);
+        stage_strip<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, true, D>(a, dt, bx, by, sb);
 }
 
-template <int BW, int MINB, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND>
+template <int BW, int MINB, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, int D>
 __global__ void __launch_bounds__(BW, MINB) cdklm_stage_kernel(const StageArgs a) {
-    __shared__ RowBufs<BW> sb;
-    stage_block<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND>(a, a.dt, blockIdx.x, blockIdx.y, sb);
+    __shared__ RowBufs<BW, D> sb;
+    stage_block<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, D>(a, a.dt, blockIdx.x, blockIdx.y, sb);
 }
 
 // Batched stage: a packed list of (member, column block, row block) tiles
@@ -647,15 +747,15 @@ __global__ void __launch_bounds__(BW, MINB) cdklm_stage_kernel(const StageArgs a
 // persistent grid.  args holds two entries per member (stage 0: h0 -> h1,
 // stage 1: h1 -> h0); dts holds the member's time step, read at launch so a
 // captured graph picks up new values.
-template <int BW, int MINB, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND>
+template <int BW, int MINB, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, int D>
 __global__ void __launch_bounds__(BW, MINB)
     cdklm_batch_kernel(const StageArgs* __restrict__ args, const float* __restrict__ dts,
                        const int4* __restrict__ tiles, const int ntiles, const int rk_step) {
-    __shared__ RowBufs<BW> sb;
+    __shared__ RowBufs<BW, D> sb;
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
         const int4 tile = tiles[ti];
         const StageArgs& a = args[2 * tile.x + rk_step];
-        stage_block<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND>(a, __ldg(dts + tile.x), tile.y, tile.z, sb);
+        stage_block<BW, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, D>(a, __ldg(dts + tile.x), tile.y, tile.z, sb);
         __syncthreads();
     }
 }

@@ -1,7 +1,8 @@
 // Kernel-variant selection shared by the single-domain and batched launchers.
 //
 // A variant is (launch shape, friction law, general grid angle, per-cell
-// wind, reciprocal quotients, land in the bathymetry).  Every variant gives
+// wind, reciprocal quotients, land in the bathymetry).  Shape 5 is the
+// 128 x 5 block with the read-ahead ring.  Every variant gives
 // the same results; the specialised ones drop work the general one would do
 // for nothing.  Instantiated set:
 //   * general: shape 4, every friction law, angle and wind combination, land
@@ -20,10 +21,12 @@ struct Variant {
 };
 
 // L is a functor with
-//   template <int BW, int MINB, int FRIC, bool GN, bool WF, bool RCP, bool LAND> cudaError_t run();
+//   template <int BW, int MINB, int FRIC, bool GN, bool WF, bool RCP, bool LAND, int D> cudaError_t run();
+// (D: rows read ahead through the shared-memory ring, 0 = register prefetch)
 template <class L>
 cudaError_t dispatch_variant(L& launcher, Variant v) {
-#define GO_V(BW, MINB, F, GN, WF, RCP, LAND) return launcher.template run<BW, MINB, F, GN, WF, RCP, LAND>()
+#define GO_VD(BW, MINB, F, GN, WF, RCP, LAND, D) return launcher.template run<BW, MINB, F, GN, WF, RCP, LAND, D>()
+#define GO_V(BW, MINB, F, GN, WF, RCP, LAND) GO_VD(BW, MINB, F, GN, WF, RCP, LAND, 0)
     if (v.gen_north || v.wind_field) {
         // general variants: shape 4, land checks on, reciprocal quotients
 #define GO_GEN(F)                                                     \
@@ -44,6 +47,7 @@ cudaError_t dispatch_variant(L& launcher, Variant v) {
             case 1: GO_V(192, 3, F, false, false, RCP, LAND);         \
             case 2: GO_V(128, 4, F, false, false, RCP, LAND);         \
             case 3: GO_V(256, 2, F, false, false, RCP, LAND);         \
+            case 5: GO_VD(128, 5, F, false, false, RCP, LAND, kReadAhead); \
             default: GO_V(128, 5, F, false, false, RCP, LAND);        \
         }                                                             \
     } while (0)
@@ -62,13 +66,24 @@ cudaError_t dispatch_variant(L& launcher, Variant v) {
 #undef GO_RL
 #undef GO_SHAPES
 #undef GO_V
+#undef GO_VD
 }
 
 inline int shape_block_width(int shape) {
     switch (shape) {
-        case 2: case 4: return 128;
+        case 2: case 4: case 5: return 128;
         case 3: return 256;
         default: return 192;
+    }
+}
+
+// Resident blocks per SM the shape is compiled for (its __launch_bounds__).
+inline int shape_blocks_per_sm(int shape) {
+    switch (shape) {
+        case 0: case 3: return 2;
+        case 1: return 3;
+        case 2: return 4;
+        default: return 5;
     }
 }
 

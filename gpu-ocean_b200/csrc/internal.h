@@ -43,6 +43,7 @@ int go_check_pitch(int pitch_bytes, int min_floats, const char* what);
 // in [2, 16] nearest below (column strips x ny) / 600, so that small grids
 // still launch enough blocks to cover the 148 SMs.
 int go_auto_rows(int nx, int ny, int shape);
+int go_auto_shape(int nx, int ny);
 
 // Kernel-variant selectors of a domain.
 int go_friction_mode(const go_domain* d);

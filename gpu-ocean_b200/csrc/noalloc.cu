@@ -100,7 +100,7 @@ int fill_domain(const go_domain_desc& s, go_domain* d) {
     k.V = s.dx / k.two_g;
     k.U = s.dy / k.two_g;
     k.two_r = two * s.r;
-    d->shape = 4;
+    d->shape = go_auto_shape(s.nx, s.ny);
     d->rows_per_block = go_auto_rows(s.nx, s.ny, d->shape);
     d->arith = GO_ARITH_RCP;
     d->has_land = 1;

@@ -8,10 +8,10 @@ namespace {
 struct SingleLaunch {
     const StageArgs* a;
     cudaStream_t s;
-    template <int BW, int MINB, int FRIC, bool GN, bool WF, bool RCP, bool LAND>
+    template <int BW, int MINB, int FRIC, bool GN, bool WF, bool RCP, bool LAND, int D>
     cudaError_t run() {
         const dim3 grid((a->k.nx + (BW - 4) - 1) / (BW - 4), (a->k.ny + a->rows_per_block - 1) / a->rows_per_block);
-        cdklm_stage_kernel<BW, MINB, FRIC, GN, WF, RCP, LAND><<<grid, BW, 0, s>>>(*a);
+        cdklm_stage_kernel<BW, MINB, FRIC, GN, WF, RCP, LAND, D><<<grid, BW, 0, s>>>(*a);
         return cudaGetLastError();
     }
 };

@@ -53,6 +53,24 @@ def test_mixed_batch_equals_member_by_member(ctx):
         assert s.t == a.t
 
 
+@pytest.mark.parametrize("launch", [(5, 16, 0), (5, 3, 148 * 5), (4, 16, 148 * 5)])
+def test_batch_launch_shapes_equal_member_by_member(ctx, launch):
+    """The batched kernel under the read-ahead shape (5) and a persistent
+    grid that walks several tiles per block gives the member-by-member
+    states bit for bit."""
+    sizes = [256, 200, 320, 128]
+    alone = _members(ctx, sizes, seed0=43000)
+    for s in alone:
+        for _ in range(6):
+            s.step(s.dt)
+    expect = _states(alone)
+    sims = _members(ctx, sizes, seed0=43000)
+    b = BatchedEnsemble.BatchedCDKLM16(sims, launch=launch)
+    b.advance(6)
+    for e, g in zip(expect, _states(sims)):
+        assert np.array_equal(e, g)
+
+
 def test_graph_replay_equals_plain_launches(ctx):
     sims_a = _members(ctx, [256] * 4, seed0=41000)
     sims_b = _members(ctx, [256] * 4, seed0=41000)
