@@ -33,8 +33,10 @@ UNIT_FLAGS = {"adjoint.cu": {"--fmad=false": "--fmad=true"}}
 
 
 def flags_for(unit):
+    """nvcc flags of one source unit; GOCEAN_NVCC_FLAGS appends more (e.g.
+    -DGO_PACKED_PAIRS for the packed-sum build of the stage kernel)."""
     sub = UNIT_FLAGS.get(unit, {})
-    return [sub.get(f, f) for f in NVCC_FLAGS]
+    return [sub.get(f, f) for f in NVCC_FLAGS] + os.environ.get("GOCEAN_NVCC_FLAGS", "").split()
 
 
 def sources():
