@@ -19,9 +19,10 @@ import numpy as np
 from . import _native
 
 DOMAIN_CANDIDATES = [(4, 2), (4, 4), (4, 8), (4, 16), (4, 24), (4, 32), (5, 8), (5, 16), (5, 24), (5, 32),
-                     (2, 4), (2, 8), (2, 16), (2, 32), (1, 8), (1, 16), (1, 32), (3, 16), (0, 16)]
-BATCH_CANDIDATES = [(4, 8, 0), (4, 16, 0), (4, 32, 0), (5, 16, 0), (5, 24, 0), (2, 16, 0), (2, 32, 0), (1, 16, 0),
-                    (4, 16, 148 * 5), (5, 16, 148 * 5)]
+                     (6, 4), (6, 8), (6, 16), (6, 24), (6, 32), (7, 16), (7, 24), (2, 4), (2, 8), (2, 16),
+                     (1, 16), (3, 16), (0, 16)]
+BATCH_CANDIDATES = [(4, 16, 0), (4, 32, 0), (5, 16, 0), (5, 24, 0), (5, 32, 0), (6, 16, 0), (6, 24, 0), (6, 32, 0),
+                    (7, 32, 0), (2, 32, 0), (1, 16, 0), (5, 32, 148 * 5)]
 GRAPH_LENGTHS = [10, 50]
 
 

@@ -50,16 +50,16 @@ int go_auto_rows(int nx, int ny, int shape) {
     return best;
 }
 
-// Default launch shape: 128 x 5 blocks, with the read-ahead ring (shape 5)
-// once the grid needs more than one wave of blocks, where the ring hides
-// the load latency; in a single wave the register prefetch (shape 4) is
-// faster (measured on a B200: 2048^2 and up gain 3-5%, 1024^2 and below
-// lose 6-9% with the ring).
+// Default launch shape: a read-ahead shape (5, or 6 for widths that 96-wide
+// blocks cover with less waste) once the grid needs more than one wave of
+// blocks, where the ring hides the load latency; in a single wave the
+// register prefetch of 128 x 5 blocks (shape 4) is faster (measured on a
+// B200: 2048^2 and up gain 3-5% with the ring, 1024^2 and below lose 6-9%).
 int go_auto_shape(int nx, int ny) {
-    const int rows = go_auto_rows(nx, ny, 4);
-    const long long strips = (nx + go::shape_block_width(4) - 5) / (go::shape_block_width(4) - 4);
-    const long long blocks = strips * ((ny + rows - 1) / rows);
-    return blocks > 148LL * go::shape_blocks_per_sm(4) ? 5 : 4;
+    const int ring = go::ring_shape(go::shape_columns(5, nx), go::shape_columns(6, nx));
+    const int rows = go_auto_rows(nx, ny, ring);
+    const long long blocks = go::shape_columns(ring, nx) / go::shape_block_width(ring) * ((ny + rows - 1) / rows);
+    return blocks > 148LL * go::shape_blocks_per_sm(ring) ? ring : 4;
 }
 
 int go_friction_mode(const go_domain* d) {
@@ -313,7 +313,7 @@ int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_ne
 
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block) {
     if (!d) return go_fail(GO_ERR_INVALID, "null domain");
-    if (shape < 0 || shape > 5) return go_fail(GO_ERR_INVALID, "launch shape %d (0..5)", shape);
+    if (shape < 0 || shape > 7) return go_fail(GO_ERR_INVALID, "launch shape %d (0..7)", shape);
     if (rows_per_block == 0) rows_per_block = go_auto_rows(d->k.nx, d->k.ny, shape);
     if (rows_per_block < 1) return go_fail(GO_ERR_INVALID, "rows_per_block must be >= 1");
     d->shape = shape;

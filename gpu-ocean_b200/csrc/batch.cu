@@ -115,19 +115,26 @@ int go_batch_create(go_domain* const* members, int n, go_batch** out) {
     const go_domain* d0 = members[0];
     b->variant = go_variant(d0);
     b->arith = d0->arith;
-    // 24-row strips (a batch launches enough blocks for long strips); the
-    // read-ahead shape once the tiles need more than one wave of blocks
-    // (measured on a B200, 100 members of 512^2: 1597 us per step with
-    // 128 x 5 blocks of 16 rows, 1540 with the ring and 24 rows)
-    b->rows = 24;
-    b->shape = d0->shape;
-    if (b->shape == 4 || b->shape == 5) {
+    // 32-row strips (a batch launches enough blocks for long strips) and,
+    // once the tiles need more than one wave of blocks, the read-ahead shape
+    // with the less column work (measured on a B200, 100 members of 512^2:
+    // 1597 us per step with 128 x 5 blocks of 16 rows and register prefetch,
+    // 1532 with the ring, 1431 with 96-wide ring blocks and 32 rows).
+    b->rows = 32;
+    {
+        long long work5 = 0, work6 = 0;
+        for (int m = 0; m < n; ++m) {
+            const Scheme& k = members[m]->k;
+            work5 += shape_columns(5, k.nx) * k.ny;
+            work6 += shape_columns(6, k.nx) * k.ny;
+        }
+        const int ring = ring_shape(work5, work6);
         long long tiles = 0;
         for (int m = 0; m < n; ++m) {
             const Scheme& k = members[m]->k;
-            tiles += (long long)((k.nx + 123) / 124) * ((k.ny + b->rows - 1) / b->rows);
+            tiles += shape_columns(ring, k.nx) / shape_block_width(ring) * ((k.ny + b->rows - 1) / b->rows);
         }
-        b->shape = tiles > 148LL * shape_blocks_per_sm(4) ? 5 : 4;
+        b->shape = tiles > 148LL * shape_blocks_per_sm(ring) ? ring : 4;
     }
     for (int m = 1; m < n; ++m) {
         const go_domain* d = members[m];
@@ -190,7 +197,7 @@ int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, f
 
 int go_batch_set_launch(go_batch* b, int shape, int rows_per_block, int blocks) {
     if (!b) return go_fail(GO_ERR_INVALID, "null batch");
-    if (shape < 0 || shape > 5) return go_fail(GO_ERR_INVALID, "launch shape %d (0..5)", shape);
+    if (shape < 0 || shape > 7) return go_fail(GO_ERR_INVALID, "launch shape %d (0..7)", shape);
     if (rows_per_block == 0) rows_per_block = 16;
     if (rows_per_block < 1 || blocks < 0) return go_fail(GO_ERR_INVALID, "rows_per_block >= 1, blocks >= 0");
     b->shape = shape;

@@ -1,8 +1,8 @@
 // Kernel-variant selection shared by the single-domain and batched launchers.
 //
 // A variant is (launch shape, friction law, general grid angle, per-cell
-// wind, reciprocal quotients, land in the bathymetry).  Shape 5 is the
-// 128 x 5 block with the read-ahead ring.  Every variant gives
+// wind, reciprocal quotients, land in the bathymetry).  Shapes 5, 6 and 7
+// (128 x 5, 96 x 6 and 192 x 3 blocks) read ahead through the ring.  Every variant gives
 // the same results; the specialised ones drop work the general one would do
 // for nothing.  Instantiated set:
 //   * general: shape 4, every friction law, angle and wind combination, land
@@ -48,6 +48,8 @@ cudaError_t dispatch_variant(L& launcher, Variant v) {
             case 2: GO_V(128, 4, F, false, false, RCP, LAND);         \
             case 3: GO_V(256, 2, F, false, false, RCP, LAND);         \
             case 5: GO_VD(128, 5, F, false, false, RCP, LAND, kReadAhead); \
+            case 6: GO_VD(96, 6, F, false, false, RCP, LAND, kReadAhead); \
+            case 7: GO_VD(192, 3, F, false, false, RCP, LAND, kReadAhead); \
             default: GO_V(128, 5, F, false, false, RCP, LAND);        \
         }                                                             \
     } while (0)
@@ -73,16 +75,31 @@ inline int shape_block_width(int shape) {
     switch (shape) {
         case 2: case 4: case 5: return 128;
         case 3: return 256;
+        case 6: return 96;
         default: return 192;
     }
 }
+
+// Columns a shape computes for an nx-wide grid (strips x block width).
+inline long long shape_columns(int shape, int nx) {
+    const int w = shape_block_width(shape);
+    return (long long)((nx + w - 5) / (w - 4)) * w;
+}
+
+// The read-ahead shape for grids whose column work (sum over grids of
+// shape_columns x ny) is work5 with 128-wide and work6 with 96-wide blocks:
+// 96-wide blocks cost ~4% more per column (measured on a B200: 4096^2 686 vs
+// 710 us per step), so shape 6 only when it computes at least 4% fewer
+// columns (a 512-wide member: 576 columns against 640).
+inline int ring_shape(long long work5, long long work6) { return work6 * 100 < work5 * 96 ? 6 : 5; }
 
 // Resident blocks per SM the shape is compiled for (its __launch_bounds__).
 inline int shape_blocks_per_sm(int shape) {
     switch (shape) {
         case 0: case 3: return 2;
-        case 1: return 3;
+        case 1: case 7: return 3;
         case 2: return 4;
+        case 6: return 6;
         default: return 5;
     }
 }

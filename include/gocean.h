@@ -93,13 +93,15 @@ int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_ne
                              const float* y_cur, const float* y_next, int pitch);
 
 /* Launch shape of the step kernel: shape 0 = 192 threads x 2 blocks/SM,
- * 1 = 192 x 3, 2 = 128 x 4, 3 = 256 x 2, 4 = 128 x 5, 5 = 128 x 5 with each
- * thread reading its column's inputs two rows ahead through shared memory
- * (cp.async).  Default: shape 5 when the grid needs more than one wave of
- * blocks, else 4.  Each block marches down a strip of rows_per_block rows
- * (0 = automatic: the height in {2, 4, 8, 16, 24} that minimises whole waves
- * of blocks times the strip length plus its 4 recomputed halo rows).  Chosen
- * by the autotuner; every shape computes identical results. */
+ * 1 = 192 x 3, 2 = 128 x 4, 3 = 256 x 2, 4 = 128 x 5; 5 = 128 x 5, 6 = 96 x 6
+ * and 7 = 192 x 3 with each thread reading its column's inputs two rows
+ * ahead through shared memory (cp.async).  Default: when the grid needs more
+ * than one wave of blocks, shape 5, or 6 where 96-wide blocks compute at
+ * least 4% fewer columns; else 4.  Each block marches down a strip of
+ * rows_per_block rows (0 = automatic: the height in {2, 4, 8, 16, 24} that
+ * minimises whole waves of blocks times the strip length plus its 4
+ * recomputed halo rows).  Chosen by the autotuner; every shape computes
+ * identical results. */
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block);
 
 /* How quotients are evaluated.  EXACT keeps every '/' of the reference
@@ -185,9 +187,8 @@ int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, f
 
 /* Launch shape (as go_domain_set_launch) and persistent grid size: blocks
  * = 0 launches one block per tile, blocks > 0 that many blocks walking the
- * tile list.  Default: 24-row strips, one block per tile, shape 5 when the
- * tiles of all members need more than one wave of blocks (else member 0's
- * shape, 4 by default). */
+ * tile list.  Default: 32-row strips, one block per tile, and the shape
+ * chosen as for a single grid from the column work of all members. */
 int go_batch_set_launch(go_batch* b, int shape, int rows_per_block, int blocks);
 int go_batch_set_arith(go_batch* b, int mode);
 

@@ -53,7 +53,7 @@ def test_mixed_batch_equals_member_by_member(ctx):
         assert s.t == a.t
 
 
-@pytest.mark.parametrize("launch", [(5, 16, 0), (5, 3, 148 * 5), (4, 16, 148 * 5)])
+@pytest.mark.parametrize("launch", [(5, 16, 0), (5, 3, 148 * 5), (4, 16, 148 * 5), (6, 24, 0), (7, 5, 148 * 3)])
 def test_batch_launch_shapes_equal_member_by_member(ctx, launch):
     """The batched kernel under the read-ahead shape (5) and a persistent
     grid that walks several tiles per block gives the member-by-member

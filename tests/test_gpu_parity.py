@@ -305,7 +305,8 @@ def test_every_launch_shape_bit_identical(ctx, bc):
     are shorter than the ring, so the ring's refills, empty groups past the
     strip and slot wrap-around all run, at walls and at periodic sides."""
     c = SC.grf(600, ny=520, dx=1000.0, bc=bc, r=3.0e-3, steps=12)
-    launches = [(4, 0), (5, 0), (5, 3), (5, 7), (5, 24), (4, 5), (0, 16), (1, 16), (2, 16), (3, 16)]
+    launches = [(4, 0), (5, 0), (5, 3), (5, 7), (5, 24), (6, 5), (6, 24), (7, 3), (7, 24), (4, 5), (0, 16),
+                (1, 16), (2, 16), (3, 16)]
     base = None
     for shape, rows in launches:
         sim = _drop_in(ctx, c)
