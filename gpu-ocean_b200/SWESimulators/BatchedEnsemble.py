@@ -50,14 +50,26 @@ class BatchedCDKLM16:
 
     def _sync_members(self):
         # work queued on the members' own streams (uploads, perturbations)
-        # completes before the batched launch reads their buffers
+        # completes before the batched launch reads their buffers; inside
+        # run_events the members are touched only through the batch stream,
+        # so the loop orders them once at its start and end
+        if getattr(self, "_owned", False):
+            return
         for s in self.sims:
             self.stream.wait_stream(s.gpu_stream)
 
+    def _release_members(self):
+        # later work on a member's own stream waits for the batch's
+        if getattr(self, "_owned", False):
+            return
+        for s in self.sims:
+            s.gpu_stream.wait_stream(self.stream)
+
     def _first_step_bc(self):
+        # on the batch stream, after _sync_members
         for s in self.sims:
             if s.t == 0:
-                s.bc_kernel.boundaryCondition(s.gpu_stream, s.gpu_data.h0, s.gpu_data.hu0, s.gpu_data.hv0)
+                s.bc_kernel.boundaryCondition(self.stream, s.gpu_data.h0, s.gpu_data.hu0, s.gpu_data.hv0)
 
     def set_dt(self, dts):
         """Per-member time steps (sequence of n floats)."""
@@ -75,6 +87,7 @@ class BatchedCDKLM16:
         """n_steps RK2 steps of every member at its own dt (graph replays
         for whole multiples of the captured length, plain launches for the
         rest)."""
+        self._sync_members()
         self._first_step_bc()
         if self._time_varying_wind():
             # wind interpolated in time: rebind every member before each step
@@ -85,7 +98,6 @@ class BatchedCDKLM16:
                 self.batch.step(1, self.stream)
                 self._account(1)
             return [s.t for s in self.sims]
-        self._sync_members()
         done = 0
         if self.graph_steps:
             while n_steps - done >= self.graph_steps:
@@ -96,11 +108,16 @@ class BatchedCDKLM16:
         return [s.t for s in self.sims]
 
     def _account(self, n_steps):
+        self._release_members()
+        # t accumulates float64(dt) once per step, as CDKLM16.step does
+        # (members sharing t and dt share the sum)
+        sums = {}
         for s in self.sims:
-            s.gpu_stream.wait_stream(self.stream)
-            # t accumulates float64(dt) once per step, as CDKLM16.step does
-            steps = np.full(int(n_steps), np.float64(np.float32(s.dt)))
-            s.t = float(np.cumsum(np.concatenate([[np.float64(s.t)], steps]))[-1])
+            key = (float(s.t), float(np.float32(s.dt)))
+            if key not in sums:
+                steps = np.full(int(n_steps), np.float64(np.float32(s.dt)))
+                sums[key] = float(np.cumsum(np.concatenate([[np.float64(s.t)], steps]))[-1])
+            s.t = sums[key]
             s.num_iterations += n_steps
 
     def step(self, t_end):
@@ -140,28 +157,22 @@ class BatchedCDKLM16:
         _native.check(lib.go_batch_grf_perturb(self.batch.handle, _native.stream_handle(self.stream),
                                                int(key0) & 0xFFFFFFFF, int(event) & 0xFFFFFFFF, float(std),
                                                float(corr_cells), _native.ptr(buf), int(buf.numel())))
-        for s in self.sims:
-            s.gpu_stream.wait_stream(self.stream)
+        self._release_members()
 
     def model_error(self, event, std=0.05, corr_cells=15.0):
         from . import ModelError
         self.perturb(ModelError.MODEL_ERROR_SEED, event, std, corr_cells)
 
     def max_dt(self):
-        """Exact CFL limit of every member (one reduction launch per member
-        on the batch stream, one device-to-host read); numpy array of n."""
+        """Exact CFL limit of every member (one batched reduction launch on
+        the batch stream, one device-to-host read); numpy array of n.  Each
+        value equals the member's own go_max_dt."""
         torch = _native.require_cuda()
         if getattr(self, "_dt_all", None) is None or self._dt_all.numel() != self.n:
             self._dt_all = torch.empty(self.n, dtype=torch.float32, device="cuda")
-        lib = _native.load()
-        sh = _native.stream_handle(self.stream)
         self._sync_members()
-        for m, s in enumerate(self.sims):
-            g = s.gpu_data
-            _native.check(lib.go_max_dt(s._domain.handle, sh, _native.ptr(g.h0.tensor), _native.ptr(g.hu0.tensor),
-                                        _native.ptr(g.hv0.tensor), int(g.h0.pitch),
-                                        _native.ptr(s.bathymetry.Bm.tensor), int(s.bathymetry.Bm.pitch),
-                                        float(s.bathymetry.mask_value), _native.ptr(self._dt_all[m:m + 1])))
+        _native.check(_native.load().go_batch_max_dt(self.batch.handle, _native.stream_handle(self.stream),
+                                                     _native.ptr(self._dt_all)))
         self.stream.synchronize()
         return self._dt_all.cpu().numpy()
 
@@ -178,12 +189,18 @@ class BatchedCDKLM16:
         the members' CFL limits -- what the reference's ensembles do member
         by member (OceanNoiseEnsemble.py:506-531).  Returns the steps taken."""
         steps = 0
-        for e in range(int(first_event), int(first_event) + int(n_events)):
-            n0 = self.sims[0].num_iterations
-            self.step(interval)
-            steps += self.sims[0].num_iterations - n0
-            self.model_error(e, std, corr_cells)
-            self.update_dt(courant)
+        self._sync_members()
+        self._owned = True
+        try:
+            for e in range(int(first_event), int(first_event) + int(n_events)):
+                n0 = self.sims[0].num_iterations
+                self.step(interval)
+                steps += self.sims[0].num_iterations - n0
+                self.model_error(e, std, corr_cells)
+                self.update_dt(courant)
+        finally:
+            self._owned = False
+            self._release_members()
         return steps
 
     def synchronize(self):

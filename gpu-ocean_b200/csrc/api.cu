@@ -126,14 +126,8 @@ __global__ void k_init_bm(const float* Hi, int ph, float* Bm, int pb, int nx, in
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= nx + 4 || j >= ny + 4) return;
-    auto dry = [&](float v) { return (fabsf(v - land) <= kDryEps) ? kDryFlag : v; };
-    const float a = dry(Hi[(size_t)j * ph + i]);
-    const float b = dry(Hi[(size_t)(j + 1) * ph + i]);
-    const float c = dry(Hi[(size_t)j * ph + i + 1]);
-    const float d = dry(Hi[(size_t)(j + 1) * ph + i + 1]);
-    const float wet = 4.0f - (float)(a == kDryFlag) - (float)(b == kDryFlag) - (float)(c == kDryFlag) -
-                      (float)(d == kDryFlag);
-    Bm[(size_t)j * pb + i] = (wet == 0.0f) ? land : (a + b + c + d) / wet;
+    Bm[(size_t)j * pb + i] = cell_mean_depth(Hi[(size_t)j * ph + i], Hi[(size_t)(j + 1) * ph + i],
+                                             Hi[(size_t)j * ph + i + 1], Hi[(size_t)(j + 1) * ph + i + 1], land);
 }
 
 // ---------------------------------------------------------------------------
@@ -164,8 +158,6 @@ __global__ void k_periodic_ew(float* e, float* u, float* v, int p, int nx, int n
 // CFL limit (max_dt.cu:42-141), exact minimum over all interior cells.
 // ---------------------------------------------------------------------------
 
-constexpr float kRefFltMax = 100000.0f;   // max_dt.cu:30 redefines FLT_MAX
-
 __global__ void k_max_dt(const float* eta, const float* hu, const float* hv, int p,
                          const float* Bm, int pb, int nx, int ny, float dx, float dy, float g,
                          float land, unsigned int* out) {
@@ -173,30 +165,10 @@ __global__ void k_max_dt(const float* eta, const float* hu, const float* hv, int
     const int n = nx * ny;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
         const int j = idx / nx + 2, i = idx % nx + 2;
-        const float e = eta[(size_t)j * p + i];
-        const float H = Bm[(size_t)j * pb + i];
-        const float h = e + H;
-        if (h <= 0.0f || fabsf(H - land) < kDryEps) continue;
-        const float u = hu[(size_t)j * p + i] / h;
-        const float v = hv[(size_t)j * p + i] / h;
-        const float c = sqrtf(g * h);
-        float d = 0.25f * dx / fabsf(u + c);
-        d = fminf(d, 0.25f * dx / fabsf(u - c));
-        d = fminf(d, 0.25f * dy / fabsf(v + c));
-        d = fminf(d, 0.25f * dy / fabsf(v - c));
-        best = fminf(best, d);
+        const size_t o = (size_t)j * p + i;
+        best = fminf(best, cell_cfl_dt(eta[o], hu[o], hv[o], Bm[(size_t)j * pb + i], dx, dy, g, land, kRefFltMax));
     }
-    for (int off = 16; off > 0; off >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, off));
-    __shared__ float warp_min[32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) warp_min[w] = best;
-    __syncthreads();
-    if (w == 0) {
-        best = (lane < (int)(blockDim.x >> 5)) ? warp_min[lane] : kRefFltMax;
-        for (int off = 16; off > 0; off >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, off));
-        // positive floats order like their bit patterns
-        if (lane == 0) atomicMin(out, __float_as_uint(best));
-    }
+    block_min_to(best, out, kRefFltMax);
 }
 
 __global__ void k_fill_u32(unsigned int* p, unsigned int v) { *p = v; }

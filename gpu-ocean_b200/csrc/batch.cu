@@ -6,6 +6,7 @@
 // (gpu_ocean/SWESimulators/OceanNoiseEnsemble.py:506-531,
 // OceanModelEnsemble.py:105-117, EnsembleFromFiles.py:302-324), which issue
 // N_members x (2 step + up to 4 boundary) launches per time step from Python.
+#include <algorithm>
 #include <vector>
 
 #include "dispatch.cuh"
@@ -86,6 +87,30 @@ int batch_launch(go_batch* b, int rk_step, cudaStream_t s) {
     const cudaError_t e = dispatch_variant(L, v);
     if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "batch stage launch failed: %s", cudaGetErrorString(e));
     return GO_OK;
+}
+
+// CFL limit of every member in one launch: blockIdx.y is the member, whose
+// current state (h0) is the input of its stage-0 arguments; the cell-mean
+// bathymetry comes from the corners as the set-up computes it.
+__global__ void k_batch_max_dt(const StageArgs* __restrict__ args, unsigned int* __restrict__ out) {
+    const StageArgs& a = args[2 * blockIdx.y];
+    const Scheme& k = a.k;
+    const int n = k.nx * k.ny;
+    float best = kRefFltMax;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const int j = idx / k.nx + 2, i = idx % k.nx + 2;
+        const size_t o = (size_t)j * a.pin + i;
+        const float* H = a.Hi + (size_t)j * a.phi + i;
+        const float Hm = cell_mean_depth(H[0], H[a.phi], H[1], H[a.phi + 1], k.land);
+        best = fminf(best, cell_cfl_dt(a.eta_in[o], a.hu_in[o], a.hv_in[o], Hm, k.dx, k.dy, k.g, k.land,
+                                       kRefFltMax));
+    }
+    block_min_to(best, out + blockIdx.y, kRefFltMax);
+}
+
+__global__ void k_fill_members(unsigned int* p, unsigned int v, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
 }
 
 void drop_graph(go_batch* b) {
@@ -282,6 +307,24 @@ int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done) {
     if (!b->graph_exec) return go_fail(GO_ERR_INVALID, "no captured graph (go_batch_graph_capture)");
     GO_CUDA(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream));
     if (steps_done) *steps_done = b->graph_steps;
+    return GO_OK;
+}
+
+int go_batch_max_dt(go_batch* b, void* stream, float* dt_dev) {
+    if (!b || !dt_dev) return go_fail(GO_ERR_INVALID, "null argument");
+    int rc = batch_commit(b);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned int* out = reinterpret_cast<unsigned int*>(dt_dev);
+    unsigned int init_bits;
+    memcpy(&init_bits, &kRefFltMax, sizeof(init_bits));
+    k_fill_members<<<(b->n + 255) / 256, 256, 0, s>>>(out, init_bits, b->n);
+    long long most = 0;
+    for (const go_domain* d : b->members) most = std::max(most, (long long)d->k.nx * d->k.ny);
+    // about 4 blocks per SM in all, spread over the members
+    const int per_member = (int)std::max(1LL, std::min((most + 255) / 256, (148LL * 4 + b->n - 1) / b->n));
+    k_batch_max_dt<<<dim3(per_member, b->n), 256, 0, s>>>(b->d_args, out);
+    GO_CUDA(cudaGetLastError());
     return GO_OK;
 }
 

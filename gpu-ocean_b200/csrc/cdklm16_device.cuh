@@ -147,4 +147,49 @@ __device__ __forceinline__ float cell_bm(float a, float b, float c, float d, flo
     return s / wet;
 }
 
+// Cell-mean bathymetry of one cell from its four corners (initBm_kernel.cu:
+// 87-104): land corners are dry, the mean over the wet ones, the land value
+// when all four are land.  Shared by the bathymetry set-up and the batched
+// CFL reduction, so both give the same float.
+__device__ __forceinline__ float cell_mean_depth(float a, float b, float c, float d, float land) {
+    auto dry = [&](float v) { return (fabsf(v - land) <= kDryEps) ? kDryFlag : v; };
+    a = dry(a); b = dry(b); c = dry(c); d = dry(d);
+    const float wet = 4.0f - (float)(a == kDryFlag) - (float)(b == kDryFlag) - (float)(c == kDryFlag) -
+                      (float)(d == kDryFlag);
+    return (wet == 0.0f) ? land : (a + b + c + d) / wet;
+}
+
+constexpr float kRefFltMax = 100000.0f;   // max_dt.cu:30 redefines FLT_MAX
+
+// CFL limit of one interior cell (max_dt.cu:42-107): min of 0.25 dx/|u +- c|
+// and 0.25 dy/|v +- c|; `none` for a dry or land cell.
+__device__ __forceinline__ float cell_cfl_dt(float e, float hu, float hv, float H, float dx, float dy, float g,
+                                             float land, float none) {
+    const float h = e + H;
+    if (h <= 0.0f || fabsf(H - land) < kDryEps) return none;
+    const float u = hu / h;
+    const float v = hv / h;
+    const float c = sqrtf(g * h);
+    float d = 0.25f * dx / fabsf(u + c);
+    d = fminf(d, 0.25f * dx / fabsf(u - c));
+    d = fminf(d, 0.25f * dy / fabsf(v + c));
+    d = fminf(d, 0.25f * dy / fabsf(v - c));
+    return d;
+}
+
+// Block minimum of a positive float, then atomicMin on its bit pattern
+// (positive floats order like their bits).  Every thread of the block calls.
+__device__ __forceinline__ void block_min_to(float best, unsigned int* out, float none) {
+    for (int off = 16; off > 0; off >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, off));
+    __shared__ float warp_min[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) warp_min[w] = best;
+    __syncthreads();
+    if (w == 0) {
+        best = (lane < (int)(blockDim.x >> 5)) ? warp_min[lane] : none;
+        for (int off = 16; off > 0; off >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, off));
+        if (lane == 0) atomicMin(out, __float_as_uint(best));
+    }
+}
+
 }  // namespace go

@@ -84,24 +84,37 @@ __global__ void k_grf_xpass(const GrfMember* __restrict__ members, const GrfMemb
 }
 
 // y pass: eta += std * field at each interior cell; the periodic ghost
-// images of the changed cells are rewritten.
+// images of the changed cells are rewritten.  One block per 32 columns x
+// kYTile rows: the block's x-filtered noise column strip (kYTile + 2R rows)
+// is staged in shared memory once, instead of each output reading its 2R+1
+// taps from global memory.
+constexpr int kYTile = 64;
 __global__ void k_grf_ypass(const GrfMember* __restrict__ members, const GrfMember single, float std_dev,
                             const float* __restrict__ scratch, const GrfWeights W) {
+    __shared__ float strip[(kYTile + kGrfMaxTaps - 1) * 32];
     const GrfMember M = members ? members[blockIdx.z] : single;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= M.nx || y >= M.ny) return;
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y0 = blockIdx.y * kYTile;
+    if (y0 >= M.ny || (int)blockIdx.x * 32 >= M.nx) return;      // whole block
     const float* tmp = scratch + M.tmp_off;
-    float acc = 0.0f;
-    for (int d = 0; d <= 2 * W.R; ++d) acc += W.w[d] * tmp[(size_t)(y + d) * M.nx + x];
-    const int j = y + 2, i = x + 2;
-    const float v = M.eta[(size_t)j * M.pitch + i] + std_dev * acc;
-    M.eta[(size_t)j * M.pitch + i] = v;
-    const int rows[2] = {j, M.periodic_y ? ((j < 4) ? j + M.ny : (j >= M.ny ? j - M.ny : -1)) : -1};
-    const int cols[2] = {i, M.periodic_x ? ((i < 4) ? i + M.nx : (i >= M.nx ? i - M.nx : -1)) : -1};
-    for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b)
-            if ((a || b) && rows[a] >= 0 && cols[b] >= 0) M.eta[(size_t)rows[a] * M.pitch + cols[b]] = v;
+    const int rows = min(kYTile, M.ny - y0) + 2 * W.R;             // <= ny + 2R - y0
+    for (int r = threadIdx.y; r < rows; r += blockDim.y)
+        strip[r * 32 + threadIdx.x] = (x < M.nx) ? tmp[(size_t)(y0 + r) * M.nx + x] : 0.0f;
+    __syncthreads();
+    if (x >= M.nx) return;
+    for (int yy = threadIdx.y; yy < kYTile && y0 + yy < M.ny; yy += blockDim.y) {
+        float acc = 0.0f;
+        for (int d = 0; d <= 2 * W.R; ++d) acc += W.w[d] * strip[(yy + d) * 32 + threadIdx.x];
+        const int j = y0 + yy + 2, i = x + 2;
+        const float v = M.eta[(size_t)j * M.pitch + i] + std_dev * acc;
+        M.eta[(size_t)j * M.pitch + i] = v;
+        const int rows_img[2] = {j, M.periodic_y ? ((j < 4) ? j + M.ny : (j >= M.ny ? j - M.ny : -1)) : -1};
+        const int cols_img[2] = {i, M.periodic_x ? ((i < 4) ? i + M.nx : (i >= M.nx ? i - M.nx : -1)) : -1};
+        for (int a2 = 0; a2 < 2; ++a2)
+            for (int b2 = 0; b2 < 2; ++b2)
+                if ((a2 || b2) && rows_img[a2] >= 0 && cols_img[b2] >= 0)
+                    M.eta[(size_t)rows_img[a2] * M.pitch + cols_img[b2]] = v;
+    }
 }
 
 }  // namespace
@@ -133,7 +146,7 @@ int grf_launch(const GrfMember* d_members, const GrfMember& single, int n_member
     if (n_members < 1) return GO_OK;
     const dim3 gx((max_nx + kChunk - 1) / kChunk, max_ny + 2 * W.R, n_members);
     k_grf_xpass<<<gx, 256, 0, s>>>(d_members, single, key0, event, scratch, W);
-    const dim3 b(32, 8), gy((max_nx + 31) / 32, (max_ny + 7) / 8, n_members);
+    const dim3 b(32, 8), gy((max_nx + 31) / 32, (max_ny + kYTile - 1) / kYTile, n_members);
     k_grf_ypass<<<gy, b, 0, s>>>(d_members, single, std_dev, scratch, W);
     GO_CUDA(cudaGetLastError());
     return GO_OK;

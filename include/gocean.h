@@ -334,6 +334,15 @@ int go_grf_perturb(go_domain* d, void* stream, float* eta, int pitch, uint32_t k
                    uint32_t key1, uint32_t event, float std_dev, float corr_cells,
                    float* scratch, size_t scratch_floats);
 
+/* go_max_dt for every member of the batch in one launch, on the members'
+ * current state (h0): writes n floats to dt_dev (device), member order.
+ * The cell-mean bathymetry is recomputed from the corners as
+ * go_init_bathymetry computes it, so each value equals go_max_dt's.
+ * Replaces the per-member CFL reductions of the reference's ensembles
+ * (gpu_ocean/SWESimulators/OceanModelEnsemble.py:112-125, one updateDt
+ * per particle). */
+int go_batch_max_dt(go_batch* b, void* stream, float* dt_dev);
+
 /* Scratch floats go_batch_grf_perturb needs for all members. */
 size_t go_batch_grf_scratch_floats(go_batch* b, float corr_cells);
 

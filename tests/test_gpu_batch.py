@@ -71,6 +71,24 @@ def test_batch_launch_shapes_equal_member_by_member(ctx, launch):
         assert np.array_equal(e, g)
 
 
+def test_batched_max_dt_equals_member_max_dt(ctx):
+    """The one-launch CFL reduction over all members gives each member's own
+    exact limit bit for bit, on uneven sizes, after steps and with land."""
+    sims = _members(ctx, [128, 300, 96, 257], seed0=44000)
+    c = SC.grf(64, ny=40, dx=1000.0, seed_bathy=44100, steps=1)
+    Hi = c.Hi.copy()
+    Hi[10:20, 10:30] = 1.0e20                        # a land patch (the mask value)
+    kw = c.kwargs()
+    kw["H"] = Hi
+    sims.append(CDKLM16.CDKLM16(ctx, dt=c.dt, **kw))
+    b = BatchedEnsemble.BatchedCDKLM16(sims)
+    b.advance(3)
+    got = b.max_dt()
+    for m, s in enumerate(sims):
+        s.updateDt(courant_number=1.0)
+        assert np.float32(got[m]) == np.float32(s.dt), (m, got[m], s.dt)
+
+
 def test_graph_replay_equals_plain_launches(ctx):
     sims_a = _members(ctx, [256] * 4, seed0=41000)
     sims_b = _members(ctx, [256] * 4, seed0=41000)
