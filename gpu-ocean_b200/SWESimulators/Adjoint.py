@@ -139,6 +139,9 @@ class MisfitProblem:
         self.land = float(sim.bathymetry.mask_value)
         self.stream = torch.cuda.Stream()
         self.sh = _native.stream_handle(self.stream)
+        self._rstream = torch.cuda.Stream()        # segment recompute, beside the reverse sweep
+        self._rsh = _native.stream_handle(self._rstream)
+        self._qn2 = self._qs2 = None               # second trajectory buffer (allocated on first use)
         Pw = _round_up(self.nx, 32)
         self.wind = torch.zeros((2, self.ny, Pw), dtype=torch.float32, device="cuda")
         self.lam_wind = torch.zeros((2, self.ny, Pw), dtype=torch.float32, device="cuda")
@@ -179,8 +182,9 @@ class MisfitProblem:
         _native.check(self._lib().go_obs_adjoint(self.sh, slab.gs(i), self.lam.gs(0), self.nx, self.ny, o.n,
                                                  _native.ptr(o.ij), _native.ptr(o.values[k]), o.w_eta, o.w_vel))
 
-    def _traj_step(self, a_slab, ai, s_slab, si, b_slab, bi):
-        _native.check(self._lib().go_traj_step(self.domain.handle, self.sh, float(self.dt), 0.0, a_slab.gs(ai),
+    def _traj_step(self, a_slab, ai, s_slab, si, b_slab, bi, sh=None):
+        sh = self.sh if sh is None else sh
+        _native.check(self._lib().go_traj_step(self.domain.handle, sh, float(self.dt), 0.0, a_slab.gs(ai),
                                                s_slab.gs(si), b_slab.gs(bi), _native.ptr(self.Hi),
                                                self.Hi_pitch, self.land))
 
@@ -254,27 +258,59 @@ class MisfitProblem:
         lw = self.lam_wind
         self.stream.synchronize()
         self.domain.status(clear=True)
+        segs = self._segments()
+        last = len(segs) - 1
+        # Segment s reads its trajectory from buffer (last - s) % 2; the last
+        # segment's is buffer 0, kept by the forward pass.  The forward
+        # recompute of segment s-1 runs on a second stream into the other
+        # buffer while the adjoint sweeps segment s, so the recompute fills
+        # the SMs the adjoint leaves idle; events order each buffer's reuse.
+        if last > 0 and self._qn2 is None:
+            self._qn2 = StateSlab(self.k + 1, self.nx, self.ny)
+            self._qs2 = StateSlab(self.k, self.nx, self.ny)
+        bufs = [(self.qn, self.qs), (self._qn2, self._qs2)]
+        ready, freed = {}, {}
+
+        def recompute(s):
+            a, b = segs[s]
+            i = (last - s) % 2
+            qn, qs = bufs[i]
+            if i in freed:
+                self._rstream.wait_event(freed[i])
+            with torch.cuda.stream(self._rstream):
+                _copy_state(qn, 0, self.ckpt, s)
+                for t in range(b - a):
+                    self._traj_step(qn, t, qs, t, qn, t + 1, sh=self._rsh)
+            ready[s] = torch.cuda.Event()
+            ready[s].record(self._rstream)
+            self.recomputed_steps += b - a
+
         with torch.cuda.stream(self.stream):
             lam.t.zero_()
             lw.zero_()
-            segs = self._segments()
-            for s in range(len(segs) - 1, -1, -1):
+            if last > 0:
+                recompute(last - 1)
+            for s in range(last, -1, -1):
                 a, b = segs[s]
-                if s != len(segs) - 1:
-                    _copy_state(self.qn, 0, self.ckpt, s)
-                    for t in range(b - a):
-                        self._traj_step(self.qn, t, self.qs, t, self.qn, t + 1)
-                    self.recomputed_steps += b - a
+                i = (last - s) % 2
+                qn, qs = bufs[i]
+                if s != last:
+                    self.stream.wait_event(ready[s])
+                    if s > 0:
+                        recompute(s - 1)
                 for n in range(b - 1, a - 1, -1):
                     t = n - a
-                    self._obs_adjoint(self.qn, t + 1, n + 1)
+                    self._obs_adjoint(qn, t + 1, n + 1)
                     _native.check(lib.go_adjoint_step(
-                        self.domain.handle, self.sh, float(self.dt), self.qn.gs(t), self.qs.gs(t),
-                        self.qn.gs(t + 1), lam.gs(0), lam.gs(0), lam.gs(1), lam.gs(2), _native.ptr(lw[0]),
+                        self.domain.handle, self.sh, float(self.dt), qn.gs(t), qs.gs(t),
+                        qn.gs(t + 1), lam.gs(0), lam.gs(0), lam.gs(1), lam.gs(2), _native.ptr(lw[0]),
                         _native.ptr(lw[1]), self.wpitch, _native.ptr(self.Hi), self.Hi_pitch))
+                freed[i] = torch.cuda.Event()
+                freed[i].record(self.stream)
             if 0 in self.obs.index:
                 _copy_state(self.qn, 0, self.ckpt, 0)
                 self._obs_adjoint(self.qn, 0, 0)
+        self._rstream.synchronize()
         self.stream.synchronize()
         if self.domain.status() & _native.GO_STATUS_ADJ_SCOPE:
             raise NotImplementedError("the adjoint met land or a cell shallower than desing_eps")
