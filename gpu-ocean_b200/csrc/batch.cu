@@ -51,11 +51,37 @@ struct BatchLaunch {
     }
 };
 
+// Kernel variant of the members as set: friction law and grid angle from
+// the domains, per-cell wind from the member arguments (a member's wind
+// field is usually handed to its domain after the batch is created), land
+// checks if any member may hold land.
+int batch_variant(go_batch* b) {
+    Variant v = go_variant(b->members[0]);
+    v.wind_field = b->args[0].wx_cur != nullptr;
+    v.land = false;
+    for (int m = 0; m < b->n; ++m) {
+        const go_domain* d = b->members[m];
+        v.land = v.land || d->has_land;
+        if (go_friction_mode(d) != v.fric || go_general_north(d) != v.gen_north ||
+            (b->args[2 * m].wx_cur != nullptr) != v.wind_field)
+            return go_fail(GO_ERR_INVALID,
+                           "member %d needs a different kernel variant (friction law, grid angle or wind "
+                           "field) than member 0; use one batch per variant", m);
+    }
+    b->variant = v;
+    return GO_OK;
+}
+
 int batch_commit(go_batch* b) {
     if (!b->dirty) return GO_OK;
     for (int m = 0; m < b->n; ++m)
         if (!b->member_set[m]) return go_fail(GO_ERR_INVALID, "batch member %d has no state set", m);
-    const int width = shape_block_width(b->shape) - 4;
+    int rc = batch_variant(b);
+    if (rc) return rc;
+    Variant v = b->variant;
+    v.shape = b->shape;
+    v.rcp = b->arith == GO_ARITH_RCP;
+    const int width = dispatch_width(v) - 4;
     std::vector<int4> tiles;
     for (int m = 0; m < b->n; ++m) {
         const Scheme& k = b->members[m]->k;
@@ -163,13 +189,11 @@ int go_batch_create(go_domain* const* members, int n, go_batch** out) {
     }
     for (int m = 1; m < n; ++m) {
         const go_domain* d = members[m];
-        b->variant.land = b->variant.land || d->has_land;
-        if (go_friction_mode(d) != b->variant.fric || go_general_north(d) != b->variant.gen_north ||
-            (d->wx_cur != nullptr) != b->variant.wind_field) {
+        if (go_friction_mode(d) != b->variant.fric || go_general_north(d) != b->variant.gen_north) {
             delete b;
             return go_fail(GO_ERR_INVALID,
-                           "member %d needs a different kernel variant (friction law, grid angle or wind "
-                           "field) than member 0; use one batch per variant", m);
+                           "member %d needs a different kernel variant (friction law or grid angle) than "
+                           "member 0; use one batch per variant", m);
         }
     }
     b->args.resize(2 * n);
@@ -223,7 +247,7 @@ int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, f
 int go_batch_set_launch(go_batch* b, int shape, int rows_per_block, int blocks) {
     if (!b) return go_fail(GO_ERR_INVALID, "null batch");
     if (shape < 0 || shape > 7) return go_fail(GO_ERR_INVALID, "launch shape %d (0..7)", shape);
-    if (rows_per_block == 0) rows_per_block = 16;
+    if (rows_per_block == 0) rows_per_block = 32;
     if (rows_per_block < 1 || blocks < 0) return go_fail(GO_ERR_INVALID, "rows_per_block >= 1, blocks >= 0");
     b->shape = shape;
     b->rows = rows_per_block;

@@ -624,9 +624,13 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
             if (h >= k.cutoff && P0.e != kDryFlag) {
                 float X, Y;
                 if (WIND_FIELD) {
+                    // one load when the current and next fields are one array
                     const size_t o = (size_t)(j - 2) * a.pw + (cl - 2);
-                    X = a.wind_t * __ldg(a.wx_next + o) + (1.0f - a.wind_t) * __ldg(a.wx_cur + o);
-                    Y = a.wind_t * __ldg(a.wy_next + o) + (1.0f - a.wind_t) * __ldg(a.wy_cur + o);
+                    const float xn = __ldg(a.wx_next + o), yn = __ldg(a.wy_next + o);
+                    const float xc = (a.wx_cur == a.wx_next) ? xn : __ldg(a.wx_cur + o);
+                    const float yc = (a.wy_cur == a.wy_next) ? yn : __ldg(a.wy_cur + o);
+                    X = a.wind_t * xn + (1.0f - a.wind_t) * xc;
+                    Y = a.wind_t * yn + (1.0f - a.wind_t) * yc;
                 } else {
                     X = a.wind_t * a.wxn + (1.0f - a.wind_t) * a.wxc;
                     Y = a.wind_t * a.wyn + (1.0f - a.wind_t) * a.wyc;

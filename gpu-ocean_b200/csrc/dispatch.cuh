@@ -28,12 +28,20 @@ cudaError_t dispatch_variant(L& launcher, Variant v) {
 #define GO_VD(BW, MINB, F, GN, WF, RCP, LAND, D) return launcher.template run<BW, MINB, F, GN, WF, RCP, LAND, D>()
 #define GO_V(BW, MINB, F, GN, WF, RCP, LAND) GO_VD(BW, MINB, F, GN, WF, RCP, LAND, 0)
     if (v.gen_north || v.wind_field) {
-        // general variants: shape 4, land checks on, reciprocal quotients
+        // general variants: 128 x 5 blocks, reciprocal quotients; a rotated
+        // grid keeps the land checks on; the per-cell wind field of a
+        // north-up grid also has the read-ahead form (shapes 5-7) and a form
+        // without land checks
 #define GO_GEN(F)                                                     \
     do {                                                              \
         if (v.gen_north && v.wind_field) GO_V(128, 5, F, true, true, true, true);   \
         if (v.gen_north) GO_V(128, 5, F, true, false, true, true);    \
-        GO_V(128, 5, F, false, true, true, true);                     \
+        if (v.shape >= 5) {                                           \
+            if (v.land) GO_VD(128, 5, F, false, true, true, true, kReadAhead);   \
+            GO_VD(128, 5, F, false, true, true, false, kReadAhead);   \
+        }                                                             \
+        if (v.land) GO_V(128, 5, F, false, true, true, true);         \
+        GO_V(128, 5, F, false, true, true, false);                    \
     } while (0)
         if (v.fric == kFricNone) GO_GEN(kFricNone);
         if (v.fric == kFricQuad) GO_GEN(kFricQuad);
@@ -78,6 +86,13 @@ inline int shape_block_width(int shape) {
         case 6: return 96;
         default: return 192;
     }
+}
+
+// Block width of the kernel dispatch_variant launches for v: the general
+// variants and '/' quotients run 128-wide blocks whatever v.shape says.
+inline int dispatch_width(const Variant& v) {
+    if (v.gen_north || v.wind_field || !v.rcp) return 128;
+    return shape_block_width(v.shape);
 }
 
 // Columns a shape computes for an nx-wide grid (strips x block width).

@@ -71,6 +71,37 @@ def test_batch_launch_shapes_equal_member_by_member(ctx, launch):
         assert np.array_equal(e, g)
 
 
+def _wind_members(ctx, sizes, seed0=45000):
+    from SWESimulators.WindStress import WindStress
+    sims = []
+    for k, n in enumerate(sizes):
+        c = SC.grf(n, dx=1000.0, seed_bathy=seed0 + k, seed_bumps=seed0 + 500 + k, steps=1)
+        rng = np.random.default_rng(seed0 + 900 + k)
+        kw = c.kwargs()
+        kw["wind_stress"] = WindStress(t=[0], X=[rng.uniform(-0.2, 0.2, (6, 5)).astype(np.float32)],
+                                       Y=[rng.uniform(-0.2, 0.2, (6, 5)).astype(np.float32)])
+        sims.append(CDKLM16.CDKLM16(ctx, dt=c.dt, **kw))
+    return sims
+
+
+@pytest.mark.parametrize("launch", [(6, 16, 0), (5, 8, 0), (0, 16, 0), (4, 16, 148 * 5)])
+def test_wind_field_batch_equals_member_by_member(ctx, launch):
+    """Members with a per-cell wind field run the general kernel variant,
+    128-wide whatever the launch shape: the tile list follows the kernel's
+    width, and the read-ahead form gives the member-by-member states."""
+    sizes = [256, 200, 130]
+    alone = _wind_members(ctx, sizes)
+    for s in alone:
+        for _ in range(5):
+            s.step(s.dt)
+    expect = _states(alone)
+    sims = _wind_members(ctx, sizes)
+    b = BatchedEnsemble.BatchedCDKLM16(sims, launch=launch)
+    b.advance(5)
+    for e, g in zip(expect, _states(sims)):
+        assert np.array_equal(e, g)
+
+
 def test_batched_max_dt_equals_member_max_dt(ctx):
     """The one-launch CFL reduction over all members gives each member's own
     exact limit bit for bit, on uneven sizes, after steps and with land."""
