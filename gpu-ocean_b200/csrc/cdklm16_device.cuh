@@ -136,15 +136,20 @@ __device__ __forceinline__ float corner(float H, const Scheme& k) {
 }
 
 // initBm (initBm_kernel.cu:87-104) for corners a=(j,i) b=(j+1,i) c=(j,i+1)
-// d=(j+1,i+1), already dry-flagged.  Also returns the plain corner sum
-// whose quarter is the kernel's own-cell Hm (CDKLM16_kernel.cu:547).
+// d=(j+1,i+1), already dry-flagged, and s = ((a + b) + c) + d, the plain
+// corner sum whose quarter is the kernel's own-cell Hm (CDKLM16_kernel.cu:547).
+// The reference builds initBm_kernel.cu with nvcc's default options
+// (Common.py:1376 passes no compile flags), so its s / wet is the IEEE
+// round-to-nearest quotient, not the approximate division the CDKLM16
+// kernel's --prec-div=false gives: __fdiv_rn keeps that rounding (they
+// differ by an ulp for some sums over 3 wet corners).
 __device__ __forceinline__ float cell_bm(float a, float b, float c, float d, float s,
                                          const Scheme& k) {
     const float wet = 4.0f - (float)(a == kDryFlag) - (float)(b == kDryFlag)
                     - (float)(c == kDryFlag) - (float)(d == kDryFlag);
     if (wet == 4.0f) return s * 0.25f;   // s/4 is exact scaling
     if (wet == 0.0f) return k.land;
-    return s / wet;
+    return __fdiv_rn(s, wet);
 }
 
 // Cell-mean bathymetry of one cell from its four corners (initBm_kernel.cu:
@@ -156,24 +161,27 @@ __device__ __forceinline__ float cell_mean_depth(float a, float b, float c, floa
     a = dry(a); b = dry(b); c = dry(c); d = dry(d);
     const float wet = 4.0f - (float)(a == kDryFlag) - (float)(b == kDryFlag) - (float)(c == kDryFlag) -
                       (float)(d == kDryFlag);
-    return (wet == 0.0f) ? land : (a + b + c + d) / wet;
+    return (wet == 0.0f) ? land : __fdiv_rn(a + b + c + d, wet);   // IEEE quotient, as cell_bm
 }
 
 constexpr float kRefFltMax = 100000.0f;   // max_dt.cu:30 redefines FLT_MAX
 
 // CFL limit of one interior cell (max_dt.cu:42-107): min of 0.25 dx/|u +- c|
-// and 0.25 dy/|v +- c|; `none` for a dry or land cell.
+// and 0.25 dy/|v +- c|; `none` for a dry or land cell.  The reference builds
+// max_dt.cu with nvcc's default options (CDKLM16.py:221 passes no compile
+// flags): its quotients and square root are IEEE round-to-nearest, kept here
+// with __fdiv_rn / __fsqrt_rn whatever this library's own flags are.
 __device__ __forceinline__ float cell_cfl_dt(float e, float hu, float hv, float H, float dx, float dy, float g,
                                              float land, float none) {
     const float h = e + H;
     if (h <= 0.0f || fabsf(H - land) < kDryEps) return none;
-    const float u = hu / h;
-    const float v = hv / h;
-    const float c = sqrtf(g * h);
-    float d = 0.25f * dx / fabsf(u + c);
-    d = fminf(d, 0.25f * dx / fabsf(u - c));
-    d = fminf(d, 0.25f * dy / fabsf(v + c));
-    d = fminf(d, 0.25f * dy / fabsf(v - c));
+    const float u = __fdiv_rn(hu, h);
+    const float v = __fdiv_rn(hv, h);
+    const float c = __fsqrt_rn(g * h);
+    float d = __fdiv_rn(0.25f * dx, fabsf(u + c));
+    d = fminf(d, __fdiv_rn(0.25f * dx, fabsf(u - c)));
+    d = fminf(d, __fdiv_rn(0.25f * dy, fabsf(v + c)));
+    d = fminf(d, __fdiv_rn(0.25f * dy, fabsf(v - c)));
     return d;
 }
 

@@ -205,6 +205,40 @@ def test_small_beta_friction_wind_periodic_vs_reference_kernel(ctx):
     assert max(e64) <= 2e-2
 
 
+@pytest.mark.parametrize("launch", [(4, 0), (5, 8), (6, 8)])
+def test_land_vs_reference_kernel(ctx, launch):
+    """Land in the bathymetry (corner depths at the land value 1e20): an
+    island and a strip along the south-west coast in the 96x80 config-2
+    physics, 200 steps against the reference kernel, under the register
+    prefetch and both read-ahead shapes."""
+    cfgd = build_ref.CONFIGS["small_beta"]
+    c = SC.grf(96, dx=500.0, steps=200)
+    ny = cfgd["ny"]
+    c.ny = ny
+    c.Hi = np.ascontiguousarray(c.Hi[: ny + 5])
+    c.eta0 = np.ascontiguousarray(c.eta0[: ny + 4])
+    c.hu0 = np.zeros_like(c.eta0)
+    c.hv0 = np.zeros_like(c.eta0)
+    c.dt = SC.cfl_dt(c)                              # before the land goes in
+    Hi = c.Hi.copy()
+    Hi[30:42, 40:58] = 1.0e20                        # island
+    Hi[2:14, 2:9] = 1.0e20                           # coast in the south-west corner
+    c.Hi = O.fix_bi_ghost_corners(Hi, c.nx, c.ny, c.bc)
+    sim = _drop_in(ctx, c)
+    sim._domain.set_launch(*launch)
+    for _ in range(c.steps):
+        sim.step(c.dt)
+    mine = sim.download()
+    assert sim.status() == 0
+    ref = _ref_for("small_beta", c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, c.bc, wind=c.wind)
+    for _ in range(c.steps):
+        ref.step(c.dt)
+    theirs = ref.download()
+    errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
+    print("land, launch", launch, "200 steps vs reference kernel:", errs)
+    assert max(errs) <= 1e-5
+
+
 def test_single_stage_each_rk_step_vs_reference_kernel(ctx):
     """One call of each RK sub-step through the kernel-level ABI
     (go_cdklm_swe_2D vs the reference cdklm_swe_2D) on a perturbed state."""
