@@ -81,13 +81,8 @@ class Simulator(object):
                                         np.asarray(ws.Y[t0_index]).reshape(-1)[0],
                                         np.asarray(ws.Y[t1_index]).reshape(-1)[0])
             else:
-                torch = _native.require_cuda()
-                arrs = [sample_at_cells(ws.X[t0_index], int(self.nx), int(self.ny)),
-                        sample_at_cells(ws.X[t1_index], int(self.nx), int(self.ny)),
-                        sample_at_cells(ws.Y[t0_index], int(self.nx), int(self.ny)),
-                        sample_at_cells(ws.Y[t1_index], int(self.nx), int(self.ny))]
-                with torch.cuda.stream(self.gpu_stream):
-                    tens = [torch.from_numpy(a).to("cuda") for a in arrs]
+                tens = [sample_at_cells(a, int(self.nx), int(self.ny), self.gpu_stream)
+                        for a in (ws.X[t0_index], ws.X[t1_index], ws.Y[t0_index], ws.Y[t1_index])]
                 self._wind_field_tensors = tens
                 domain.set_wind_field(*tens)
         elapsed_since_t0 = (self.t - new_t0)

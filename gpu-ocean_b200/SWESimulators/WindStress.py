@@ -33,32 +33,21 @@ class WindStress:
         return all(np.asarray(a).size == 1 for a in self.X) and all(np.asarray(a).size == 1 for a in self.Y)
 
 
-def sample_at_cells(field, nx, ny):
-    """Sample a wind array the way the reference's normalized, bilinear,
-    clamped texture lookup does at each interior cell
-    (common.cu:616-650 called with ti+0.5, tj+0.5 and NX, NY at
-    CDKLM16_kernel.cu:827-828): s = (i+2+0.5)/nx, t = (j+2+0.5)/ny for
-    interior indices i, j.  Weights are exact here; the texture unit
-    quantises them to 1/256.  Returns an (ny, nx) float32 array."""
-    a = np.asarray(field, dtype=np.float64)
-    H, W = a.shape
-    s = (np.arange(nx) + 2.5) / float(nx)
-    t = (np.arange(ny) + 2.5) / float(ny)
-    x = s * W - 0.5
-    y = t * H - 0.5
-    x0 = np.floor(x).astype(np.int64)
-    y0 = np.floor(y).astype(np.int64)
-    ax = x - x0
-    ay = y - y0
-    xi0 = np.clip(x0, 0, W - 1)
-    xi1 = np.clip(x0 + 1, 0, W - 1)
-    yi0 = np.clip(y0, 0, H - 1)
-    yi1 = np.clip(y0 + 1, 0, H - 1)
-    v00 = a[np.ix_(yi0, xi0)]
-    v01 = a[np.ix_(yi0, xi1)]
-    v10 = a[np.ix_(yi1, xi0)]
-    v11 = a[np.ix_(yi1, xi1)]
-    AX = ax[None, :]
-    AY = ay[:, None]
-    out = (1 - AY) * ((1 - AX) * v00 + AX * v01) + AY * ((1 - AX) * v10 + AX * v11)
-    return out.astype(np.float32)
+def sample_at_cells(field, nx, ny, stream=None):
+    """The wind array sampled at each interior cell of an nx x ny grid the
+    way the reference's kernel reads its wind texture (common.cu:616-650
+    called with ti+0.5, tj+0.5 and NX, NY at CDKLM16_kernel.cu:827-828):
+    a bilinear, clamped, normalised texture lookup at
+    ((i+2+0.5)/nx, (j+2+0.5)/ny), done on the GPU by go_sample_wind so the
+    texture unit's fixed-point filter weights are the reference's.
+    Returns a (ny, nx) float32 device tensor."""
+    from . import _native
+    torch = _native.require_cuda()
+    a = np.ascontiguousarray(np.asarray(field, dtype=np.float32))
+    if a.ndim != 2:
+        raise ValueError("a wind stress field is a 2-D array")
+    out = torch.empty((int(ny), int(nx)), dtype=torch.float32, device="cuda")
+    _native.check(_native.load().go_sample_wind(
+        _native.stream_handle(stream), a.ctypes.data_as(_native.ctypes.c_void_p), int(a.shape[1]),
+        int(a.shape[0]), int(nx), int(ny), _native.ptr(out), int(nx) * 4))
+    return out

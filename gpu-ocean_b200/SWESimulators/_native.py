@@ -95,6 +95,7 @@ SIGNATURES = {
     "go_batch_grf_perturb": (_I, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, _F, _F, _P, ctypes.c_size_t]),
     "go_max_dt": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _F, _P]),
     "go_batch_max_dt": (_I, [_P, _P, _P]),
+    "go_sample_wind": (_I, [_P, _P, _I, _I, _I, _I, _P, _I]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),
     "go_batch_destroy": (_I, [_P]),

@@ -92,6 +92,18 @@ int go_domain_set_wind_uniform(go_domain* d, float x_cur, float x_next,
 int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_next,
                              const float* y_cur, const float* y_next, int pitch);
 
+/* Samples a wind stress array (host, h rows x w columns, row-major) at the
+ * interior cells of an nx x ny grid into out (device, ny rows, pitch in
+ * bytes) the way the reference's kernel reads its wind textures
+ * (gpu_ocean/SWESimulators/gpu_kernels/common.cu:616-650,
+ * gpu_ocean/SWESimulators/Simulator.py:171-213): one bilinear, clamped,
+ * normalised texture lookup per cell at ((i + 2.5) / nx, (j + 2.5) / ny),
+ * so the values equal the reference's.  Synchronises the stream (a set-up
+ * call, once per wind interval).  Hand the result to
+ * go_domain_set_wind_field. */
+int go_sample_wind(void* stream, const float* field, int w, int h, int nx, int ny, float* out,
+                   int out_pitch);
+
 /* Launch shape of the step kernel: shape 0 = 192 threads x 2 blocks/SM,
  * 1 = 192 x 3, 2 = 128 x 4, 3 = 256 x 2, 4 = 128 x 5; 5 = 128 x 5, 6 = 96 x 6
  * and 7 = 192 x 3 with each thread reading its column's inputs two rows

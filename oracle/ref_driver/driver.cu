@@ -77,6 +77,17 @@ int ref_setup(const float* f_host, int fw, int fh, float angle, float wxc, float
     return e;
 }
 
+// Non-uniform wind: current/next X and Y arrays (host, h x w each) bound as
+// the wind textures (Simulator.py:171-213 setTexture).
+int ref_set_wind(const float* xc, const float* xn, const float* yc, const float* yn, int w, int h) {
+    int e = make_tex(g_wxc, xc, w, h);
+    if (!e) e = make_tex(g_wxn, xn, w, h);
+    if (!e) e = make_tex(g_wyc, yc, w, h);
+    if (!e) e = make_tex(g_wyn, yn, w, h);
+    if (!e) e = refk_set_textures(g_angle.obj, g_f.obj, g_wxc.obj, g_wxn.obj, g_wyc.obj, g_wyn.obj);
+    return e;
+}
+
 int ref_bathymetry(void* s, int bc_north, int bc_east, float* Bi, int pbi, float land, float* Bm, int pbm) {
     return refb_bathymetry((cudaStream_t)s, NX, NY, bc_north == 2, bc_east == 2, Bi, pbi, land, Bm, pbm);
 }

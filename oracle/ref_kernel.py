@@ -34,6 +34,7 @@ def _load(cfg, fmad=False):
     lib = ctypes.CDLL(path)
     lib.ref_config.argtypes = [ctypes.POINTER(_I), ctypes.POINTER(_I)] + [ctypes.POINTER(_F)] * 4
     lib.ref_setup.argtypes = [ctypes.POINTER(_F), _I, _I, _F, _F, _F, _F, _F]
+    lib.ref_set_wind.argtypes = [ctypes.POINTER(_F)] * 4 + [_I, _I]
     lib.ref_bathymetry.argtypes = [_P, _I, _I, _P, _I, _F, _P, _I]
     lib.ref_boundary.argtypes = [_P, _I, _I, _P, _P, _P, _I]
     lib.ref_stage.argtypes = [_P, _F, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _I, _F, _F, _I]
@@ -56,7 +57,7 @@ class RefKernelSim:
     beta-plane, uniform wind, angle 0)."""
 
     def __init__(self, cfg, eta0, hu0, hv0, Hi, dt, f, coriolis_beta=0.0, bc=(1, 1, 1, 1),
-                 wind=(0.0, 0.0), fmad=False, f_rows=None):
+                 wind=(0.0, 0.0), fmad=False, f_rows=None, wind_fields=None):
         import torch
         self.torch = torch
         self.lib = _load(cfg, fmad)
@@ -74,6 +75,13 @@ class RefKernelSim:
         fh, fw = ftex.shape
         _chk(self.lib.ref_setup(ftex.ctypes.data_as(ctypes.POINTER(_F)), fw, fh, 0.0,
                                 float(wind[0]), float(wind[0]), float(wind[1]), float(wind[1])), "setup")
+        if wind_fields is not None:
+            # (X current, X next, Y current, Y next) arrays of one shape
+            arrs = [np.ascontiguousarray(np.asarray(a, dtype=np.float32)) for a in wind_fields]
+            wh, ww = arrs[0].shape
+            _chk(self.lib.ref_set_wind(*[a.ctypes.data_as(ctypes.POINTER(_F)) for a in arrs], ww, wh),
+                 "set_wind")
+            self._wind_fields = arrs
         dev = "cuda"
         self.stream = torch.cuda.current_stream()
         s = ctypes.c_void_p(int(self.stream.cuda_stream))

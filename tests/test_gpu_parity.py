@@ -239,6 +239,67 @@ def test_land_vs_reference_kernel(ctx, launch):
     assert max(errs) <= 1e-5
 
 
+def test_wind_field_vs_reference_kernel(ctx):
+    """Non-uniform wind stress (6 x 7 arrays, bilinear texture lookup in the
+    reference): the drop-in simulator over 120 steps, and single RK
+    sub-steps with different current and next fields at time weight 0.37,
+    against the reference kernel, bit for bit."""
+    from SWESimulators.WindStress import WindStress, sample_at_cells
+    cfgd = build_ref.CONFIGS["small_beta"]
+    nx, ny = cfgd["nx"], cfgd["ny"]
+    c = SC.grf(96, dx=500.0, steps=120)
+    c.ny = ny
+    c.Hi = O.fix_bi_ghost_corners(np.ascontiguousarray(c.Hi[: ny + 5]), nx, ny, c.bc)
+    c.eta0 = np.ascontiguousarray(c.eta0[: ny + 4])
+    c.hu0 = np.zeros_like(c.eta0)
+    c.hv0 = np.zeros_like(c.eta0)
+    c.dt = SC.cfl_dt(c)
+    rng = np.random.default_rng(11)
+    Xc, Xn, Yc, Yn = (rng.uniform(-3e-4, 3e-4, (6, 7)).astype(np.float32) for _ in range(4))
+    kw = c.kwargs()
+    kw["wind_stress"] = WindStress(t=[0], X=[Xc], Y=[Yc])
+    sim = CDKLM16.CDKLM16(ctx, dt=c.dt, **kw)
+    for _ in range(c.steps):
+        sim.step(c.dt)
+    mine = sim.download()
+    if not ref_kernel.available(cfgd):
+        pytest.skip("reference kernel library not built")
+    ref = ref_kernel.RefKernelSim(cfgd, c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, c.bc,
+                                  wind_fields=(Xc, Xc, Yc, Yc))
+    for _ in range(c.steps):
+        ref.step(c.dt)
+    theirs = ref.download()
+    errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
+    print("wind field, 120 steps vs reference kernel:", errs)
+    assert max(errs) == 0.0
+
+    # single sub-steps, current != next, wind_t = 0.37
+    ref = ref_kernel.RefKernelSim(cfgd, c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, c.bc,
+                                  wind_fields=(Xc, Xn, Yc, Yn))
+    for _ in range(10):
+        ref.step(c.dt)
+    dom = _native.Domain(nx, ny, 500.0, 500.0, 9.81, 3e-3, bc=c.bc)
+    dom.set_coriolis(O.coriolis_rows(c.f, c.beta, ny, 500.0))
+    fields = [sample_at_cells(a, nx, ny) for a in (Xc, Xn, Yc, Yn)]
+    dom.set_wind_field(*fields)
+    Hi_t = torch.from_numpy(c.Hi).cuda()
+    dt = float(np.float32(c.dt))
+    for k in (0, 1):
+        qin = [a.clone() for a in ref.h0]
+        qout = [a.clone() for a in ref.h0]
+        ref.boundary(qin)
+        mine_out = [a.clone() for a in qout]
+        ref.stage(k, dt, qin, qout, wind_t=0.37)
+        p = (nx + 4) * 4
+        _native.check(_native.load().go_cdklm_swe_2D(
+            dom.handle, None, dt, k, _native.ptr(qin[0]), p, _native.ptr(qin[1]), p, _native.ptr(qin[2]), p,
+            _native.ptr(mine_out[0]), p, _native.ptr(mine_out[1]), p, _native.ptr(mine_out[2]), p,
+            _native.ptr(Hi_t), (nx + 5) * 4, None, 0, 1e20, 0.37, dom.bc_packed))
+        torch.cuda.synchronize()
+        for a, b in zip(mine_out, qout):
+            assert torch.equal(a[2:-2, 2:-2], b[2:-2, 2:-2]), k
+
+
 def test_single_stage_each_rk_step_vs_reference_kernel(ctx):
     """One call of each RK sub-step through the kernel-level ABI
     (go_cdklm_swe_2D vs the reference cdklm_swe_2D) on a perturbed state."""
