@@ -80,7 +80,9 @@ class CDKLM16(Simulator.Simulator):
             desing_eps=desingularization_eps, flux_slope_eps=flux_slope_eps, depth_cutoff=depth_cutoff,
             bc=boundary_conditions.codes(),
             friction_law=_native.GO_FRICTION_LINEAR if linear_friction else _native.GO_FRICTION_QUADRATIC,
-            north=(np.float32(north[0]), np.float32(north[1])))
+            # the kernel's north vector: sinf/cosf of the float angle on the
+            # device, as the reference's getNorth (CDKLM16_kernel.cu:68-77)
+            north=_native.north_vector(np.float32(a0)) if a0 != 0.0 else (np.float32(0.0), np.float32(1.0)))
 
         self.bathymetry = Common.Bathymetry(gpu_ctx, self.gpu_stream, nx, ny, ghost_cells_x, ghost_cells_y,
                                             H, boundary_conditions)

@@ -96,6 +96,7 @@ SIGNATURES = {
     "go_max_dt": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _F, _P]),
     "go_batch_max_dt": (_I, [_P, _P, _P]),
     "go_sample_wind": (_I, [_P, _P, _I, _I, _I, _I, _P, _I]),
+    "go_north_vector": (_I, [_F, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),
     "go_batch_destroy": (_I, [_P]),
@@ -156,6 +157,14 @@ def stream_handle(stream):
     if stream is None:
         return ctypes.c_void_p(0)
     return ctypes.c_void_p(int(stream.cuda_stream))
+
+
+def north_vector(angle):
+    """(sin a, cos a) of a float32 grid angle as the device computes it
+    (go_north_vector)."""
+    nx_, ny_ = ctypes.c_float(), ctypes.c_float()
+    check(load().go_north_vector(float(np.float32(angle)), ctypes.byref(nx_), ctypes.byref(ny_)))
+    return np.float32(nx_.value), np.float32(ny_.value)
 
 
 def pack_bc(north, east, south, west):

@@ -1,4 +1,5 @@
-// Wind stress sampled at the cells, as the reference's kernel samples it.
+// Wind stress sampled at the cells, and the north vector of a constant grid
+// angle, as the reference's kernel forms them from its textures.
 //
 // The reference binds each wind array (any size) to a texture with bilinear
 // filtering, clamped addressing and normalised coordinates
@@ -29,7 +30,29 @@ __global__ void k_sample_wind(cudaTextureObject_t tex, int nx, int ny, float* ou
     out[(size_t)j * pitch + i] = tex2D<float>(tex, s, t);
 }
 
+// North vector of a constant grid angle, as getNorth forms it on the device
+// (CDKLM16_kernel.cu:68-77): sinf and cosf of the float angle.
+__global__ void k_north(float angle, float* out) {
+    out[0] = sinf(angle);
+    out[1] = cosf(angle);
+}
+
 }  // namespace
+
+extern "C" int go_north_vector(float angle, float* north_x, float* north_y) {
+    if (!north_x || !north_y) return go_fail(GO_ERR_INVALID, "null argument");
+    float* d = nullptr;
+    GO_CUDA(cudaMalloc(&d, 2 * sizeof(float)));
+    float h[2] = {0.0f, 1.0f};
+    k_north<<<1, 1>>>(angle, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "north vector: %s", cudaGetErrorString(e));
+    *north_x = h[0];
+    *north_y = h[1];
+    return GO_OK;
+}
 
 extern "C" int go_sample_wind(void* stream, const float* field, int w, int h, int nx, int ny, float* out,
                               int out_pitch) {

@@ -92,6 +92,12 @@ int go_domain_set_wind_uniform(go_domain* d, float x_cur, float x_next,
 int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_next,
                              const float* y_cur, const float* y_next, int pitch);
 
+/* North vector (sin a, cos a) of a constant grid angle a, computed on the
+ * device with sinf/cosf as the reference's kernel forms it from its angle
+ * texture (gpu_ocean/SWESimulators/gpu_kernels/CDKLM16_kernel.cu:68-77), for
+ * go_domain_desc.north_x / north_y.  Synchronous (a set-up call). */
+int go_north_vector(float angle, float* north_x, float* north_y);
+
 /* Samples a wind stress array (host, h rows x w columns, row-major) at the
  * interior cells of an nx x ny grid into out (device, ny rows, pitch in
  * bytes) the way the reference's kernel reads its wind textures

@@ -54,10 +54,10 @@ def _p(t):
 
 class RefKernelSim:
     """Reference CDKLM16 RK2 simulation on the GPU (wall/periodic, f- or
-    beta-plane, uniform wind, angle 0)."""
+    beta-plane, uniform wind or wind arrays, a constant grid angle)."""
 
     def __init__(self, cfg, eta0, hu0, hv0, Hi, dt, f, coriolis_beta=0.0, bc=(1, 1, 1, 1),
-                 wind=(0.0, 0.0), fmad=False, f_rows=None, wind_fields=None):
+                 wind=(0.0, 0.0), fmad=False, f_rows=None, wind_fields=None, angle=0.0):
         import torch
         self.torch = torch
         self.lib = _load(cfg, fmad)
@@ -73,7 +73,7 @@ class RefKernelSim:
         if f_rows is not None:
             ftex = np.ascontiguousarray(np.repeat(np.asarray(f_rows, np.float32)[:, None], nx + 4, axis=1))
         fh, fw = ftex.shape
-        _chk(self.lib.ref_setup(ftex.ctypes.data_as(ctypes.POINTER(_F)), fw, fh, 0.0,
+        _chk(self.lib.ref_setup(ftex.ctypes.data_as(ctypes.POINTER(_F)), fw, fh, float(np.float32(angle)),
                                 float(wind[0]), float(wind[0]), float(wind[1]), float(wind[1])), "setup")
         if wind_fields is not None:
             # (X current, X next, Y current, Y next) arrays of one shape
