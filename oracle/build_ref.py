@@ -41,6 +41,9 @@ CONFIGS = {
     "bump256": dict(nx=256, ny=256, dx=200.0, dy=200.0, g=9.81, r=0.0),
     "small_beta": dict(nx=96, ny=80, dx=500.0, dy=500.0, g=9.81, r=3e-3),
     "grf4096": dict(nx=4096, ny=4096, dx=500.0, dy=500.0, g=9.81, r=3e-3),
+    # the kernel's linear friction branch (CDKLM16_kernel.cu:884-886), which
+    # the reference host never enables, built with use_linear_friction
+    "small_linear": dict(nx=96, ny=80, dx=500.0, dy=500.0, g=9.81, r=3e-3, linear=True),
 }
 
 
@@ -52,6 +55,8 @@ def _fmt(x):
 
 def lib_name(cfg, fmad=False):
     tag = "nx%d_ny%d_dx%g_dy%g_g%g_r%g" % (cfg["nx"], cfg["ny"], cfg["dx"], cfg["dy"], cfg["g"], cfg["r"])
+    if cfg.get("linear"):
+        tag += "_linear"
     return os.path.join(OUT, "libref_cdklm16_%s%s.so" % (tag, "_fmad" if fmad else ""))
 
 
@@ -97,6 +102,8 @@ def build_one(src_dir, cfg, fmad=False):
                  "-DKPSIMULATOR_DEPTH_CUTOFF=" + _fmt(1e-5), "-DTHETA=" + _fmt(1.3), "-DRK_ORDER=2",
                  "-DNX=%d" % cfg["nx"], "-DNY=%d" % cfg["ny"], "-DDX=" + _fmt(cfg["dx"]),
                  "-DDY=" + _fmt(cfg["dy"]), "-DGRAV=" + _fmt(cfg["g"]), "-DFRIC=" + _fmt(cfg["r"])]
+        if cfg.get("linear"):
+            cdefs.append("-Duse_linear_friction")
         flags = list(CDKLM_FLAGS)
         if fmad:
             flags[-1] = "--fmad=true"

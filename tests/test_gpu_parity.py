@@ -334,6 +334,34 @@ def test_rotated_grid_vs_reference_kernel(ctx, angle):
     assert max(errs) == 0.0
 
 
+def test_linear_friction_vs_reference_kernel(ctx):
+    """The linear friction law (GO_FRICTION_LINEAR, C = 2 r dt / (eta + Hm))
+    against the reference kernel built with use_linear_friction
+    (CDKLM16_kernel.cu:884-886): the 96x80 config-2 physics, 200 steps."""
+    cfgd = build_ref.CONFIGS["small_linear"]
+    if not ref_kernel.available(cfgd):
+        pytest.skip("reference kernel library not built")
+    nx, ny = cfgd["nx"], cfgd["ny"]
+    c = SC.grf(96, dx=500.0, steps=200)
+    c.ny = ny
+    c.Hi = O.fix_bi_ghost_corners(np.ascontiguousarray(c.Hi[: ny + 5]), nx, ny, c.bc)
+    c.eta0 = np.ascontiguousarray(c.eta0[: ny + 4])
+    c.hu0 = np.zeros_like(c.eta0)
+    c.hv0 = np.zeros_like(c.eta0)
+    c.dt = SC.cfl_dt(c)
+    sim = CDKLM16.CDKLM16(ctx, dt=c.dt, linear_friction=True, **c.kwargs())
+    for _ in range(c.steps):
+        sim.step(c.dt)
+    mine = sim.download()
+    ref = ref_kernel.RefKernelSim(cfgd, c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, c.bc, wind=c.wind)
+    for _ in range(c.steps):
+        ref.step(c.dt)
+    theirs = ref.download()
+    errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
+    print("linear friction 200 steps vs reference kernel:", errs)
+    assert max(errs) == 0.0
+
+
 def test_single_stage_each_rk_step_vs_reference_kernel(ctx):
     """One call of each RK sub-step through the kernel-level ABI
     (go_cdklm_swe_2D vs the reference cdklm_swe_2D) on a perturbed state."""
