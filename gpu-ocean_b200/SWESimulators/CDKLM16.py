@@ -198,8 +198,13 @@ class CDKLM16(Simulator.Simulator):
         return self.t
 
     def drifterStep(self, dt):
+        """Advances the attached drifters through the new state
+        (CDKLM16.py:600-610)."""
         if self.hasDrifters:
-            raise NotImplementedError("device drifters are not built")
+            self.drifters.drift(self.gpu_data.h0, self.gpu_data.hu0, self.gpu_data.hv0, self.bathymetry.Bm,
+                                self.nx, self.ny, self.t, self.dx, self.dy, dt, np.int32(2), np.int32(2))
+            self.drifter_t += dt
+            return self.drifter_t
 
     def callKernel(self, h_in, hu_in, hv_in, h_out, hu_out, hv_out, local_dt, wind_stress_t, rk_step):
         """One sub-step (CDKLM16.py:613-639) through go_cdklm_swe_2D."""

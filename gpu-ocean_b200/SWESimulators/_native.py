@@ -97,6 +97,12 @@ SIGNATURES = {
     "go_batch_max_dt": (_I, [_P, _P, _P]),
     "go_sample_wind": (_I, [_P, _P, _I, _I, _I, _I, _P, _I]),
     "go_north_vector": (_I, [_F, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "go_wind_texture_create": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_uint64)]),
+    "go_wind_texture_destroy": (_I, [ctypes.c_uint64]),
+    "go_drift_passive": (_I, [_P, _I, _I, _F, _F, _F, _I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I, _I, _P, _I,
+                              _F, _F, _F, _P]),
+    "go_drift_enforce_bc": (_I, [_P, _F, _F, _I, _I, _I, _P, _I]),
+    "go_observe_flow": (_I, [_P, _I, _I, _F, _F, _I, _I, _P, _I, _P, _I, _I, _P, _I, _P, _I]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),
     "go_batch_destroy": (_I, [_P]),

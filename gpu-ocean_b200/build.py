@@ -4,7 +4,8 @@
 
 The floating-point flags are the reference's own (gpu_ocean/SWESimulators/
 CDKLM16.py:196-200): --ftz=true --prec-div=false --prec-sqrt=false
---fmad=false (the adjoint unit contracts FMAs, see UNIT_FLAGS).
+--fmad=false (the adjoint unit contracts FMAs and the drifter unit uses
+nvcc's defaults as the reference's drifter kernels do, see UNIT_FLAGS).
 """
 
 import os
@@ -29,7 +30,10 @@ NVCC_FLAGS = [
 # Units whose flags differ: the adjoint is not bit-compared with the
 # reference and keeps the forward's rounding only where a branch depends on
 # it (written out with __fmul_rn in the source), so it may contract FMAs.
-UNIT_FLAGS = {"adjoint.cu": {"--fmad=false": "--fmad=true"}}
+UNIT_FLAGS = {"adjoint.cu": {"--fmad=false": "--fmad=true"},
+              # the reference builds its drifter kernels with nvcc's defaults
+              "drifters.cu": {"--ftz=true": "--ftz=false", "--prec-div=false": "--prec-div=true",
+                              "--prec-sqrt=false": "--prec-sqrt=true", "--fmad=false": "--fmad=true"}}
 
 
 def flags_for(unit):

@@ -92,6 +92,44 @@ int go_domain_set_wind_uniform(go_domain* d, float x_cur, float x_next,
 int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_next,
                              const float* y_cur, const float* y_next, int pitch);
 
+/* ---------------------------------------------------------------------
+ * Drifters (gpu_ocean/SWESimulators/GPUDrifterCollection.py) and flow
+ * observation at drifter cells.  positions: (num_drifters + 1) rows of
+ * (x, y) floats in metres from the south-west interior corner (the last row
+ * is the observation's position), device, pitch in bytes.
+ * --------------------------------------------------------------------- */
+
+/* A wind field (host, h rows x w columns) as a bilinear, clamped,
+ * normalised texture for wind drift (GPUDrifterCollection.py:120-176); the
+ * handle is passed to go_drift_passive.  go_wind_texture_destroy frees it. */
+int go_wind_texture_create(const float* field, int w, int h, uint64_t* texture);
+int go_wind_texture_destroy(uint64_t texture);
+
+/* One Euler step of every drifter and the observation position with the
+ * flow velocity bilinear between the four nearest cell centres, plus
+ * wind_drift_factor x the wind (textures: X current, X next, Y current,
+ * Y next; may be NULL when the factor is 0), then the periodic wrap
+ * (passiveDrifterKernel, gpu_ocean/SWESimulators/gpu_kernels/
+ * driftKernels.cu:108-207; called from GPUDrifterCollection.py:209-232).
+ * Cells outside the arrays are clamped (the reference reads there). */
+int go_drift_passive(void* stream, int nx, int ny, float dx, float dy, float dt, int x_zero_cell,
+                     int y_zero_cell, const float* eta, int eta_pitch, const float* hu, int hu_pitch,
+                     const float* hv, int hv_pitch, const float* Hm, int Hm_pitch, int periodic_north_south,
+                     int periodic_east_west, int num_drifters, float* positions, int positions_pitch,
+                     float sensitivity, float wind_t, float wind_drift_factor, const uint64_t* wind_textures);
+
+/* Periodic wrap of every position (enforceBoundaryConditions,
+ * driftKernels.cu:211-250). */
+int go_drift_enforce_bc(void* stream, float domain_size_x, float domain_size_y, int periodic_north_south,
+                        int periodic_east_west, int num_drifters, float* positions, int positions_pitch);
+
+/* (hu, hv) of the cell under each drifter into observation (device,
+ * num_drifters rows of 2 floats, pitch in bytes) (observeUnderlyingFlow,
+ * gpu_ocean/SWESimulators/gpu_kernels/observationKernels.cu:29-81). */
+int go_observe_flow(void* stream, int nx, int ny, float dx, float dy, int x_zero_cell, int y_zero_cell,
+                    const float* hu, int hu_pitch, const float* hv, int hv_pitch, int num_drifters,
+                    const float* positions, int positions_pitch, float* observation, int observation_pitch);
+
 /* North vector (sin a, cos a) of a constant grid angle a, computed on the
  * device with sinf/cosf as the reference's kernel forms it from its angle
  * texture (gpu_ocean/SWESimulators/gpu_kernels/CDKLM16_kernel.cu:68-77), for

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+extern "C" int refr_set_drift_wind(cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t,
+                                   cudaTextureObject_t);
 extern "C" int refk_set_textures(cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t,
                                  cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t);
 extern "C" int refk_cdklm_swe_2D(cudaStream_t, float, int, float*, int, float*, int, float*, int, float*,
@@ -26,6 +28,7 @@ struct Tex {
 };
 
 Tex g_angle, g_f, g_wxc, g_wxn, g_wyc, g_wyn;
+Tex g_dwxc, g_dwxn, g_dwyc, g_dwyn;     // wind of the drift kernel
 
 void release(Tex& t) {
     if (t.obj) cudaDestroyTextureObject(t.obj);
@@ -85,6 +88,16 @@ int ref_set_wind(const float* xc, const float* xn, const float* yc, const float*
     if (!e) e = make_tex(g_wyc, yc, w, h);
     if (!e) e = make_tex(g_wyn, yn, w, h);
     if (!e) e = refk_set_textures(g_angle.obj, g_f.obj, g_wxc.obj, g_wxn.obj, g_wyc.obj, g_wyn.obj);
+    return e;
+}
+
+// Wind textures of the drift kernel (GPUDrifterCollection.py:120-176).
+int ref_set_drift_wind(const float* xc, const float* xn, const float* yc, const float* yn, int w, int h) {
+    int e = make_tex(g_dwxc, xc, w, h);
+    if (!e) e = make_tex(g_dwxn, xn, w, h);
+    if (!e) e = make_tex(g_dwyc, yc, w, h);
+    if (!e) e = make_tex(g_dwyn, yn, w, h);
+    if (!e) e = refr_set_drift_wind(g_dwxc.obj, g_dwxn.obj, g_dwyc.obj, g_dwyn.obj);
     return e;
 }
 

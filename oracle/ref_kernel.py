@@ -40,6 +40,11 @@ def _load(cfg, fmad=False):
     lib.ref_stage.argtypes = [_P, _F, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _I, _F, _F, _I]
     lib.ref_step.argtypes = [_P, _I, _F, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _I, _F, _I]
     lib.ref_max_dt.argtypes = [_P, _P, _P, _P, _I, _P, _I, _F, _P, _P]
+    lib.ref_set_drift_wind.argtypes = [ctypes.POINTER(_F)] * 4 + [_I, _I]
+    lib.refr_drift.argtypes = [_P, _I, _I, _F, _F, _F, _I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I, _I, _P, _I,
+                               _F, _F, _F]
+    lib.refr_enforce_bc.argtypes = [_P, _F, _F, _I, _I, _I, _P, _I]
+    lib.refr_observe.argtypes = [_P, _I, _I, _F, _F, _I, _I, _P, _I, _P, _I, _P, _I, _F, _I, _P, _I, _P, _I]
     return lib
 
 
@@ -144,3 +149,48 @@ class RefKernelSim:
     def download_prev(self):
         self.torch.cuda.synchronize()
         return tuple(a.cpu().numpy() for a in self.h1)
+
+
+class RefDrifters:
+    """The reference's drifter kernels (passiveDrifterKernel,
+    enforceBoundaryConditions, observeUnderlyingFlow) on their own device
+    positions: (n + 1) x 2 float32, the last row the observation.  Flow
+    arrays are (tensor, pitch in bytes) pairs of the ghost-inclusive grid."""
+
+    def __init__(self, cfg, positions, observation, wind_fields=None):
+        import torch
+        self.torch = torch
+        self.lib = _load(cfg)
+        rows = np.concatenate([np.asarray(positions, np.float32).reshape(-1, 2),
+                               np.asarray(observation, np.float32).reshape(1, 2)])
+        self.n = rows.shape[0] - 1
+        self.pos = torch.from_numpy(np.ascontiguousarray(rows)).cuda()
+        self.s = ctypes.c_void_p(int(torch.cuda.current_stream().cuda_stream))
+        if wind_fields is not None:
+            arrs = [np.ascontiguousarray(np.asarray(a, dtype=np.float32)) for a in wind_fields]
+            wh, ww = arrs[0].shape
+            _chk(self.lib.ref_set_drift_wind(*[a.ctypes.data_as(ctypes.POINTER(_F)) for a in arrs], ww, wh),
+                 "set_drift_wind")
+            self._wind = arrs
+
+    def drift(self, eta, hu, hv, Hm, nx, ny, dx, dy, dt, periodic_ns, periodic_ew, sensitivity=1.0,
+              wind_t=0.0, wind_drift_factor=0.0):
+        _chk(self.lib.refr_drift(self.s, nx, ny, float(dx), float(dy), float(dt), 2, 2, _p(eta[0]), eta[1],
+                                 _p(hu[0]), hu[1], _p(hv[0]), hv[1], _p(Hm[0]), Hm[1], int(periodic_ns),
+                                 int(periodic_ew), self.n, _p(self.pos), 8, float(sensitivity), float(wind_t),
+                                 float(wind_drift_factor)), "drift")
+
+    def enforce_bc(self, size_x, size_y, periodic_ns, periodic_ew):
+        _chk(self.lib.refr_enforce_bc(self.s, float(size_x), float(size_y), int(periodic_ns), int(periodic_ew),
+                                      self.n, _p(self.pos), 8), "enforce_bc")
+
+    def observe(self, eta, hu, hv, nx, ny, dx, dy):
+        out = self.torch.zeros((max(self.n, 1), 2), dtype=self.torch.float32, device="cuda")
+        _chk(self.lib.refr_observe(self.s, nx, ny, float(dx), float(dy), 2, 2, _p(eta[0]), eta[1], _p(hu[0]), hu[1],
+                                   _p(hv[0]), hv[1], 0.0, self.n, _p(self.pos), 8, _p(out), 8), "observe")
+        self.torch.cuda.synchronize()
+        return out[:self.n].cpu().numpy()
+
+    def positions(self):
+        self.torch.cuda.synchronize()
+        return self.pos.cpu().numpy()
