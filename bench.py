@@ -369,6 +369,58 @@ def run_ensemble(ctx, n_members=100, n=512, target_steps=300, graph_steps=10):
                     "cells), dt = 0.7 CFL min over members; both paths from the same perturbed states"}
 
 
+def run_drifters(ctx, n_drifters=100000, steps=100):
+    """Drifters on the headline 4096^2 case: the drift launch alone
+    (drifter-steps/s, one thread per drifter plus the observation row) and
+    CDKLM16.step(dt) with and without the drifters attached."""
+    import torch
+    from SWESimulators import CDKLM16, Common
+    from SWESimulators.GPUDrifterCollection import GPUDrifterCollection
+
+    c = make_case("grf4096")
+    sim = CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs())
+    sim.step(c.dt)
+    stream = sim.gpu_stream
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    timed(lambda: [sim.step(c.dt) for _ in range(5)])
+    plain_ms = timed(lambda: [sim.step(c.dt) for _ in range(steps)])
+    Lx, Ly = c.nx * c.dx, c.ny * c.dy
+    d = GPUDrifterCollection(ctx, n_drifters, boundaryConditions=Common.BoundaryConditions(*c.bc),
+                             domain_size_x=Lx, domain_size_y=Ly, gpu_stream=stream)
+    rng = np.random.default_rng(7)
+    d.setDrifterPositions(np.stack([rng.uniform(0.05, 0.95, n_drifters) * Lx,
+                                    rng.uniform(0.05, 0.95, n_drifters) * Ly], axis=1))
+    d.setObservationPosition([0.5 * Lx, 0.5 * Ly])
+    g = sim.gpu_data
+
+    def drift_only():
+        for _ in range(steps):
+            d.drift(g.h0, g.hu0, g.hv0, sim.bathymetry.Bm, c.nx, c.ny, sim.t, c.dx, c.dy, np.float32(c.dt), 2, 2)
+
+    timed(drift_only)
+    drift_ms = timed(drift_only)
+    sim.attachDrifters(d)
+    timed(lambda: [sim.step(c.dt) for _ in range(5)])
+    with_ms = timed(lambda: [sim.step(c.dt) for _ in range(steps)])
+    return {"workload": "drifters", "grid": "4096x4096", "drifters": n_drifters, "steps": steps,
+            "drift_us_per_launch": 1e3 * drift_ms / steps,
+            "drifter_steps_per_s": n_drifters * steps / (drift_ms * 1e-3),
+            "step_ms_plain": plain_ms / steps, "step_ms_with_drifters": with_ms / steps,
+            "overhead": with_ms / plain_ms - 1.0,
+            "note": "CUDA events on the simulator's stream; drifters uniform over the interior; the step loop "
+                    "launches each step separately once drifters are attached (as CDKLM16.step does)"}
+
+
 def run_adjoint(ctx, n=512, n_steps=500, k=50, kind=0, rows=0):
     """Gradient of the observation misfit (64 cells, steps 50..500, truth
     bumps seed 50001, background 50002) w.r.t. the initial state and the
@@ -592,7 +644,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage",
+    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage", "drifters",
                                            "adjoint_batch"],
                     default="grf4096")
     ap.add_argument("--grid", type=int, default=2048, help="grid size of the adjoint_stage workload")
@@ -635,7 +687,7 @@ def main():
         print(json.dumps(line))
         return
 
-    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch"):
+    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch", "drifters"):
         if rank != 0:
             return
         from SWESimulators import Common
@@ -648,6 +700,8 @@ def main():
             r = run_adjoint(ctx, kind=args.adj_kind, rows=args.adj_rows)
         elif args.workload == "adjoint_batch":
             r = run_adjoint_batch(ctx)
+        elif args.workload == "drifters":
+            r = run_drifters(ctx)
         else:
             r = run_adjoint_stages(ctx, args.grid, reps=args.steps if args.steps < 2000 else 20,
                                    kind=args.adj_kind, rows=args.adj_rows)
@@ -665,6 +719,8 @@ def main():
             value, ms = r["batched_gcell_steps_s"], r["batched_ms"] / max(r["steps"], 1)
         elif args.workload == "adjoint_batch":
             value, ms = r["forward_adjoint_gcell_steps_s"], r["forward_adjoint_ms"] / r["steps"]
+        elif args.workload == "drifters":
+            value, ms = 4096 * 4096 / (r["step_ms_with_drifters"] * 1e-3) / 1e9, r["step_ms_with_drifters"]
         else:
             cells_steps = 512 * 512 * r["steps"]
             value, ms = cells_steps / (r["forward_adjoint_ms_k50"] * 1e-3) / 1e9, r["forward_adjoint_ms_k50"] / r["steps"]
@@ -702,7 +758,7 @@ def main():
         ctx = Common.CUDAContext(local)
         secondary = {}
         for name, fn in (("ensemble100", run_ensemble), ("adjoint512", run_adjoint),
-                         ("adjoint_batch", run_adjoint_batch)):
+                         ("adjoint_batch", run_adjoint_batch), ("drifters", run_drifters)):
             try:
                 secondary[name] = fn(ctx)
             except Exception as e:      # a secondary failure must not lose the headline line
