@@ -111,6 +111,8 @@ class MisfitProblem:
         d = sim._domain.desc
         if abs(float(d.north_x)) > 0.0 or float(d.north_y) != 1.0:
             raise NotImplementedError("the adjoint is built for north-up grids only")
+        if max(d.bc_north, d.bc_east, d.bc_south, d.bc_west) > 2:
+            raise NotImplementedError("the adjoint is built for wall and periodic boundaries only")
         Bm = sim.downloadBathymetry()[1]
         if np.any(np.abs(Bm - np.float32(sim.bathymetry.mask_value)) < 1e-3):
             raise NotImplementedError("the adjoint is built for bathymetry without land")
@@ -449,6 +451,8 @@ class BatchedMisfitProblem:
             d = s._domain.desc
             if abs(float(d.north_x)) > 0.0 or float(d.north_y) != 1.0:
                 raise NotImplementedError("the adjoint is built for north-up grids only")
+            if max(d.bc_north, d.bc_east, d.bc_south, d.bc_west) > 2:
+                raise NotImplementedError("the adjoint is built for wall and periodic boundaries only")
         self.n_steps = int(n_steps)
         self.dt = np.float32(s0.dt if dt is None else dt)
         self.obs = obs

@@ -7,7 +7,7 @@ attributes other modules read (``gpu_data.h0 ...``, ``bathymetry``,
 ``gpu_stream``, ``t``, ``num_iterations``, ...).
 
 What is not built raises ``NotImplementedError`` at construction:
-open boundaries (codes 3/4), a spatially varying grid angle, ``latitude``,
+a spatially varying grid angle, ``latitude``,
 the stochastic model error (``small_scale_perturbation``), NetCDF output,
 ``rk_order`` other than 2.  The Coriolis table is always full-resolution
 (``subsample_f``/``subsample_angle`` are accepted and ignored; the
@@ -48,8 +48,6 @@ class CDKLM16(Simulator.Simulator):
             raise NotImplementedError("NetCDF output is not built (netCDF4 is not available)")
         if latitude is not None:
             raise NotImplementedError("a latitude field (2-D Coriolis) is not built")
-        if boundary_conditions.isSponge():
-            raise NotImplementedError("open boundaries (codes 3 and 4) are not built")
         angle = np.asarray(angle)
         if angle.size != 1 and not np.all(angle == angle.reshape(-1)[0]):
             raise NotImplementedError("a spatially varying grid angle is not built")
@@ -102,6 +100,8 @@ class CDKLM16(Simulator.Simulator):
         self.bc_kernel = Common.BoundaryConditionsArakawaA(gpu_ctx, self.nx, self.ny, ghost_cells_x,
                                                            ghost_cells_y, self.boundary_conditions,
                                                            boundary_conditions_data)
+        # open boundaries: the step domain runs the ghost sequence after each stage
+        self.bc_kernel.use_domain(self._domain)
 
         # Coriolis per ghost-inclusive row (CDKLM16.py:310-345), full resolution
         self.coriolis_rows = self._coriolis_rows(eta0, angle, a0)
@@ -166,7 +166,9 @@ class CDKLM16(Simulator.Simulator):
     def step(self, t_end=0.0, apply_stochastic_term=True, write_now=True, update_dt=False):
         """Advance by t_end seconds in steps of self.dt; the last step is
         shortened to land on t_end (CDKLM16.py:494-598)."""
+        open_bc = self.boundary_conditions.isSponge()
         if self.t == 0:
+            self.bc_kernel.update_bc_values(self.gpu_stream, self.t)
             self.bc_kernel.boundaryCondition(self.gpu_stream, self.gpu_data.h0, self.gpu_data.hu0,
                                              self.gpu_data.hv0)
         t_now = 0.0
@@ -181,12 +183,16 @@ class CDKLM16(Simulator.Simulator):
             local_dt = np.float32(min(self.dt, np.float32(t_end - t_now)))
             wind_t = np.float32(self.update_wind_stress())
             if pending_n and (local_dt != pending_dt or wind_t != pending_w or time_varying_wind
-                              or self.hasDrifters):
+                              or self.hasDrifters or open_bc):
                 self._launch_steps(pending_n, pending_dt, pending_w)
                 pending_n = 0
             pending_n += 1
             pending_dt, pending_w = local_dt, wind_t
-            if self.hasDrifters or time_varying_wind:
+            if self.hasDrifters or time_varying_wind or open_bc:
+                # one launch per step: the drifters move between steps, the
+                # wind or the exterior solution of this step's time
+                if open_bc:
+                    self.bc_kernel.update_bc_values(self.gpu_stream, self.t)
                 self._launch_steps(pending_n, pending_dt, pending_w)
                 pending_n = 0
                 self.drifterStep(local_dt)

@@ -7,7 +7,7 @@ simulator and its callers use:
 * ``CUDAArray2D``                  (Common.py:503-631)  -- torch-backed, padded pitch
 * ``SWEDataArakawaA``              (Common.py:634-690)
 * ``BoundaryConditions`` / ``BoundaryConditionsData`` (Common.py:824-1014)
-* ``BoundaryConditionsArakawaA``   (Common.py:1019-1309) -- wall and periodic
+* ``BoundaryConditionsArakawaA``   (Common.py:1019-1309) -- wall, periodic and open (3/4)
 * ``Bathymetry``                   (Common.py:1313-1459)
 
 Device memory is allocated by PyTorch; every kernel is the in-tree CUDA
@@ -15,6 +15,8 @@ library reached through ``_native`` (no CPU fallback).
 """
 
 import logging
+
+import ctypes
 
 import numpy as np
 
@@ -288,22 +290,105 @@ class BoundaryConditionsData:
 
 
 class BoundaryConditionsArakawaA:
-    """Ghost-cell refresh for unstaggered grids (Common.py:1019-1309).  Wall
-    sides are mirrored inside the step kernel and need no launch here;
-    periodic sides copy the opposite interior rows, north-south first."""
+    """Ghost-cell refresh for unstaggered grids (Common.py:1019-1309): north-
+    south first, then east-west; per axis the periodic copy, or the open
+    kinds of its two sides (3: flow relaxation towards the exterior solution
+    in ``bc_data``, 4: linear interpolation over the sponge).  Wall sides are
+    mirrored inside the step kernel and need no launch here.  With open
+    boundaries the simulator's own step domain is attached (``use_domain``)
+    so that its RK stages apply the same sequence."""
 
     def __init__(self, gpu_ctx, nx, ny, halo_x, halo_y, boundary_conditions,
                  bc_data=None, block_width=16, block_height=16):
-        if boundary_conditions.isSponge():
-            raise NotImplementedError("open (sponge) boundaries 3/4 are not built")
         self.boundary_conditions = boundary_conditions
         self.nx, self.ny = np.int32(nx), np.int32(ny)
         self.halo_x, self.halo_y = np.int32(halo_x), np.int32(halo_y)
-        self.bc_data = bc_data
+        self.bc_data = bc_data if bc_data is not None else BoundaryConditionsData()
         self._domain = _native.Domain(nx, ny, 1.0, 1.0, 1.0, bc=boundary_conditions.codes())
+        self._domains = [self._domain]
+        self.bc_timestamps = [None, None]
+        self.bc_t = np.float32(0.0)
+        self._textures = None
+        if boundary_conditions.isSponge():
+            sp = boundary_conditions.getSponge()
+            self._domain.set_sponge(sp["north"], sp["east"], sp["south"], sp["west"])
+
+    def use_domain(self, domain):
+        """Also keep `domain` (the simulator's step domain) up to date with
+        the sponge widths and the exterior solution."""
+        if self.boundary_conditions.isSponge():
+            sp = self.boundary_conditions.getSponge()
+            domain.set_sponge(sp["north"], sp["east"], sp["south"], sp["west"])
+            if self._textures is not None:
+                domain.set_open_bc(self._textures, self.bc_t)
+        self._domains.append(domain)
+
+    def _relaxes(self):
+        bc = self.boundary_conditions
+        return 3 in (int(bc.north), int(bc.south), int(bc.east), int(bc.west))
+
+    @staticmethod
+    def _pack(side_a, side_b, t_index, along_x):
+        """Texels (h, hu, hv, 0) of two sides at one time: rows (south,
+        north) of one texel per column, or columns (west, east) of one texel
+        per row (Common.py:1105-1137)."""
+        def rgba(side):
+            h = np.squeeze(side.h[t_index])
+            hu = np.squeeze(side.hu[t_index])
+            hv = np.squeeze(side.hv[t_index])
+            if h.ndim != 1:
+                raise ValueError("boundary data of a side must be one row or column")
+            return np.stack([h, hu, hv, np.zeros_like(h)], axis=1).astype(np.float32)
+        a, b = rgba(side_a), rgba(side_b)
+        if along_x:
+            return np.ascontiguousarray(np.stack([a, b], axis=0))      # 2 x L x 4
+        return np.ascontiguousarray(np.stack([a, b], axis=1))          # L x 2 x 4
 
     def update_bc_values(self, gpu_stream, t):
-        return
+        """Exterior solution of the interval around t as textures (rebuilt
+        when the interval changes) and the time weight of this step
+        (Common.py:1073-1216)."""
+        if not self._relaxes():
+            return
+        d = self.bc_data
+        t1_index = min(len(d.t) - 1, int(np.searchsorted(d.t, t)))
+        t0_index = max(0, int(np.searchsorted(d.t, t)) - 1)
+        new_t0, new_t1 = d.t[t0_index], d.t[t1_index]
+        if [new_t0, new_t1] != self.bc_timestamps or self._textures is None:
+            lib = _native.load()
+            handles = []
+            for k in (t0_index, t1_index):
+                for along_x, (a, b) in ((True, (d.south, d.north)), (False, (d.west, d.east))):
+                    texels = self._pack(a, b, k, along_x)
+                    h = ctypes.c_uint64(0)
+                    _native.check(lib.go_bc_texture_create(texels.ctypes.data_as(ctypes.c_void_p),
+                                                           int(texels.shape[1]), int(texels.shape[0]),
+                                                           ctypes.byref(h)))
+                    handles.append(h.value)
+            # order: NS current, NS next, EW current, EW next
+            new = (handles[0], handles[2], handles[1], handles[3])
+            if gpu_stream is not None:
+                gpu_stream.synchronize()
+            self._release()
+            self._textures = new
+            self.bc_timestamps = [new_t0, new_t1]
+        interval = max(1.0e-10, new_t1 - new_t0)
+        self.bc_t = np.float32(max(0.0, min(1.0, (t - new_t0) / interval)))
+        for dom in self._domains:
+            dom.set_open_bc(self._textures, self.bc_t)
+
+    def _release(self):
+        if self._textures is not None:
+            lib = _native.load()
+            for h in self._textures:
+                lib.go_wind_texture_destroy(ctypes.c_uint64(h))
+            self._textures = None
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:
+            pass
 
     def boundaryCondition(self, gpu_stream, h, u, v):
         assert h.pitch == u.pitch == v.pitch

@@ -103,6 +103,9 @@ SIGNATURES = {
                               _F, _F, _F, _P]),
     "go_drift_enforce_bc": (_I, [_P, _F, _F, _I, _I, _I, _P, _I]),
     "go_observe_flow": (_I, [_P, _I, _I, _F, _F, _I, _I, _P, _I, _P, _I, _I, _P, _I, _P, _I]),
+    "go_domain_set_sponge": (_I, [_P, _I, _I, _I, _I]),
+    "go_bc_texture_create": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_uint64)]),
+    "go_domain_set_open_bc": (_I, [_P, _P, _F]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),
     "go_batch_destroy": (_I, [_P]),
@@ -228,6 +231,13 @@ class Domain:
         for t in (x_next, y_cur, y_next):
             assert t.stride(0) * 4 == pitch
         check(load().go_domain_set_wind_field(self.handle, ptr(x_cur), ptr(x_next), ptr(y_cur), ptr(y_next), pitch))
+
+    def set_sponge(self, north, east, south, west):
+        check(load().go_domain_set_sponge(self.handle, int(north), int(east), int(south), int(west)))
+
+    def set_open_bc(self, textures, bc_t):
+        arr = (ctypes.c_uint64 * 4)(*[int(t) for t in textures])
+        check(load().go_domain_set_open_bc(self.handle, arr, float(np.float32(bc_t))))
 
     def set_launch(self, shape=0, rows_per_block=0):
         check(load().go_domain_set_launch(self.handle, int(shape), int(rows_per_block)))

@@ -34,6 +34,8 @@ UNIT_FLAGS = {"adjoint.cu": {"--fmad=false": "--fmad=true"},
               # the reference builds its drifter kernels with nvcc's defaults
               "drifters.cu": {"--ftz=true": "--ftz=false", "--prec-div=false": "--prec-div=true",
                               "--prec-sqrt=false": "--prec-sqrt=true", "--fmad=false": "--fmad=true"}}
+# ... and its boundary kernels (open boundaries) the same way
+UNIT_FLAGS["open_boundaries.cu"] = UNIT_FLAGS["drifters.cu"]
 
 
 def flags_for(unit):

@@ -193,8 +193,9 @@ int go_domain_create(const go_domain_desc* desc, go_domain** out) {
     if (s.rk_order != 2) return go_fail(GO_ERR_UNSUPPORTED, "rk_order %d: only 2 (Heun) is built", s.rk_order);
     const int bcs[4] = {s.bc_north, s.bc_east, s.bc_south, s.bc_west};
     for (int b : bcs)
-        if (b != GO_BC_WALL && b != GO_BC_PERIODIC)
-            return go_fail(GO_ERR_UNSUPPORTED, "boundary code %d: only wall (1) and periodic (2) are built", b);
+        if (b < GO_BC_WALL || b > GO_BC_LINEAR_SPONGE)
+            return go_fail(GO_ERR_UNSUPPORTED, "boundary code %d: wall (1), periodic (2), flow relaxation (3) "
+                           "and linear sponge (4) are built", b);
     if ((s.bc_north == GO_BC_PERIODIC) != (s.bc_south == GO_BC_PERIODIC) ||
         (s.bc_east == GO_BC_PERIODIC) != (s.bc_west == GO_BC_PERIODIC))
         return go_fail(GO_ERR_INVALID, "periodic boundaries must be set on both opposite sides");
@@ -329,10 +330,19 @@ int go_boundary_condition(go_domain* d, void* stream, float* eta, float* hu, flo
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     const int nx = d->k.nx, ny = d->k.ny, p = pitch / 4;
-    if (d->k.bcN == GO_BC_PERIODIC)
+    // north-south (periodic copy, or the open kinds), then east-west
+    if (d->k.bcN == GO_BC_PERIODIC) {
         k_periodic_ns<<<dim3((nx + 4 + 127) / 128, 4), 128, 0, s>>>(eta, hu, hv, p, nx, ny);
-    if (d->k.bcE == GO_BC_PERIODIC)
+    } else {
+        rc = go_open_bc_ns(d, s, eta, hu, hv, p);
+        if (rc) return rc;
+    }
+    if (d->k.bcE == GO_BC_PERIODIC) {
         k_periodic_ew<<<dim3((ny + 4 + 127) / 128, 4), 128, 0, s>>>(eta, hu, hv, p, nx, ny);
+    } else {
+        rc = go_open_bc_ew(d, s, eta, hu, hv, p);
+        if (rc) return rc;
+    }
     GO_CUDA(cudaGetLastError());
     return GO_OK;
 }
@@ -381,10 +391,16 @@ int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_
                                        Hi_pitch / 4, land_value, wind_stress_t);
     const StageArgs a1 = go_stage_args(d, dt, 1, eta1, hu1, hv1, pitch1 / 4, eta0, hu0, hv0, pitch0 / 4, Hi,
                                        Hi_pitch / 4, land_value, wind_stress_t);
+    const bool open = go_has_open_bc(d);
     for (int n = 0; n < n_steps; ++n) {
         rc = go_launch_stage(d, s, a0);
+        // open boundaries: the reference's ghost sequence after each stage
+        // (CDKLM16.py:537-540, 585-586); the stage kernel's own periodic
+        // images are redone in order after the open kinds of the other axis
+        if (!rc && open) rc = go_boundary_condition(d, stream, eta1, hu1, hv1, pitch1);
         if (rc) return rc;
         rc = go_launch_stage(d, s, a1);
+        if (!rc && open) rc = go_boundary_condition(d, stream, eta0, hu0, hv0, pitch0);
         if (rc) return rc;
     }
     return GO_OK;

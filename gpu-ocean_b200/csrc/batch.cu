@@ -187,8 +187,12 @@ int go_batch_create(go_domain* const* members, int n, go_batch** out) {
         }
         b->shape = tiles > 148LL * shape_blocks_per_sm(ring) ? ring : 4;
     }
-    for (int m = 1; m < n; ++m) {
+    for (int m = 0; m < n; ++m) {
         const go_domain* d = members[m];
+        if (go_has_open_bc(d)) {
+            delete b;
+            return go_fail(GO_ERR_UNSUPPORTED, "member %d has open boundaries, which the batch does not run", m);
+        }
         if (go_friction_mode(d) != b->variant.fric || go_general_north(d) != b->variant.gen_north) {
             delete b;
             return go_fail(GO_ERR_INVALID,

@@ -25,6 +25,9 @@ struct go_domain {
     int has_land;            // bathymetry may hold land cells (checks on)
     int adj_kind;            // GO_ADJ_* launch form of the adjoint stage
     int adj_rows;            // rows per strip of the marching adjoint (0: automatic)
+    int sponge[4];           // open-boundary sponge widths: north, east, south, west
+    uint64_t bc_tex[4];      // exterior solution textures: NS cur, NS next, EW cur, EW next
+    float bc_t;              // their time weight
 };
 
 // Records the message of a failed call (go_last_error) and returns code.
@@ -44,6 +47,12 @@ int go_check_pitch(int pitch_bytes, int min_floats, const char* what);
 // still launch enough blocks to cover the 148 SMs.
 int go_auto_rows(int nx, int ny, int shape);
 int go_auto_shape(int nx, int ny);
+// Open kinds (codes 3/4) of one axis (csrc/open_boundaries.cu).
+int go_open_bc_ns(const go_domain* d, cudaStream_t s, float* h, float* u, float* v, int p);
+int go_open_bc_ew(const go_domain* d, cudaStream_t s, float* h, float* u, float* v, int p);
+inline bool go_has_open_bc(const go_domain* d) {
+    return d->k.bcN > 2 || d->k.bcE > 2 || d->k.bcS > 2 || d->k.bcW > 2;
+}
 
 // Kernel-variant selectors of a domain.
 int go_friction_mode(const go_domain* d);

@@ -78,7 +78,8 @@ int fill_domain(const go_domain_desc& s, go_domain* d) {
     const int bcs[4] = {s.bc_north, s.bc_east, s.bc_south, s.bc_west};
     for (int b : bcs)
         if (b != GO_BC_WALL && b != GO_BC_PERIODIC)
-            return go_fail(GO_ERR_UNSUPPORTED, "boundary code %d: only wall (1) and periodic (2) are built", b);
+            return go_fail(GO_ERR_UNSUPPORTED, "boundary code %d: the allocation-free step takes wall (1) and "
+                           "periodic (2) boundaries only", b);
     if ((s.bc_north == GO_BC_PERIODIC) != (s.bc_south == GO_BC_PERIODIC) ||
         (s.bc_east == GO_BC_PERIODIC) != (s.bc_west == GO_BC_PERIODIC))
         return go_fail(GO_ERR_INVALID, "periodic boundaries must be set on both opposite sides");

@@ -37,6 +37,8 @@ extern "C" {
 /* Boundary codes, gpu_ocean/SWESimulators/Common.py:824-857. */
 #define GO_BC_WALL 1
 #define GO_BC_PERIODIC 2
+#define GO_BC_FLOW_RELAXATION 3   /* open: relaxation towards an exterior solution over a sponge */
+#define GO_BC_LINEAR_SPONGE 4     /* open: linear between the outer and inner sponge edges */
 
 /* Bottom friction law.  QUADRATIC is what the reference kernel compiles
  * (CDKLM16_kernel.cu:884-900 without use_linear_friction); LINEAR is the
@@ -129,6 +131,29 @@ int go_drift_enforce_bc(void* stream, float domain_size_x, float domain_size_y, 
 int go_observe_flow(void* stream, int nx, int ny, float dx, float dy, int x_zero_cell, int y_zero_cell,
                     const float* hu, int hu_pitch, const float* hv, int hv_pitch, int num_drifters,
                     const float* positions, int positions_pitch, float* observation, int observation_pitch);
+
+/* ---------------------------------------------------------------------
+ * Open boundaries (codes 3 and 4; gpu_ocean/SWESimulators/gpu_kernels/
+ * boundary_kernels.cu:264-539, Common.py:1073-1309).  go_boundary_condition
+ * and go_cdklm_step (after each RK stage) then run the reference's ghost
+ * sequence: north-south periodic copy or open kinds, then east-west.
+ * --------------------------------------------------------------------- */
+
+/* Sponge widths in ghost-inclusive cells from the outer edge (the
+ * reference's spongeCells). */
+int go_domain_set_sponge(go_domain* d, int north, int east, int south, int west);
+
+/* A float4 (h, hu, hv, unused) texture of w x h texels (host, row-major)
+ * for the flow relaxation's exterior solution, bilinear, clamped,
+ * normalised (Common.py:1098-1103).  Free with go_wind_texture_destroy. */
+int go_bc_texture_create(const float* texels, int w, int h, uint64_t* texture);
+
+/* Exterior solution of the flow relaxation: textures {NS current, NS next,
+ * EW current, EW next} (NS: row 0 south, row 1 north; EW: column 0 west,
+ * column 1 east) and the time weight bc_t in [0, 1] used by the following
+ * launches (BoundaryConditionsArakawaA.update_bc_values,
+ * Common.py:1073-1216).  The caller keeps the textures alive. */
+int go_domain_set_open_bc(go_domain* d, const uint64_t* textures, float bc_t);
 
 /* North vector (sin a, cos a) of a constant grid angle a, computed on the
  * device with sinf/cosf as the reference's kernel forms it from its angle

@@ -9,6 +9,10 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+extern "C" int refb_set_open_bc_tex(cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t,
+                                    cudaTextureObject_t);
+extern "C" int refb_boundary(cudaStream_t, int, int, int, int, int, int, int, int, int, int, float, float*, int,
+                             float*, int, float*, int);
 extern "C" int refr_set_drift_wind(cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t,
                                    cudaTextureObject_t);
 extern "C" int refk_set_textures(cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t,
@@ -29,6 +33,8 @@ struct Tex {
 
 Tex g_angle, g_f, g_wxc, g_wxn, g_wyc, g_wyn;
 Tex g_dwxc, g_dwxn, g_dwyc, g_dwyn;     // wind of the drift kernel
+Tex g_ns0, g_ns1, g_ew0, g_ew1;         // exterior solution of the flow relaxation
+
 
 void release(Tex& t) {
     if (t.obj) cudaDestroyTextureObject(t.obj);
@@ -42,6 +48,34 @@ int make_tex(Tex& t, const float* host, int w, int h) {
     cudaError_t e = cudaMallocArray(&t.arr, &ch, w, h);
     if (e) return (int)e;
     e = cudaMemcpy2DToArray(t.arr, 0, 0, host, w * sizeof(float), w * sizeof(float), h, cudaMemcpyHostToDevice);
+    if (e) return (int)e;
+    cudaResourceDesc res;
+    memset(&res, 0, sizeof(res));
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = t.arr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    return (int)cudaCreateTextureObject(&t.obj, &res, &td, nullptr);
+}
+
+struct OpenBC {
+    int active = 0;
+    int codes[4] = {1, 1, 1, 1};        // north, east, south, west
+    int sponge[4] = {0, 0, 0, 0};
+    float bc_t = 0.0f;
+} g_open;
+
+int make_tex4(Tex& t, const float* host, int w, int h) {
+    release(t);
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
+    cudaError_t e = cudaMallocArray(&t.arr, &ch, w, h);
+    if (e) return (int)e;
+    e = cudaMemcpy2DToArray(t.arr, 0, 0, host, w * sizeof(float4), w * sizeof(float4), h, cudaMemcpyHostToDevice);
     if (e) return (int)e;
     cudaResourceDesc res;
     memset(&res, 0, sizeof(res));
@@ -106,7 +140,32 @@ int ref_bathymetry(void* s, int bc_north, int bc_east, float* Bi, int pbi, float
 }
 
 int ref_boundary(void* s, int bc_north, int bc_east, float* h, float* u, float* v, int p) {
+    if (g_open.active)
+        return refb_boundary((cudaStream_t)s, NX, NY, g_open.codes[0], g_open.codes[1], g_open.codes[2],
+                             g_open.codes[3], g_open.sponge[0], g_open.sponge[1], g_open.sponge[2], g_open.sponge[3],
+                             g_open.bc_t, h, p, u, p, v, p);
     return refb_periodic((cudaStream_t)s, NX, NY, bc_north == 2, bc_east == 2, h, p, u, p, v, p);
+}
+
+// Open boundaries for ref_boundary / ref_step: codes and sponge widths
+// (north, east, south, west), exterior textures (NS: w_ns x 2 float4 texels,
+// EW: 2 x h_ew) of the current and next time, and the time weight.
+int ref_set_open_bc(const int* codes, const int* sponge, const float* ns0, const float* ns1, int w_ns,
+                    const float* ew0, const float* ew1, int h_ew, float bc_t) {
+    for (int i = 0; i < 4; ++i) { g_open.codes[i] = codes[i]; g_open.sponge[i] = sponge[i]; }
+    g_open.bc_t = bc_t;
+    g_open.active = 1;
+    int e = make_tex4(g_ns0, ns0, w_ns, 2);
+    if (!e) e = make_tex4(g_ns1, ns1, w_ns, 2);
+    if (!e) e = make_tex4(g_ew0, ew0, 2, h_ew);
+    if (!e) e = make_tex4(g_ew1, ew1, 2, h_ew);
+    if (!e) e = refb_set_open_bc_tex(g_ns0.obj, g_ns1.obj, g_ew0.obj, g_ew1.obj);
+    return e;
+}
+
+int ref_set_bc_t(float bc_t) {
+    g_open.bc_t = bc_t;
+    return 0;
 }
 
 int ref_stage(void* s, float dt, int rk_step, float* e0, float* u0, float* v0, int p0,

@@ -34,3 +34,43 @@ extern "C" int refb_bathymetry(cudaStream_t s, int nx, int ny, int periodic_ns, 
     refb::initBm<<<grid, block, 0, s>>>(nx + 4, ny + 4, Bi, pbi, land, Bm, pbm);
     return (int)cudaGetLastError();
 }
+
+// Exterior-solution textures of the flow relaxation (Common.py:1098-1216).
+extern "C" int refb_set_open_bc_tex(cudaTextureObject_t ns0, cudaTextureObject_t ns1, cudaTextureObject_t ew0,
+                                    cudaTextureObject_t ew1) {
+    cudaError_t e = cudaMemcpyToSymbol(refb::bc_tex_NS_current, &ns0, sizeof(ns0));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(refb::bc_tex_NS_next, &ns1, sizeof(ns1));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(refb::bc_tex_EW_current, &ew0, sizeof(ew0));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(refb::bc_tex_EW_next, &ew1, sizeof(ew1));
+    return (int)e;
+}
+
+// BoundaryConditionsArakawaA.boundaryCondition (Common.py:1219-1239) for any
+// codes: north-south periodic or open kinds, then east-west.
+extern "C" int refb_boundary(cudaStream_t s, int nx, int ny, int north, int east, int south, int west,
+                             int sp_north, int sp_east, int sp_south, int sp_west, float bc_t,
+                             float* h, int ph, float* u, int pu, float* v, int pv) {
+    dim3 block(16, 16);
+    dim3 grid = grid_for(nx + 2 * 2 + 1, ny + 2 * 2 + 1);
+    if (north == 2) {
+        refb::periodicBoundary_NS<<<grid, block, 0, s>>>(nx, ny, 2, 2, h, ph, u, pu, v, pv);
+    } else {
+        if (north == 3 || south == 3)
+            refb::flowRelaxationScheme_NS<<<grid, block, 0, s>>>(north, south, nx, ny, 2, 2, sp_north, sp_south,
+                                                                h, ph, u, pu, v, pv, bc_t);
+        if (north == 4 || south == 4)
+            refb::linearInterpolation_NS<<<grid, block, 0, s>>>(north, south, nx, ny, 2, 2, sp_north, sp_south,
+                                                               h, ph, u, pu, v, pv);
+    }
+    if (east == 2) {
+        refb::periodicBoundary_EW<<<grid, block, 0, s>>>(nx, ny, 2, 2, h, ph, u, pu, v, pv);
+    } else {
+        if (east == 3 || west == 3)
+            refb::flowRelaxationScheme_EW<<<grid, block, 0, s>>>(east, west, nx, ny, 2, 2, sp_east, sp_west,
+                                                                h, ph, u, pu, v, pv, bc_t);
+        if (east == 4 || west == 4)
+            refb::linearInterpolation_EW<<<grid, block, 0, s>>>(east, west, nx, ny, 2, 2, sp_east, sp_west,
+                                                               h, ph, u, pu, v, pv);
+    }
+    return (int)cudaGetLastError();
+}

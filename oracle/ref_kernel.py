@@ -41,6 +41,9 @@ def _load(cfg, fmad=False):
     lib.ref_step.argtypes = [_P, _I, _F, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _I, _F, _I]
     lib.ref_max_dt.argtypes = [_P, _P, _P, _P, _I, _P, _I, _F, _P, _P]
     lib.ref_set_drift_wind.argtypes = [ctypes.POINTER(_F)] * 4 + [_I, _I]
+    lib.ref_set_open_bc.argtypes = [ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_F), ctypes.POINTER(_F),
+                                    _I, ctypes.POINTER(_F), ctypes.POINTER(_F), _I, _F]
+    lib.ref_set_bc_t.argtypes = [_F]
     lib.refr_drift.argtypes = [_P, _I, _I, _F, _F, _F, _I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I, _I, _P, _I,
                                _F, _F, _F]
     lib.refr_enforce_bc.argtypes = [_P, _F, _F, _I, _I, _I, _P, _I]
@@ -123,13 +126,38 @@ class RefKernelSim:
                                 _p(Qout[0]), _p(Qout[1]), _p(Qout[2]), self.pitch, _p(self.Hi), (self.nx + 5) * 4,
                                 _p(self.Bm), self.pitch, float(self.land), float(wind_t), self.bc_packed), "stage")
 
+    def set_open_bc(self, codes, sponge, t, ns, ew):
+        """Open boundaries: codes and sponge widths (north, east, south,
+        west); the exterior solution at two times t = (t0, t1) as NS texels
+        [(2, L, 4) per time: row 0 south, row 1 north] and EW texels
+        [(L, 2, 4): column 0 west, column 1 east], as
+        BoundaryConditionsArakawaA.update_bc_values packs them."""
+        self._open_t = (float(t[0]), float(t[1]))
+        ns = [np.ascontiguousarray(a, dtype=np.float32) for a in ns]
+        ew = [np.ascontiguousarray(a, dtype=np.float32) for a in ew]
+        self._open_data = (ns, ew)
+        c = (_I * 4)(*[int(x) for x in codes])
+        sp = (_I * 4)(*[int(x) for x in sponge])
+        P = lambda a: a.ctypes.data_as(ctypes.POINTER(_F))
+        _chk(self.lib.ref_set_open_bc(c, sp, P(ns[0]), P(ns[1]), ns[0].shape[1], P(ew[0]), P(ew[1]), ew[0].shape[0],
+                                      float(self._bc_t(0.0))), "set_open_bc")
+
+    def _bc_t(self, t):
+        t0, t1 = self._open_t
+        return np.float32(max(0.0, min(1.0, (t - t0) / max(1.0e-10, t1 - t0))))
+
     def step(self, t_end):
         """CDKLM16.step(t_end) (CDKLM16.py:494-598) with constant wind."""
+        open_bc = getattr(self, "_open_t", None) is not None
         if self.t == 0:
+            if open_bc:
+                self.lib.ref_set_bc_t(float(self._bc_t(self.t)))
             self.boundary(self.h0)
         t_now = 0.0
         while t_now < t_end:
             local_dt = np.float32(min(self.dt, np.float32(t_end - t_now)))
+            if open_bc:
+                self.lib.ref_set_bc_t(float(self._bc_t(self.t)))
             self.run_steps(1, local_dt)
             self.t += np.float64(local_dt)
             t_now += np.float64(local_dt)

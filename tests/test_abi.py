@@ -64,7 +64,7 @@ def _desc(**kw):
     (dict(dx=0.0), -1),
     (dict(r=-1.0), -1),
     (dict(rk_order=3), -3),
-    (dict(bc_north=3), -3),
+    (dict(bc_north=5), -3),          # no boundary kind 5
     (dict(bc_north=2), -1),          # periodic on one side only
     (dict(friction_law=7), -1),
 ])

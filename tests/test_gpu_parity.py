@@ -362,6 +362,66 @@ def test_linear_friction_vs_reference_kernel(ctx):
     assert max(errs) == 0.0
 
 
+def _open_bc_data(nx, ny, t1, seed):
+    """Exterior solutions at t = 0 and t1: smooth profiles along each side
+    (rows of nx + 4 for north/south, columns of ny + 4 for east/west)."""
+    rng = np.random.default_rng(seed)
+
+    def side(n):
+        x = np.linspace(0.0, 1.0, n)
+        lev = []
+        for _ in range(2):
+            a, b, c = rng.uniform(-0.3, 0.3, 3)
+            lev.append(tuple((v * np.sin(np.pi * (k + 1) * x) + 0.05).astype(np.float32).reshape(1, n)
+                             for k, v in enumerate((a, b, c))))
+        return Common.SingleBoundaryConditionData(h=[lev[0][0], lev[1][0]], hu=[lev[0][1], lev[1][1]],
+                                                  hv=[lev[0][2], lev[1][2]])
+    return Common.BoundaryConditionsData(t=[0.0, t1], north=side(nx + 4), south=side(nx + 4), east=side(ny + 4),
+                                         west=side(ny + 4))
+
+
+@pytest.mark.parametrize("codes", [(3, 3, 3, 3), (4, 4, 4, 4), (3, 2, 3, 2), (1, 3, 1, 4)])
+def test_open_boundaries_vs_reference_kernel(ctx, codes):
+    """Open boundaries (3: flow relaxation towards a time-interpolated
+    exterior solution over 10-cell sponges, 4: linear sponge), alone and
+    beside periodic and wall sides: 120 steps against the reference kernel
+    with the reference's boundary kernels after each stage."""
+    cfgd = build_ref.CONFIGS["small_beta"]
+    if not ref_kernel.available(cfgd):
+        pytest.skip("reference kernel library not built")
+    nx, ny = cfgd["nx"], cfgd["ny"]
+    c = SC.grf(96, dx=500.0, steps=120)
+    c.ny = ny
+    c.bc = codes
+    c.Hi = O.fix_bi_ghost_corners(np.ascontiguousarray(c.Hi[: ny + 5]), nx, ny, codes)
+    c.eta0 = np.ascontiguousarray(c.eta0[: ny + 4])
+    c.hu0 = np.zeros_like(c.eta0)
+    c.hv0 = np.zeros_like(c.eta0)
+    c.dt = SC.cfl_dt(c)
+    t1 = 40.0 * c.dt
+    sponge = tuple(10 if k in (3, 4) else 0 for k in codes)
+    data = _open_bc_data(nx, ny, t1, seed=sum(codes))
+    kw = c.kwargs()
+    kw["boundary_conditions"] = Common.BoundaryConditions(*codes, spongeCells={
+        "north": sponge[0], "east": sponge[1], "south": sponge[2], "west": sponge[3]})
+    kw["boundary_conditions_data"] = data
+    sim = CDKLM16.CDKLM16(ctx, dt=c.dt, **kw)
+    for _ in range(c.steps):
+        sim.step(c.dt)
+    mine = sim.download()
+    assert sim.status() == 0
+    ref = ref_kernel.RefKernelSim(cfgd, c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, codes, wind=c.wind)
+    pack = Common.BoundaryConditionsArakawaA._pack
+    ref.set_open_bc(codes, sponge, (0.0, t1), [pack(data.south, data.north, k, True) for k in (0, 1)],
+                    [pack(data.west, data.east, k, False) for k in (0, 1)])
+    for _ in range(c.steps):
+        ref.step(c.dt)
+    theirs = ref.download()
+    errs = [rel_max(a, b) for a, b in zip(mine, theirs)]       # ghost cells included
+    print("open boundaries", codes, "120 steps vs reference kernel:", errs)
+    assert max(errs) == 0.0
+
+
 def test_single_stage_each_rk_step_vs_reference_kernel(ctx):
     """One call of each RK sub-step through the kernel-level ABI
     (go_cdklm_swe_2D vs the reference cdklm_swe_2D) on a perturbed state."""
