@@ -421,6 +421,50 @@ def run_drifters(ctx, n_drifters=100000, steps=100):
                     "launches each step separately once drifters are attached (as CDKLM16.step does)"}
 
 
+def run_open_bc(ctx, steps=100, sponge=10):
+    """Open boundaries on the headline 4096^2 physics: flow relaxation over
+    10-cell sponges on all four sides towards a time-interpolated exterior
+    solution, against the same grid with walls, CDKLM16.step(dt) per step."""
+    import torch
+    from SWESimulators import CDKLM16, Common
+
+    c = make_case("grf4096")
+    rng = np.random.default_rng(11)
+
+    def side(n):
+        lev = [[(rng.uniform(-0.2, 0.2) * np.ones((1, n))).astype(np.float32) for _ in range(3)] for _ in range(2)]
+        return Common.SingleBoundaryConditionData(h=[lev[0][0], lev[1][0]], hu=[lev[0][1], lev[1][1]],
+                                                  hv=[lev[0][2], lev[1][2]])
+
+    def timed(sim):
+        stream = sim.gpu_stream
+        sim.step(c.dt)
+        for _ in range(5):
+            sim.step(c.dt)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            sim.step(c.dt)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / steps
+
+    kw = c.kwargs()
+    kw["boundary_conditions"] = Common.BoundaryConditions(1, 1, 1, 1)
+    walls_ms = timed(CDKLM16.CDKLM16(ctx, dt=c.dt, **kw))
+    kw["boundary_conditions"] = Common.BoundaryConditions(3, 3, 3, 3, spongeCells={
+        "north": sponge, "east": sponge, "south": sponge, "west": sponge})
+    kw["boundary_conditions_data"] = Common.BoundaryConditionsData(
+        t=[0.0, 1000.0 * c.dt], north=side(c.nx + 4), south=side(c.nx + 4), east=side(c.ny + 4), west=side(c.ny + 4))
+    open_ms = timed(CDKLM16.CDKLM16(ctx, dt=c.dt, **kw))
+    return {"workload": "open_bc", "grid": "4096x4096", "sponge_cells": sponge, "steps": steps,
+            "step_ms_walls": walls_ms, "step_ms_open": open_ms, "overhead": open_ms / walls_ms - 1.0,
+            "note": "CUDA events on the simulator's stream; open: relaxation kernels after each RK stage, "
+                    "exterior solution interpolated in time, one step per launch"}
+
+
 def run_adjoint(ctx, n=512, n_steps=500, k=50, kind=0, rows=0):
     """Gradient of the observation misfit (64 cells, steps 50..500, truth
     bumps seed 50001, background 50002) w.r.t. the initial state and the
@@ -644,7 +688,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage", "drifters",
+    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage", "drifters", "open_bc",
                                            "adjoint_batch"],
                     default="grf4096")
     ap.add_argument("--grid", type=int, default=2048, help="grid size of the adjoint_stage workload")
@@ -687,7 +731,7 @@ def main():
         print(json.dumps(line))
         return
 
-    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch", "drifters"):
+    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch", "drifters", "open_bc"):
         if rank != 0:
             return
         from SWESimulators import Common
@@ -702,6 +746,8 @@ def main():
             r = run_adjoint_batch(ctx)
         elif args.workload == "drifters":
             r = run_drifters(ctx)
+        elif args.workload == "open_bc":
+            r = run_open_bc(ctx)
         else:
             r = run_adjoint_stages(ctx, args.grid, reps=args.steps if args.steps < 2000 else 20,
                                    kind=args.adj_kind, rows=args.adj_rows)
@@ -721,6 +767,8 @@ def main():
             value, ms = r["forward_adjoint_gcell_steps_s"], r["forward_adjoint_ms"] / r["steps"]
         elif args.workload == "drifters":
             value, ms = 4096 * 4096 / (r["step_ms_with_drifters"] * 1e-3) / 1e9, r["step_ms_with_drifters"]
+        elif args.workload == "open_bc":
+            value, ms = 4096 * 4096 / (r["step_ms_open"] * 1e-3) / 1e9, r["step_ms_open"]
         else:
             cells_steps = 512 * 512 * r["steps"]
             value, ms = cells_steps / (r["forward_adjoint_ms_k50"] * 1e-3) / 1e9, r["forward_adjoint_ms_k50"] / r["steps"]
@@ -758,7 +806,8 @@ def main():
         ctx = Common.CUDAContext(local)
         secondary = {}
         for name, fn in (("ensemble100", run_ensemble), ("adjoint512", run_adjoint),
-                         ("adjoint_batch", run_adjoint_batch), ("drifters", run_drifters)):
+                         ("adjoint_batch", run_adjoint_batch), ("drifters", run_drifters),
+                         ("open_bc", run_open_bc)):
             try:
                 secondary[name] = fn(ctx)
             except Exception as e:      # a secondary failure must not lose the headline line

@@ -23,10 +23,10 @@ namespace {
 
 constexpr int kHalo = 2;
 
-__global__ void k_frs_ns(int bc_north, int bc_south, int nx, int ny, int sponge_north, int sponge_south, float* h,
+__global__ void k_frs_ns(int row0, int bc_north, int bc_south, int nx, int ny, int sponge_north, int sponge_south, float* h,
                          float* u, float* v, int p, cudaTextureObject_t cur, cudaTextureObject_t next, float bc_t) {
     const int ti = blockIdx.x * blockDim.x + threadIdx.x;
-    const int tj = blockIdx.y * blockDim.y + threadIdx.y;
+    const int tj = row0 + blockIdx.y * blockDim.y + threadIdx.y;   // a band of rows
     if (!(((bc_south == 3 && tj < sponge_south && tj >= 0) ||
            (bc_north == 3 && tj > ny + 2 * kHalo - 1 - sponge_north && tj < ny + 2 * kHalo)) &&
           (ti >= 0 && ti < nx + 2 * kHalo)))
@@ -47,9 +47,9 @@ __global__ void k_frs_ns(int bc_north, int bc_south, int nx, int ny, int sponge_
     v[o] = (1.0f - alpha) * v[o] + alpha * ev;
 }
 
-__global__ void k_frs_ew(int bc_east, int bc_west, int nx, int ny, int sponge_east, int sponge_west, float* h,
+__global__ void k_frs_ew(int col0, int bc_east, int bc_west, int nx, int ny, int sponge_east, int sponge_west, float* h,
                          float* u, float* v, int p, cudaTextureObject_t cur, cudaTextureObject_t next, float bc_t) {
-    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ti = col0 + blockIdx.x * blockDim.x + threadIdx.x;   // a band of columns
     const int tj = blockIdx.y * blockDim.y + threadIdx.y;
     if (!(((bc_west == 3 && ti < sponge_west && ti >= 0) ||
            (bc_east == 3 && ti > nx + 2 * kHalo - 1 - sponge_east && ti < nx + 2 * kHalo)) &&
@@ -72,10 +72,10 @@ __global__ void k_frs_ew(int bc_east, int bc_west, int nx, int ny, int sponge_ea
 
 // Linear between the outer edge and the inner edge of the sponge; the edges
 // themselves keep their values.
-__global__ void k_lin_ns(int bc_north, int bc_south, int nx, int ny, int sponge_north, int sponge_south, float* h,
+__global__ void k_lin_ns(int row0, int bc_north, int bc_south, int nx, int ny, int sponge_north, int sponge_south, float* h,
                          float* u, float* v, int p) {
     const int ti = blockIdx.x * blockDim.x + threadIdx.x;
-    const int tj = blockIdx.y * blockDim.y + threadIdx.y;
+    const int tj = row0 + blockIdx.y * blockDim.y + threadIdx.y;   // a band of rows
     if (!(((bc_south == 4 && tj < sponge_south && tj > 0) ||
            (bc_north == 4 && tj > ny + 2 * kHalo - 1 - sponge_north && tj < ny + 2 * kHalo - 1)) &&
           (ti > 0) && (ti < nx + 2 * kHalo - 1)))
@@ -94,9 +94,9 @@ __global__ void k_lin_ns(int bc_north, int bc_south, int nx, int ny, int sponge_
     v[o] = ov + ratio * (iv - ov);
 }
 
-__global__ void k_lin_ew(int bc_east, int bc_west, int nx, int ny, int sponge_east, int sponge_west, float* h,
+__global__ void k_lin_ew(int col0, int bc_east, int bc_west, int nx, int ny, int sponge_east, int sponge_west, float* h,
                          float* u, float* v, int p) {
-    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ti = col0 + blockIdx.x * blockDim.x + threadIdx.x;   // a band of columns
     const int tj = blockIdx.y * blockDim.y + threadIdx.y;
     if (!(((bc_west == 4 && ti < sponge_west && ti > 0) ||
            (bc_east == 4 && ti > nx + 2 * kHalo - 1 - sponge_east && ti < nx + 2 * kHalo - 1)) &&
@@ -122,32 +122,51 @@ __global__ void k_lin_ew(int bc_east, int bc_west, int nx, int ny, int sponge_ea
 // run (go_boundary_condition calls this for the non-periodic axes).
 int go_open_bc_ns(const go_domain* d, cudaStream_t s, float* h, float* u, float* v, int p) {
     const go::Scheme& k = d->k;
-    const dim3 b(16, 16), g((k.nx + 2 * kHalo + 15) / 16, (k.ny + 2 * kHalo + 15) / 16);
-    if (k.bcN == 3 || k.bcS == 3) {
-        if (!d->bc_tex[0] || !d->bc_tex[1])
-            return go_fail(GO_ERR_INVALID, "flow relaxation north/south needs its exterior textures "
-                                           "(go_domain_set_open_bc)");
-        k_frs_ns<<<g, b, 0, s>>>(k.bcN, k.bcS, k.nx, k.ny, d->sponge[0], d->sponge[2], h, u, v, p,
-                                 (cudaTextureObject_t)d->bc_tex[0], (cudaTextureObject_t)d->bc_tex[1], d->bc_t);
+    if ((k.bcN == 3 || k.bcS == 3) && (!d->bc_tex[0] || !d->bc_tex[1]))
+        return go_fail(GO_ERR_INVALID, "flow relaxation north/south needs its exterior textures "
+                                       "(go_domain_set_open_bc)");
+    // Only the sponge bands are launched: every thread of the reference's
+    // full-grid launch outside them does nothing, and a thread's result
+    // depends on its own cell and on rows no thread of the launch writes.
+    const int rows = k.ny + 2 * kHalo;
+    const int south_end = min(d->sponge[2] + 1, rows);
+    const int bands[2][2] = {{0, south_end},                                          // south
+                             {max(rows - 1 - d->sponge[0], south_end), rows}};        // north, disjoint
+    const dim3 b(16, 16);
+    for (const auto& band : bands) {
+        const int n = band[1] - band[0];
+        if (n <= 0) continue;
+        const dim3 g((k.nx + 2 * kHalo + 15) / 16, (n + 15) / 16);
+        if (k.bcN == 3 || k.bcS == 3)
+            k_frs_ns<<<g, b, 0, s>>>(band[0], k.bcN, k.bcS, k.nx, k.ny, d->sponge[0], d->sponge[2], h, u, v, p,
+                                     (cudaTextureObject_t)d->bc_tex[0], (cudaTextureObject_t)d->bc_tex[1], d->bc_t);
+        if (k.bcN == 4 || k.bcS == 4)
+            k_lin_ns<<<g, b, 0, s>>>(band[0], k.bcN, k.bcS, k.nx, k.ny, d->sponge[0], d->sponge[2], h, u, v, p);
     }
-    if (k.bcN == 4 || k.bcS == 4)
-        k_lin_ns<<<g, b, 0, s>>>(k.bcN, k.bcS, k.nx, k.ny, d->sponge[0], d->sponge[2], h, u, v, p);
     GO_CUDA(cudaGetLastError());
     return GO_OK;
 }
 
 int go_open_bc_ew(const go_domain* d, cudaStream_t s, float* h, float* u, float* v, int p) {
     const go::Scheme& k = d->k;
-    const dim3 b(16, 16), g((k.nx + 2 * kHalo + 15) / 16, (k.ny + 2 * kHalo + 15) / 16);
-    if (k.bcE == 3 || k.bcW == 3) {
-        if (!d->bc_tex[2] || !d->bc_tex[3])
-            return go_fail(GO_ERR_INVALID, "flow relaxation east/west needs its exterior textures "
-                                           "(go_domain_set_open_bc)");
-        k_frs_ew<<<g, b, 0, s>>>(k.bcE, k.bcW, k.nx, k.ny, d->sponge[1], d->sponge[3], h, u, v, p,
-                                 (cudaTextureObject_t)d->bc_tex[2], (cudaTextureObject_t)d->bc_tex[3], d->bc_t);
+    if ((k.bcE == 3 || k.bcW == 3) && (!d->bc_tex[2] || !d->bc_tex[3]))
+        return go_fail(GO_ERR_INVALID, "flow relaxation east/west needs its exterior textures "
+                                       "(go_domain_set_open_bc)");
+    const int cols = k.nx + 2 * kHalo;
+    const int west_end = min(d->sponge[3] + 1, cols);
+    const int bands[2][2] = {{0, west_end},                                           // west
+                             {max(cols - 1 - d->sponge[1], west_end), cols}};         // east, disjoint
+    const dim3 b(16, 16);
+    for (const auto& band : bands) {
+        const int n = band[1] - band[0];
+        if (n <= 0) continue;
+        const dim3 g((n + 15) / 16, (k.ny + 2 * kHalo + 15) / 16);
+        if (k.bcE == 3 || k.bcW == 3)
+            k_frs_ew<<<g, b, 0, s>>>(band[0], k.bcE, k.bcW, k.nx, k.ny, d->sponge[1], d->sponge[3], h, u, v, p,
+                                     (cudaTextureObject_t)d->bc_tex[2], (cudaTextureObject_t)d->bc_tex[3], d->bc_t);
+        if (k.bcE == 4 || k.bcW == 4)
+            k_lin_ew<<<g, b, 0, s>>>(band[0], k.bcE, k.bcW, k.nx, k.ny, d->sponge[1], d->sponge[3], h, u, v, p);
     }
-    if (k.bcE == 4 || k.bcW == 4)
-        k_lin_ew<<<g, b, 0, s>>>(k.bcE, k.bcW, k.nx, k.ny, d->sponge[1], d->sponge[3], h, u, v, p);
     GO_CUDA(cudaGetLastError());
     return GO_OK;
 }
