@@ -7,9 +7,10 @@ attributes other modules read (``gpu_data.h0 ...``, ``bathymetry``,
 ``gpu_stream``, ``t``, ``num_iterations``, ...).
 
 What is not built raises ``NotImplementedError`` at construction:
-a spatially varying grid angle, ``latitude``,
-the stochastic model error (``small_scale_perturbation``), NetCDF output,
-``rk_order`` other than 2.  The Coriolis table is always full-resolution
+a spatially varying grid angle, ``latitude``, NetCDF output,
+``rk_order`` other than 2.  The stochastic model error
+(``small_scale_perturbation``) runs on OceanStateNoise after each step.
+The Coriolis table is always full-resolution
 (``subsample_f``/``subsample_angle`` are accepted and ignored; the
 reference's subsampler calls ``scipy.interpolate.interp2d``, which the
 installed SciPy no longer provides).
@@ -19,7 +20,7 @@ import logging
 
 import numpy as np
 
-from . import Common, Simulator, WindStress, _native
+from . import Common, OceanStateNoise, Simulator, WindStress, _native
 
 
 class CDKLM16(Simulator.Simulator):
@@ -42,8 +43,6 @@ class CDKLM16(Simulator.Simulator):
         self.logger = logging.getLogger(__name__)
         if rk_order != 2:
             raise NotImplementedError("only rk_order=2 (Heun) is built")
-        if small_scale_perturbation:
-            raise NotImplementedError("the stochastic model error (OceanStateNoise) is not built")
         if write_netcdf:
             raise NotImplementedError("NetCDF output is not built (netCDF4 is not available)")
         if latitude is not None:
@@ -60,6 +59,7 @@ class CDKLM16(Simulator.Simulator):
 
         # CDKLM16.py:146-148 -- f compensated to the first interior cell
         a0 = float(angle.reshape(-1)[0])
+        self._angle0 = np.float32(a0)
         north = np.array([np.sin(a0), np.cos(a0)])
         f = f - coriolis_beta * (x_zero_reference_cell * dx * north[0] + y_zero_reference_cell * dy * north[1])
         x_zero_reference_cell = 0
@@ -107,9 +107,16 @@ class CDKLM16(Simulator.Simulator):
         self.coriolis_rows = self._coriolis_rows(eta0, angle, a0)
         self._domain.set_coriolis(self.coriolis_rows)
 
-        self.small_scale_perturbation = False
+        # stochastic model error (CDKLM16.py:355-367)
+        self.small_scale_perturbation = small_scale_perturbation
         self.small_scale_model_error = None
         self.small_scale_perturbation_interpolation_factor = small_scale_perturbation_interpolation_factor
+        if small_scale_perturbation:
+            self.small_scale_model_error = OceanStateNoise.OceanStateNoise.fromsim(
+                self, soar_q0=small_scale_perturbation_amplitude,
+                interpolation_factor=small_scale_perturbation_interpolation_factor, use_lcg=use_lcg,
+                xorwow_seed=xorwow_seed, block_width=block_width_model_error,
+                block_height=block_height_model_error)
         self.model_time_step = model_time_step
         self.total_time_steps = 0
         if model_time_step is None:
@@ -146,6 +153,8 @@ class CDKLM16(Simulator.Simulator):
             self.gpu_data.release()
         if getattr(self, "bathymetry", None) is not None:
             self.bathymetry.release()
+        if getattr(self, "small_scale_model_error", None) is not None:
+            self.small_scale_model_error.cleanUp()
         self.gpu_ctx = None
 
     @classmethod
@@ -167,6 +176,7 @@ class CDKLM16(Simulator.Simulator):
         """Advance by t_end seconds in steps of self.dt; the last step is
         shortened to land on t_end (CDKLM16.py:494-598)."""
         open_bc = self.boundary_conditions.isSponge()
+        perturb = self.small_scale_perturbation and apply_stochastic_term
         if self.t == 0:
             self.bc_kernel.update_bc_values(self.gpu_stream, self.t)
             self.bc_kernel.boundaryCondition(self.gpu_stream, self.gpu_data.h0, self.gpu_data.hu0,
@@ -183,18 +193,23 @@ class CDKLM16(Simulator.Simulator):
             local_dt = np.float32(min(self.dt, np.float32(t_end - t_now)))
             wind_t = np.float32(self.update_wind_stress())
             if pending_n and (local_dt != pending_dt or wind_t != pending_w or time_varying_wind
-                              or self.hasDrifters or open_bc):
+                              or self.hasDrifters or open_bc or perturb):
                 self._launch_steps(pending_n, pending_dt, pending_w)
                 pending_n = 0
             pending_n += 1
             pending_dt, pending_w = local_dt, wind_t
-            if self.hasDrifters or time_varying_wind or open_bc:
+            if self.hasDrifters or time_varying_wind or open_bc or perturb:
                 # one launch per step: the drifters move between steps, the
-                # wind or the exterior solution of this step's time
+                # wind or the exterior solution of this step's time, the
+                # model error perturbs each step's result before its
+                # boundary conditions (CDKLM16.py:580-586)
                 if open_bc:
                     self.bc_kernel.update_bc_values(self.gpu_stream, self.t)
                 self._launch_steps(pending_n, pending_dt, pending_w)
                 pending_n = 0
+                if perturb:
+                    self.small_scale_model_error.perturbSim(self)
+                    self.applyBoundaryConditions()
                 self.drifterStep(local_dt)
             self.t += np.float64(local_dt)
             t_now += np.float64(local_dt)
@@ -227,8 +242,21 @@ class CDKLM16(Simulator.Simulator):
             float(self.bathymetry.mask_value), float(wind_stress_t), packed))
 
     def perturbState(self, q0_scale=1):
+        """Adds one model-error perturbation (CDKLM16.py:642-644)."""
         if self.small_scale_perturbation:
-            raise NotImplementedError("the stochastic model error is not built")
+            self.small_scale_model_error.perturbSim(self, q0_scale=q0_scale)
+
+    def angle_texture_field(self):
+        """The grid angle as the reference's 1 x 1 angle texture."""
+        return np.array([[self._angle0]], dtype=np.float32)
+
+    def coriolis_texture_field(self):
+        """The Coriolis parameter per ghost-inclusive row as a one-column
+        texture (rows vary; the kernels read it where f is zero)."""
+        rows = np.asarray(self.coriolis_rows, dtype=np.float32)
+        if np.all(rows == rows[0]):
+            return rows[:1].reshape(1, 1)
+        return np.ascontiguousarray(rows.reshape(-1, 1))
 
     def applyBoundaryConditions(self):
         self.bc_kernel.boundaryCondition(self.gpu_stream, self.gpu_data.h0, self.gpu_data.hu0, self.gpu_data.hv0)

@@ -107,6 +107,18 @@ SIGNATURES = {
     "go_bc_texture_create": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_uint64)]),
     "go_domain_set_open_bc": (_I, [_P, _P, _F]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
+    "go_noise_lcg": (_I, [_P, _I, _I, _I, _I, _P, _I, _P, _I]),
+    "go_noise_xorwow_state_bytes": (ctypes.c_size_t, []),
+    "go_noise_xorwow_init": (_I, [_P, ctypes.c_uint64, _I, _P]),
+    "go_noise_xorwow_fill": (_I, [_P, _I, _I, _P, _I, _I, _P, _I]),
+    "go_noise_soar": (_I, [_P, _I, _I, _F, _F, _F, _F, _F, _I, _I, _P, _I, _P, _I, _I]),
+    "go_noise_geostrophic": (_I, [_P, _I, _I, _F, _F, _I, _I, _F, _F, _F, _F, _P, _I, _P, _I, _P, _I, _P, _I,
+                                  _P, _I, _F, ctypes.c_uint64, ctypes.c_uint64]),
+    "go_noise_bicubic": (_I, [_P, _I, _I, _I, _I, _F, _F, _I, _I, _I, _I, _F, _F, _I, _I, _F, _F, _F, _F, _P, _I,
+                              _P, _I, _P, _I, _P, _I, _P, _I, _F, ctypes.c_uint64, ctypes.c_uint64]),
+    "go_noise_reduce_scratch_bytes": (ctypes.c_size_t, []),
+    "go_noise_square_sums": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _P, ctypes.c_size_t]),
+    "go_noise_make_perpendicular": (_I, [_P, _I, _I, _P, _I, _P, _I, _P]),
     "go_batch_create": (_I, [ctypes.POINTER(ctypes.c_void_p), _I, ctypes.POINTER(ctypes.c_void_p)]),
     "go_batch_destroy": (_I, [_P]),
     "go_batch_set_member": (_I, [_P, _I, _F, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _F, _F]),

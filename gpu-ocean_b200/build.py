@@ -36,6 +36,10 @@ UNIT_FLAGS = {"adjoint.cu": {"--fmad=false": "--fmad=true"},
                               "--prec-sqrt=false": "--prec-sqrt=true", "--fmad=false": "--fmad=true"}}
 # ... and its boundary kernels (open boundaries) the same way
 UNIT_FLAGS["open_boundaries.cu"] = UNIT_FLAGS["drifters.cu"]
+# the model-error kernels with --use_fast_math (OceanStateNoise.py:222-227):
+# flush to zero, approximate division and square root (already set), FMA
+# contraction and the fast intrinsics for logf, expf, sinf, cosf
+UNIT_FLAGS["ocean_noise.cu"] = {"--fmad=false": "--use_fast_math"}
 
 
 def flags_for(unit):

@@ -1,0 +1,624 @@
+// Stochastic model error of OceanStateNoise: random fields (LCG or XORWOW),
+// SOAR-correlated perturbation of eta on a coarse grid, and the
+// geostrophically balanced perturbation of (eta, hu, hv) on the model grid,
+// directly (interpolation factor 1) or through bicubic interpolation.
+//
+// Restates, kernel by kernel:
+//   gpu_ocean/SWESimulators/gpu_kernels/ocean_noise.cu:81-118   (ansic_lcg, boxMuller)
+//   gpu_ocean/SWESimulators/gpu_kernels/ocean_noise.cu:121-200  (uniformDistribution, normalDistribution)
+//   gpu_ocean/SWESimulators/gpu_kernels/ocean_noise.cu:206-241  (makePerpendicular)
+//   gpu_ocean/SWESimulators/gpu_kernels/ocean_noise.cu:249-372  (soar_covariance, SOAR)
+//   gpu_ocean/SWESimulators/gpu_kernels/ocean_noise.cu:379-508  (geostrophicBalance)
+//   gpu_ocean/SWESimulators/gpu_kernels/ocean_noise.cu:522-772  (bicubicInterpolation)
+//   gpu_ocean/SWESimulators/gpu_kernels/common.cu:696-819       (bicubic coefficients, evaluation)
+//   gpu_ocean/SWESimulators/gpu_kernels/reductions.cu           (squareSum, squareSumDouble)
+// The reference compiles ocean_noise.cu with --use_fast_math
+// (OceanStateNoise.py:222-227), so this unit is built with the same option
+// (build.py UNIT_FLAGS) and writes each expression with the reference's
+// operand order: approximate logf/expf/sqrtf/division and FMA contraction
+// then round the same way.
+//
+// What differs from the reference's kernels, by design:
+//  * SOAR: the 25 covariance weights depend only on the tap offset, so each
+//    block evaluates them once (the reference's expression, per offset) into
+//    shared memory instead of once per tap per cell; the sum runs in the
+//    reference's tap order with the same fused multiply-adds.
+//  * Per-cell indexing: every kernel computes each cell's sources from its
+//    own global index (clamped or wrapped as the reference's shared tiles
+//    are filled), so the launch shape is free and no thread reads past the
+//    arrays (the reference's tiles read one row past the random buffer, and
+//    its bicubic tile origin depends on the block).
+//  * Reductions: many blocks with double accumulators and a fixed-order
+//    finish by the last block, instead of one 128-thread block in float.
+//  * XORWOW: curand's XORWOW device generator with one persistent state per
+//    generator (pycuda's XORWOWRandomNumberGenerator uses the same
+//    generator; its seeds and stream layout are its own, so the XORWOW path
+//    matches the reference in distribution, not draw for draw).
+#include "internal.h"
+
+#include <curand_kernel.h>
+
+namespace {
+
+constexpr int kCutoff = 2;             // OceanStateNoise.py:96 (config.soar_cutoff)
+constexpr int kBW = 32, kBH = 8;       // 2-D blocks of the per-cell kernels
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+__device__ __forceinline__ int wrap(int v, int n) { return ((v % n) + n) % n; }
+
+// ---- random numbers ---------------------------------------------------------
+
+// ANSI C LCG, two draws (ocean_noise.cu:81-99): seed <- (seed a + c) mod m,
+// u = seed / 2^31 rounded to float.
+__device__ __forceinline__ float2 lcg_pair(unsigned long long& seed) {
+    const unsigned long long m = 2147483647ULL;
+    seed = ((seed * 1103515245ULL) + 12345ULL) % m;
+    const float u1 = (float)((double)seed / 2147483648.0);
+    seed = ((seed * 1103515245ULL) + 12345ULL) % m;
+    const float u2 = (float)((double)seed / 2147483648.0);
+    return make_float2(u1, u2);
+}
+
+// Box-Muller (ocean_noise.cu:106-116).
+__device__ __forceinline__ float2 box_muller(float2 u) {
+    const float r = sqrtf(-2.0f * logf(u.x));
+    return make_float2(r * cospif(2 * u.y), r * sinpif(2 * u.y));
+}
+
+// One thread per seed; writes its pair into columns 2i, 2i+1 of its row
+// (ocean_noise.cu:121-200).  The reference's branch for a lone last column
+// (2i == random_nx) is met by no thread, so an odd width keeps its last
+// column unwritten; kept as it is for parity.
+__global__ void k_lcg(int normal, int seed_nx, int seed_ny, int random_nx, unsigned long long* __restrict__ seed,
+                      int sp, float* __restrict__ rnd, int rp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= seed_nx || j >= seed_ny) return;
+    unsigned long long s = seed[(size_t)j * sp + i];
+    float2 u = lcg_pair(s);
+    if (normal) u = box_muller(u);
+    seed[(size_t)j * sp + i] = s;
+    float* row = rnd + (size_t)j * rp;
+    if (2 * i + 1 < random_nx) {
+        row[2 * i] = u.x;
+        row[2 * i + 1] = u.y;
+    } else if (2 * i == random_nx) {
+        row[2 * i] = u.x;
+    }
+}
+
+__global__ void k_xorwow_init(unsigned long long seed, int n, curandStateXORWOW_t* __restrict__ states) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    curandStateXORWOW_t st;
+    curand_init(seed, (unsigned long long)g, 0ULL, &st);
+    states[g] = st;
+}
+
+// Generator g fills the element pairs g, g + n, g + 2n, ... of the row-major
+// nx x ny field (pitched rows).
+__global__ void k_xorwow_fill(int normal, int n, curandStateXORWOW_t* __restrict__ states, int nx, int ny,
+                              float* __restrict__ out, int op) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    curandStateXORWOW_t st = states[g];
+    const long long total = (long long)nx * ny;
+    for (long long e = 2LL * g; e < total; e += 2LL * n) {
+        float2 v;
+        if (normal) {
+            v = curand_normal2(&st);
+        } else {
+            v.x = curand_uniform(&st);
+            v.y = curand_uniform(&st);
+        }
+        const int j0 = (int)(e / nx), i0 = (int)(e % nx);
+        out[(size_t)j0 * op + i0] = v.x;
+        if (e + 1 < total) {
+            const int j1 = (int)((e + 1) / nx), i1 = (int)((e + 1) % nx);
+            out[(size_t)j1 * op + i1] = v.y;
+        }
+    }
+    states[g] = st;
+}
+
+// ---- SOAR covariance on the coarse grid ---------------------------------------
+
+// soar_covariance of ocean_noise.cu:249-255 for the tap offset (ox, oy) =
+// (a_x - b_x, a_y - b_y).
+__device__ __forceinline__ float soar_weight(int ox, int oy, float dx, float dy, float q0, float L) {
+    const float dist = sqrtf(dx * dx * ox * ox + dy * dy * oy * oy);
+    return q0 * (1.0f + dist / L) * expf(-dist / L);
+}
+
+// Row (or column) of the random buffer behind coarse index c, tap k in
+// [0, 4] (ocean_noise.cu:300-330): wrapped over the n interior values when
+// periodic, else c + k in a buffer with 4 extra values on each side.
+__device__ __forceinline__ int random_src(int c, int k, int n, int periodic) {
+    return periodic ? wrap(c + k - 2 * kCutoff, n) : min(c + k, n + 4 * kCutoff - 1);
+}
+
+// One thread per coarse cell, ghost cells included ((nx+4) x (ny+4)):
+// coarse = scale * sum_taps Q(tap) xi(tap), or += when additive
+// (ocean_noise.cu:264-372).
+__global__ void __launch_bounds__(kBW* kBH) k_soar(int nx, int ny, float dx, float dy, float q0, float L, float scale,
+                                                   int pns, int pew, const float* __restrict__ rnd, int rp,
+                                                   float* __restrict__ coarse, int cp, int additive) {
+    constexpr int TW = kBW + 2 * kCutoff, TH = kBH + 2 * kCutoff;
+    __shared__ float xi[TH][TW];
+    __shared__ float w[2 * kCutoff + 1][2 * kCutoff + 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int t = ty * kBW + tx;
+    const int bx = blockIdx.x * kBW, by = blockIdx.y * kBH;
+    if (t < (2 * kCutoff + 1) * (2 * kCutoff + 1)) {
+        const int ky = t / (2 * kCutoff + 1), kx = t % (2 * kCutoff + 1);
+        w[ky][kx] = soar_weight(kCutoff - kx, kCutoff - ky, dx, dy, q0, L);
+    }
+    for (int j = ty; j < TH; j += kBH) {
+        const int gj = random_src(by + j, 0, ny, pns);
+        const float* row = rnd + (size_t)gj * rp;
+        for (int i = tx; i < TW; i += kBW) xi[j][i] = __ldg(row + random_src(bx + i, 0, nx, pew));
+    }
+    __syncthreads();
+    const int ti = bx + tx, tj = by + ty;
+    if (ti >= nx + 4 || tj >= ny + 4) return;
+    float acc = 0.0f;
+#pragma unroll
+    for (int ky = 0; ky <= 2 * kCutoff; ++ky) {
+#pragma unroll
+        for (int kx = 0; kx <= 2 * kCutoff; ++kx) acc = __fmaf_rn(w[ky][kx], xi[ty + ky][tx + kx], acc);
+    }
+    float* out = coarse + (size_t)tj * cp + ti;
+    if (additive > 0)
+        *out = __fmaf_rn(scale, acc, *out);
+    else
+        *out = scale * acc;
+}
+
+// ---- geostrophic balance -------------------------------------------------------
+
+struct BalanceArgs {
+    int nx, ny, gx, gy;
+    float dx, dy, g, f, beta;
+    const float* coarse;
+    int cp;
+    float *eta, *hu, *hv;
+    int pe, pu, pv;
+    const float* Hi;
+    int ph;
+    float land;
+    cudaTextureObject_t angle, coriolis;
+};
+
+// H at the cell centre and whether a corner is land (ocean_noise.cu:418-438).
+__device__ __forceinline__ void cell_depth(const BalanceArgs& a, int ti, int tj, float& H_mid, bool& dry) {
+    const int j0 = clampi(tj, 0, a.ny + 4), j1 = clampi(tj + 1, 0, a.ny + 4);
+    const int i0 = clampi(ti, 0, a.nx + 4), i1 = clampi(ti + 1, 0, a.nx + 4);
+    const float h00 = __ldg(a.Hi + (size_t)j0 * a.ph + i0), h01 = __ldg(a.Hi + (size_t)j0 * a.ph + i1);
+    const float h10 = __ldg(a.Hi + (size_t)j1 * a.ph + i0), h11 = __ldg(a.Hi + (size_t)j1 * a.ph + i1);
+    dry = (h00 == a.land) || (h01 == a.land) || (h10 == a.land) || (h11 == a.land);
+    H_mid = 0.25f * (h00 + h01 + h10 + h11);
+}
+
+// Coriolis parameter at cell (ti, tj) (ocean_noise.cu:471-476, 38-67): the
+// beta plane along the texture's north vector, or the Coriolis texture
+// when f is zero.
+__device__ __forceinline__ float cell_coriolis(const BalanceArgs& a, int ti, int tj) {
+    const float s = (ti + 0.5f) / (a.nx + 4.0f);
+    const float t = (tj + 0.5f) / (a.ny + 4.0f);
+    const float angle = tex2D<float>(a.angle, s, t);
+    const float2 north = make_float2(sinf(angle), cosf(angle));
+    float coriolis = a.f + a.beta * ((ti + 0.5f) * a.dx * north.x + (tj + 0.5f) * a.dy * north.y);
+    if (a.f == 0) coriolis = tex2D<float>(a.coriolis, s, t);
+    return coriolis;
+}
+
+// Interior cells of the model grid; the coarse grid is the model grid
+// (ocean_noise.cu:379-508).
+__global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a) {
+    const int ti = blockIdx.x * kBW + threadIdx.x + a.gx;
+    const int tj = blockIdx.y * kBH + threadIdx.y + a.gy;
+    if (!(ti > 1 && tj > 1 && ti < a.nx + 2 && tj < a.ny + 2)) return;
+    float H_mid;
+    bool dry;
+    cell_depth(a, ti, tj, H_mid, dry);
+    auto c = [&](int i, int j) {
+        return __ldg(a.coarse + (size_t)clampi(j, 0, a.ny + 3) * a.cp + clampi(i, 0, a.nx + 3));
+    };
+    const float d = c(ti, tj);
+    const float coriolis = cell_coriolis(a, ti, tj);
+    float* eta = a.eta + (size_t)tj * a.pe + ti;
+    float* hu = a.hu + (size_t)tj * a.pu + ti;
+    float* hv = a.hv + (size_t)tj * a.pv + ti;
+    const float h_mid = d + H_mid + *eta;
+    const float eta_diff_x = (c(ti + 1, tj) - c(ti - 1, tj)) / (2.0f * a.dx);
+    const float eta_diff_y = (c(ti, tj + 1) - c(ti, tj - 1)) / (2.0f * a.dy);
+    const float d_hu = -(a.g / coriolis) * h_mid * eta_diff_y;
+    const float d_hv = (a.g / coriolis) * h_mid * eta_diff_x;
+    if (dry) {
+        *eta = 0.0f;
+        *hu = 0.0f;
+        *hv = 0.0f;
+    } else {
+        *eta += d;
+        *hu += d_hu;
+        *hv += d_hv;
+    }
+}
+
+// ---- bicubic interpolation from the coarse grid ---------------------------------
+
+struct M4 {
+    float4 r0, r1, r2, r3;
+};
+
+__device__ __forceinline__ float dot4(const float4 a, const float4 b) {
+    return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
+}
+
+// Coefficients B F B^T of the bicubic patch for corner values and
+// derivatives F (common.cu:723-801; B = [[1,0,0,0],[0,0,1,0],[-3,3,-2,-1],
+// [2,-2,1,1]]), as dot products of F's rows with B's rows, then B's rows
+// with those.
+__device__ __forceinline__ M4 bicubic_coefficients(const M4 f) {
+    const float4 b0 = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+    const float4 b1 = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    const float4 b2 = make_float4(-3.0f, 3.0f, -2.0f, -1.0f);
+    const float4 b3 = make_float4(2.0f, -2.0f, 1.0f, 1.0f);
+    M4 ft;   // (F B^T)^T
+    ft.r0 = make_float4(dot4(f.r0, b0), dot4(f.r1, b0), dot4(f.r2, b0), dot4(f.r3, b0));
+    ft.r1 = make_float4(dot4(f.r0, b1), dot4(f.r1, b1), dot4(f.r2, b1), dot4(f.r3, b1));
+    ft.r2 = make_float4(dot4(f.r0, b2), dot4(f.r1, b2), dot4(f.r2, b2), dot4(f.r3, b2));
+    ft.r3 = make_float4(dot4(f.r0, b3), dot4(f.r1, b3), dot4(f.r2, b3), dot4(f.r3, b3));
+    M4 o;
+    o.r0 = make_float4(dot4(b0, ft.r0), dot4(b0, ft.r1), dot4(b0, ft.r2), dot4(b0, ft.r3));
+    o.r1 = make_float4(dot4(b1, ft.r0), dot4(b1, ft.r1), dot4(b1, ft.r2), dot4(b1, ft.r3));
+    o.r2 = make_float4(dot4(b2, ft.r0), dot4(b2, ft.r1), dot4(b2, ft.r2), dot4(b2, ft.r3));
+    o.r3 = make_float4(dot4(b3, ft.r0), dot4(b3, ft.r1), dot4(b3, ft.r2), dot4(b3, ft.r3));
+    return o;
+}
+
+// x^T C y (common.cu:803-819).
+__device__ __forceinline__ float bicubic_eval(const float4 x, const float4 y, const M4 c) {
+    const float4 tmp = make_float4(dot4(c.r0, y), dot4(c.r1, y), dot4(c.r2, y), dot4(c.r3, y));
+    return dot4(x, tmp);
+}
+
+struct InterpArgs {
+    BalanceArgs b;
+    int cnx, cny, cgx, cgy;
+    float cdx, cdy;
+    int off_i, off_j;
+};
+
+// d_eta at ghost-inclusive model cell (ti, tj): the coarse cell below-left
+// of the cell centre, its 4x4 neighbourhood (clamped to the coarse array),
+// central differences for the derivatives and the bicubic patch
+// (ocean_noise.cu:610-705).
+__device__ float interpolate(const InterpArgs& a, int ti, int tj) {
+    const float x = (ti - a.b.gx + 0.5f + a.off_i) * a.b.dx;
+    const float y = (tj - a.b.gy + 0.5f + a.off_j) * a.b.dy;
+    int ci = (int)(floorf((x / a.cdx) + a.cgx - 0.5f));
+    int cj = (int)(floorf((y / a.cdy) + a.cgy - 0.5f));
+    if (ci > a.cnx + 1) ci -= 1;
+    if (cj > a.cny + 1) cj -= 1;
+    const float coarse_x = (ci - a.cgx + 0.5f) * a.cdx;
+    const float coarse_y = (cj - a.cgy + 0.5f) * a.cdy;
+    auto c = [&](int di, int dj) {
+        return __ldg(a.b.coarse + (size_t)clampi(cj + dj, 0, a.cny + 3) * a.b.cp + clampi(ci + di, 0, a.cnx + 3));
+    };
+    M4 f;
+    f.r0.x = c(0, 0);
+    f.r0.y = c(0, 1);
+    f.r1.x = c(1, 0);
+    f.r1.y = c(1, 1);
+    f.r2.x = (c(1, 0) - c(-1, 0)) / 2.0f;
+    f.r2.y = (c(1, 1) - c(-1, 1)) / 2.0f;
+    f.r3.x = (c(2, 0) - c(0, 0)) / 2.0f;
+    f.r3.y = (c(2, 1) - c(0, 1)) / 2.0f;
+    f.r0.z = (c(0, 1) - c(0, -1)) / 2.0f;
+    f.r0.w = (c(0, 2) - c(0, 0)) / 2.0f;
+    f.r1.z = (c(1, 1) - c(1, -1)) / 2.0f;
+    f.r1.w = (c(1, 2) - c(1, 0)) / 2.0f;
+    const float fy_10 = (c(-1, 1) - c(-1, -1)) / 2.0f;
+    const float fy_11 = (c(-1, 2) - c(-1, 0)) / 2.0f;
+    const float fy20 = (c(2, 1) - c(2, -1)) / 2.0f;
+    const float fy21 = (c(2, 2) - c(2, 0)) / 2.0f;
+    f.r2.z = (f.r1.z - fy_10) / 2.0f;
+    f.r2.w = (f.r1.w - fy_11) / 2.0f;
+    f.r3.z = (fy20 - f.r0.z) / 2.0f;
+    f.r3.w = (fy21 - f.r0.w) / 2.0f;
+    const float rel_x = (x - coarse_x) / a.cdx;
+    const float rel_y = (y - coarse_y) / a.cdy;
+    const M4 coef = bicubic_coefficients(f);
+    const float4 xv = make_float4(1.0f, rel_x, rel_x * rel_x, rel_x * rel_x * rel_x);
+    const float4 yv = make_float4(1.0f, rel_y, rel_y * rel_y, rel_y * rel_y * rel_y);
+    return bicubic_eval(xv, yv, coef);
+}
+
+// Interior cells: d_eta interpolated on the block and a one-cell halo into
+// shared memory, then the geostrophic balance from its central differences
+// (ocean_noise.cu:522-772).
+__global__ void __launch_bounds__(kBW* kBH) k_interp_balance(const InterpArgs a) {
+    __shared__ float d_eta[kBH + 2][kBW + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int bx = blockIdx.x * kBW + a.b.gx, by = blockIdx.y * kBH + a.b.gy;
+    for (int j = ty; j < kBH + 2; j += kBH)
+        for (int i = tx; i < kBW + 2; i += kBW) d_eta[j][i] = interpolate(a, bx + i - 1, by + j - 1);
+    __syncthreads();
+    const int ti = bx + tx, tj = by + ty;
+    if (!(ti > 1 && tj > 1 && ti < a.b.nx + 2 && tj < a.b.ny + 2)) return;
+    float H_mid;
+    bool dry;
+    cell_depth(a.b, ti, tj, H_mid, dry);
+    const float coriolis = cell_coriolis(a.b, ti, tj);
+    const int ex = tx + 1, ey = ty + 1;
+    const float eta_diff_x = (d_eta[ey][ex + 1] - d_eta[ey][ex - 1]) / (2.0f * a.b.dx);
+    const float eta_diff_y = (d_eta[ey + 1][ex] - d_eta[ey - 1][ex]) / (2.0f * a.b.dy);
+    float d = d_eta[ey][ex];
+    float d_hu = -(a.b.g / coriolis) * (H_mid + d) * eta_diff_y;
+    float d_hv = (a.b.g / coriolis) * (H_mid + d) * eta_diff_x;
+    if (dry) {
+        d = 0.0f;
+        d_hu = 0.0f;
+        d_hv = 0.0f;
+    }
+    a.b.eta[(size_t)tj * a.b.pe + ti] += d;
+    a.b.hu[(size_t)tj * a.b.pu + ti] += d_hu;
+    a.b.hv[(size_t)tj * a.b.pv + ti] += d_hv;
+}
+
+// ---- reductions and the perpendicular field ------------------------------------
+
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocksMax = 1184;    // 148 SMs x 8
+
+struct RedScratch {
+    unsigned int ticket;
+    unsigned int pad;
+    double part[kRedBlocksMax][3];
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block sums of a^2 (and b^2, a b when b is given) over an nx x ny pitched
+// field; the last block to finish adds the partials in block order and
+// writes the floats (reductions.cu: squareSum, squareSumDouble).
+__global__ void __launch_bounds__(kRedThreads) k_square_sums(int nx, int ny, const float* __restrict__ a, int pa,
+                                                             const float* __restrict__ b, int pb,
+                                                             float* __restrict__ result, RedScratch* s) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    const long long total = (long long)nx * ny;
+    for (long long e = (long long)blockIdx.x * kRedThreads + threadIdx.x; e < total;
+         e += (long long)gridDim.x * kRedThreads) {
+        const int j = (int)(e / nx), i = (int)(e % nx);
+        const double x = __ldg(a + (size_t)j * pa + i);
+        s0 += x * x;
+        if (b) {
+            const double y = __ldg(b + (size_t)j * pb + i);
+            s1 += y * y;
+            s2 += x * y;
+        }
+    }
+    __shared__ double red[3][kRedThreads / 32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    if (lane == 0) {
+        red[0][warp] = s0;
+        red[1][warp] = s1;
+        red[2][warp] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+        for (int w = 0; w < kRedThreads / 32; ++w) {
+            t0 += red[0][w];
+            t1 += red[1][w];
+            t2 += red[2][w];
+        }
+        s->part[blockIdx.x][0] = t0;
+        s->part[blockIdx.x][1] = t1;
+        s->part[blockIdx.x][2] = t2;
+        __threadfence();
+        last = (atomicAdd(&s->ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    for (unsigned int k = 0; k < gridDim.x; ++k) {
+        t0 += ((volatile double*)s->part[k])[0];
+        t1 += ((volatile double*)s->part[k])[1];
+        t2 += ((volatile double*)s->part[k])[2];
+    }
+    result[0] = (float)t0;
+    if (b) {
+        result[1] = (float)t1;
+        result[2] = (float)t2;
+    }
+    s->ticket = 0;
+}
+
+// nu <- sqrt(|nu|^2 / |nu_perp|^2) (nu - (xi.nu / |xi|^2) xi)
+// (ocean_noise.cu:206-241), from the three sums in red.
+__global__ void k_make_perpendicular(int nx, int ny, const float* __restrict__ xi, int px, float* __restrict__ nu,
+                                     int pn, const float* __restrict__ red) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    const float xi_norm = red[0];
+    const float nu_norm = red[1];
+    const float dot_product = red[2];
+    const float parallel_factor = dot_product / xi_norm;
+    const float perpendicular_norm = nu_norm - parallel_factor * dot_product;
+    float* n = nu + (size_t)j * pn + i;
+    *n = sqrtf(nu_norm / perpendicular_norm) * (*n - (parallel_factor * xi[(size_t)j * px + i]));
+}
+
+int check_field(int pitch_bytes, int width, const char* what) { return go_check_pitch(pitch_bytes, width, what); }
+
+}  // namespace
+
+extern "C" {
+
+int go_noise_lcg(void* stream, int normal, int seed_nx, int seed_ny, int random_nx, uint64_t* seed,
+                 int seed_pitch, float* random, int random_pitch) {
+    if (!seed || !random) return go_fail(GO_ERR_INVALID, "null argument");
+    if (seed_nx < 1 || seed_ny < 1 || random_nx < 1 || (random_nx + 1) / 2 > seed_nx)
+        return go_fail(GO_ERR_INVALID, "seed grid %d x %d cannot fill %d random columns", seed_nx, seed_ny,
+                       random_nx);
+    if (seed_pitch < 8 * seed_nx || seed_pitch % 8)
+        return go_fail(GO_ERR_INVALID, "seed pitch %d for %d seeds", seed_pitch, seed_nx);
+    int rc = check_field(random_pitch, random_nx, "random");
+    if (rc) return rc;
+    const dim3 block(64, 4);
+    const dim3 grid((seed_nx + 63) / 64, (seed_ny + 3) / 4);
+    k_lcg<<<grid, block, 0, (cudaStream_t)stream>>>(normal, seed_nx, seed_ny, random_nx,
+                                                    (unsigned long long*)seed, seed_pitch / 8, random,
+                                                    random_pitch / 4);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+size_t go_noise_xorwow_state_bytes(void) { return sizeof(curandStateXORWOW_t); }
+
+int go_noise_xorwow_init(void* stream, uint64_t seed, int n_generators, void* states) {
+    if (!states || n_generators < 1) return go_fail(GO_ERR_INVALID, "no generator states");
+    k_xorwow_init<<<(n_generators + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+        (unsigned long long)seed, n_generators, (curandStateXORWOW_t*)states);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+int go_noise_xorwow_fill(void* stream, int normal, int n_generators, void* states, int nx, int ny, float* out,
+                         int out_pitch) {
+    if (!states || !out || n_generators < 1) return go_fail(GO_ERR_INVALID, "null argument");
+    if (nx < 1 || ny < 1) return go_fail(GO_ERR_INVALID, "empty field");
+    int rc = check_field(out_pitch, nx, "random");
+    if (rc) return rc;
+    k_xorwow_fill<<<(n_generators + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+        normal, n_generators, (curandStateXORWOW_t*)states, nx, ny, out, out_pitch / 4);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+int go_noise_soar(void* stream, int coarse_nx, int coarse_ny, float coarse_dx, float coarse_dy, float soar_q0,
+                  float soar_L, float perturbation_scale, int periodic_north_south, int periodic_east_west,
+                  const float* random, int random_pitch, float* coarse, int coarse_pitch, int additive) {
+    if (!random || !coarse) return go_fail(GO_ERR_INVALID, "null argument");
+    if (coarse_nx < 1 || coarse_ny < 1) return go_fail(GO_ERR_INVALID, "empty coarse grid");
+    const int rnx = periodic_east_west ? coarse_nx : coarse_nx + 4 * kCutoff;
+    int rc = check_field(random_pitch, rnx, "random");
+    if (!rc) rc = check_field(coarse_pitch, coarse_nx + 4, "coarse");
+    if (rc) return rc;
+    const dim3 grid((coarse_nx + 4 + kBW - 1) / kBW, (coarse_ny + 4 + kBH - 1) / kBH);
+    k_soar<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(
+        coarse_nx, coarse_ny, coarse_dx, coarse_dy, soar_q0, soar_L, perturbation_scale, periodic_north_south,
+        periodic_east_west, random, random_pitch / 4, coarse, coarse_pitch / 4, additive);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+static int fill_balance(BalanceArgs& a, int nx, int ny, float dx, float dy, int ghost_x, int ghost_y, float g, float f,
+                        float beta, const float* coarse, int coarse_pitch, int coarse_width, float* eta,
+                        int eta_pitch, float* hu, int hu_pitch, float* hv, int hv_pitch, const float* Hi,
+                        int Hi_pitch, float land_value, uint64_t angle_texture, uint64_t coriolis_texture) {
+    if (!coarse || !eta || !hu || !hv || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
+    if (nx < 1 || ny < 1) return go_fail(GO_ERR_INVALID, "empty grid");
+    if (!angle_texture || !coriolis_texture) return go_fail(GO_ERR_INVALID, "angle and Coriolis textures needed");
+    int rc = check_field(coarse_pitch, coarse_width, "coarse");
+    if (!rc) rc = check_field(eta_pitch, nx + 4, "eta");
+    if (!rc) rc = check_field(hu_pitch, nx + 4, "hu");
+    if (!rc) rc = check_field(hv_pitch, nx + 4, "hv");
+    if (!rc) rc = check_field(Hi_pitch, nx + 5, "Hi");
+    if (rc) return rc;
+    a.nx = nx; a.ny = ny; a.gx = ghost_x; a.gy = ghost_y;
+    a.dx = dx; a.dy = dy; a.g = g; a.f = f; a.beta = beta;
+    a.coarse = coarse; a.cp = coarse_pitch / 4;
+    a.eta = eta; a.hu = hu; a.hv = hv;
+    a.pe = eta_pitch / 4; a.pu = hu_pitch / 4; a.pv = hv_pitch / 4;
+    a.Hi = Hi; a.ph = Hi_pitch / 4; a.land = land_value;
+    a.angle = (cudaTextureObject_t)angle_texture;
+    a.coriolis = (cudaTextureObject_t)coriolis_texture;
+    return GO_OK;
+}
+
+int go_noise_geostrophic(void* stream, int nx, int ny, float dx, float dy, int ghost_x, int ghost_y, float g,
+                         float f, float beta, float y0_reference_cell, const float* coarse, int coarse_pitch,
+                         float* eta, int eta_pitch, float* hu, int hu_pitch, float* hv, int hv_pitch,
+                         const float* Hi, int Hi_pitch, float land_value, uint64_t angle_texture,
+                         uint64_t coriolis_texture) {
+    (void)y0_reference_cell;   // accepted and unused, as in the reference kernel
+    BalanceArgs a;
+    int rc = fill_balance(a, nx, ny, dx, dy, ghost_x, ghost_y, g, f, beta, coarse, coarse_pitch, nx + 4, eta,
+                          eta_pitch, hu, hu_pitch, hv, hv_pitch, Hi, Hi_pitch, land_value, angle_texture,
+                          coriolis_texture);
+    if (rc) return rc;
+    const dim3 grid((nx + kBW - 1) / kBW, (ny + kBH - 1) / kBH);
+    k_balance<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(a);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+int go_noise_bicubic(void* stream, int nx, int ny, int ghost_x, int ghost_y, float dx, float dy, int coarse_nx,
+                     int coarse_ny, int coarse_ghost_x, int coarse_ghost_y, float coarse_dx, float coarse_dy,
+                     int offset_i, int offset_j, float g, float f, float beta, float y0_reference_cell,
+                     const float* coarse, int coarse_pitch, float* eta, int eta_pitch, float* hu, int hu_pitch,
+                     float* hv, int hv_pitch, const float* Hi, int Hi_pitch, float land_value,
+                     uint64_t angle_texture, uint64_t coriolis_texture) {
+    (void)y0_reference_cell;
+    if (coarse_nx < 1 || coarse_ny < 1) return go_fail(GO_ERR_INVALID, "empty coarse grid");
+    InterpArgs a;
+    int rc = fill_balance(a.b, nx, ny, dx, dy, ghost_x, ghost_y, g, f, beta, coarse, coarse_pitch, coarse_nx + 4,
+                          eta, eta_pitch, hu, hu_pitch, hv, hv_pitch, Hi, Hi_pitch, land_value, angle_texture,
+                          coriolis_texture);
+    if (rc) return rc;
+    a.cnx = coarse_nx; a.cny = coarse_ny; a.cgx = coarse_ghost_x; a.cgy = coarse_ghost_y;
+    a.cdx = coarse_dx; a.cdy = coarse_dy; a.off_i = offset_i; a.off_j = offset_j;
+    const dim3 grid((nx + kBW - 1) / kBW, (ny + kBH - 1) / kBH);
+    k_interp_balance<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(a);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+size_t go_noise_reduce_scratch_bytes(void) { return sizeof(RedScratch); }
+
+int go_noise_square_sums(void* stream, int nx, int ny, const float* a, int a_pitch, const float* b, int b_pitch,
+                         float* result, void* scratch, size_t scratch_bytes) {
+    if (!a || !result || !scratch) return go_fail(GO_ERR_INVALID, "null argument");
+    if (nx < 1 || ny < 1) return go_fail(GO_ERR_INVALID, "empty field");
+    if (scratch_bytes < sizeof(RedScratch))
+        return go_fail(GO_ERR_INVALID, "reduction scratch of %zu bytes, %zu needed", scratch_bytes,
+                       sizeof(RedScratch));
+    int rc = check_field(a_pitch, nx, "a");
+    if (!rc && b) rc = check_field(b_pitch, nx, "b");
+    if (rc) return rc;
+    const long long total = (long long)nx * ny;
+    const int blocks = (int)std::min<long long>(kRedBlocksMax, (total + kRedThreads - 1) / kRedThreads);
+    k_square_sums<<<blocks, kRedThreads, 0, (cudaStream_t)stream>>>(nx, ny, a, a_pitch / 4, b, b ? b_pitch / 4 : 0,
+                                                                    result, (RedScratch*)scratch);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+int go_noise_make_perpendicular(void* stream, int nx, int ny, const float* xi, int xi_pitch, float* nu,
+                                int nu_pitch, const float* reduction) {
+    if (!xi || !nu || !reduction) return go_fail(GO_ERR_INVALID, "null argument");
+    if (nx < 1 || ny < 1) return go_fail(GO_ERR_INVALID, "empty field");
+    int rc = check_field(xi_pitch, nx, "xi");
+    if (!rc) rc = check_field(nu_pitch, nx, "nu");
+    if (rc) return rc;
+    const dim3 grid((nx + kBW - 1) / kBW, (ny + kBH - 1) / kBH);
+    k_make_perpendicular<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(nx, ny, xi, xi_pitch / 4, nu,
+                                                                            nu_pitch / 4, reduction);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+}  // extern "C"

@@ -155,6 +155,78 @@ int go_bc_texture_create(const float* texels, int w, int h, uint64_t* texture);
  * Common.py:1073-1216).  The caller keeps the textures alive. */
 int go_domain_set_open_bc(go_domain* d, const uint64_t* textures, float bc_t);
 
+/*
+ * Stochastic model error (OceanStateNoise): SOAR-correlated perturbations of
+ * eta on a coarse grid, geostrophically balanced hu and hv.  Replaces the
+ * kernels of gpu_ocean/SWESimulators/gpu_kernels/ocean_noise.cu and
+ * reductions.cu as gpu_ocean/SWESimulators/OceanStateNoise.py:343-571
+ * launches them.  All arrays are device memory, row-major, pitches in bytes;
+ * every call is asynchronous on its stream.
+ */
+
+/* LCG random numbers (ocean_noise.cu:81-200, OceanStateNoise.py:343-372):
+ * each of the seed_nx x seed_ny 64-bit seeds advances twice and writes a
+ * pair of N(0,1) numbers (normal != 0, Box-Muller) or U[0,1) numbers into
+ * columns 2i, 2i+1 of its row of the random_nx-wide buffer. */
+int go_noise_lcg(void* stream, int normal, int seed_nx, int seed_ny, int random_nx, uint64_t* seed,
+                 int seed_pitch, float* random, int random_pitch);
+
+/* XORWOW generators (the reference's default, pycuda's
+ * XORWOWRandomNumberGenerator, OceanStateNoise.py:160-168): bytes of one
+ * generator state, seeding of n generators (subsequence g for generator g),
+ * and a fill of an nx x ny field with N(0,1) (normal != 0) or U(0,1]. */
+size_t go_noise_xorwow_state_bytes(void);
+int go_noise_xorwow_init(void* stream, uint64_t seed, int n_generators, void* states);
+int go_noise_xorwow_fill(void* stream, int normal, int n_generators, void* states, int nx, int ny, float* out,
+                         int out_pitch);
+
+/* SOAR covariance with cut-off 2 applied to the random field, written (or
+ * added, additive != 0) times perturbation_scale to all (coarse_nx + 4) x
+ * (coarse_ny + 4) cells of the coarse buffer (ocean_noise.cu:249-372).  The
+ * random field is coarse_nx (+8 unless periodic east-west) by coarse_ny
+ * (+8 unless periodic north-south). */
+int go_noise_soar(void* stream, int coarse_nx, int coarse_ny, float coarse_dx, float coarse_dy, float soar_q0,
+                  float soar_L, float perturbation_scale, int periodic_north_south, int periodic_east_west,
+                  const float* random, int random_pitch, float* coarse, int coarse_pitch, int additive);
+
+/* Adds the coarse perturbation (coarse grid = model grid) to eta and the
+ * geostrophically balanced d_hu, d_hv to hu, hv in the interior cells;
+ * cells with a land corner in Hi become 0 (ocean_noise.cu:379-508).  The
+ * angle and Coriolis textures are handles of go_wind_texture_create (the
+ * reference's angle_tex and coriolis_f_tex: bilinear, clamped, normalised
+ * over the ghost-inclusive grid); the Coriolis texture is read where f == 0.
+ * y0_reference_cell is accepted and unused, as in the reference. */
+int go_noise_geostrophic(void* stream, int nx, int ny, float dx, float dy, int ghost_x, int ghost_y, float g,
+                         float f, float beta, float y0_reference_cell, const float* coarse, int coarse_pitch,
+                         float* eta, int eta_pitch, float* hu, int hu_pitch, float* hv, int hv_pitch,
+                         const float* Hi, int Hi_pitch, float land_value, uint64_t angle_texture,
+                         uint64_t coriolis_texture);
+
+/* As go_noise_geostrophic with a coarser perturbation grid: d_eta is the
+ * bicubic interpolation of the coarse buffer, shifted by (offset_i,
+ * offset_j) model cells; land cells are left unchanged
+ * (ocean_noise.cu:522-772, common.cu:696-819). */
+int go_noise_bicubic(void* stream, int nx, int ny, int ghost_x, int ghost_y, float dx, float dy, int coarse_nx,
+                     int coarse_ny, int coarse_ghost_x, int coarse_ghost_y, float coarse_dx, float coarse_dy,
+                     int offset_i, int offset_j, float g, float f, float beta, float y0_reference_cell,
+                     const float* coarse, int coarse_pitch, float* eta, int eta_pitch, float* hu, int hu_pitch,
+                     float* hv, int hv_pitch, const float* Hi, int Hi_pitch, float land_value,
+                     uint64_t angle_texture, uint64_t coriolis_texture);
+
+/* result[0] = sum a^2 over an nx x ny field; with b also result[1] = sum
+ * b^2 and result[2] = sum a b (reductions.cu squareSum, squareSumDouble).
+ * Accumulates in double, deterministic order.  scratch: device bytes of
+ * go_noise_reduce_scratch_bytes(), zeroed once before first use (the call
+ * leaves it ready for the next). */
+size_t go_noise_reduce_scratch_bytes(void);
+int go_noise_square_sums(void* stream, int nx, int ny, const float* a, int a_pitch, const float* b, int b_pitch,
+                         float* result, void* scratch, size_t scratch_bytes);
+
+/* nu <- nu made perpendicular to xi and rescaled to its former norm, from
+ * the three sums of go_noise_square_sums (ocean_noise.cu:206-241). */
+int go_noise_make_perpendicular(void* stream, int nx, int ny, const float* xi, int xi_pitch, float* nu,
+                                int nu_pitch, const float* reduction);
+
 /* North vector (sin a, cos a) of a constant grid angle a, computed on the
  * device with sinf/cosf as the reference's kernel forms it from its angle
  * texture (gpu_ocean/SWESimulators/gpu_kernels/CDKLM16_kernel.cu:68-77), for

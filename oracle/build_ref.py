@@ -6,8 +6,8 @@ The reference (metno/gpu-ocean) JIT-compiles gpu_ocean/SWESimulators/
 gpu_kernels/*.cu with PyCUDA.  Those files use legacy texture references
 (``texture<float, cudaTextureType2D> x;`` / ``tex2D(x, s, t)``), which CUDA 12
 removed.  This recipe copies CDKLM16_kernel.cu, common.cu, max_dt.cu,
-boundary_kernels.cu, initBm_kernel.cu, driftKernels.cu and
-observationKernels.cu into a temporary directory,
+boundary_kernels.cu, initBm_kernel.cu, driftKernels.cu,
+observationKernels.cu and ocean_noise.cu into a temporary directory,
 rewrites each texture reference into a ``__constant__ cudaTextureObject_t``
 read with ``tex2D<T>``, and compiles them with the wrapper translation units
 in oracle/ref_driver/ into one shared library per compile-time
@@ -30,7 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 DRIVER = os.path.join(HERE, "ref_driver")
 KERNEL_FILES = ["CDKLM16_kernel.cu", "common.cu", "max_dt.cu", "boundary_kernels.cu", "initBm_kernel.cu",
-                "driftKernels.cu", "observationKernels.cu"]
+                "driftKernels.cu", "observationKernels.cu", "ocean_noise.cu"]
 
 # Compile flags of the CDKLM16 module (CDKLM16.py:196-200); the other
 # modules are compiled with PyCUDA's defaults.
@@ -115,6 +115,8 @@ def build_one(src_dir, cfg, fmad=False):
             ("tu_bc.cu", ["-Dblock_width=16", "-Dblock_height=16"]),
             ("tu_maxdt.cu", ["-Dblock_width=12", "-Dblock_height=32", "-DNUM_THREADS=256"]),
             ("tu_drift.cu", ["-Dblock_width=64", "-Dblock_height=1"]),
+            # OceanStateNoise.py:222-227
+            ("tu_noise.cu", ["-Dblock_width=16", "-Dblock_height=16", "--use_fast_math", "--maxrregcount=32"]),
             ("driver.cu", cdefs),
         ]
         for src, extra in jobs:

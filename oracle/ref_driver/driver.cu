@@ -15,6 +15,7 @@ extern "C" int refb_boundary(cudaStream_t, int, int, int, int, int, int, int, in
                              float*, int, float*, int);
 extern "C" int refr_set_drift_wind(cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t,
                                    cudaTextureObject_t);
+extern "C" int refn_set_textures(cudaTextureObject_t, cudaTextureObject_t);
 extern "C" int refk_set_textures(cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t,
                                  cudaTextureObject_t, cudaTextureObject_t, cudaTextureObject_t);
 extern "C" int refk_cdklm_swe_2D(cudaStream_t, float, int, float*, int, float*, int, float*, int, float*,
@@ -34,6 +35,7 @@ struct Tex {
 Tex g_angle, g_f, g_wxc, g_wxn, g_wyc, g_wyn;
 Tex g_dwxc, g_dwxn, g_dwyc, g_dwyn;     // wind of the drift kernel
 Tex g_ns0, g_ns1, g_ew0, g_ew1;         // exterior solution of the flow relaxation
+Tex g_nangle, g_nf;                     // angle and Coriolis textures of the model-error kernels
 
 
 void release(Tex& t) {
@@ -132,6 +134,15 @@ int ref_set_drift_wind(const float* xc, const float* xn, const float* yc, const 
     if (!e) e = make_tex(g_dwyc, yc, w, h);
     if (!e) e = make_tex(g_dwyn, yn, w, h);
     if (!e) e = refr_set_drift_wind(g_dwxc.obj, g_dwxn.obj, g_dwyc.obj, g_dwyn.obj);
+    return e;
+}
+
+// Angle and Coriolis textures of the model-error kernels
+// (OceanStateNoise.py:284-320), host arrays of h rows x w columns.
+int ref_noise_textures(const float* angle, int aw, int ah, const float* coriolis, int cw, int ch) {
+    int e = make_tex(g_nangle, angle, aw, ah);
+    if (!e) e = make_tex(g_nf, coriolis, cw, ch);
+    if (!e) e = refn_set_textures(g_nangle.obj, g_nf.obj);
     return e;
 }
 

@@ -48,6 +48,14 @@ def _load(cfg, fmad=False):
                                _F, _F, _F]
     lib.refr_enforce_bc.argtypes = [_P, _F, _F, _I, _I, _I, _P, _I]
     lib.refr_observe.argtypes = [_P, _I, _I, _F, _F, _I, _I, _P, _I, _P, _I, _P, _I, _F, _I, _P, _I, _P, _I]
+    lib.ref_noise_textures.argtypes = [ctypes.POINTER(_F), _I, _I, ctypes.POINTER(_F), _I, _I]
+    lib.refn_lcg.argtypes = [_P, _I, _I, _I, _I, _P, _I, _P, _I]
+    lib.refn_soar.argtypes = [_P, _I, _I, _F, _F, _F, _F, _F, _I, _I, _P, _I, _P, _I, _I]
+    lib.refn_geostrophic.argtypes = [_P, _I, _I, _F, _F, _I, _I, _F, _F, _F, _F, _P, _I, _P, _I, _P, _I, _P, _I,
+                                     _P, _I, _F]
+    lib.refn_bicubic.argtypes = [_P, _I, _I, _I, _I, _F, _F, _I, _I, _I, _I, _F, _F, _I, _I, _F, _F, _F, _F, _P, _I,
+                                 _P, _I, _P, _I, _P, _I, _P, _I, _F]
+    lib.refn_make_perpendicular.argtypes = [_P, _I, _I, _P, _I, _P, _I, _P]
     return lib
 
 
@@ -222,3 +230,47 @@ class RefDrifters:
     def positions(self):
         self.torch.cuda.synchronize()
         return self.pos.cpu().numpy()
+
+
+class RefNoise:
+    """The reference's model-error kernels (normalDistribution,
+    uniformDistribution, SOAR, geostrophicBalance, bicubicInterpolation,
+    makePerpendicular from ocean_noise.cu, --use_fast_math) on caller
+    tensors given as (tensor, pitch in bytes) pairs, on the current torch
+    stream.  The angle and Coriolis textures are host arrays."""
+
+    def __init__(self, cfg, angle=((0.0,),), coriolis=((0.0,),)):
+        import torch
+        self.torch = torch
+        self.lib = _load(cfg)
+        self.s = ctypes.c_void_p(int(torch.cuda.current_stream().cuda_stream))
+        a = np.ascontiguousarray(np.asarray(angle, dtype=np.float32))
+        c = np.ascontiguousarray(np.asarray(coriolis, dtype=np.float32))
+        self._tex = (a, c)
+        _chk(self.lib.ref_noise_textures(a.ctypes.data_as(ctypes.POINTER(_F)), a.shape[1], a.shape[0],
+                                         c.ctypes.data_as(ctypes.POINTER(_F)), c.shape[1], c.shape[0]), "textures")
+
+    def lcg(self, normal, seed_nx, seed_ny, random_nx, seed, random):
+        _chk(self.lib.refn_lcg(self.s, int(normal), seed_nx, seed_ny, random_nx, _p(seed[0]), seed[1],
+                               _p(random[0]), random[1]), "lcg")
+
+    def soar(self, cnx, cny, cdx, cdy, q0, L, scale, pns, pew, random, coarse, additive=0):
+        _chk(self.lib.refn_soar(self.s, cnx, cny, float(cdx), float(cdy), float(q0), float(L), float(scale),
+                                int(pns), int(pew), _p(random[0]), random[1], _p(coarse[0]), coarse[1],
+                                int(additive)), "soar")
+
+    def geostrophic(self, nx, ny, dx, dy, g, f, beta, coarse, eta, hu, hv, Hi, land=1e20, gx=2, gy=2):
+        _chk(self.lib.refn_geostrophic(self.s, nx, ny, float(dx), float(dy), gx, gy, float(g), float(f),
+                                       float(beta), 0.0, _p(coarse[0]), coarse[1], _p(eta[0]), eta[1], _p(hu[0]),
+                                       hu[1], _p(hv[0]), hv[1], _p(Hi[0]), Hi[1], float(land)), "geostrophic")
+
+    def bicubic(self, nx, ny, dx, dy, cnx, cny, cdx, cdy, oi, oj, g, f, beta, coarse, eta, hu, hv, Hi, land=1e20,
+                gx=2, gy=2):
+        _chk(self.lib.refn_bicubic(self.s, nx, ny, gx, gy, float(dx), float(dy), cnx, cny, gx, gy, float(cdx),
+                                   float(cdy), int(oi), int(oj), float(g), float(f), float(beta), 0.0, _p(coarse[0]),
+                                   coarse[1], _p(eta[0]), eta[1], _p(hu[0]), hu[1], _p(hv[0]), hv[1], _p(Hi[0]),
+                                   Hi[1], float(land)), "bicubic")
+
+    def make_perpendicular(self, nx, ny, xi, nu, red):
+        _chk(self.lib.refn_make_perpendicular(self.s, nx, ny, _p(xi[0]), xi[1], _p(nu[0]), nu[1], _p(red)),
+             "make_perpendicular")
