@@ -465,6 +465,66 @@ def run_open_bc(ctx, steps=100, sponge=10):
                     "exterior solution interpolated in time, one step per launch"}
 
 
+def run_model_error(ctx, steps=50, reps=20, n=4096):
+    """Stochastic model error on the headline 4096^2 case: CDKLM16.step(dt)
+    with small_scale_perturbation (LCG draws, SOAR, geostrophic balance
+    after every step) against the plain step, and the perturbation alone
+    (draws, SOAR, balance) with its HBM roofline.  Algorithmic bytes per
+    cell: draws 12 (seed read and write 16 per pair of cells, 4 written),
+    SOAR 8 (xi read, coarse written), balance 32 (coarse, Hi, eta, hu, hv
+    read; eta, hu, hv written)."""
+    import torch
+    from SWESimulators import CDKLM16, Common
+    from SWESimulators.OceanStateNoise import OceanStateNoise
+
+    c = make_case("grf4096")
+    if n != c.nx:
+        from SWESimulators import SyntheticCases as SC
+        c = SC.grf(n, dx=c.dx, steps=1)
+    peak, _ = measured_peak()
+
+    def timed(stream, fn, n):
+        fn()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
+    plain = CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs())
+    plain_ms = timed(plain.gpu_stream, lambda: plain.step(c.dt), steps)
+    del plain
+    sim = CDKLM16.CDKLM16(ctx, dt=c.dt, small_scale_perturbation=True, small_scale_perturbation_amplitude=1e-4,
+                          use_lcg=True, **c.kwargs())
+    with_ms = timed(sim.gpu_stream, lambda: sim.step(c.dt), steps)
+    noise = sim.small_scale_model_error
+    s = sim.gpu_stream
+    draw_ms = timed(s, noise.generateNormalDistribution, reps)
+    soar_bal_ms = timed(s, lambda: noise.perturbSim(sim, update_random_field=False), reps)
+    all_ms = timed(s, lambda: noise.perturbSim(sim), reps)
+    cells = c.nx * c.ny
+    traffic = 52.0 * cells
+    out = {"workload": "model_error", "grid": "%dx%d" % (c.nx, c.ny), "generator": "lcg", "interpolation_factor": 1,
+           "steps": steps, "step_ms_plain": plain_ms, "step_ms_with_model_error": with_ms,
+           "cells": cells, "overhead": with_ms / plain_ms - 1.0, "perturb_ms": all_ms, "draws_ms": draw_ms,
+           "soar_balance_ms": soar_bal_ms,
+           "roofline": {"bound": "hbm", "achieved": traffic / (all_ms * 1e-3) / 1e9, "unit": "GB/s",
+                        "bytes_per_cell": 52, "peak": peak,
+                        "frac": traffic / (all_ms * 1e-3) / 1e9 / peak},
+           "note": "CUDA events on the simulator's stream; perturb = draws + SOAR + balance (3 launches); "
+                   "peak = measured copy bandwidth"}
+    del sim, noise
+    # XORWOW draws (the reference's default generator)
+    x = OceanStateNoise(ctx, s, c.nx, c.ny, c.dx, c.dy, Common.BoundaryConditions(*c.bc), False, use_lcg=False,
+                        xorwow_seed=1)
+    out["xorwow_draws_ms"] = timed(s, x.generateNormalDistribution, reps)
+    return out
+
+
 def run_adjoint(ctx, n=512, n_steps=500, k=50, kind=0, rows=0):
     """Gradient of the observation misfit (64 cells, steps 50..500, truth
     bumps seed 50001, background 50002) w.r.t. the initial state and the
@@ -689,9 +749,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage", "drifters", "open_bc",
-                                           "adjoint_batch"],
+                                           "adjoint_batch", "model_error"],
                     default="grf4096")
-    ap.add_argument("--grid", type=int, default=2048, help="grid size of the adjoint_stage workload")
+    ap.add_argument("--grid", type=int, default=None,
+                    help="grid size of the adjoint_stage (default 2048) and model_error (default 4096) workloads")
     ap.add_argument("--adj-kind", type=int, default=0, help="adjoint launch form (include/gocean.h GO_ADJ_*)")
     ap.add_argument("--adj-rows", type=int, default=0, help="rows per strip of the marching adjoint (0: automatic)")
     ap.add_argument("--rows", type=int, default=0, help="rows per block strip (0: library default)")
@@ -731,7 +792,8 @@ def main():
         print(json.dumps(line))
         return
 
-    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch", "drifters", "open_bc"):
+    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch", "drifters", "open_bc",
+                         "model_error"):
         if rank != 0:
             return
         from SWESimulators import Common
@@ -748,12 +810,14 @@ def main():
             r = run_drifters(ctx)
         elif args.workload == "open_bc":
             r = run_open_bc(ctx)
+        elif args.workload == "model_error":
+            r = run_model_error(ctx, n=args.grid or 4096)
         else:
-            r = run_adjoint_stages(ctx, args.grid, reps=args.steps if args.steps < 2000 else 20,
+            r = run_adjoint_stages(ctx, args.grid or 2048, reps=args.steps if args.steps < 2000 else 20,
                                    kind=args.adj_kind, rows=args.adj_rows)
         clocks = sampler.stop()
         if args.workload == "adjoint_stage":
-            cells = args.grid * args.grid
+            cells = (args.grid or 2048) ** 2
             us = r["adjoint_stage0_us"] + r["adjoint_stage1_us"]
             print(json.dumps({"metric": METRIC, "value": cells / (us * 1e-6) / 1e9, "unit": UNIT, "n_gpus": 1,
                               "steps": r["reps"], "warmup": 3, "ms_per_step": us * 1e-3,
@@ -769,6 +833,9 @@ def main():
             value, ms = 4096 * 4096 / (r["step_ms_with_drifters"] * 1e-3) / 1e9, r["step_ms_with_drifters"]
         elif args.workload == "open_bc":
             value, ms = 4096 * 4096 / (r["step_ms_open"] * 1e-3) / 1e9, r["step_ms_open"]
+        elif args.workload == "model_error":
+            value = r["cells"] / (r["step_ms_with_model_error"] * 1e-3) / 1e9
+            ms = r["step_ms_with_model_error"]
         else:
             cells_steps = 512 * 512 * r["steps"]
             value, ms = cells_steps / (r["forward_adjoint_ms_k50"] * 1e-3) / 1e9, r["forward_adjoint_ms_k50"] / r["steps"]
@@ -807,7 +874,7 @@ def main():
         secondary = {}
         for name, fn in (("ensemble100", run_ensemble), ("adjoint512", run_adjoint),
                          ("adjoint_batch", run_adjoint_batch), ("drifters", run_drifters),
-                         ("open_bc", run_open_bc)):
+                         ("open_bc", run_open_bc), ("model_error", run_model_error)):
             try:
                 secondary[name] = fn(ctx)
             except Exception as e:      # a secondary failure must not lose the headline line

@@ -48,13 +48,26 @@ __device__ __forceinline__ int wrap(int v, int n) { return ((v % n) + n) % n; }
 
 // ---- random numbers ---------------------------------------------------------
 
-// ANSI C LCG, two draws (ocean_noise.cu:81-99): seed <- (seed a + c) mod m,
-// u = seed / 2^31 rounded to float.
-__device__ __forceinline__ float2 lcg_pair(unsigned long long& seed) {
+// One LCG step, (seed a + c) mod m with m = 2^31 - 1, the product wrapping
+// at 2^64 as the reference's unsigned long long arithmetic does.  For seeds
+// below 2^32 the sum is below 2^63 and m is a Mersenne prime, so the
+// remainder folds with shifts and adds (x = h 2^31 + l = h + l mod m);
+// larger seeds take the division.
+__device__ __forceinline__ unsigned long long lcg_next(unsigned long long seed) {
     const unsigned long long m = 2147483647ULL;
-    seed = ((seed * 1103515245ULL) + 12345ULL) % m;
+    const unsigned long long x = seed * 1103515245ULL + 12345ULL;
+    if (seed >> 32) return x % m;
+    unsigned long long r = (x & m) + (x >> 31);
+    r = (r & m) + (r >> 31);
+    return r >= m ? r - m : r;
+}
+
+// ANSI C LCG, two draws (ocean_noise.cu:81-99): u = seed / 2^31 rounded to
+// float (the quotient by a power of two is exact in double).
+__device__ __forceinline__ float2 lcg_pair(unsigned long long& seed) {
+    seed = lcg_next(seed);
     const float u1 = (float)((double)seed / 2147483648.0);
-    seed = ((seed * 1103515245ULL) + 12345ULL) % m;
+    seed = lcg_next(seed);
     const float u2 = (float)((double)seed / 2147483648.0);
     return make_float2(u1, u2);
 }
@@ -62,7 +75,9 @@ __device__ __forceinline__ float2 lcg_pair(unsigned long long& seed) {
 // Box-Muller (ocean_noise.cu:106-116).
 __device__ __forceinline__ float2 box_muller(float2 u) {
     const float r = sqrtf(-2.0f * logf(u.x));
-    return make_float2(r * cospif(2 * u.y), r * sinpif(2 * u.y));
+    float s, c;
+    sincospif(2 * u.y, &s, &c);
+    return make_float2(r * c, r * s);
 }
 
 // One thread per seed; writes its pair into columns 2i, 2i+1 of its row
@@ -130,48 +145,107 @@ __device__ __forceinline__ float soar_weight(int ox, int oy, float dx, float dy,
     return q0 * (1.0f + dist / L) * expf(-dist / L);
 }
 
-// Row (or column) of the random buffer behind coarse index c, tap k in
-// [0, 4] (ocean_noise.cu:300-330): wrapped over the n interior values when
-// periodic, else c + k in a buffer with 4 extra values on each side.
-__device__ __forceinline__ int random_src(int c, int k, int n, int periodic) {
-    return periodic ? wrap(c + k - 2 * kCutoff, n) : min(c + k, n + 4 * kCutoff - 1);
+constexpr int kTaps = 2 * kCutoff + 1;
+constexpr int kSoarRows = 8;                  // coarse rows per thread
+constexpr int kSoarTY = 4;                    // thread rows per block
+constexpr int kSoarBH = kSoarRows * kSoarTY;  // 32 coarse rows per block
+
+// Index into the random buffer behind tile position c (coarse index plus
+// tap) along one axis (ocean_noise.cu:300-330): wrapped over the n interior
+// values when periodic (c - 4), else c itself in a buffer with 4 extra
+// values on each side.  -1 for positions no written cell reads (beyond
+// c - 4 = n + 3, or c = n + 7).
+__device__ __forceinline__ int random_src(int c, int n, int periodic) {
+    if (periodic) {
+        int v = c - 2 * kCutoff;
+        if (v > n + 3) return -1;
+        if (n < 2 * kCutoff) return wrap(v, n);
+        return v < 0 ? v + n : (v >= n ? v - n : v);
+    }
+    return c > n + 4 * kCutoff - 1 ? -1 : c;
 }
 
-// One thread per coarse cell, ghost cells included ((nx+4) x (ny+4)):
-// coarse = scale * sum_taps Q(tap) xi(tap), or += when additive
-// (ocean_noise.cu:264-372).
-__global__ void __launch_bounds__(kBW* kBH) k_soar(int nx, int ny, float dx, float dy, float q0, float L, float scale,
-                                                   int pns, int pew, const float* __restrict__ rnd, int rp,
-                                                   float* __restrict__ coarse, int cp, int additive) {
-    constexpr int TW = kBW + 2 * kCutoff, TH = kBH + 2 * kCutoff;
+// Coarse cells, ghost cells included ((nx+4) x (ny+4)): coarse = scale *
+// sum_taps Q(tap) xi(tap), or += when additive (ocean_noise.cu:264-372).
+// A block covers 32 x 32 cells; the random values behind them (36 x 36) sit
+// in shared memory and each thread sums a strip of 8 cells down one column
+// from registers, taps in the reference's order (rows outer, columns inner).
+__global__ void __launch_bounds__(kBW* kSoarTY) k_soar(int nx, int ny, float dx, float dy, float q0, float L,
+                                                       float scale, int pns, int pew,
+                                                       const float* __restrict__ rnd, int rp,
+                                                       float* __restrict__ coarse, int cp, int additive,
+                                                       int aligned16) {
+    constexpr int TW = kBW + 2 * kCutoff, TH = kSoarBH + 2 * kCutoff;
+    static_assert(TW % 4 == 0 && (2 * kCutoff) % 4 == 0, "float4 tile rows");
     __shared__ float xi[TH][TW];
-    __shared__ float w[2 * kCutoff + 1][2 * kCutoff + 1];
+    __shared__ float w[kTaps * kTaps];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int t = ty * kBW + tx;
-    const int bx = blockIdx.x * kBW, by = blockIdx.y * kBH;
-    if (t < (2 * kCutoff + 1) * (2 * kCutoff + 1)) {
-        const int ky = t / (2 * kCutoff + 1), kx = t % (2 * kCutoff + 1);
-        w[ky][kx] = soar_weight(kCutoff - kx, kCutoff - ky, dx, dy, q0, L);
-    }
-    for (int j = ty; j < TH; j += kBH) {
-        const int gj = random_src(by + j, 0, ny, pns);
-        const float* row = rnd + (size_t)gj * rp;
-        for (int i = tx; i < TW; i += kBW) xi[j][i] = __ldg(row + random_src(bx + i, 0, nx, pew));
+    const int bx = blockIdx.x * kBW, by = blockIdx.y * kSoarBH;
+    if (t < kTaps * kTaps) w[t] = soar_weight(kCutoff - t % kTaps, kCutoff - t / kTaps, dx, dy, q0, L);
+    // First random row and column behind the tile, and whether the whole
+    // tile lies inside the random buffer without wrapping: then its rows are
+    // read as 9 aligned float4 each (the first column is a multiple of 4;
+    // aligned16 says the buffer and pitch are 16-byte aligned).
+    const int row0 = pns ? by - 2 * kCutoff : by;
+    const int col0 = pew ? bx - 2 * kCutoff : bx;
+    const int rows_avail = pns ? ny : ny + 4 * kCutoff;
+    const int cols_avail = pew ? nx : nx + 4 * kCutoff;
+    if (aligned16 && row0 >= 0 && col0 >= 0 && row0 + TH <= rows_avail && col0 + TW <= cols_avail) {
+        constexpr int V = TW / 4;
+        for (int k = t; k < TH * V; k += kBW * kSoarTY) {
+            const int j = k / V, v = k % V;
+            const float4 q = __ldg(reinterpret_cast<const float4*>(rnd + (size_t)(row0 + j) * rp + col0) + v);
+            xi[j][4 * v] = q.x;
+            xi[j][4 * v + 1] = q.y;
+            xi[j][4 * v + 2] = q.z;
+            xi[j][4 * v + 3] = q.w;
+        }
+    } else {
+        // edge tiles: each thread fills tile columns tx and tx + 32 (tx < 4)
+        const int gi0 = random_src(bx + tx, nx, pew);
+        const int gi1 = tx < TW - kBW ? random_src(bx + kBW + tx, nx, pew) : -1;
+        for (int j = ty; j < TH; j += kSoarTY) {
+            const int gj = random_src(by + j, ny, pns);
+            const float* row = rnd + (size_t)max(gj, 0) * rp;
+            xi[j][tx] = (gj >= 0 && gi0 >= 0) ? __ldg(row + gi0) : 0.0f;
+            if (tx < TW - kBW) xi[j][kBW + tx] = (gj >= 0 && gi1 >= 0) ? __ldg(row + gi1) : 0.0f;
+        }
     }
     __syncthreads();
-    const int ti = bx + tx, tj = by + ty;
-    if (ti >= nx + 4 || tj >= ny + 4) return;
-    float acc = 0.0f;
+    float wr[kTaps * kTaps];
 #pragma unroll
-    for (int ky = 0; ky <= 2 * kCutoff; ++ky) {
+    for (int k = 0; k < kTaps * kTaps; ++k) wr[k] = w[k];
+    const int ti = bx + tx;
+    const int r0 = ty * kSoarRows;
+    // The tile rows q = r0 .. r0 + 11 are read once each, in order; row q
+    // is tap row ky = q - r of cell r, so every cell still receives its taps
+    // rows first, columns second, as the reference sums them.
+    float acc[kSoarRows];
 #pragma unroll
-        for (int kx = 0; kx <= 2 * kCutoff; ++kx) acc = __fmaf_rn(w[ky][kx], xi[ty + ky][tx + kx], acc);
+    for (int r = 0; r < kSoarRows; ++r) acc[r] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < kSoarRows + kTaps - 1; ++q) {
+        float x[kTaps];
+#pragma unroll
+        for (int kx = 0; kx < kTaps; ++kx) x[kx] = xi[r0 + q][tx + kx];
+#pragma unroll
+        for (int r = 0; r < kSoarRows; ++r) {
+            const int ky = q - r;
+            if (ky < 0 || ky >= kTaps) continue;
+#pragma unroll
+            for (int kx = 0; kx < kTaps; ++kx) acc[r] = __fmaf_rn(wr[ky * kTaps + kx], x[kx], acc[r]);
+        }
     }
-    float* out = coarse + (size_t)tj * cp + ti;
-    if (additive > 0)
-        *out = __fmaf_rn(scale, acc, *out);
-    else
-        *out = scale * acc;
+    if (ti >= nx + 4) return;
+#pragma unroll
+    for (int r = 0; r < kSoarRows; ++r) {
+        const int tj = by + r0 + r;
+        if (tj < ny + 4) {
+            float* out = coarse + (size_t)tj * cp + ti;
+            *out = additive > 0 ? __fmaf_rn(scale, acc[r], *out) : scale * acc[r];
+        }
+    }
 }
 
 // ---- geostrophic balance -------------------------------------------------------
@@ -199,49 +273,91 @@ __device__ __forceinline__ void cell_depth(const BalanceArgs& a, int ti, int tj,
     H_mid = 0.25f * (h00 + h01 + h10 + h11);
 }
 
-// Coriolis parameter at cell (ti, tj) (ocean_noise.cu:471-476, 38-67): the
-// beta plane along the texture's north vector, or the Coriolis texture
-// when f is zero.
-__device__ __forceinline__ float cell_coriolis(const BalanceArgs& a, int ti, int tj) {
-    const float s = (ti + 0.5f) / (a.nx + 4.0f);
-    const float t = (tj + 0.5f) / (a.ny + 4.0f);
-    const float angle = tex2D<float>(a.angle, s, t);
-    const float2 north = make_float2(sinf(angle), cosf(angle));
-    float coriolis = a.f + a.beta * ((ti + 0.5f) * a.dx * north.x + (tj + 0.5f) * a.dy * north.y);
-    if (a.f == 0) coriolis = tex2D<float>(a.coriolis, s, t);
-    return coriolis;
+// How the Coriolis parameter of a cell is found (ocean_noise.cu:471-476):
+// the reference evaluates f + beta (north . x) with the north vector from
+// the angle texture, then takes the Coriolis texture instead when f == 0.
+// With beta == 0 and f != 0 that is f + 0 * (finite) = f exactly, so the
+// texture and trigonometry are only needed in the two other cases.
+enum CoriolisMode { kCorF = 0, kCorBeta = 1, kCorTexture = 2 };
+
+__host__ __device__ __forceinline__ int coriolis_mode(float f, float beta) {
+    return f == 0.0f ? kCorTexture : (beta == 0.0f ? kCorF : kCorBeta);
 }
 
+__device__ __forceinline__ float cell_coriolis(const BalanceArgs& a, int mode, int ti, int tj) {
+    if (mode == kCorF) return a.f;
+    const float s = (ti + 0.5f) / (a.nx + 4.0f);
+    const float t = (tj + 0.5f) / (a.ny + 4.0f);
+    if (mode == kCorTexture) return tex2D<float>(a.coriolis, s, t);
+    const float angle = tex2D<float>(a.angle, s, t);
+    const float2 north = make_float2(sinf(angle), cosf(angle));
+    return a.f + a.beta * ((ti + 0.5f) * a.dx * north.x + (tj + 0.5f) * a.dy * north.y);
+}
+
+constexpr int kBalRows = 4;                   // cells per thread, down a column
+
 // Interior cells of the model grid; the coarse grid is the model grid
-// (ocean_noise.cu:379-508).
-__global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a) {
+// (ocean_noise.cu:379-508).  Each thread marches kBalRows cells down one
+// column, carrying the coarse values of the rows above and below and the
+// lower corner pair of Hi from one cell to the next.
+__global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a, int mode) {
     const int ti = blockIdx.x * kBW + threadIdx.x + a.gx;
-    const int tj = blockIdx.y * kBH + threadIdx.y + a.gy;
-    if (!(ti > 1 && tj > 1 && ti < a.nx + 2 && tj < a.ny + 2)) return;
-    float H_mid;
-    bool dry;
-    cell_depth(a, ti, tj, H_mid, dry);
+    const int tj0 = (blockIdx.y * kBH + threadIdx.y) * kBalRows + a.gy;
+    if (ti < 2 || ti >= a.nx + 2) return;
+    const float* __restrict__ coarse = a.coarse;
+    const float* __restrict__ Hi = a.Hi;
+    float* __restrict__ eta_p = a.eta;
+    float* __restrict__ hu_p = a.hu;
+    float* __restrict__ hv_p = a.hv;
     auto c = [&](int i, int j) {
-        return __ldg(a.coarse + (size_t)clampi(j, 0, a.ny + 3) * a.cp + clampi(i, 0, a.nx + 3));
+        return __ldg(coarse + (size_t)clampi(j, 0, a.ny + 3) * a.cp + clampi(i, 0, a.nx + 3));
     };
-    const float d = c(ti, tj);
-    const float coriolis = cell_coriolis(a, ti, tj);
-    float* eta = a.eta + (size_t)tj * a.pe + ti;
-    float* hu = a.hu + (size_t)tj * a.pu + ti;
-    float* hv = a.hv + (size_t)tj * a.pv + ti;
-    const float h_mid = d + H_mid + *eta;
-    const float eta_diff_x = (c(ti + 1, tj) - c(ti - 1, tj)) / (2.0f * a.dx);
-    const float eta_diff_y = (c(ti, tj + 1) - c(ti, tj - 1)) / (2.0f * a.dy);
-    const float d_hu = -(a.g / coriolis) * h_mid * eta_diff_y;
-    const float d_hv = (a.g / coriolis) * h_mid * eta_diff_x;
-    if (dry) {
-        *eta = 0.0f;
-        *hu = 0.0f;
-        *hv = 0.0f;
-    } else {
-        *eta += d;
-        *hu += d_hu;
-        *hv += d_hv;
+    auto h = [&](int i, int j) { return __ldg(Hi + (size_t)clampi(j, 0, a.ny + 4) * a.ph + clampi(i, 0, a.nx + 4)); };
+    // every input of the column strip first (independent loads in flight),
+    // then the cells; rows past the grid load clamped values and are skipped
+    float cc[kBalRows + 2], cl[kBalRows], cr[kBalRows], hl[kBalRows + 1], hr[kBalRows + 1];
+    float e[kBalRows], u[kBalRows], v[kBalRows];
+#pragma unroll
+    for (int k = 0; k < kBalRows + 2; ++k) cc[k] = c(ti, tj0 - 1 + k);
+#pragma unroll
+    for (int k = 0; k < kBalRows + 1; ++k) {
+        hl[k] = h(ti, tj0 + k);
+        hr[k] = h(ti + 1, tj0 + k);
+    }
+#pragma unroll
+    for (int r = 0; r < kBalRows; ++r) {
+        const int tj = min(tj0 + r, a.ny + 3);
+        cl[r] = c(ti - 1, tj);
+        cr[r] = c(ti + 1, tj);
+        e[r] = eta_p[(size_t)tj * a.pe + ti];
+        u[r] = hu_p[(size_t)tj * a.pu + ti];
+        v[r] = hv_p[(size_t)tj * a.pv + ti];
+    }
+#pragma unroll
+    for (int r = 0; r < kBalRows; ++r) {
+        const int tj = tj0 + r;
+        if (tj < 2 || tj >= a.ny + 2) continue;
+        const float h00 = hl[r], h01 = hr[r], h10 = hl[r + 1], h11 = hr[r + 1];
+        const bool dry = (h00 == a.land) || (h01 == a.land) || (h10 == a.land) || (h11 == a.land);
+        const float H_mid = 0.25f * (h00 + h01 + h10 + h11);
+        const float coriolis = cell_coriolis(a, mode, ti, tj);
+        const float d = cc[r + 1];
+        const float h_mid = d + H_mid + e[r];
+        const float eta_diff_x = (cr[r] - cl[r]) / (2.0f * a.dx);
+        const float eta_diff_y = (cc[r + 2] - cc[r]) / (2.0f * a.dy);
+        // d_hu = -(g / f) h_mid d_y eta and d_hv = (g / f) h_mid d_x eta; the
+        // reference's hu += d_hu contracts into one fused multiply-add with
+        // the last product (ocean_noise.cu:480-493 under --use_fast_math),
+        // written out here so the rounding does not depend on the compiler.
+        float en = 0.0f, un = 0.0f, vn = 0.0f;
+        if (!dry) {
+            en = e[r] + d;
+            un = __fmaf_rn(-(a.g / coriolis) * h_mid, eta_diff_y, u[r]);
+            vn = __fmaf_rn((a.g / coriolis) * h_mid, eta_diff_x, v[r]);
+        }
+        eta_p[(size_t)tj * a.pe + ti] = en;
+        hu_p[(size_t)tj * a.pu + ti] = un;
+        hv_p[(size_t)tj * a.pv + ti] = vn;
     }
 }
 
@@ -350,7 +466,7 @@ __global__ void __launch_bounds__(kBW* kBH) k_interp_balance(const InterpArgs a)
     float H_mid;
     bool dry;
     cell_depth(a.b, ti, tj, H_mid, dry);
-    const float coriolis = cell_coriolis(a.b, ti, tj);
+    const float coriolis = cell_coriolis(a.b, coriolis_mode(a.b.f, a.b.beta), ti, tj);
     const int ex = tx + 1, ey = ty + 1;
     const float eta_diff_x = (d_eta[ey][ex + 1] - d_eta[ey][ex - 1]) / (2.0f * a.b.dx);
     const float eta_diff_y = (d_eta[ey + 1][ex] - d_eta[ey - 1][ex]) / (2.0f * a.b.dy);
@@ -362,9 +478,14 @@ __global__ void __launch_bounds__(kBW* kBH) k_interp_balance(const InterpArgs a)
         d_hu = 0.0f;
         d_hv = 0.0f;
     }
-    a.b.eta[(size_t)tj * a.b.pe + ti] += d;
-    a.b.hu[(size_t)tj * a.b.pu + ti] += d_hu;
-    a.b.hv[(size_t)tj * a.b.pv + ti] += d_hv;
+    // here the land test selects d_hu before the sum, so the reference adds
+    // the rounded product (no contraction, ocean_noise.cu:758-770)
+    float* eta = a.b.eta + (size_t)tj * a.b.pe + ti;
+    float* hu = a.b.hu + (size_t)tj * a.b.pu + ti;
+    float* hv = a.b.hv + (size_t)tj * a.b.pv + ti;
+    *eta = __fadd_rn(*eta, d);
+    *hu = __fadd_rn(*hu, d_hu);
+    *hv = __fadd_rn(*hv, d_hv);
 }
 
 // ---- reductions and the perpendicular field ------------------------------------
@@ -517,10 +638,11 @@ int go_noise_soar(void* stream, int coarse_nx, int coarse_ny, float coarse_dx, f
     int rc = check_field(random_pitch, rnx, "random");
     if (!rc) rc = check_field(coarse_pitch, coarse_nx + 4, "coarse");
     if (rc) return rc;
-    const dim3 grid((coarse_nx + 4 + kBW - 1) / kBW, (coarse_ny + 4 + kBH - 1) / kBH);
-    k_soar<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(
+    const dim3 grid((coarse_nx + 4 + kBW - 1) / kBW, (coarse_ny + 4 + kSoarBH - 1) / kSoarBH);
+    k_soar<<<grid, dim3(kBW, kSoarTY), 0, (cudaStream_t)stream>>>(
         coarse_nx, coarse_ny, coarse_dx, coarse_dy, soar_q0, soar_L, perturbation_scale, periodic_north_south,
-        periodic_east_west, random, random_pitch / 4, coarse, coarse_pitch / 4, additive);
+        periodic_east_west, random, random_pitch / 4, coarse, coarse_pitch / 4, additive,
+        (((uintptr_t)random | (uintptr_t)random_pitch) & 15) == 0);
     GO_CUDA(cudaGetLastError());
     return GO_OK;
 }
@@ -560,8 +682,8 @@ int go_noise_geostrophic(void* stream, int nx, int ny, float dx, float dy, int g
                           eta_pitch, hu, hu_pitch, hv, hv_pitch, Hi, Hi_pitch, land_value, angle_texture,
                           coriolis_texture);
     if (rc) return rc;
-    const dim3 grid((nx + kBW - 1) / kBW, (ny + kBH - 1) / kBH);
-    k_balance<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(a);
+    const dim3 grid((nx + kBW - 1) / kBW, (ny + kBH * kBalRows - 1) / (kBH * kBalRows));
+    k_balance<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(a, coriolis_mode(f, beta));
     GO_CUDA(cudaGetLastError());
     return GO_OK;
 }

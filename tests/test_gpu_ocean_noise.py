@@ -156,11 +156,10 @@ def test_geostrophic_vs_reference(ctx, case):
     eta0 = np.random.RandomState(3).uniform(-0.1, 0.1, (NY + 4, NX + 4)).astype(np.float32)
     eta, Hi = _state(NX, NY, land, eta0)
     a = _arrays(ctx, NX, NY, eta, Hi)
-    n.perturbOceanState(*a, f, beta=beta, g=G, ghost_cells_x=2, ghost_cells_y=2)
-    coarse = n.getCoarseBuffer()
-    rc = _pitched(coarse)
     re, rhu, rhv, rH = _pitched(eta), _pitched(np.zeros_like(eta)), _pitched(np.zeros_like(eta)), _pitched(Hi)
-    ref.geostrophic(NX, NY, DX, DX, G, f, beta, rc, re, rhu, rhv, rH)
+    for _ in range(3):    # repeated: hu, hv non-zero from the second on
+        n.perturbOceanState(*a, f, beta=beta, g=G, ghost_cells_x=2, ghost_cells_y=2)
+        ref.geostrophic(NX, NY, DX, DX, G, f, beta, _pitched(n.getCoarseBuffer()), re, rhu, rhv, rH)
     for mine, theirs in zip((a[0], a[1], a[2]), (re, rhu, rhv)):
         m = mine.download(torch.cuda.current_stream())
         t = _host(theirs, m.shape)
@@ -175,13 +174,13 @@ def test_bicubic_vs_reference(ctx, factor, align):
     n = _noise(ctx, nx, ny, factor=factor)
     eta, Hi = _state(nx, ny, land=[(7, 9)])
     a = _arrays(ctx, nx, ny, eta, Hi)
-    n.perturbOceanState(*a, F, g=G, ghost_cells_x=2, ghost_cells_y=2, align_with_cell_i=align,
-                        align_with_cell_j=align)
     oi, oj = n._obtain_coarse_grid_offset(align, align)
-    rc = _pitched(n.getCoarseBuffer())
     re, rhu, rhv, rH = _pitched(eta), _pitched(np.zeros_like(eta)), _pitched(np.zeros_like(eta)), _pitched(Hi)
-    ref.bicubic(nx, ny, DX, DX, int(n.coarse_nx), int(n.coarse_ny), n.coarse_dx, n.coarse_dy, oi, oj, G, F, 0.0,
-                rc, re, rhu, rhv, rH)
+    for _ in range(3):
+        n.perturbOceanState(*a, F, g=G, ghost_cells_x=2, ghost_cells_y=2, align_with_cell_i=align,
+                            align_with_cell_j=align)
+        ref.bicubic(nx, ny, DX, DX, int(n.coarse_nx), int(n.coarse_ny), n.coarse_dx, n.coarse_dy, oi, oj, G, F,
+                    0.0, _pitched(n.getCoarseBuffer()), re, rhu, rhv, rH)
     for mine, theirs in zip(a[:3], (re, rhu, rhv)):
         m = mine.download(torch.cuda.current_stream())
         t = _host(theirs, m.shape)
@@ -353,3 +352,48 @@ def test_simulator_small_scale_perturbation(ctx):
     assert np.abs(eta).max() > 0
     a.perturbState(q0_scale=0.5)
     assert not np.array_equal(a.download()[0], eta)
+
+
+@pytest.mark.parametrize("pns, pew", [(True, True), (False, False)])
+def test_large_grid_vs_reference_with_timing(ctx, pns, pew):
+    """2048 x 2048 model grid: three draws, SOAR and balance against the
+    reference's kernels on copies of the same seeds and state, bit for bit;
+    prints both sides' device times (CUDA events, 10 repetitions)."""
+    n_cells = 2048
+    ref = _ref()
+    n = _noise(ctx, n_cells, n_cells, pns, pew)
+    eta, Hi = _state(n_cells, n_cells, land=[(100, 200), (1500, 7)])
+    a = _arrays(ctx, n_cells, n_cells, eta, Hi)
+    rs = _pitched(n.getSeed().astype(np.int64), dtype=np.int64)
+    rr = _pitched(np.zeros((n.rand_ny, n.rand_nx)))
+    rc = _pitched(np.zeros((n.coarse_ny + 4, n.coarse_nx + 4)))
+    re, rhu, rhv, rH = _pitched(eta), _pitched(np.zeros_like(eta)), _pitched(np.zeros_like(eta)), _pitched(Hi)
+
+    def mine():
+        n.perturbOceanState(*a, F, 0.0, G, ghost_cells_x=2, ghost_cells_y=2)
+
+    def theirs():
+        ref.lcg(True, int(n.seed_nx), int(n.seed_ny), int(n.rand_nx), rs, rr)
+        ref.soar(int(n.coarse_nx), int(n.coarse_ny), n.coarse_dx, n.coarse_dy, n.soar_q0, n.soar_L, 1.0, pns, pew,
+                 rr, rc)
+        ref.geostrophic(n_cells, n_cells, DX, DX, G, F, 0.0, rc, re, rhu, rhv, rH)
+
+    def timed(fn, reps=10):
+        s = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for _ in range(3):
+        mine()
+        theirs()
+    for x, y in zip(a[:3], (re, rhu, rhv)):
+        m = x.download(torch.cuda.current_stream())
+        assert np.array_equal(m, _host(y, m.shape))
+    t_mine, t_ref = timed(mine), timed(theirs)
+    print("2048^2 perturbation (draws + SOAR + balance): ours %.3f ms, reference kernels %.3f ms (x%.2f)"
+          % (t_mine, t_ref, t_ref / t_mine))
