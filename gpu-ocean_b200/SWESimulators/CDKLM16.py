@@ -7,9 +7,10 @@ attributes other modules read (``gpu_data.h0 ...``, ``bathymetry``,
 ``gpu_stream``, ``t``, ``num_iterations``, ...).
 
 What is not built raises ``NotImplementedError`` at construction:
-a spatially varying grid angle, ``latitude``, NetCDF output,
-``rk_order`` other than 2.  The stochastic model error
-(``small_scale_perturbation``) runs on OceanStateNoise after each step.
+a spatially varying grid angle, ``latitude``, ``rk_order`` other than 2.
+The stochastic model error (``small_scale_perturbation``) runs on
+OceanStateNoise after each step; NetCDF output (``write_netcdf``) and
+``fromfilename`` use SimWriter and SimReader.
 The Coriolis table is always full-resolution
 (``subsample_f``/``subsample_angle`` are accepted and ignored; the
 reference's subsampler calls ``scipy.interpolate.interp2d``, which the
@@ -20,7 +21,7 @@ import logging
 
 import numpy as np
 
-from . import Common, OceanStateNoise, Simulator, WindStress, _native
+from . import Common, OceanStateNoise, SimReader, Simulator, SimWriter, WindStress, _native
 
 
 class CDKLM16(Simulator.Simulator):
@@ -43,8 +44,6 @@ class CDKLM16(Simulator.Simulator):
         self.logger = logging.getLogger(__name__)
         if rk_order != 2:
             raise NotImplementedError("only rk_order=2 (Heun) is built")
-        if write_netcdf:
-            raise NotImplementedError("NetCDF output is not built (netCDF4 is not available)")
         if latitude is not None:
             raise NotImplementedError("a latitude field (2-D Coriolis) is not built")
         angle = np.asarray(angle)
@@ -121,6 +120,12 @@ class CDKLM16(Simulator.Simulator):
         self.total_time_steps = 0
         if model_time_step is None:
             self.model_time_step = self.dt
+        # NetCDF output, the initial state as the first record (CDKLM16.py:375-377)
+        if self.write_netcdf:
+            self.sim_writer = SimWriter.SimNetCDFWriter(self, super_dir_name=super_dir_name,
+                                                        filename=netcdf_filename,
+                                                        ignore_ghostcells=self.ignore_ghostcells,
+                                                        offset_x=self.offset_x, offset_y=self.offset_y)
         if self.dt <= 0:
             self.updateDt()
 
@@ -149,6 +154,8 @@ class CDKLM16(Simulator.Simulator):
         return np.ascontiguousarray(coriolis_f[:, 0])
 
     def cleanUp(self):
+        if getattr(self, "sim_writer", None) is not None:
+            self.closeNetCDF()
         if getattr(self, "gpu_data", None) is not None:
             self.gpu_data.release()
         if getattr(self, "bathymetry", None) is not None:
@@ -160,7 +167,52 @@ class CDKLM16(Simulator.Simulator):
     @classmethod
     def fromfilename(cls, gpu_ctx, filename, cont_write_netcdf=True, use_lcg=False, xorwow_seed=None,
                      new_netcdf_filename=None, time0=None):
-        raise NotImplementedError("NetCDF restart is not built (netCDF4 is not available)")
+        """A simulator hot-started from the last record (or the record at
+        time0) of a NetCDF file written by SimWriter (CDKLM16.py:411-490):
+        the file's parameters, bathymetry, boundary conditions and state.
+        As in the reference, the wind is not restored (the file names only
+        its source) and the Coriolis parameter read back is the one the
+        writer stored, which the constructor shifts again for a beta plane."""
+        sim_reader = SimReader.SimNetCDFReader(filename, ignore_ghostcells=False)
+        try:
+            sim_name = str(sim_reader.get("simulator_short"))
+            assert sim_name == cls.__name__, \
+                "Trying to initialize a " + cls.__name__ + " simulator with netCDF file based on " + sim_name + \
+                " results."
+            H = sim_reader.getH()
+            if time0 is None:
+                eta0, hu0, hv0, time0 = sim_reader.getLastTimeStep()
+            else:
+                eta0, hu0, hv0, time0 = sim_reader.getStateAtTime(time0)
+            if len(H.shape) == 3:
+                H = H[0, :, :]
+            sim_params = {
+                "gpu_ctx": gpu_ctx, "eta0": eta0, "hu0": hu0, "hv0": hv0, "H": H,
+                "nx": int(sim_reader.get("nx")), "ny": int(sim_reader.get("ny")),
+                "dx": sim_reader.get("dx"), "dy": sim_reader.get("dy"), "dt": sim_reader.get("dt"),
+                "g": sim_reader.get("g"), "f": sim_reader.get("coriolis_force"),
+                "r": sim_reader.get("bottom_friction_r"), "t": float(time0),
+                "theta": sim_reader.get("minmod_theta"), "rk_order": int(sim_reader.get("time_integrator")),
+                "coriolis_beta": sim_reader.get("coriolis_beta"), "write_netcdf": cont_write_netcdf,
+                "use_lcg": use_lcg, "xorwow_seed": xorwow_seed, "netcdf_filename": new_netcdf_filename,
+            }
+            wind_type = sim_reader.get("wind_stress_type")
+            sim_params["wind_stress"] = WindStress.WindStress()
+            if wind_type != "not found":
+                raise NotImplementedError("wind_stress_type %s: typed wind parameters are not built" % wind_type)
+            sim_params["boundary_conditions"] = sim_reader.getBC()
+            if sim_reader.has("small_scale_perturbation"):
+                sim_params["small_scale_perturbation"] = sim_reader.get("small_scale_perturbation") == "True"
+                if sim_params["small_scale_perturbation"]:
+                    sim_params["small_scale_perturbation_amplitude"] = \
+                        sim_reader.get("small_scale_perturbation_amplitude")
+                    sim_params["small_scale_perturbation_interpolation_factor"] = \
+                        int(sim_reader.get("small_scale_perturbation_interpolation_factor"))
+            if sim_reader.has("model_time_step"):
+                sim_params["model_time_step"] = sim_reader.get("model_time_step")
+        finally:
+            sim_reader.close()
+        return cls(**sim_params)
 
     # -- stepping -----------------------------------------------------------
     def _launch_steps(self, n, dt, wind_t):
@@ -216,6 +268,8 @@ class CDKLM16(Simulator.Simulator):
             self.num_iterations += 1
         if pending_n:
             self._launch_steps(pending_n, pending_dt, pending_w)
+        if self.write_netcdf and write_now:
+            self.sim_writer.writeTimestep(self)
         return self.t
 
     def drifterStep(self, dt):
@@ -286,11 +340,15 @@ class CDKLM16(Simulator.Simulator):
             self.total_time_steps += 1
             if self.total_time_steps % 5 == 0:
                 self.updateDt(courant_number=courant_number)
+        if self.write_netcdf and write_now:
+            self.sim_writer.writeTimestep(self)
         assert round(observation_time) == round(self.t), \
             'The simulation time is not the same as observation time after dataAssimilationStep!'
 
     def writeState(self):
-        return
+        """Appends the current state to the NetCDF file (CDKLM16.py:706-708)."""
+        if self.write_netcdf:
+            self.sim_writer.writeTimestep(self)
 
     # -- time step ----------------------------------------------------------
     def maxDtDevice(self):

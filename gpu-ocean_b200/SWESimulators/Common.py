@@ -18,6 +18,8 @@ import logging
 
 import ctypes
 
+import re
+
 import numpy as np
 
 from . import _native
@@ -215,7 +217,7 @@ class SWEDataArakawaA:
 
 class BoundaryConditions:
     """Boundary codes per side (Common.py:824-946): 1 wall, 2 periodic,
-    3 flow relaxation, 4 linear interpolation (3 and 4 are not built)."""
+    3 flow relaxation, 4 linear interpolation."""
 
     def __init__(self, north=1, east=1, south=1, west=1,
                  spongeCells={'north': 0, 'south': 0, 'east': 0, 'west': 0}):
@@ -254,9 +256,27 @@ class BoundaryConditions:
                 4: "Open_Linear_Interpolation"}.get(int(cond), "Invalid_:|")
 
     def __str__(self):
+        # plain ints in the sponge dict, so the string reads back with
+        # fromstring (NumPy 2 would print np.int32(..))
+        sponge = {k: int(v) for k, v in self.spongeCells.items()}
         return ("north: " + self._toString(self.north) + ", east: " + self._toString(self.east) +
                 ", south: " + self._toString(self.south) + ", west: " + self._toString(self.west) +
-                ", spongeCells: " + str(self.spongeCells))
+                ", spongeCells: " + str(sponge))
+
+    @classmethod
+    def fromstring(cls, bc_string):
+        """Inverse of __str__, the form SimWriter stores in NetCDF files
+        (Common.py:908-946): four side keywords, then the sponge widths as
+        a dict or as four numbers in north, east, south, west order."""
+        codes = {"Wall": 1, "Periodic": 2, "Flow_Relaxation_Scheme": 3, "Open_Linear_Interpolation": 4}
+        words = [w for w in re.split(r"[\s,:{}\[\]']+", str(bc_string)) if w]
+        sides = [codes.get(words[k], -1) for k in (1, 3, 5, 7)]
+        rest = words[9:]
+        if len(rest) >= 8:
+            sponge = {rest[k]: int(rest[k + 1]) for k in range(0, 8, 2)}
+        else:
+            sponge = dict(zip(("north", "east", "south", "west"), (int(w) for w in rest[:4])))
+        return cls(*sides, spongeCells=sponge)
 
     def codes(self):
         return (int(self.north), int(self.east), int(self.south), int(self.west))

@@ -156,8 +156,8 @@ class OceanStateNoise(object):
         self.reduction_buffer = Common.CUDAArray2D(gpu_stream, 3, 1, 0, 0, np.zeros((1, 3), dtype=np.float32))
         self._red_scratch = torch.zeros(int(self.lib.go_noise_reduce_scratch_bytes()), dtype=torch.uint8,
                                         device="cuda")
-        self.angle_tex = self._texture(angle)
-        self.coriolis_tex = self._texture(coriolis_f)
+        self._angle_tex = self._texture(angle)
+        self._coriolis_tex = self._texture(coriolis_f)
 
     def _texture(self, field):
         arr = np.ascontiguousarray(np.asarray(field, dtype=np.float32))
@@ -289,7 +289,7 @@ class OceanStateNoise(object):
         tail = (_native.ptr(cb.tensor), int(cb.pitch), _native.ptr(eta.tensor), int(eta.pitch),
                 _native.ptr(hu.tensor), int(hu.pitch), _native.ptr(hv.tensor), int(hv.pitch),
                 _native.ptr(H.tensor), int(H.pitch), float(np.float32(land_mask_value)),
-                ctypes.c_uint64(self.angle_tex), ctypes.c_uint64(self.coriolis_tex))
+                ctypes.c_uint64(self._angle_tex), ctypes.c_uint64(self._coriolis_tex))
         phys = (float(np.float32(g)), float(np.float32(f)), float(np.float32(beta)),
                 float(np.float32(y0_reference_cell)))
         if self.interpolation_factor > 1:
