@@ -70,15 +70,19 @@ def _copy_state(dst, i, src, k):
 
 
 class Observations:
-    """Observed cells and values.  ij: (n, 2) interior (i, j) indices;
-    steps: the step numbers (1..n_steps) after which J sums the misfit;
-    values: (len(steps), n, 3) observed (eta, hu, hv)."""
+    """Observed cells and values.  ij: (n, 2) interior (i, j) indices, the
+    same cells at every observation time, or (len(steps), n, 2) cells per
+    time (observations that move, such as drifters); steps: the step
+    numbers (1..n_steps) after which J sums the misfit; values:
+    (len(steps), n, 3) observed (eta, hu, hv)."""
 
     def __init__(self, ij, steps, values, w_eta=100.0, w_vel=1.0):
         torch = _native.require_cuda()
-        ij = np.ascontiguousarray(np.asarray(ij, dtype=np.int32).reshape(-1, 2))
-        values = np.asarray(values, dtype=np.float32).reshape(len(steps), ij.shape[0], 3)
-        self.n = ij.shape[0]
+        ij = np.asarray(ij, dtype=np.int32)
+        self.per_step = ij.ndim == 3
+        ij = np.ascontiguousarray(ij.reshape(len(steps), -1, 2) if self.per_step else ij.reshape(-1, 2))
+        self.n = ij.shape[-2]
+        values = np.asarray(values, dtype=np.float32).reshape(len(steps), self.n, 3)
         self.steps = [int(s) for s in steps]
         if sorted(set(self.steps)) != self.steps:
             raise ValueError("observation steps must be increasing and distinct")
@@ -88,6 +92,36 @@ class Observations:
         self.index = {s: k for k, s in enumerate(self.steps)}
         self.w_eta = float(w_eta)
         self.w_vel = float(w_vel)
+
+    def cells(self, k):
+        """Device (n, 2) cells of observation time k."""
+        return self.ij[k] if self.per_step else self.ij
+
+    @classmethod
+    def drifter_cells(cls, positions, nx, ny, dx, dy):
+        """Interior cells under drifter positions (..., 2) in metres from the
+        south-west interior corner: floor(x / dx), floor(y / dy) in float32,
+        the cell the reference's observation kernel reads
+        (observationKernels.cu:53-64, go_observe_flow), clamped to the
+        interior (a drifter exactly on the east or north edge)."""
+        p = np.asarray(positions, dtype=np.float32)
+        i = np.floor(p[..., 0] / np.float32(dx)).astype(np.int64)
+        j = np.floor(p[..., 1] / np.float32(dy)).astype(np.int64)
+        return np.stack([np.clip(i, 0, nx - 1), np.clip(j, 0, ny - 1)], axis=-1).astype(np.int32)
+
+    @classmethod
+    def from_drifters(cls, positions, steps, currents, nx, ny, dx, dy, w_vel=1.0):
+        """A misfit of drifter-observed currents: at each observation step
+        s_k the (hu, hv) a drifter at positions[k] would observe
+        (GPUDrifterCollection.observeUnderlyingFlow, observationKernels.cu:
+        29-81) against currents[k], weight w_vel, eta unobserved.  The
+        positions are given (the observed trajectories); the dependence of
+        the positions on the flow is not differentiated."""
+        pos = np.asarray(positions, dtype=np.float32).reshape(len(steps), -1, 2)
+        cur = np.asarray(currents, dtype=np.float32).reshape(len(steps), -1, 2)
+        values = np.zeros(cur.shape[:2] + (3,), dtype=np.float32)
+        values[..., 1:] = cur
+        return cls(cls.drifter_cells(pos, nx, ny, dx, dy), steps, values, w_eta=0.0, w_vel=w_vel)
 
     @staticmethod
     def sample(states_by_step, ij):
@@ -125,8 +159,8 @@ class MisfitProblem:
             if s < 0 or s > self.n_steps:
                 raise ValueError("observation step %d outside 0..%d" % (s, self.n_steps))
         ij = obs.ij_host
-        if ij.size and (ij[:, 0].min() < 0 or ij[:, 0].max() >= self.nx or ij[:, 1].min() < 0
-                        or ij[:, 1].max() >= self.ny):
+        if ij.size and (ij[..., 0].min() < 0 or ij[..., 0].max() >= self.nx or ij[..., 1].min() < 0
+                        or ij[..., 1].max() >= self.ny):
             raise ValueError("observation cells must be interior cells (0 <= i < nx, 0 <= j < ny)")
         self.k = max(1, min(int(checkpoint_every), self.n_steps))
         self.domain = _native.Domain(self.nx, self.ny, d.dx, d.dy, d.g, d.r, theta=d.theta,
@@ -172,7 +206,7 @@ class MisfitProblem:
             return
         o = self.obs
         k = o.index[step]
-        _native.check(self._lib().go_obs_misfit(self.sh, slab.gs(i), self.nx, self.ny, o.n, _native.ptr(o.ij),
+        _native.check(self._lib().go_obs_misfit(self.sh, slab.gs(i), self.nx, self.ny, o.n, _native.ptr(o.cells(k)),
                                                 _native.ptr(o.values[k]), o.w_eta, o.w_vel,
                                                 _native.ptr(self.J_dev)))
 
@@ -182,7 +216,7 @@ class MisfitProblem:
         o = self.obs
         k = o.index[step]
         _native.check(self._lib().go_obs_adjoint(self.sh, slab.gs(i), self.lam.gs(0), self.nx, self.ny, o.n,
-                                                 _native.ptr(o.ij), _native.ptr(o.values[k]), o.w_eta, o.w_vel))
+                                                 _native.ptr(o.cells(k)), _native.ptr(o.values[k]), o.w_eta, o.w_vel))
 
     def _traj_step(self, a_slab, ai, s_slab, si, b_slab, bi, sh=None):
         sh = self.sh if sh is None else sh
@@ -457,8 +491,8 @@ class BatchedMisfitProblem:
         self.dt = np.float32(s0.dt if dt is None else dt)
         self.obs = obs
         ij = obs.ij_host
-        if ij.size and (ij[:, 0].min() < 0 or ij[:, 0].max() >= self.nx or ij[:, 1].min() < 0
-                        or ij[:, 1].max() >= self.ny):
+        if ij.size and (ij[..., 0].min() < 0 or ij[..., 0].max() >= self.nx or ij[..., 1].min() < 0
+                        or ij[..., 1].max() >= self.ny):
             raise ValueError("observation cells must be interior cells")
         self.stream = torch.cuda.Stream()
         self.sh = _native.stream_handle(self.stream)
@@ -525,7 +559,7 @@ class BatchedMisfitProblem:
         o, lib = self.obs, _native.load()
         k = o.index[step]
         for m in range(self.M):
-            _native.check(lib.go_obs_misfit(self.sh, self.h0.gs(m), self.nx, self.ny, o.n, _native.ptr(o.ij),
+            _native.check(lib.go_obs_misfit(self.sh, self.h0.gs(m), self.nx, self.ny, o.n, _native.ptr(o.cells(k)),
                                             _native.ptr(o.values[k]), o.w_eta, o.w_vel,
                                             _native.ptr(self.J_dev[m:m + 1])))
 
@@ -536,7 +570,7 @@ class BatchedMisfitProblem:
         k = o.index[step]
         for m in range(self.M):
             _native.check(lib.go_obs_adjoint(self.sh, self.h0.gs(m), self.lam.gs(m), self.nx, self.ny, o.n,
-                                             _native.ptr(o.ij), _native.ptr(o.values[k]), o.w_eta, o.w_vel))
+                                             _native.ptr(o.cells(k)), _native.ptr(o.values[k]), o.w_eta, o.w_vel))
 
     def _advance(self, a, b):
         """h0: Q^a -> Q^b; the misfit of states reached for the first time."""

@@ -106,3 +106,15 @@ def test_initialize_uniform_inside_domain():
     p = d.getDrifterPositions()
     assert p[:, 0].min() >= 0 and p[:, 0].max() <= 10.3
     assert p[:, 1].min() >= 0 and p[:, 1].max() <= 5.4
+
+
+def test_drifter_cells_for_the_misfit():
+    # Observations.drifter_cells: floor(x / dx) in float32 as the observation
+    # kernel reads its cell, clamped to the interior at the east/north edge
+    from SWESimulators.Adjoint import Observations
+    dx, dy, nx, ny = 500.0, 400.0, 10, 8
+    pos = np.array([[0.0, 0.0], [3 * dx, 2 * dy], [3 * dx - 1e-3, 2 * dy - 1e-3], [nx * dx, ny * dy],
+                    [4.5 * dx, 7.99 * dy]])
+    cells = Observations.drifter_cells(pos, nx, ny, dx, dy)
+    assert cells.tolist() == [[0, 0], [3, 2], [2, 1], [nx - 1, ny - 1], [4, 7]]
+    assert Observations.drifter_cells(pos.reshape(1, 5, 2), nx, ny, dx, dy).shape == (1, 5, 2)

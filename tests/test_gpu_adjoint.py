@@ -503,3 +503,53 @@ def test_batched_adjoint_independent_of_snapshots(ctx):
     for J, g, gw in res[1:]:
         assert np.allclose(J, res[0][0], rtol=1e-12)
         assert torch.equal(g, res[0][1]) and torch.equal(gw, res[0][2])
+
+
+def test_drifter_misfit(ctx):
+    """Drifter-observed currents as the misfit (Observations.from_drifters):
+    a truth run with drifters attached gives their positions and the
+    currents go_observe_flow reads under them; those are the truth's hu, hv
+    at Observations.drifter_cells; and the misfit over moving cells has the
+    J and gradient of the sum of one fixed-cell problem per observation
+    time (the adjoint is linear in the observation forcing)."""
+    from SWESimulators.GPUDrifterCollection import GPUDrifterCollection
+
+    n, dx, n_steps, steps = 40, 4000.0, 12, [4, 8, 12]
+    c, sim = make_sim(ctx, n, n, dx=dx, seed=20241, seed_bumps=50002)
+    ct, truth = make_sim(ctx, n, n, dx=dx, seed=20241, seed_bumps=50001)
+    d = GPUDrifterCollection(ctx, 30, boundaryConditions=truth.boundary_conditions, domain_size_x=n * dx,
+                             domain_size_y=n * dx)
+    rng = np.random.default_rng(7)
+    d.setDrifterPositions(rng.uniform(0.1, 0.9, (30, 2)) * n * dx)
+    truth.attachDrifters(d)
+    pos, cur = [], []
+    for s in range(1, n_steps + 1):
+        truth.step(ct.dt)
+        if s in steps:
+            p = d.getDrifterPositions()
+            g = truth.gpu_data
+            o = d.observeUnderlyingFlow(g.hu0, g.hv0, n, n, dx, dx)
+            _, u, v = truth.download(interior_domain_only=True)
+            cells = Adjoint.Observations.drifter_cells(p, n, n, dx, dx)
+            assert np.array_equal(o[:, 0], u[cells[:, 1], cells[:, 0]])
+            assert np.array_equal(o[:, 1], v[cells[:, 1], cells[:, 0]])
+            pos.append(p)
+            cur.append(o)
+    assert not np.array_equal(pos[0], pos[-1])
+    obs = Adjoint.Observations.from_drifters(pos, steps, cur, n, n, dx, dx)
+    assert obs.per_step and obs.w_eta == 0.0
+    x0 = [torch.as_tensor(np.ascontiguousarray(a), device="cuda") for a in sim.download(interior_domain_only=True)]
+    X, Y = wind_field(c, 9)
+    J, *g = Adjoint.MisfitProblem(sim, n_steps, obs, dt=c.dt, checkpoint_every=5).gradient(*x0, X, Y)
+    J_sum, g_sum = 0.0, None
+    vals = obs.values.cpu().numpy()
+    for k, s in enumerate(steps):
+        ok = Adjoint.Observations(obs.ij_host[k], [s], vals[k:k + 1], w_eta=0.0, w_vel=1.0)
+        Jk, *gk = Adjoint.MisfitProblem(sim, n_steps, ok, dt=c.dt, checkpoint_every=5).gradient(*x0, X, Y)
+        J_sum += float(Jk)
+        g_sum = gk if g_sum is None else [a + b for a, b in zip(g_sum, gk)]
+    print("drifter misfit J %.6e, sum of fixed-cell misfits %.6e" % (float(J), J_sum))
+    assert float(J) > 0 and abs(float(J) - J_sum) <= 1e-12 * abs(J_sum)
+    errs = [rel(a, b) for a, b in zip(g, g_sum)]
+    print("gradient rel. differences", ["%.2e" % e for e in errs])
+    assert max(errs) < 1e-5, errs
