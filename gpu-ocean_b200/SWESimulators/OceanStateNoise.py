@@ -273,6 +273,12 @@ class OceanStateNoise(object):
         offset_i, offset_j = coarse_grid_offset(int(self.interpolation_factor), align_with_cell_i,
                                                 align_with_cell_j)
         rn, cb = self.random_numbers, self.coarse_buffer
+        phys = (float(np.float32(g)), float(np.float32(f)), float(np.float32(beta)),
+                float(np.float32(y0_reference_cell)))
+        tail = (_native.ptr(cb.tensor), int(cb.pitch), _native.ptr(eta.tensor), int(eta.pitch),
+                _native.ptr(hu.tensor), int(hu.pitch), _native.ptr(hv.tensor), int(hv.pitch),
+                _native.ptr(H.tensor), int(H.pitch), float(np.float32(land_mask_value)),
+                ctypes.c_uint64(self._angle_tex), ctypes.c_uint64(self._coriolis_tex))
         _native.check(self.lib.go_noise_soar(s, int(self.coarse_nx), int(self.coarse_ny), float(self.coarse_dx),
                                              float(self.coarse_dy), float(soar_q0), float(self.soar_L),
                                              float(np.float32(perturbation_scale)), int(self.periodicNorthSouth),
@@ -286,12 +292,6 @@ class OceanStateNoise(object):
                                                  int(self.periodicNorthSouth), int(self.periodicEastWest),
                                                  _native.ptr(pn.tensor), int(pn.pitch), _native.ptr(cb.tensor),
                                                  int(cb.pitch), 1))
-        tail = (_native.ptr(cb.tensor), int(cb.pitch), _native.ptr(eta.tensor), int(eta.pitch),
-                _native.ptr(hu.tensor), int(hu.pitch), _native.ptr(hv.tensor), int(hv.pitch),
-                _native.ptr(H.tensor), int(H.pitch), float(np.float32(land_mask_value)),
-                ctypes.c_uint64(self._angle_tex), ctypes.c_uint64(self._coriolis_tex))
-        phys = (float(np.float32(g)), float(np.float32(f)), float(np.float32(beta)),
-                float(np.float32(y0_reference_cell)))
         if self.interpolation_factor > 1:
             _native.check(self.lib.go_noise_bicubic(s, int(self.nx), int(self.ny), int(ghost_cells_x),
                                                     int(ghost_cells_y), float(self.dx), float(self.dy),

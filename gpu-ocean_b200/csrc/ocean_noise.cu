@@ -38,6 +38,8 @@
 
 #include <curand_kernel.h>
 
+#include <algorithm>
+
 namespace {
 
 constexpr int kCutoff = 2;             // OceanStateNoise.py:96 (config.soar_cutoff)
@@ -254,6 +256,8 @@ struct BalanceArgs {
     int nx, ny, gx, gy;
     float dx, dy, g, f, beta;
     const float* coarse;
+    // interior cells perturbed: [i_lo, i_hi) x [j_lo, j_hi)
+    int i_lo, i_hi, j_lo, j_hi;
     int cp;
     float *eta, *hu, *hv;
     int pe, pu, pv;
@@ -296,14 +300,36 @@ __device__ __forceinline__ float cell_coriolis(const BalanceArgs& a, int mode, i
 
 constexpr int kBalRows = 4;                   // cells per thread, down a column
 
+// One interior cell's balance (ocean_noise.cu:418-508): corner depths
+// h00..h11 (rows tj, tj+1 x columns ti, ti+1), the coarse perturbation d at
+// the cell and its neighbours (cl, cr west and east, cdn, cup south and
+// north), the cell's (e, u, v); returns the new (eta, hu, hv).
+__device__ __forceinline__ float3 balance_cell(const BalanceArgs& a, int mode, int ti, int tj, float h00, float h01,
+                                               float h10, float h11, float d, float cl, float cr, float cdn,
+                                               float cup, float e, float u, float v) {
+    const bool dry = (h00 == a.land) || (h01 == a.land) || (h10 == a.land) || (h11 == a.land);
+    if (dry) return make_float3(0.0f, 0.0f, 0.0f);
+    const float H_mid = 0.25f * (h00 + h01 + h10 + h11);
+    const float coriolis = cell_coriolis(a, mode, ti, tj);
+    const float h_mid = d + H_mid + e;
+    const float eta_diff_x = (cr - cl) / (2.0f * a.dx);
+    const float eta_diff_y = (cup - cdn) / (2.0f * a.dy);
+    // d_hu = -(g / f) h_mid d_y eta and d_hv = (g / f) h_mid d_x eta; the
+    // reference's hu += d_hu contracts into one fused multiply-add with the
+    // last product (ocean_noise.cu:480-493 under --use_fast_math), written
+    // out here so the rounding does not depend on the compiler.
+    return make_float3(e + d, __fmaf_rn(-(a.g / coriolis) * h_mid, eta_diff_y, u),
+                       __fmaf_rn((a.g / coriolis) * h_mid, eta_diff_x, v));
+}
+
 // Interior cells of the model grid; the coarse grid is the model grid
 // (ocean_noise.cu:379-508).  Each thread marches kBalRows cells down one
 // column, carrying the coarse values of the rows above and below and the
 // lower corner pair of Hi from one cell to the next.
 __global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a, int mode) {
-    const int ti = blockIdx.x * kBW + threadIdx.x + a.gx;
-    const int tj0 = (blockIdx.y * kBH + threadIdx.y) * kBalRows + a.gy;
-    if (ti < 2 || ti >= a.nx + 2) return;
+    const int ti = blockIdx.x * kBW + threadIdx.x + a.i_lo;
+    const int tj0 = (blockIdx.y * kBH + threadIdx.y) * kBalRows + a.j_lo;
+    if (ti >= a.i_hi) return;
     const float* __restrict__ coarse = a.coarse;
     const float* __restrict__ Hi = a.Hi;
     float* __restrict__ eta_p = a.eta;
@@ -336,28 +362,12 @@ __global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a, int m
 #pragma unroll
     for (int r = 0; r < kBalRows; ++r) {
         const int tj = tj0 + r;
-        if (tj < 2 || tj >= a.ny + 2) continue;
-        const float h00 = hl[r], h01 = hr[r], h10 = hl[r + 1], h11 = hr[r + 1];
-        const bool dry = (h00 == a.land) || (h01 == a.land) || (h10 == a.land) || (h11 == a.land);
-        const float H_mid = 0.25f * (h00 + h01 + h10 + h11);
-        const float coriolis = cell_coriolis(a, mode, ti, tj);
-        const float d = cc[r + 1];
-        const float h_mid = d + H_mid + e[r];
-        const float eta_diff_x = (cr[r] - cl[r]) / (2.0f * a.dx);
-        const float eta_diff_y = (cc[r + 2] - cc[r]) / (2.0f * a.dy);
-        // d_hu = -(g / f) h_mid d_y eta and d_hv = (g / f) h_mid d_x eta; the
-        // reference's hu += d_hu contracts into one fused multiply-add with
-        // the last product (ocean_noise.cu:480-493 under --use_fast_math),
-        // written out here so the rounding does not depend on the compiler.
-        float en = 0.0f, un = 0.0f, vn = 0.0f;
-        if (!dry) {
-            en = e[r] + d;
-            un = __fmaf_rn(-(a.g / coriolis) * h_mid, eta_diff_y, u[r]);
-            vn = __fmaf_rn((a.g / coriolis) * h_mid, eta_diff_x, v[r]);
-        }
-        eta_p[(size_t)tj * a.pe + ti] = en;
-        hu_p[(size_t)tj * a.pu + ti] = un;
-        hv_p[(size_t)tj * a.pv + ti] = vn;
+        if (tj >= a.j_hi) continue;
+        const float3 q = balance_cell(a, mode, ti, tj, hl[r], hr[r], hl[r + 1], hr[r + 1], cc[r + 1], cl[r], cr[r],
+                                      cc[r], cc[r + 2], e[r], u[r], v[r]);
+        eta_p[(size_t)tj * a.pe + ti] = q.x;
+        hu_p[(size_t)tj * a.pu + ti] = q.y;
+        hv_p[(size_t)tj * a.pv + ti] = q.z;
     }
 }
 
@@ -457,12 +467,12 @@ __device__ float interpolate(const InterpArgs& a, int ti, int tj) {
 __global__ void __launch_bounds__(kBW* kBH) k_interp_balance(const InterpArgs a) {
     __shared__ float d_eta[kBH + 2][kBW + 2];
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int bx = blockIdx.x * kBW + a.b.gx, by = blockIdx.y * kBH + a.b.gy;
+    const int bx = blockIdx.x * kBW + a.b.i_lo, by = blockIdx.y * kBH + a.b.j_lo;
     for (int j = ty; j < kBH + 2; j += kBH)
         for (int i = tx; i < kBW + 2; i += kBW) d_eta[j][i] = interpolate(a, bx + i - 1, by + j - 1);
     __syncthreads();
     const int ti = bx + tx, tj = by + ty;
-    if (!(ti > 1 && tj > 1 && ti < a.b.nx + 2 && tj < a.b.ny + 2)) return;
+    if (ti >= a.b.i_hi || tj >= a.b.j_hi) return;
     float H_mid;
     bool dry;
     cell_depth(a.b, ti, tj, H_mid, dry);
@@ -666,6 +676,15 @@ static int fill_balance(BalanceArgs& a, int nx, int ny, float dx, float dy, int 
     a.eta = eta; a.hu = hu; a.hv = hv;
     a.pe = eta_pitch / 4; a.pu = hu_pitch / 4; a.pv = hv_pitch / 4;
     a.Hi = Hi; a.ph = Hi_pitch / 4; a.land = land_value;
+    // The reference launches one 16 x 16 block per 16 x 16 cells from the
+    // ghost offset and perturbs the interior cells its threads reach
+    // (OceanStateNoise.py:279-282, ocean_noise.cu:462): with offsets 0 or
+    // 1 that can stop short of the last interior cells.  Same cells here.
+    constexpr int kRefBlock = 16;
+    a.i_lo = ghost_x > 2 ? ghost_x : 2;
+    a.j_lo = ghost_y > 2 ? ghost_y : 2;
+    a.i_hi = std::min(nx + 2, ghost_x + kRefBlock * ((nx + kRefBlock - 1) / kRefBlock));
+    a.j_hi = std::min(ny + 2, ghost_y + kRefBlock * ((ny + kRefBlock - 1) / kRefBlock));
     a.angle = (cudaTextureObject_t)angle_texture;
     a.coriolis = (cudaTextureObject_t)coriolis_texture;
     return GO_OK;
@@ -682,7 +701,9 @@ int go_noise_geostrophic(void* stream, int nx, int ny, float dx, float dy, int g
                           eta_pitch, hu, hu_pitch, hv, hv_pitch, Hi, Hi_pitch, land_value, angle_texture,
                           coriolis_texture);
     if (rc) return rc;
-    const dim3 grid((nx + kBW - 1) / kBW, (ny + kBH * kBalRows - 1) / (kBH * kBalRows));
+    const int ci = a.i_hi - a.i_lo, cj = a.j_hi - a.j_lo;
+    if (ci <= 0 || cj <= 0) return GO_OK;
+    const dim3 grid((ci + kBW - 1) / kBW, (cj + kBH * kBalRows - 1) / (kBH * kBalRows));
     k_balance<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(a, coriolis_mode(f, beta));
     GO_CUDA(cudaGetLastError());
     return GO_OK;
@@ -703,7 +724,9 @@ int go_noise_bicubic(void* stream, int nx, int ny, int ghost_x, int ghost_y, flo
     if (rc) return rc;
     a.cnx = coarse_nx; a.cny = coarse_ny; a.cgx = coarse_ghost_x; a.cgy = coarse_ghost_y;
     a.cdx = coarse_dx; a.cdy = coarse_dy; a.off_i = offset_i; a.off_j = offset_j;
-    const dim3 grid((nx + kBW - 1) / kBW, (ny + kBH - 1) / kBH);
+    const int ci = a.b.i_hi - a.b.i_lo, cj = a.b.j_hi - a.b.j_lo;
+    if (ci <= 0 || cj <= 0) return GO_OK;
+    const dim3 grid((ci + kBW - 1) / kBW, (cj + kBH - 1) / kBH);
     k_interp_balance<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(a);
     GO_CUDA(cudaGetLastError());
     return GO_OK;

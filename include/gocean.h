@@ -195,7 +195,9 @@ int go_noise_soar(void* stream, int coarse_nx, int coarse_ny, float coarse_dx, f
  * angle and Coriolis textures are handles of go_wind_texture_create (the
  * reference's angle_tex and coriolis_f_tex: bilinear, clamped, normalised
  * over the ghost-inclusive grid); the Coriolis texture is read where f == 0.
- * y0_reference_cell is accepted and unused, as in the reference. */
+ * y0_reference_cell is accepted and unused, as in the reference.  The cells
+ * perturbed are the interior cells the reference's 16 x 16-block launch
+ * reaches from the ghost offset (all of them for ghost offset 2). */
 int go_noise_geostrophic(void* stream, int nx, int ny, float dx, float dy, int ghost_x, int ghost_y, float g,
                          float f, float beta, float y0_reference_cell, const float* coarse, int coarse_pitch,
                          float* eta, int eta_pitch, float* hu, int hu_pitch, float* hv, int hv_pitch,

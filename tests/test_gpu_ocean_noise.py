@@ -397,3 +397,31 @@ def test_large_grid_vs_reference_with_timing(ctx, pns, pew):
     t_mine, t_ref = timed(mine), timed(theirs)
     print("2048^2 perturbation (draws + SOAR + balance): ours %.3f ms, reference kernels %.3f ms (x%.2f)"
           % (t_mine, t_ref, t_ref / t_mine))
+
+
+@pytest.mark.parametrize("ghost", [0, 1, 2])
+@pytest.mark.parametrize("n, factor", [(47, 1), (63, 3)])
+def test_ghost_offsets_vs_reference(ctx, ghost, n, factor):
+    """Ghost offsets 0 and 1 (the reference's defaults of perturbOceanState)
+    on grids of 16k - 1 cells, where the reference's 16 x 16 launch stops
+    short of the last interior cells: the same cells change, bit for bit,
+    through the direct (factor 1) and bicubic (factor 3) balance."""
+    ref = _ref()
+    nn = _noise(ctx, n, n, factor=factor)
+    eta, Hi = _state(n, n)
+    a = _arrays(ctx, n, n, eta, Hi)
+    re, rhu, rhv, rH = _pitched(eta), _pitched(np.zeros_like(eta)), _pitched(np.zeros_like(eta)), _pitched(Hi)
+    for _ in range(2):
+        nn.perturbOceanState(*a, F, 0.0, G, ghost_cells_x=ghost, ghost_cells_y=ghost)
+        rc = _pitched(nn.getCoarseBuffer())
+        if factor == 1:
+            ref.geostrophic(n, n, DX, DX, G, F, 0.0, rc, re, rhu, rhv, rH, gx=ghost, gy=ghost)
+        else:
+            ref.bicubic(n, n, DX, DX, int(nn.coarse_nx), int(nn.coarse_ny), nn.coarse_dx, nn.coarse_dy, 0, 0, G, F,
+                        0.0, rc, re, rhu, rhv, rH, gx=ghost, gy=ghost)
+    s = torch.cuda.current_stream()
+    for x, y in zip(a[:3], (re, rhu, rhv)):
+        m = x.download(s)
+        assert np.array_equal(m, _host(y, m.shape))
+    if ghost == 0:
+        assert not a[1].download(s)[2:-2, -3].any()      # column n + 1 untouched, as in the reference
