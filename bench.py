@@ -522,7 +522,44 @@ def run_model_error(ctx, steps=50, reps=20, n=4096):
     x = OceanStateNoise(ctx, s, c.nx, c.ny, c.dx, c.dy, Common.BoundaryConditions(*c.bc), False, use_lcg=False,
                         xorwow_seed=1)
     out["xorwow_draws_ms"] = timed(s, x.generateNormalDistribution, reps)
+    del x
+    out["ensemble"] = run_model_error_ensemble(ctx)
     return out
+
+
+def run_model_error_ensemble(ctx, members=32, n=512, steps=20):
+    """The reference's ensemble with model error (OceanNoiseEnsemble.step:
+    every member steps and is perturbed after every step): 32 members of
+    512^2, LCG, member by member (CDKLM16.step per member, 5 launches a
+    step each) against BatchedCDKLM16.step (2 step launches and 3 model-error
+    launches a step for all members, plus the members' boundary updates).
+    Wall time around synchronised loops, per step."""
+    import time
+    import torch
+    from SWESimulators import CDKLM16, SyntheticCases as SC
+    from SWESimulators.BatchedEnsemble import BatchedCDKLM16
+
+    c = SC.grf(n, dx=1000.0, bc=(2, 2, 2, 2), steps=1)
+    sims = [CDKLM16.CDKLM16(ctx, dt=c.dt, small_scale_perturbation=True, small_scale_perturbation_amplitude=1e-4,
+                            use_lcg=True, **c.kwargs()) for _ in range(members)]
+
+    def wall(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / steps
+
+    loop_ms = wall(lambda: [s.step(steps * c.dt) for s in sims])
+    ens = BatchedCDKLM16(sims)
+    batched_ms = wall(lambda: ens.step(steps * c.dt))
+    cells = members * n * n
+    return {"members": members, "grid": "%dx%d" % (n, n), "steps": steps, "loop_ms_per_step": loop_ms,
+            "batched_ms_per_step": batched_ms, "speedup": loop_ms / batched_ms,
+            "batched_gcell_steps_s": cells / (batched_ms * 1e-3) / 1e9,
+            "loop_gcell_steps_s": cells / (loop_ms * 1e-3) / 1e9,
+            "note": "wall clock around synchronised loops; model error after every step"}
 
 
 def run_adjoint(ctx, n=512, n_steps=500, k=50, kind=0, rows=0):

@@ -120,12 +120,15 @@ class BatchedCDKLM16:
             s.t = sums[key]
             s.num_iterations += n_steps
 
-    def step(self, t_end):
+    def step(self, t_end, apply_stochastic_term=True):
         """Every member advances by t_end with the reference's step() loop
-        semantics (CDKLM16.py:494-598); the members must share dt."""
+        semantics (CDKLM16.py:494-598); the members must share dt.  Members
+        built with small_scale_perturbation get their model error after
+        every step (CDKLM16.py:580-586), all members in one batched pass."""
         dts = {float(np.float32(s.dt)) for s in self.sims}
         if len(dts) != 1:
             raise ValueError("step(t_end) needs a common dt; use advance(n) for per-member dt")
+        perturb = apply_stochastic_term and self._has_model_error()
         dt = np.float32(self.sims[0].dt)
         t_now = 0.0
         full = 0
@@ -135,14 +138,77 @@ class BatchedCDKLM16:
                 break
             full += 1
             t_now += np.float64(local_dt)
-        if full:
+        if full and perturb:
+            for _ in range(full):
+                self.advance(1)
+                self.perturb_members(boundary_conditions=True)
+        elif full:
             self.advance(full)
         if t_now < t_end:
             last = np.float32(min(dt, np.float32(t_end - t_now)))
             self.set_dt([last] * self.n)
             self.advance(1)
+            if perturb:
+                self.perturb_members(boundary_conditions=True)
             self.set_dt([dt] * self.n)
         return self.sims[0].t
+
+    # -- the members' own model error (OceanStateNoise) ----------------------
+    def _has_model_error(self):
+        flags = [bool(getattr(s, "small_scale_perturbation", False)) for s in self.sims]
+        if any(flags) and not all(flags):
+            raise ValueError("either every member or none has small_scale_perturbation")
+        return all(flags)
+
+    def _noise_batch(self):
+        """go_noise_batch over the members' OceanStateNoise objects (built
+        once; the descriptors point at the members' own buffers)."""
+        if getattr(self, "_noise", None) is not None:
+            return self._noise
+        import ctypes
+        errs = [s.small_scale_model_error for s in self.sims]
+        e0, s0 = errs[0], self.sims[0]
+        for e, s in zip(errs, self.sims):
+            same = (int(e.nx), int(e.ny), int(e.interpolation_factor), bool(e.use_lcg), int(e.periodicNorthSouth),
+                    int(e.periodicEastWest), float(e.soar_L), float(e.dx), float(e.dy)) == \
+                   (int(e0.nx), int(e0.ny), 1, bool(e0.use_lcg), int(e0.periodicNorthSouth),
+                    int(e0.periodicEastWest), float(e0.soar_L), float(e0.dx), float(e0.dy))
+            if not same or int(s.ghost_cells_x) != int(s0.ghost_cells_x):
+                raise ValueError("batched model error needs one grid, generator, boundary kinds, soar_L and "
+                                 "interpolation factor 1 for all members")
+        descs = (_native.GoNoiseMember * self.n)(*[e.member_desc(s) for e, s in zip(errs, self.sims)])
+        h = ctypes.c_void_p()
+        _native.check(_native.load().go_noise_batch_create(
+            ctypes.cast(descs, ctypes.c_void_p), self.n, int(e0.nx), int(e0.ny), float(e0.dx), float(e0.dy),
+            int(s0.ghost_cells_x), int(s0.ghost_cells_y), float(e0.soar_L), int(e0.periodicNorthSouth),
+            int(e0.periodicEastWest), int(bool(e0.use_lcg)), ctypes.byref(h)))
+        self._noise = h
+        return h
+
+    def perturb_members(self, q0_scale=1.0, perturbation_scale=1.0, boundary_conditions=False):
+        """Every member's OceanStateNoise.perturbSim (OceanStateNoise.py:
+        376-397) in three launches for all members (go_noise_batch_perturb),
+        each member bit for bit as alone: CDKLM16.perturbState of every
+        member (CDKLM16.py:642-644).  boundary_conditions=True also refreshes
+        the ghost cells afterwards, as the step loop does (CDKLM16.py:
+        580-586)."""
+        h = self._noise_batch()
+        self._sync_members()
+        _native.check(_native.load().go_noise_batch_perturb(h, _native.stream_handle(self.stream), float(q0_scale),
+                                                            float(np.float32(perturbation_scale)), 1))
+        if boundary_conditions:
+            for s in self.sims:
+                s.bc_kernel.boundaryCondition(self.stream, s.gpu_data.h0, s.gpu_data.hu0, s.gpu_data.hv0)
+        self._release_members()
+
+    def __del__(self):
+        h = getattr(self, "_noise", None)
+        if h is not None:
+            try:
+                _native.load().go_noise_batch_destroy(h)
+            except Exception:
+                pass
+            self._noise = None
 
     def perturb(self, key0, event, std=0.05, corr_cells=15.0):
         """Every member's eta += std * field(key (key0, m), event): one

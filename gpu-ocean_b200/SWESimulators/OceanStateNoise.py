@@ -269,7 +269,9 @@ class OceanStateNoise(object):
         if update_random_field:
             self.generateNormalDistribution()
         s = self._s(stream)
-        soar_q0 = np.float32(self.soar_q0 * q0_scale)
+        # q0 x q0_scale in double, then float (the reference's NumPy 1
+        # scalar arithmetic; go_noise_batch_perturb forms it the same way)
+        soar_q0 = np.float32(np.float64(self.soar_q0) * np.float64(q0_scale))
         offset_i, offset_j = coarse_grid_offset(int(self.interpolation_factor), align_with_cell_i,
                                                 align_with_cell_j)
         rn, cb = self.random_numbers, self.coarse_buffer
@@ -303,6 +305,28 @@ class OceanStateNoise(object):
             _native.check(self.lib.go_noise_geostrophic(s, int(self.nx), int(self.ny), float(self.dx),
                                                         float(self.dy), int(ghost_cells_x), int(ghost_cells_y),
                                                         *phys, *tail))
+
+    def member_desc(self, sim):
+        """The go_noise_member descriptor of this perturbation applied to
+        sim's state (for go_noise_batch_create)."""
+        m = _native.GoNoiseMember()
+        if self.use_lcg:
+            m.seed, m.seed_pitch = int(self.seed.tensor.data_ptr()), int(self.seed.pitch)
+        else:
+            m.xorwow_states, m.n_generators = int(self.rng.data_ptr()), int(self._n_generators)
+        m.random, m.random_pitch = int(self.random_numbers.tensor.data_ptr()), int(self.random_numbers.pitch)
+        m.coarse, m.coarse_pitch = int(self.coarse_buffer.tensor.data_ptr()), int(self.coarse_buffer.pitch)
+        g = sim.gpu_data
+        m.eta, m.eta_pitch = int(g.h0.tensor.data_ptr()), int(g.h0.pitch)
+        m.hu, m.hu_pitch = int(g.hu0.tensor.data_ptr()), int(g.hu0.pitch)
+        m.hv, m.hv_pitch = int(g.hv0.tensor.data_ptr()), int(g.hv0.pitch)
+        Bi = sim.bathymetry.Bi
+        m.Hi, m.Hi_pitch = int(Bi.tensor.data_ptr()), int(Bi.pitch)
+        m.angle_texture, m.coriolis_texture = self._angle_tex, self._coriolis_tex
+        m.soar_q0 = float(self.soar_q0)
+        m.g, m.f, m.beta = float(np.float32(sim.g)), float(np.float32(sim.f)), float(np.float32(sim.coriolis_beta))
+        m.land_value = float(np.float32(sim.bathymetry.mask_value))
+        return m
 
     def _obtain_coarse_grid_offset(self, fine_index_i, fine_index_j):
         return coarse_grid_offset(int(self.interpolation_factor), fine_index_i, fine_index_j)

@@ -56,6 +56,18 @@ class GoState(ctypes.Structure):
 
 _SP = ctypes.POINTER(GoState)
 
+
+class GoNoiseMember(ctypes.Structure):
+    """go_noise_member: one ensemble member's model-error buffers."""
+    _fields_ = [("seed", ctypes.c_void_p), ("xorwow_states", ctypes.c_void_p), ("random", ctypes.c_void_p),
+                ("coarse", ctypes.c_void_p), ("eta", ctypes.c_void_p), ("hu", ctypes.c_void_p),
+                ("hv", ctypes.c_void_p), ("Hi", ctypes.c_void_p), ("angle_texture", ctypes.c_uint64),
+                ("coriolis_texture", ctypes.c_uint64), ("seed_pitch", ctypes.c_int), ("random_pitch", ctypes.c_int),
+                ("coarse_pitch", ctypes.c_int), ("eta_pitch", ctypes.c_int), ("hu_pitch", ctypes.c_int),
+                ("hv_pitch", ctypes.c_int), ("Hi_pitch", ctypes.c_int), ("n_generators", ctypes.c_int),
+                ("soar_q0", ctypes.c_float), ("g", ctypes.c_float), ("f", ctypes.c_float), ("beta", ctypes.c_float),
+                ("land_value", ctypes.c_float), ("reserved", ctypes.c_float)]
+
 # name -> (restype, argtypes)
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -116,6 +128,9 @@ SIGNATURES = {
                                   _P, _I, _F, ctypes.c_uint64, ctypes.c_uint64]),
     "go_noise_bicubic": (_I, [_P, _I, _I, _I, _I, _F, _F, _I, _I, _I, _I, _F, _F, _I, _I, _F, _F, _F, _F, _P, _I,
                               _P, _I, _P, _I, _P, _I, _P, _I, _F, ctypes.c_uint64, ctypes.c_uint64]),
+    "go_noise_batch_create": (_I, [_P, _I, _I, _I, _F, _F, _I, _I, _F, _I, _I, _I, ctypes.POINTER(ctypes.c_void_p)]),
+    "go_noise_batch_destroy": (_I, [_P]),
+    "go_noise_batch_perturb": (_I, [_P, _P, ctypes.c_double, _F, _I]),
     "go_noise_reduce_scratch_bytes": (ctypes.c_size_t, []),
     "go_noise_square_sums": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _P, ctypes.c_size_t]),
     "go_noise_make_perpendicular": (_I, [_P, _I, _I, _P, _I, _P, _I, _P]),

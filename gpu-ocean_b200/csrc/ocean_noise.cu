@@ -86,8 +86,9 @@ __device__ __forceinline__ float2 box_muller(float2 u) {
 // (ocean_noise.cu:121-200).  The reference's branch for a lone last column
 // (2i == random_nx) is met by no thread, so an odd width keeps its last
 // column unwritten; kept as it is for parity.
-__global__ void k_lcg(int normal, int seed_nx, int seed_ny, int random_nx, unsigned long long* __restrict__ seed,
-                      int sp, float* __restrict__ rnd, int rp) {
+__device__ __forceinline__ void lcg_body(int normal, int seed_nx, int seed_ny, int random_nx,
+                                         unsigned long long* __restrict__ seed, int sp, float* __restrict__ rnd,
+                                         int rp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= seed_nx || j >= seed_ny) return;
@@ -104,6 +105,11 @@ __global__ void k_lcg(int normal, int seed_nx, int seed_ny, int random_nx, unsig
     }
 }
 
+__global__ void k_lcg(int normal, int seed_nx, int seed_ny, int random_nx, unsigned long long* __restrict__ seed,
+                      int sp, float* __restrict__ rnd, int rp) {
+    lcg_body(normal, seed_nx, seed_ny, random_nx, seed, sp, rnd, rp);
+}
+
 __global__ void k_xorwow_init(unsigned long long seed, int n, curandStateXORWOW_t* __restrict__ states) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
@@ -114,8 +120,8 @@ __global__ void k_xorwow_init(unsigned long long seed, int n, curandStateXORWOW_
 
 // Generator g fills the element pairs g, g + n, g + 2n, ... of the row-major
 // nx x ny field (pitched rows).
-__global__ void k_xorwow_fill(int normal, int n, curandStateXORWOW_t* __restrict__ states, int nx, int ny,
-                              float* __restrict__ out, int op) {
+__device__ __forceinline__ void xorwow_body(int normal, int n, curandStateXORWOW_t* __restrict__ states, int nx,
+                                            int ny, float* __restrict__ out, int op) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     curandStateXORWOW_t st = states[g];
@@ -136,6 +142,11 @@ __global__ void k_xorwow_fill(int normal, int n, curandStateXORWOW_t* __restrict
         }
     }
     states[g] = st;
+}
+
+__global__ void k_xorwow_fill(int normal, int n, curandStateXORWOW_t* __restrict__ states, int nx, int ny,
+                              float* __restrict__ out, int op) {
+    xorwow_body(normal, n, states, nx, ny, out, op);
 }
 
 // ---- SOAR covariance on the coarse grid ---------------------------------------
@@ -172,11 +183,9 @@ __device__ __forceinline__ int random_src(int c, int n, int periodic) {
 // A block covers 32 x 32 cells; the random values behind them (36 x 36) sit
 // in shared memory and each thread sums a strip of 8 cells down one column
 // from registers, taps in the reference's order (rows outer, columns inner).
-__global__ void __launch_bounds__(kBW* kSoarTY) k_soar(int nx, int ny, float dx, float dy, float q0, float L,
-                                                       float scale, int pns, int pew,
-                                                       const float* __restrict__ rnd, int rp,
-                                                       float* __restrict__ coarse, int cp, int additive,
-                                                       int aligned16) {
+__device__ __forceinline__ void soar_body(int nx, int ny, float dx, float dy, float q0, float L, float scale, int pns,
+                                          int pew, const float* __restrict__ rnd, int rp, float* __restrict__ coarse,
+                                          int cp, int additive, int aligned16) {
     constexpr int TW = kBW + 2 * kCutoff, TH = kSoarBH + 2 * kCutoff;
     static_assert(TW % 4 == 0 && (2 * kCutoff) % 4 == 0, "float4 tile rows");
     __shared__ float xi[TH][TW];
@@ -248,6 +257,14 @@ __global__ void __launch_bounds__(kBW* kSoarTY) k_soar(int nx, int ny, float dx,
             *out = additive > 0 ? __fmaf_rn(scale, acc[r], *out) : scale * acc[r];
         }
     }
+}
+
+__global__ void __launch_bounds__(kBW* kSoarTY) k_soar(int nx, int ny, float dx, float dy, float q0, float L,
+                                                       float scale, int pns, int pew,
+                                                       const float* __restrict__ rnd, int rp,
+                                                       float* __restrict__ coarse, int cp, int additive,
+                                                       int aligned16) {
+    soar_body(nx, ny, dx, dy, q0, L, scale, pns, pew, rnd, rp, coarse, cp, additive, aligned16);
 }
 
 // ---- geostrophic balance -------------------------------------------------------
@@ -326,7 +343,7 @@ __device__ __forceinline__ float3 balance_cell(const BalanceArgs& a, int mode, i
 // (ocean_noise.cu:379-508).  Each thread marches kBalRows cells down one
 // column, carrying the coarse values of the rows above and below and the
 // lower corner pair of Hi from one cell to the next.
-__global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a, int mode) {
+__device__ __forceinline__ void balance_body(const BalanceArgs& a, int mode) {
     const int ti = blockIdx.x * kBW + threadIdx.x + a.i_lo;
     const int tj0 = (blockIdx.y * kBH + threadIdx.y) * kBalRows + a.j_lo;
     if (ti >= a.i_hi) return;
@@ -370,6 +387,8 @@ __global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a, int m
         hv_p[(size_t)tj * a.pv + ti] = q.z;
     }
 }
+
+__global__ void __launch_bounds__(kBW* kBH) k_balance(const BalanceArgs a, int mode) { balance_body(a, mode); }
 
 // ---- bicubic interpolation from the coarse grid ---------------------------------
 
@@ -763,6 +782,160 @@ int go_noise_make_perpendicular(void* stream, int nx, int ny, const float* xi, i
     k_make_perpendicular<<<grid, dim3(kBW, kBH), 0, (cudaStream_t)stream>>>(nx, ny, xi, xi_pitch / 4, nu,
                                                                             nu_pitch / 4, reduction);
     GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+}  // extern "C"
+
+// ---- the model error of an ensemble, batched across members ---------------------
+//
+// One launch per kernel over all members (blockIdx.z = member); each block
+// runs the single-member kernel's body on its member's buffers and
+// parameters, so each member gets exactly its own perturbation.
+
+namespace {
+
+__global__ void k_lcg_batch(const go_noise_member* __restrict__ m, int seed_nx, int seed_ny, int random_nx) {
+    const go_noise_member& a = m[blockIdx.z];
+    lcg_body(1, seed_nx, seed_ny, random_nx, reinterpret_cast<unsigned long long*>(a.seed), a.seed_pitch / 8,
+             a.random, a.random_pitch / 4);
+}
+
+__global__ void k_xorwow_batch(const go_noise_member* __restrict__ m, int nx, int ny) {
+    const go_noise_member& a = m[blockIdx.z];
+    xorwow_body(1, a.n_generators, reinterpret_cast<curandStateXORWOW_t*>(a.xorwow_states), nx, ny, a.random,
+                a.random_pitch / 4);
+}
+
+__global__ void __launch_bounds__(kBW* kSoarTY) k_soar_batch(const go_noise_member* __restrict__ m, int nx, int ny,
+                                                             float dx, float dy, float L, double q0_scale,
+                                                             float scale, int pns, int pew, int aligned16) {
+    const go_noise_member& a = m[blockIdx.z];
+    const float q0 = (float)((double)a.soar_q0 * q0_scale);
+    soar_body(nx, ny, dx, dy, q0, L, scale, pns, pew, a.random, a.random_pitch / 4, a.coarse, a.coarse_pitch / 4, 0,
+              aligned16);
+}
+
+__global__ void __launch_bounds__(kBW* kBH) k_balance_batch(const go_noise_member* __restrict__ m,
+                                                            const BalanceArgs geom) {
+    const go_noise_member& mm = m[blockIdx.z];
+    BalanceArgs a = geom;
+    a.g = mm.g;
+    a.f = mm.f;
+    a.beta = mm.beta;
+    a.coarse = mm.coarse;
+    a.cp = mm.coarse_pitch / 4;
+    a.eta = mm.eta;
+    a.hu = mm.hu;
+    a.hv = mm.hv;
+    a.pe = mm.eta_pitch / 4;
+    a.pu = mm.hu_pitch / 4;
+    a.pv = mm.hv_pitch / 4;
+    a.Hi = mm.Hi;
+    a.ph = mm.Hi_pitch / 4;
+    a.land = mm.land_value;
+    a.angle = (cudaTextureObject_t)mm.angle_texture;
+    a.coriolis = (cudaTextureObject_t)mm.coriolis_texture;
+    balance_body(a, coriolis_mode(a.f, a.beta));
+}
+
+}  // namespace
+
+struct go_noise_batch {
+    int n, nx, ny, pns, pew, use_lcg, n_gen, aligned16;
+    int seed_nx, seed_ny, rand_nx, rand_ny;
+    float dx, dy, L;
+    BalanceArgs geom;                 // shared geometry of the balance (cells, dx, dy)
+    go_noise_member* d_members;
+};
+
+extern "C" {
+
+int go_noise_batch_create(const go_noise_member* members, int n, int nx, int ny, float dx, float dy, int ghost_x,
+                          int ghost_y, float soar_L, int periodic_north_south, int periodic_east_west, int use_lcg,
+                          go_noise_batch** out) {
+    if (!members || !out || n < 1) return go_fail(GO_ERR_INVALID, "no members");
+    if (n > 65535) return go_fail(GO_ERR_INVALID, "%d members, at most 65535", n);
+    if (nx < 1 || ny < 1) return go_fail(GO_ERR_INVALID, "empty grid");
+    *out = nullptr;
+    const int rnx = periodic_east_west ? nx : nx + 4 * kCutoff;
+    const int rny = periodic_north_south ? ny : ny + 4 * kCutoff;
+    const int snx = (rnx + 1) / 2;
+    int aligned = 1;
+    for (int k = 0; k < n; ++k) {
+        const go_noise_member& m = members[k];
+        if (!m.random || !m.coarse || !m.eta || !m.hu || !m.hv || !m.Hi)
+            return go_fail(GO_ERR_INVALID, "member %d: null buffer", k);
+        if (!m.angle_texture || !m.coriolis_texture)
+            return go_fail(GO_ERR_INVALID, "member %d: angle and Coriolis textures needed", k);
+        if (use_lcg) {
+            if (!m.seed || m.seed_pitch < 8 * snx || m.seed_pitch % 8)
+                return go_fail(GO_ERR_INVALID, "member %d: seeds", k);
+        } else if (!m.xorwow_states || m.n_generators < 1 || m.n_generators != members[0].n_generators) {
+            return go_fail(GO_ERR_INVALID, "member %d: XORWOW states", k);
+        }
+        int rc = check_field(m.random_pitch, rnx, "random");
+        if (!rc) rc = check_field(m.coarse_pitch, nx + 4, "coarse");
+        if (!rc) rc = check_field(m.eta_pitch, nx + 4, "eta");
+        if (!rc) rc = check_field(m.hu_pitch, nx + 4, "hu");
+        if (!rc) rc = check_field(m.hv_pitch, nx + 4, "hv");
+        if (!rc) rc = check_field(m.Hi_pitch, nx + 5, "Hi");
+        if (rc) return rc;
+        if (((uintptr_t)m.random | (uintptr_t)m.random_pitch) & 15) aligned = 0;
+    }
+    go_noise_batch* b = new go_noise_batch();
+    b->n = n; b->nx = nx; b->ny = ny; b->pns = periodic_north_south; b->pew = periodic_east_west;
+    b->use_lcg = use_lcg; b->n_gen = members[0].n_generators; b->aligned16 = aligned;
+    b->seed_nx = snx; b->seed_ny = rny; b->rand_nx = rnx; b->rand_ny = rny;
+    b->dx = dx; b->dy = dy; b->L = soar_L;
+    const go_noise_member& m0 = members[0];
+    int rc = fill_balance(b->geom, nx, ny, dx, dy, ghost_x, ghost_y, m0.g, m0.f, m0.beta, m0.coarse,
+                          m0.coarse_pitch, nx + 4, m0.eta, m0.eta_pitch, m0.hu, m0.hu_pitch, m0.hv, m0.hv_pitch,
+                          m0.Hi, m0.Hi_pitch, m0.land_value, m0.angle_texture, m0.coriolis_texture);
+    cudaError_t e = cudaSuccess;
+    if (!rc) e = cudaMalloc(&b->d_members, sizeof(go_noise_member) * n);
+    if (!rc && e == cudaSuccess)
+        e = cudaMemcpy(b->d_members, members, sizeof(go_noise_member) * n, cudaMemcpyHostToDevice);
+    if (rc || e != cudaSuccess) {
+        if (b->d_members) cudaFree(b->d_members);
+        delete b;
+        return rc ? rc : go_fail(GO_ERR_CUDA, "noise batch: %s", cudaGetErrorString(e));
+    }
+    *out = b;
+    return GO_OK;
+}
+
+int go_noise_batch_destroy(go_noise_batch* b) {
+    if (!b) return GO_OK;
+    cudaFree(b->d_members);
+    delete b;
+    return GO_OK;
+}
+
+int go_noise_batch_perturb(go_noise_batch* b, void* stream, double q0_scale, float perturbation_scale,
+                           int update_random_field) {
+    if (!b) return go_fail(GO_ERR_INVALID, "null batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (update_random_field) {
+        if (b->use_lcg) {
+            const dim3 grid((b->seed_nx + 63) / 64, (b->seed_ny + 3) / 4, b->n);
+            k_lcg_batch<<<grid, dim3(64, 4), 0, s>>>(b->d_members, b->seed_nx, b->seed_ny, b->rand_nx);
+        } else {
+            const dim3 grid((b->n_gen + 127) / 128, 1, b->n);
+            k_xorwow_batch<<<grid, 128, 0, s>>>(b->d_members, b->rand_nx, b->rand_ny);
+        }
+        GO_CUDA(cudaGetLastError());
+    }
+    const dim3 gs((b->nx + 4 + kBW - 1) / kBW, (b->ny + 4 + kSoarBH - 1) / kSoarBH, b->n);
+    k_soar_batch<<<gs, dim3(kBW, kSoarTY), 0, s>>>(b->d_members, b->nx, b->ny, b->dx, b->dy, b->L, q0_scale,
+                                                   perturbation_scale, b->pns, b->pew, b->aligned16);
+    GO_CUDA(cudaGetLastError());
+    const int ci = b->geom.i_hi - b->geom.i_lo, cj = b->geom.j_hi - b->geom.j_lo;
+    if (ci > 0 && cj > 0) {
+        const dim3 gb((ci + kBW - 1) / kBW, (cj + kBH * kBalRows - 1) / (kBH * kBalRows), b->n);
+        k_balance_batch<<<gb, dim3(kBW, kBH), 0, s>>>(b->d_members, b->geom);
+        GO_CUDA(cudaGetLastError());
+    }
     return GO_OK;
 }
 

@@ -215,6 +215,45 @@ int go_noise_bicubic(void* stream, int nx, int ny, int ghost_x, int ghost_y, flo
                      float* hv, int hv_pitch, const float* Hi, int Hi_pitch, float land_value,
                      uint64_t angle_texture, uint64_t coriolis_texture);
 
+/* The model error of an ensemble, batched across members: every member's
+ * draws, SOAR field and balanced perturbation (coarse grid = model grid, one
+ * field, not additive) in one launch per kernel, each member bit for bit
+ * what go_noise_lcg (or go_noise_xorwow_fill), go_noise_soar and
+ * go_noise_geostrophic give it alone.  Replaces the per-member perturbSim of
+ * the reference's ensembles (OceanNoiseEnsemble.py:506-531 through
+ * CDKLM16.py:580-582).  The members share the grid, the boundary kinds, the
+ * generator kind and soar_L; each has its own buffers and parameters. */
+typedef struct go_noise_member {
+    uint64_t* seed;           /* LCG seeds, seed_ny x seed_nx (NULL with XORWOW) */
+    void* xorwow_states;      /* XORWOW states (NULL with LCG) */
+    float* random;            /* random field */
+    float* coarse;            /* coarse buffer, (ny+4) x (nx+4) */
+    float* eta;
+    float* hu;
+    float* hv;
+    const float* Hi;          /* (ny+5) x (nx+5) */
+    uint64_t angle_texture;   /* go_wind_texture_create handles */
+    uint64_t coriolis_texture;
+    int seed_pitch, random_pitch, coarse_pitch, eta_pitch, hu_pitch, hv_pitch, Hi_pitch; /* bytes */
+    int n_generators;         /* XORWOW generators */
+    float soar_q0, g, f, beta, land_value, reserved;
+} go_noise_member;
+
+typedef struct go_noise_batch go_noise_batch;
+
+/* Checks the members (host array of n) against the shared geometry and
+ * copies their descriptors to the device (synchronous). */
+int go_noise_batch_create(const go_noise_member* members, int n, int nx, int ny, float dx, float dy,
+                          int ghost_x, int ghost_y, float soar_L, int periodic_north_south,
+                          int periodic_east_west, int use_lcg, go_noise_batch** out);
+int go_noise_batch_destroy(go_noise_batch* b);
+
+/* One perturbation of every member: new normal draws (update_random_field
+ * != 0), SOAR with amplitude (float)((double)soar_q0 x q0_scale) and
+ * perturbation_scale, then the balance. */
+int go_noise_batch_perturb(go_noise_batch* b, void* stream, double q0_scale, float perturbation_scale,
+                           int update_random_field);
+
 /* result[0] = sum a^2 over an nx x ny field; with b also result[1] = sum
  * b^2 and result[2] = sum a b (reductions.cu squareSum, squareSumDouble).
  * Accumulates in double, deterministic order.  scratch: device bytes of

@@ -175,3 +175,49 @@ def test_autotune_batch(ctx, tmp_path, monkeypatch):
     assert res["graph_steps"] in (0, 4)
     b.advance(6)
     assert sims[0].num_iterations == 6
+
+
+@pytest.mark.parametrize("lcg", [True, False])
+def test_batched_model_error_equals_member_by_member(ctx, lcg):
+    """Members with the reference's small-scale model error
+    (small_scale_perturbation, OceanStateNoise): BatchedCDKLM16.step perturbs
+    all of them after every step in three launches (go_noise_batch_perturb);
+    each member ends bit for bit where its twin stepped alone with
+    CDKLM16.step ends.  Members differ in f, amplitude and draws; then one
+    more perturbation with q0_scale against perturbState."""
+    from SWESimulators import CDKLM16, SyntheticCases as SC
+    from SWESimulators.BatchedEnsemble import BatchedCDKLM16
+    M = 5
+    c = SC.grf(64, ny=48, dx=1000.0, bc=(2, 2, 2, 2), steps=1)
+
+    def member(m):
+        kw = c.kwargs()
+        kw["f"] = np.float32(c.f * (1.0 + 0.1 * m))
+        return CDKLM16.CDKLM16(ctx, dt=c.dt, small_scale_perturbation=True,
+                               small_scale_perturbation_amplitude=1e-4 * (1 + m), use_lcg=lcg,
+                               xorwow_seed=1000 + m, **kw)
+
+    sims = [member(m) for m in range(M)]
+    twins = [member(m) for m in range(M)]
+    if lcg:
+        for s, t in zip(sims, twins):
+            seeds = s.small_scale_model_error.getSeed()
+            t.small_scale_model_error.seed.upload(t.gpu_stream, seeds)
+    ens = BatchedCDKLM16(sims)
+    ens.step(7.5 * c.dt)                  # 7 steps and a half step, each perturbed
+    ens.synchronize()
+    for t in twins:
+        t.step(7.5 * c.dt)
+    for s, t in zip(sims, twins):
+        for x, y in zip(s.download(), t.download()):
+            assert np.array_equal(x, y)
+        assert s.num_iterations == t.num_iterations == 8
+    ens.perturb_members(q0_scale=0.37)
+    ens.synchronize()
+    for t in twins:
+        t.perturbState(q0_scale=0.37)
+    for s, t in zip(sims, twins):
+        for x, y in zip(s.download(), t.download()):
+            assert np.array_equal(x, y)
+    e0, e1 = sims[0].download()[0], sims[1].download()[0]
+    assert not np.array_equal(e0, e1)
