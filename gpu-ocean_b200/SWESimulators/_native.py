@@ -80,6 +80,7 @@ SIGNATURES = {
     "go_domain_set_wind_field": (_I, [_P, _P, _P, _P, _P, _I]),
     "go_domain_set_launch": (_I, [_P, _I, _I]),
     "go_domain_set_arith": (_I, [_P, _I]),
+    "go_check_quotients": (_I, [_P, _P, _P, _I, _P, _P]),
     "go_domain_set_land": (_I, [_P, _I]),
     "go_init_bathymetry": (_I, [_P, _P, _P, _I, _P, _I, _F]),
     "go_boundary_condition": (_I, [_P, _P, _P, _P, _P, _I]),

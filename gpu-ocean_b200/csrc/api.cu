@@ -40,11 +40,19 @@ int go_auto_rows(int nx, int ny, int shape) {
     const long long strips = (nx + useful - 1) / useful;
     const long long slots = 148LL * go::shape_blocks_per_sm(shape);
     static const int kRows[] = {2, 4, 8, 16, 24};
-    int best = 2;
+    // column-pair shapes: heights in whole ring chunks of 3 rows; priming a
+    // strip costs about 2 rows
+    static const int kPairRows[] = {3, 6, 12, 24, 36, 48, 72, 96};
+    const bool pair = go_pair_shape(shape);
+    const int* rows = pair ? kPairRows : kRows;
+    const int n = pair ? 8 : 5;
+    const int extra = pair ? 2 : 4;
+    int best = rows[0];
     long long best_cost = -1;
-    for (int r : kRows) {
+    for (int i = 0; i < n; ++i) {
+        const int r = rows[i];
         const long long blocks = strips * ((ny + r - 1) / r);
-        const long long cost = ((blocks + slots - 1) / slots) * (r + 4);
+        const long long cost = ((blocks + slots - 1) / slots) * (r + extra);
         if (best_cost < 0 || cost <= best_cost) { best = r; best_cost = cost; }
     }
     return best;
@@ -286,7 +294,7 @@ int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_ne
 
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block) {
     if (!d) return go_fail(GO_ERR_INVALID, "null domain");
-    if (shape < 0 || shape > 7) return go_fail(GO_ERR_INVALID, "launch shape %d (0..7)", shape);
+    if (shape < 0 || shape > GO_SHAPE_PAIR96) return go_fail(GO_ERR_INVALID, "launch shape %d (0..10)", shape);
     if (rows_per_block == 0) rows_per_block = go_auto_rows(d->k.nx, d->k.ny, shape);
     if (rows_per_block < 1) return go_fail(GO_ERR_INVALID, "rows_per_block must be >= 1");
     d->shape = shape;

@@ -69,3 +69,7 @@ go::Variant go_variant(const go_domain* d);
 
 // One single-domain stage launch (stage_launch.cu).
 int go_launch_stage(go_domain* d, cudaStream_t s, const go::StageArgs& a);
+
+// Column-pair shapes (pair_launch.cu).
+bool go_pair_shape(int shape);
+int go_pair_threads(int shape);

@@ -1,4 +1,5 @@
 // Single-domain stage launches: every kernel variant of the marching stage.
+#include "cdklm16_pair.cuh"
 #include "dispatch.cuh"
 
 using namespace go;
@@ -29,7 +30,17 @@ Variant go_variant(const go_domain* d) {
     return v;
 }
 
+int go_prepare_pair(const StageArgs& a, int shape, PairMapParams* mp, bool* tma);
+int go_launch_pair(go_domain* d, cudaStream_t s, const StageArgs& a, const PairMapParams& mp, bool tma);
+
 int go_launch_stage(go_domain* d, cudaStream_t s, const StageArgs& a) {
+    if (go_pair_shape(d->shape)) {
+        PairMapParams mp;
+        bool tma = false;
+        int rc = go_prepare_pair(a, d->shape, &mp, &tma);
+        if (!rc) rc = go_launch_pair(d, s, a, mp, tma);
+        return rc;
+    }
     SingleLaunch L{&a, s};
     const cudaError_t e = dispatch_variant(L, go_variant(d));
     if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));

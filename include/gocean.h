@@ -297,6 +297,12 @@ int go_sample_wind(void* stream, const float* field, int w, int h, int nx, int n
  * recomputed halo rows).  Chosen by the autotuner; every shape computes
  * identical results. */
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block);
+/* Column-pair shapes: blocks of 32, 64 or 96 threads, each thread two
+ * adjacent columns in packed FP32x2 arithmetic, inputs of boundary-free
+ * blocks staged by TMA tile loads (16-byte aligned arrays and pitches). */
+#define GO_SHAPE_PAIR32 8
+#define GO_SHAPE_PAIR64 9
+#define GO_SHAPE_PAIR96 10
 
 /* How quotients are evaluated.  EXACT keeps every '/' of the reference
  * kernel (div.full.f32 under its --prec-div=false).  RCP (the default)
@@ -306,6 +312,13 @@ int go_domain_set_launch(go_domain* d, int shape, int rows_per_block);
 #define GO_ARITH_EXACT 0
 #define GO_ARITH_RCP 1
 int go_domain_set_arith(go_domain* d, int mode);
+
+/* Self-check of the two quotient modes: writes a[i] / b[i] as the stage
+ * kernel evaluates it under GO_ARITH_EXACT to q_div and under GO_ARITH_RCP
+ * to q_rcp, for n device floats each (compiled with the stage kernel's
+ * flags).  No counterpart in the reference; tests use it to pin the
+ * equivalence of the two modes over the scheme's denominators. */
+int go_check_quotients(void* stream, const float* a, const float* b, int n, float* q_div, float* q_rcp);
 
 /* Whether the bathymetry may hold land (corners equal to the land value,
  * Common.py:1333-1337).  1 (the default) keeps every land test of the

@@ -171,6 +171,68 @@ def test_bump256_1000_steps_vs_reference_kernel_and_fp64(ctx):
     assert abs(s1 - s0) / float(np.sum(np.abs(c.eta0[2:-2, 2:-2]))) < 1e-5
 
 
+def _run_steps(sim, n, dt):
+    for _ in range(n):
+        sim.step(dt)
+
+
+def test_grf4096_1000_steps_vs_reference_kernel_and_fp64(ctx):
+    """The headline workload exactly as bench.py builds it: 4096^2, GRF
+    bathymetry, 8 bumps, beta plane, uniform wind, quadratic friction,
+    walls north/south, periodic east/west; 1000 RK2 steps on the library's
+    default launch (reciprocal quotients, read-ahead shape, boundary-free
+    blocks) against the reference kernel (CDKLM16_kernel.cu:429-1006 rebuilt
+    for this GPU), whole arrays with ghost cells.  The same run under '/'
+    quotients must give the same bits; the error against the FP64
+    restatement and the mass balance are stated."""
+    c = SC.grf4096()
+    steps = 1000
+    cfg = build_ref.CONFIGS["grf4096"]
+    if not ref_kernel.available(cfg):
+        pytest.skip("reference kernel library not built")
+    Hi = O.fix_bi_ghost_corners(c.Hi, c.nx, c.ny, c.bc)
+    sim = _drop_in(ctx, c)
+    _run_steps(sim, steps, c.dt)
+    mine = sim.download()
+    assert sim.num_iterations == steps
+    assert sim.status() == 0
+    ref = ref_kernel.RefKernelSim(cfg, c.eta0, c.hu0, c.hv0, Hi, c.dt, c.f, c.beta, c.bc, wind=c.wind)
+    _run_steps(ref, steps, c.dt)
+    theirs = ref.download()
+    del ref
+    e_ref = [rel_max(a, b) for a, b in zip(mine, theirs)]
+    e_int = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
+    print("grf4096 1000 steps vs reference kernel, whole arrays:", e_ref, "interior:", e_int)
+    assert max(e_ref) <= 1e-5
+    # '/' quotients: the same bits
+    sim2 = _drop_in(ctx, c)
+    sim2._domain.set_arith(_native.GO_ARITH_EXACT)
+    _run_steps(sim2, steps, c.dt)
+    exact_mode = sim2.download()
+    del sim2
+    for a, b in zip(mine, exact_mode):
+        assert np.array_equal(a, b)
+    # wall north/south + periodic east/west conserve the interior mass
+    Bm = O.init_bm(Hi)
+    s0 = float(np.sum(np.maximum(c.eta0, -Bm)[2:-2, 2:-2].astype(np.float64)))
+    s1 = float(np.sum(mine[0][2:-2, 2:-2].astype(np.float64)))
+    s1r = float(np.sum(theirs[0][2:-2, 2:-2].astype(np.float64)))
+    scale = float(np.sum(np.abs(c.eta0[2:-2, 2:-2].astype(np.float64))))
+    print("  mass drift relative to sum|eta0|: this build %.3e, reference %.3e" % ((s1 - s0) / scale,
+                                                                                 (s1r - s0) / scale))
+    assert abs(s1 - s0) / scale < 1e-4
+    # the FP64 restatement on the GPU
+    fp64 = O.OracleSim(c.eta0, c.hu0, c.hv0, c.Hi, c.nx, c.ny, c.dx, c.dy, c.dt, c.g, c.f, c.r,
+                       coriolis_beta=c.beta, bc=c.bc, wind=c.wind, device="cuda")
+    _run_steps(fp64, steps, c.dt)
+    exact = fp64.download()
+    del fp64
+    e64 = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, exact)]
+    e64_ref = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(theirs, exact)]
+    print("  vs FP64:", e64, "| reference vs FP64:", e64_ref)
+    assert max(e64) <= 1.5 * max(e64_ref) + 1e-7
+
+
 def test_small_beta_friction_wind_periodic_vs_reference_kernel(ctx):
     """Config-2 physics (beta plane, quadratic friction, wind, periodic E/W,
     walls N/S) on a 96x80 grid: 200 steps against the reference kernel."""
