@@ -37,6 +37,44 @@ class BatchedCDKLM16:
         if graph_steps:
             self.capture(graph_steps)
 
+    # -- failure isolation ------------------------------------------------
+    def member_status(self, clear=False):
+        """Each member's status word (GO_STATUS_* bits, member order); a
+        member whose state went non-finite is flagged alone."""
+        self.stream.synchronize()
+        return self.batch.status(clear)
+
+    def failed_members(self):
+        """Indices of the members whose state went non-finite."""
+        return [m for m, w in enumerate(self.member_status()) if w & _native.GO_STATUS_NONFINITE]
+
+    def drop(self, members):
+        """Removes members (indices into the current member list) from the
+        ensemble, as the reference's ensembles stop stepping dead particles
+        (BaseOceanStateEnsemble.py:108-110, EnsembleFromFiles.py:315); the
+        batch is rebuilt over the remaining members, which step on bit for
+        bit as before.  Returns the removed simulators."""
+        gone = sorted(set(int(m) for m in members))
+        if any(m < 0 or m >= self.n for m in gone):
+            raise IndexError("member index out of range")
+        self.stream.synchronize()
+        removed = [self.sims[m] for m in gone]
+        self.sims = [s for m, s in enumerate(self.sims) if m not in gone]
+        self.n = len(self.sims)
+        self.invalidate_model_error()
+        launch = getattr(self.batch, "launch", None)
+        self.batch.close()
+        self.batch = _native.Batch([s._domain for s in self.sims])
+        if launch is not None:
+            self.batch.set_launch(*launch)
+        for m, s in enumerate(self.sims):
+            self._bind(m, s)
+        steps = self.graph_steps
+        self.graph_steps = 0
+        if steps:
+            self.capture(steps)
+        return removed
+
     def _bind(self, m, s):
         # the member's wind at its current time (Simulator.update_wind_stress)
         wind_t = np.float32(s.update_wind_stress())
@@ -161,21 +199,29 @@ class BatchedCDKLM16:
         return all(flags)
 
     def _noise_batch(self):
-        """go_noise_batch over the members' OceanStateNoise objects (built
-        once; the descriptors point at the members' own buffers)."""
-        if getattr(self, "_noise", None) is not None:
-            return self._noise
-        import ctypes
+        """go_noise_batch over the members' OceanStateNoise objects.  The
+        descriptors point at the members' own buffers and hold each member's
+        f, beta, g and q0, so the set is rebuilt when a member's
+        OceanStateNoise object is replaced; after changing a member's
+        physical parameters or buffers in place, call
+        invalidate_model_error()."""
         errs = [s.small_scale_model_error for s in self.sims]
+        key = tuple(map(id, errs))
+        if getattr(self, "_noise", None) is not None:
+            if key == self._noise_key:
+                return self._noise
+            self.invalidate_model_error()
+        import ctypes
         e0, s0 = errs[0], self.sims[0]
         for e, s in zip(errs, self.sims):
             same = (int(e.nx), int(e.ny), int(e.interpolation_factor), bool(e.use_lcg), int(e.periodicNorthSouth),
                     int(e.periodicEastWest), float(e.soar_L), float(e.dx), float(e.dy)) == \
                    (int(e0.nx), int(e0.ny), 1, bool(e0.use_lcg), int(e0.periodicNorthSouth),
                     int(e0.periodicEastWest), float(e0.soar_L), float(e0.dx), float(e0.dy))
-            if not same or int(s.ghost_cells_x) != int(s0.ghost_cells_x):
-                raise ValueError("batched model error needs one grid, generator, boundary kinds, soar_L and "
-                                 "interpolation factor 1 for all members")
+            if not same or int(s.ghost_cells_x) != int(s0.ghost_cells_x) or \
+                    int(s.ghost_cells_y) != int(s0.ghost_cells_y):
+                raise ValueError("batched model error needs one grid, ghost cells, generator, boundary kinds, "
+                                 "soar_L and interpolation factor 1 for all members")
         descs = (_native.GoNoiseMember * self.n)(*[e.member_desc(s) for e, s in zip(errs, self.sims)])
         h = ctypes.c_void_p()
         _native.check(_native.load().go_noise_batch_create(
@@ -183,7 +229,17 @@ class BatchedCDKLM16:
             int(s0.ghost_cells_x), int(s0.ghost_cells_y), float(e0.soar_L), int(e0.periodicNorthSouth),
             int(e0.periodicEastWest), int(bool(e0.use_lcg)), ctypes.byref(h)))
         self._noise = h
+        self._noise_key = key
         return h
+
+    def invalidate_model_error(self):
+        """Drops the batched model-error descriptors; the next perturbation
+        rebuilds them from the members' current OceanStateNoise state."""
+        h = getattr(self, "_noise", None)
+        self._noise = None
+        if h is not None:
+            self.stream.synchronize()   # no perturbation in flight reads the descriptors
+            _native.load().go_noise_batch_destroy(h)
 
     def perturb_members(self, q0_scale=1.0, perturbation_scale=1.0, boundary_conditions=False):
         """Every member's OceanStateNoise.perturbSim (OceanStateNoise.py:
@@ -218,11 +274,12 @@ class BatchedCDKLM16:
         n = lib.go_batch_grf_scratch_floats(self.batch.handle, float(corr_cells))
         if n == 0:
             raise ValueError("invalid correlation length")
-        buf = ModelError._scratch_for(n)
         self._sync_members()
+        buf = ModelError._scratch_for(n, self.stream)
         _native.check(lib.go_batch_grf_perturb(self.batch.handle, _native.stream_handle(self.stream),
                                                int(key0) & 0xFFFFFFFF, int(event) & 0xFFFFFFFF, float(std),
                                                float(corr_cells), _native.ptr(buf), int(buf.numel())))
+        ModelError._scratch_used(self.stream)
         self._release_members()
 
     def model_error(self, event, std=0.05, corr_cells=15.0):

@@ -121,14 +121,45 @@ class ShardedEnsemble:
         self.members = local_members(self.n_members, self.world, self.rank)
         self.sims = [make_member(m) for m in self.members]
         self.device = torch.device("cuda", torch.cuda.current_device())
+        # collectives run on the device over NCCL; gloo (CPU tests, several
+        # ranks on one GPU) takes host tensors
+        gloo = dist.is_initialized() and dist.get_backend(group) == "gloo"
+        self.comm_device = torch.device("cpu") if gloo else self.device
         self.batch = BatchedEnsemble.BatchedCDKLM16(self.sims, graph_steps=graph_steps) if self.sims else None
 
     def update_dt(self, courant=0.7):
         local = float(np.min(self.batch.max_dt())) if self.batch else float("inf")
-        dt = np.float32(courant * global_min(local, self.device, self.group))
+        dt = np.float32(courant * global_min(local, self.comm_device, self.group))
         if self.batch:
             self.batch.set_dt([dt] * len(self.sims))
         return dt
+
+    def states(self):
+        """{global member: [eta, hu, hv]} of this rank's members (the
+        ghost-inclusive device arrays of Q^n)."""
+        return {m: [s.gpu_data.h0.tensor, s.gpu_data.hu0.tensor, s.gpu_data.hv0.tensor]
+                for m, s in zip(self.members, self.sims)}
+
+    def resample(self, pairs):
+        """Resampling after an analysis (MPIOceanModelEnsemble.py:244-258,
+        281-287): for each (src, dst) pair of global members, member dst
+        takes member src's state.  Over gloo the states travel through host
+        copies."""
+        import torch
+        for s in self.sims:
+            s.gpu_stream.synchronize()
+        if self.batch:
+            self.batch.stream.synchronize()
+        dev = self.states()
+        if self.comm_device.type == "cpu":
+            host = {m: [t.cpu() for t in ts] for m, ts in dev.items()}
+            exchange_members(self.n_members, pairs, host, self.group)
+            for m, ts in dev.items():
+                for t, h in zip(ts, host[m]):
+                    t.copy_(h)
+        else:
+            exchange_members(self.n_members, pairs, dev, self.group)
+        torch.cuda.synchronize()
 
     def run_events(self, first_event, n_events, interval=60.0, std=0.05, corr_cells=15.0, courant=0.7):
         """BatchedCDKLM16.run_events with the member keys of the global
@@ -152,4 +183,4 @@ class ShardedEnsemble:
             self.batch.stream.wait_stream(s.gpu_stream)
 
     def gather(self, local_values):
-        return gather_member_scalars(self.n_members, local_values, self.device, self.group)
+        return gather_member_scalars(self.n_members, local_values, self.comm_device, self.group)

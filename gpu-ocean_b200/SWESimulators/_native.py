@@ -19,6 +19,7 @@ GO_FRICTION_QUADRATIC = 0
 GO_FRICTION_LINEAR = 1
 GO_STATUS_NONFINITE = 0x1
 GO_STATUS_ADJ_SCOPE = 0x2
+GO_STATUS_TIMEOUT = 0x4
 GO_ERR_INVALID = -1
 GO_ERR_CUDA = -2
 GO_ERR_UNSUPPORTED = -3
@@ -120,6 +121,7 @@ SIGNATURES = {
     "go_bc_texture_create": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_uint64)]),
     "go_domain_set_open_bc": (_I, [_P, _P, _F]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
+    "go_batch_status": (_I, [_P, _P, _I]),
     "go_noise_lcg": (_I, [_P, _I, _I, _I, _I, _P, _I, _P, _I]),
     "go_noise_xorwow_state_bytes": (ctypes.c_size_t, []),
     "go_noise_xorwow_init": (_I, [_P, ctypes.c_uint64, _I, _P]),
@@ -316,6 +318,7 @@ class Batch:
 
     def set_launch(self, shape=0, rows_per_block=0, blocks=0):
         check(load().go_batch_set_launch(self.handle, int(shape), int(rows_per_block), int(blocks)))
+        self.launch = (int(shape), int(rows_per_block), int(blocks))
 
     def set_arith(self, mode):
         check(load().go_batch_set_arith(self.handle, int(mode)))
@@ -330,6 +333,12 @@ class Batch:
         n = ctypes.c_int()
         check(load().go_batch_tiles(self.handle, ctypes.byref(n)))
         return n.value
+
+    def status(self, clear=False):
+        """Per-member status words (GO_STATUS_* bits), member order."""
+        out = (ctypes.c_uint32 * self.n)()
+        check(load().go_batch_status(self.handle, ctypes.cast(out, ctypes.c_void_p), int(bool(clear))))
+        return [int(v) for v in out]
 
     def step(self, n_steps, stream=None):
         check(load().go_batch_step(self.handle, stream_handle(stream), int(n_steps)))

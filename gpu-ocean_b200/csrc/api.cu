@@ -5,7 +5,7 @@
 // --ftz=true --prec-div=false --prec-sqrt=false --fmad=false.
 #include <string>
 
-#include "dispatch.cuh"
+#include "pair_dispatch.cuh"
 
 using namespace go;
 
@@ -98,6 +98,8 @@ StageArgs go_stage_args(const go_domain* d, float dt, int rk_step, const float* 
     a.pw = d->wpitch;
     a.rows_per_block = d->rows_per_block;
     a.status = d->d_status;
+    a.neg_zero = -0.0f;
+    a.fric = go_friction_mode(d);
     return a;
 }
 
@@ -211,6 +213,7 @@ int go_domain_create(const go_domain_desc* desc, go_domain** out) {
         return go_fail(GO_ERR_INVALID, "unknown friction law %d", s.friction_law);
 
     go_domain* d = new go_domain();
+    d->own_side = 1;
     d->desc = s;
     Scheme& k = d->k;
     k.nx = s.nx; k.ny = s.ny;
@@ -248,6 +251,9 @@ int go_domain_create(const go_domain_desc* desc, go_domain** out) {
 
 int go_domain_destroy(go_domain* d) {
     if (!d) return GO_OK;
+    if (d->side) cudaStreamDestroy(d->side);
+    if (d->ev_fork) cudaEventDestroy(d->ev_fork);
+    if (d->ev_join) cudaEventDestroy(d->ev_join);
     cudaFree(d->d_frows);
     cudaFree(d->d_status);
     delete d;
@@ -294,7 +300,7 @@ int go_domain_set_wind_field(go_domain* d, const float* x_cur, const float* x_ne
 
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block) {
     if (!d) return go_fail(GO_ERR_INVALID, "null domain");
-    if (shape < 0 || shape > GO_SHAPE_PAIR96) return go_fail(GO_ERR_INVALID, "launch shape %d (0..10)", shape);
+    if (shape < 0 || shape > GO_SHAPE_PAIR) return go_fail(GO_ERR_INVALID, "launch shape %d (0..8)", shape);
     if (rows_per_block == 0) rows_per_block = go_auto_rows(d->k.nx, d->k.ny, shape);
     if (rows_per_block < 1) return go_fail(GO_ERR_INVALID, "rows_per_block must be >= 1");
     d->shape = shape;
@@ -400,14 +406,18 @@ int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_
     const StageArgs a1 = go_stage_args(d, dt, 1, eta1, hu1, hv1, pitch1 / 4, eta0, hu0, hv0, pitch0 / 4, Hi,
                                        Hi_pitch / 4, land_value, wind_stress_t);
     const bool open = go_has_open_bc(d);
+    PreparedStage p0, p1;
+    rc = go_prepare_stage(d, a0, &p0);
+    if (!rc) rc = go_prepare_stage(d, a1, &p1);
+    if (rc) return rc;
     for (int n = 0; n < n_steps; ++n) {
-        rc = go_launch_stage(d, s, a0);
+        rc = go_launch_prepared(d, s, p0);
         // open boundaries: the reference's ghost sequence after each stage
         // (CDKLM16.py:537-540, 585-586); the stage kernel's own periodic
         // images are redone in order after the open kinds of the other axis
         if (!rc && open) rc = go_boundary_condition(d, stream, eta1, hu1, hv1, pitch1);
         if (rc) return rc;
-        rc = go_launch_stage(d, s, a1);
+        rc = go_launch_prepared(d, s, p1);
         if (!rc && open) rc = go_boundary_condition(d, stream, eta0, hu0, hv0, pitch0);
         if (rc) return rc;
     }

@@ -9,8 +9,8 @@
 #include <algorithm>
 #include <vector>
 
-#include "dispatch.cuh"
 #include "grf.cuh"
+#include "pair_dispatch.cuh"
 
 using namespace go;
 
@@ -24,6 +24,14 @@ struct go_batch {
     float* d_dt = nullptr;
     int4* d_tiles = nullptr;
     int ntiles = 0;
+    // column-pair shape: boundary-free tiles (d_tiles, TMA maps in d_maps)
+    // and boundary-frame tiles (d_tiles_frame) launched as two kernels, the
+    // frame on a high-priority side stream
+    int4* d_tiles_frame = nullptr;
+    int ntiles_frame = 0;
+    PairMapParams* d_maps = nullptr;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int shape = 4, rows = 32, blocks = 0;
     int arith = 0;
     Variant variant;
@@ -72,6 +80,63 @@ int batch_variant(go_batch* b) {
     return GO_OK;
 }
 
+// Tiles of the column-pair kernel: per member its boundary-free rectangle
+// (when every array of the member qualifies for TMA) and its boundary frame
+// in short strips, with the member's TMA maps for both stages.
+int batch_commit_pair(go_batch* b) {
+    std::vector<int4> ti, tf;
+    std::vector<PairMapParams> maps(2 * b->n);
+    for (int m = 0; m < b->n; ++m) {
+        const Scheme& k = b->members[m]->k;
+        b->args[2 * m].rows_per_block = b->rows;
+        b->args[2 * m + 1].rows_per_block = b->rows;
+        bool t0 = false, t1 = false;
+        int rc = go_prepare_pair(b->args[2 * m], &maps[2 * m], &t0);
+        if (!rc) rc = go_prepare_pair(b->args[2 * m + 1], &maps[2 * m + 1], &t1);
+        if (rc) return rc;
+        const PairGrid g = pair_grid(k, b->rows, t0 && t1);
+        for (int by = 0; by < g.nby; ++by) {
+            const int r0 = 4 + by * g.rows;
+            const int r1 = std::min(r0 + g.rows, k.ny);
+            for (int bx = g.bx0; bx < g.bx1; ++bx) ti.push_back(make_int4(m, bx, r0, r1));
+        }
+        const int nf = pair_frame_count(g);
+        for (int i = 0; i < nf; ++i) {
+            int bx, r0, r1;
+            pair_frame_block(g, i, bx, r0, r1);
+            tf.push_back(make_int4(m, bx, r0, r1));
+        }
+    }
+    cudaFree(b->d_tiles);
+    cudaFree(b->d_tiles_frame);
+    cudaFree(b->d_maps);
+    b->d_tiles = b->d_tiles_frame = nullptr;
+    b->d_maps = nullptr;
+    if (!ti.empty()) {
+        GO_CUDA(cudaMalloc(&b->d_tiles, sizeof(int4) * ti.size()));
+        GO_CUDA(cudaMemcpy(b->d_tiles, ti.data(), sizeof(int4) * ti.size(), cudaMemcpyHostToDevice));
+    }
+    if (!tf.empty()) {
+        GO_CUDA(cudaMalloc(&b->d_tiles_frame, sizeof(int4) * tf.size()));
+        GO_CUDA(cudaMemcpy(b->d_tiles_frame, tf.data(), sizeof(int4) * tf.size(), cudaMemcpyHostToDevice));
+    }
+    GO_CUDA(cudaMalloc(&b->d_maps, sizeof(PairMapParams) * maps.size()));
+    GO_CUDA(cudaMemcpy(b->d_maps, maps.data(), sizeof(PairMapParams) * maps.size(), cudaMemcpyHostToDevice));
+    if (!b->side) {
+        int least = 0, greatest = 0;
+        GO_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        GO_CUDA(cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, greatest));
+        GO_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        GO_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+    }
+    GO_CUDA(cudaMemcpy(b->d_args, b->args.data(), sizeof(StageArgs) * b->args.size(), cudaMemcpyHostToDevice));
+    GO_CUDA(cudaMemcpy(b->d_dt, b->dt.data(), sizeof(float) * b->n, cudaMemcpyHostToDevice));
+    b->ntiles = (int)ti.size();
+    b->ntiles_frame = (int)tf.size();
+    b->dirty = false;
+    return GO_OK;
+}
+
 int batch_commit(go_batch* b) {
     if (!b->dirty) return GO_OK;
     for (int m = 0; m < b->n; ++m)
@@ -81,6 +146,7 @@ int batch_commit(go_batch* b) {
     Variant v = b->variant;
     v.shape = b->shape;
     v.rcp = b->arith == GO_ARITH_RCP;
+    if (go_pair_shape(b->shape)) return batch_commit_pair(b);
     const int width = dispatch_width(v) - 4;
     std::vector<int4> tiles;
     for (int m = 0; m < b->n; ++m) {
@@ -103,7 +169,47 @@ int batch_commit(go_batch* b) {
     return GO_OK;
 }
 
+int batch_launch_pair(go_batch* b, int rk_step, cudaStream_t s) {
+    Variant v = b->variant;
+    v.shape = b->shape;
+    v.rcp = b->arith == GO_ARITH_RCP;
+    const bool fork_join = b->ntiles > 0 && b->ntiles_frame > 0;
+    PairBatchReq r{b->d_args, b->d_dt, b->d_tiles_frame, b->ntiles_frame, b->ntiles_frame, rk_step, b->d_maps, s};
+    if (fork_join) {
+        GO_CUDA(cudaEventRecord(b->ev_fork, s));
+        GO_CUDA(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+        r.s = b->side;
+    }
+    if (b->ntiles_frame > 0) {
+        const cudaError_t e = pair_batch_launch_frame(r, v);
+        if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "batch stage launch (frame) failed: %s", cudaGetErrorString(e));
+    }
+    if (b->ntiles > 0) {
+        r.s = s;
+        r.tiles = b->d_tiles;
+        r.ntiles = b->ntiles;
+        r.grid = (b->blocks > 0 && b->blocks < b->ntiles) ? b->blocks : b->ntiles;
+        const cudaError_t e = pair_batch_launch_interior(r, v);
+        if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "batch stage launch failed: %s", cudaGetErrorString(e));
+    }
+    if (fork_join) {
+        GO_CUDA(cudaEventRecord(b->ev_join, b->side));
+        GO_CUDA(cudaStreamWaitEvent(s, b->ev_join, 0));
+    }
+    if (b->ntiles > 0) {
+        // periodic east/west ghost columns of every member (the kernel skips
+        // the others): the region's strips leave them to this copy
+        StageArgs none;
+        memset(&none, 0, sizeof(none));
+        int most = 0;
+        for (const go_domain* d : b->members) most = std::max(most, d->k.ny);
+        GO_CUDA(pair_launch_periodic_columns(b->d_args, b->n, most, rk_step, none, s));
+    }
+    return GO_OK;
+}
+
 int batch_launch(go_batch* b, int rk_step, cudaStream_t s) {
+    if (go_pair_shape(b->shape)) return batch_launch_pair(b, rk_step, s);
     int grid = b->ntiles;
     if (b->blocks > 0 && b->blocks < grid) grid = b->blocks;
     BatchLaunch L{b, rk_step, grid, s};
@@ -218,6 +324,11 @@ int go_batch_create(go_domain* const* members, int n, go_batch** out) {
 int go_batch_destroy(go_batch* b) {
     if (!b) return GO_OK;
     drop_graph(b);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    cudaFree(b->d_tiles_frame);
+    cudaFree(b->d_maps);
     cudaFree(b->d_args);
     cudaFree(b->d_dt);
     cudaFree(b->d_tiles);
@@ -250,7 +361,7 @@ int go_batch_set_member(go_batch* b, int m, float dt, float* eta0, float* hu0, f
 
 int go_batch_set_launch(go_batch* b, int shape, int rows_per_block, int blocks) {
     if (!b) return go_fail(GO_ERR_INVALID, "null batch");
-    if (shape < 0 || shape > 7) return go_fail(GO_ERR_INVALID, "launch shape %d (0..7)", shape);
+    if (shape < 0 || shape > GO_SHAPE_PAIR) return go_fail(GO_ERR_INVALID, "launch shape %d (0..8)", shape);
     if (rows_per_block == 0) rows_per_block = 32;
     if (rows_per_block < 1 || blocks < 0) return go_fail(GO_ERR_INVALID, "rows_per_block >= 1, blocks >= 0");
     b->shape = shape;
@@ -287,7 +398,7 @@ int go_batch_tiles(go_batch* b, int* ntiles) {
     if (!b || !ntiles) return go_fail(GO_ERR_INVALID, "null argument");
     int rc = batch_commit(b);
     if (rc) return rc;
-    *ntiles = b->ntiles;
+    *ntiles = b->ntiles + b->ntiles_frame;
     return GO_OK;
 }
 
@@ -353,6 +464,15 @@ int go_batch_max_dt(go_batch* b, void* stream, float* dt_dev) {
     const int per_member = (int)std::max(1LL, std::min((most + 255) / 256, (148LL * 4 + b->n - 1) / b->n));
     k_batch_max_dt<<<dim3(per_member, b->n), 256, 0, s>>>(b->d_args, out);
     GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+int go_batch_status(go_batch* b, uint32_t* status_host, int clear) {
+    if (!b || !status_host) return go_fail(GO_ERR_INVALID, "null argument");
+    for (int m = 0; m < b->n; ++m) {
+        int rc = go_domain_status(b->members[m], &status_host[m], clear);
+        if (rc) return rc;
+    }
     return GO_OK;
 }
 

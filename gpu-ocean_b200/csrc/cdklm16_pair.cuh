@@ -35,31 +35,24 @@
 #include <cuda.h>
 
 #include "cdklm16_stage.cuh"
+#include "gocean.h"
 
 namespace go {
 
 // ---- packed FP32x2 arithmetic ---------------------------------------------
-__device__ __forceinline__ float2 padd(float2 a, float2 b) {
-    float2 d;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "add.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return d;
-}
-__device__ __forceinline__ float2 psub(float2 a, float2 b) {
-    float2 d;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "sub.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return d;
-}
-__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
-    float2 d;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "mul.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return d;
-}
+// Sums issue as FADD2 (add.rn.ftz.f32x2 under --ftz=true), differences as
+// FFMA2(b, -1, a) = round(a - b), products as FFMA2(a, b, nz) with nz = -0
+// taken from the kernel arguments: round(a b + (-0)) = round(a b) for every
+// a, b (a zero product keeps its sign), so each lane rounds exactly as the
+// scalar add/sub/mul.rn.ftz of the reference's build.  A packed multiply
+// is not used because ptxas contracts mul.f32x2 followed by add.f32x2 into
+// one FFMA2 (measured on a B200: 7% of a*b+c and half of 16-step x*b+c
+// chains differ from the separately rounded scalar operations, with
+// --fmad=false and explicit .rn), while an FMA whose addend it cannot see
+// leaves nothing to contract.
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ float2 pmul_nz(float2 a, float2 b, float2 nz) { return __ffma2_rn(a, b, nz); }
 __device__ __forceinline__ float2 pb(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float2 psel(bool cx, bool cy, float2 a, float2 b) {
     return make_float2(cx ? a.x : b.x, cy ? a.y : b.y);
@@ -89,13 +82,14 @@ __device__ __forceinline__ float2 pminmod(float2 b, float2 c, float2 f) {
 }
 
 // minmodSlope (common.cu:532-542) per lane.
-__device__ __forceinline__ float2 pslope(float2 l, float2 c, float2 r, float2 theta) {
+__device__ __forceinline__ float2 pslope(float2 l, float2 c, float2 r, float2 theta, float2 nz) {
+    auto pmul = [&](float2 x, float2 y) { return pmul_nz(x, y, nz); };
     return pminmod(pmul(psub(c, l), theta), pmul(psub(r, l), pb(0.5f)), pmul(psub(r, c), theta));
 }
 
 template <bool RCP>
-__device__ __forceinline__ float2 prcp_or_div(float2 a, float2 b) {
-    if (RCP) return pmul(a, make_float2(rcp_approx(b.x), rcp_approx(b.y)));
+__device__ __forceinline__ float2 prcp_or_div(float2 a, float2 b, float2 nz) {
+    if (RCP) return pmul_nz(a, make_float2(rcp_approx(b.x), rcp_approx(b.y)), nz);
     return make_float2(a.x / b.x, a.y / b.y);
 }
 
@@ -103,9 +97,10 @@ __device__ __forceinline__ float2 prcp_or_div(float2 a, float2 b) {
 template <bool RCP>
 struct PDiv {
     float c, inv;
-    __device__ __forceinline__ explicit PDiv(float c_) : c(c_), inv(RCP ? rcp_approx(c_) : 0.0f) {}
+    float2 nz;
+    __device__ __forceinline__ PDiv(float c_, float2 nz_) : c(c_), inv(RCP ? rcp_approx(c_) : 0.0f), nz(nz_) {}
     __device__ __forceinline__ float2 operator()(float2 a) const {
-        if (RCP) return pmul(a, pb(inv));
+        if (RCP) return pmul_nz(a, pb(inv), nz);
         return make_float2(a.x / c, a.y / c);
     }
 };
@@ -115,7 +110,8 @@ struct PDiv {
 // momentum, tangential momentum) fluxes.
 template <bool RCP>
 __device__ __forceinline__ void pflux(float2 hm, float2 um, float2 vm, float2 hp, float2 up, float2 vp,
-                                      const Scheme& k, float2& F0, float2& F1, float2& F2) {
+                                      const Scheme& k, float2 nz, float2& F0, float2& F1, float2& F2) {
+    auto pmul = [&](float2 x, float2 y) { return pmul_nz(x, y, nz); };
     const bool wpx = hp.x > k.cutoff, wpy = hp.y > k.cutoff;
     const bool wmx = hm.x > k.cutoff, wmy = hm.y > k.cutoff;
     const float2 z = pb(0.0f);
@@ -160,6 +156,12 @@ __device__ __forceinline__ void pflux(float2 hm, float2 um, float2 vm, float2 hp
         F0 = psel(zx, zy, z, F0); F1 = psel(zx, zy, z, F1); F2 = psel(zx, zy, z, F2);
     }
 }
+
+// Face states of two faces (one float2 lane each): minus side (hm, um, vm),
+// plus side (hp, up, vp); un normal, ut tangential.
+struct PFace {
+    float2 hm, um, vm, hp, up, vp;
+};
 
 // Cell state of one lane from conserved variables (CDKLM16_kernel.cu:551-593).
 template <bool RCP, bool LAND>
@@ -273,11 +275,10 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-// Waits are bounded: about a second of polling, after which the block
-// reports GO_STATUS_TIMEOUT-style failure through the status word and
-// abandons its strip.
+// Waits are bounded: about a second of polling, after which the block sets
+// GO_STATUS_TIMEOUT in the status word and abandons its strip.
 constexpr int kWaitPolls = 1 << 20;
-constexpr unsigned kStatusTimeout = 0x4u;
+constexpr unsigned kStatusTimeout = GO_STATUS_TIMEOUT;
 
 template <int T>
 __device__ __forceinline__ void pair_sync() {
@@ -291,30 +292,42 @@ struct PairSmem {
     uint64_t bar[4];
 };
 
-// True when the strip [r0, r1) of the columns cl0 .. cl0+2T-1 touches no
-// ghost cell, wall flip or periodic image, and its corners need no clamp.
+// True when the column block from cl0 (2T columns) needs no wall logic: it
+// reaches no ghost column of a wall side (periodic and open sides are read
+// as they are; the periodic images of its cells are written after the
+// stage).  Rows [4, ny) need none either.  Such strips run the TMA path.
 template <int T>
-__device__ __forceinline__ bool pair_interior(const Scheme& k, int cl0, int r0, int r1) {
-    return cl0 >= 4 && cl0 + 2 * T - 1 <= k.nx - 1 && r0 >= 4 && r1 <= k.ny;
+__host__ __device__ __forceinline__ bool pair_fast_cols(const Scheme& k, int cl0) {
+    return (k.bcW != kWall || cl0 >= 4) && (k.bcE != kWall || cl0 + 2 * T - 1 <= k.nx - 1);
+}
+__host__ __device__ __forceinline__ bool pair_fast_rows(const Scheme& k, int r0, int r1) {
+    return r0 >= 4 && r1 <= k.ny;
 }
 
 // One block strip of the column-pair stage.
 //   ring: dynamic shared memory for NS chunks (TMA launches), else null
 //   chunk_base: running chunk counter of this block (mbarrier phases)
-template <int T, int NS, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, bool EDGE, bool TMA>
+// FRIC: kFric* or -1 for the law in StageArgs::fric; WIND: 0 uniform wind,
+// 1 per-cell wind field, -1 whichever StageArgs holds.  The boundary-free
+// kernels fix both at compile time: deciding them at run time costs that
+// kernel 10% (measured at 4096^2: 586 against 524 us per step).
+template <int T, int NS, int UNR, int FRIC, int WIND, bool GEN_NORTH, bool RCP, bool LAND, bool EDGE, bool TMA>
 __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& maps, const float dt, const int bx,
-                                           const int by, PairSmem<T>& sm, float* ring, unsigned& chunk_base) {
+                                           const int r0, const int r1, PairSmem<T>& sm, float* ring,
+                                           unsigned& chunk_base) {
     const Scheme& k = a.k;
     const int t = threadIdx.x;
     const int cl0 = bx * (2 * T - 4);
     const int cl = cl0 + 2 * t;            // lane x column; lane y is cl + 1
-    const int r0 = 2 + by * a.rows_per_block;
-    const int r1 = min(r0 + a.rows_per_block, k.ny + 2);
     const bool stage1 = (a.rk_step == 1);
+    const int fric = FRIC >= 0 ? FRIC : a.fric;                         // friction law
+    const bool wind_field = WIND >= 0 ? (WIND == 1) : (a.wx_cur != nullptr);
 
-    const PDiv<RCP> by2g(k.two_g);
-    const PDiv<RCP> bydx(k.dx);
-    const PDiv<RCP> bydy(k.dy);
+    const float2 NZ = pb(a.neg_zero);      // -0, opaque to the compiler
+    auto pmul = [&](float2 x, float2 y) { return pmul_nz(x, y, NZ); };
+    const PDiv<RCP> by2g(k.two_g, NZ);
+    const PDiv<RCP> bydx(k.dx, NZ);
+    const PDiv<RCP> bydy(k.dy, NZ);
     const float2 theta2 = pb(k.theta);
     const float2 thg2 = pb(k.theta_g);
     const float2 hg2 = pb(k.half_g);
@@ -324,6 +337,13 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     int qcx = cl, qcy = cl + 1;
     float husx = 1.0f, husy = 1.0f;
     int hc0 = cl, hc1 = cl + 1, hc2 = cl + 2;
+    // TMA path: the last column block at a periodic or open east side can
+    // reach past the array; its prime loads pairs from a clamped column
+    // (lanes past column nx+3 are never written nor read by a written
+    // cell).  A pair starting at column nx+3 (odd nx) ends in the row's
+    // padding: TMA launches have pitches of whole 16-byte units, so the
+    // padding exists.  (The ring's tile loads fill such columns with zeros.)
+    const int clq = !EDGE ? min(cl, k.nx + 2 + (k.nx & 1)) : cl;   // even, pair within the row's pitch
     if (EDGE) {
         auto mirror_col = [&](int c, int& qc, float& s) {
             qc = min(c, k.nx + 3);
@@ -344,9 +364,10 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     const bool flipFp_x = EDGE && k.bcE == kWall && cl == k.nx + 2, flipFp_y = EDGE && k.bcE == kWall && cl + 1 == k.nx + 2;
     auto flipLy = [&](int r) { return EDGE && ((k.bcS == kWall && r < 2) || (k.bcN == kWall && r > k.ny + 1)); };
     auto flipAdjY = [&](int r) { return EDGE && ((k.bcS == kWall && r < 2) || (k.bcN == kWall && r > k.ny + 2)); };
-    const bool wr_x = (t >= 1) && (t < T - 1) && (!EDGE || cl <= k.nx + 1);          // lane writes its cell
-    const bool wr_y = (t >= 1) && (t < T - 1) && (!EDGE || cl + 1 <= k.nx + 1);
+    const bool wr_x = (t >= 1) && (t < T - 1) && cl <= k.nx + 1;          // lane writes its cell
+    const bool wr_y = (t >= 1) && (t < T - 1) && cl + 1 <= k.nx + 1;
     const bool writer = wr_x || wr_y;
+
 
     const float* __restrict__ frow = a.f_rows;
 
@@ -365,9 +386,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         const int rr = mirror_row(r, hv_sgn);
         const size_t o = (size_t)rr * a.pin;
         if (!EDGE && TMA) {   // 8-byte aligned pairs
-            e = __ldg(reinterpret_cast<const float2*>(a.eta_in + o + cl));
-            hu = __ldg(reinterpret_cast<const float2*>(a.hu_in + o + cl));
-            hv = __ldg(reinterpret_cast<const float2*>(a.hv_in + o + cl));
+            e = __ldg(reinterpret_cast<const float2*>(a.eta_in + o + clq));
+            hu = __ldg(reinterpret_cast<const float2*>(a.hu_in + o + clq));
+            hv = __ldg(reinterpret_cast<const float2*>(a.hv_in + o + clq));
         } else {
             e = make_float2(__ldg(a.eta_in + o + qcx), __ldg(a.eta_in + o + qcy));
             hu = make_float2(__ldg(a.hu_in + o + qcx), __ldg(a.hu_in + o + qcy));
@@ -386,9 +407,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     auto load_h = [&](int r, float2& Ha, float2& Hb) {
         const float* row = a.Hi + (size_t)r * a.phi;
         float h2;
-        if (!EDGE && TMA) {
-            Ha = __ldg(reinterpret_cast<const float2*>(row + cl));
-            h2 = __ldg(row + cl + 2);
+        if (!EDGE && TMA) {   // corners 0 .. nx+4 of the row
+            Ha = __ldg(reinterpret_cast<const float2*>(row + clq));
+            h2 = __ldg(row + min(clq + 2, k.nx + 4));
         } else {
             Ha = make_float2(__ldg(row + hc0), __ldg(row + hc1));
             h2 = __ldg(row + hc2);
@@ -435,8 +456,8 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     // the corner rows r (south) and r+1 (north)
     auto y_slope = [&](const PRow& lo, const PRow& c, const PRow& up, const PRow& cn, int r, float2& du,
                        float2& dv, float2& L) {
-        du = pslope(lo.u, c.u, up.u, theta2);
-        dv = pslope(lo.v, c.v, up.v, theta2);
+        du = pslope(lo.u, c.u, up.u, theta2, NZ);
+        dv = pslope(lo.v, c.v, up.v, theta2, NZ);
         const float2 U2 = pb(k.U);
         const float2 backward = pmul(thg2, padd(psub(c.e, lo.e), pmul(U2, padd(c.fu, lo.fu))));
         const float2 central =
@@ -477,7 +498,7 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         const float2 hm0 = make_float2(fmaxf(0.0f, hm.x), fmaxf(0.0f, hm.y));
         float2 F0, F1, F2;
         pflux<RCP>(hm0, padd(lo.v, pmul(half, vy_lo)), padd(lo.u, pmul(half, uy_lo)), hp0,
-                   psub(hi.v, pmul(half, vy_hi)), psub(hi.u, pmul(half, uy_hi)), k, F0, F1, F2);
+                   psub(hi.v, pmul(half, vy_hi)), psub(hi.u, pmul(half, uy_hi)), k, NZ, F0, F1, F2);
         {   // a land (dry-flag) cell on either side: zero flux (:271-273)
             const bool dx_ = hi.e.x == kDryFlag || lo.e.x == kDryFlag;
             const bool dy_ = hi.e.y == kDryFlag || lo.e.y == kDryFlag;
@@ -487,6 +508,49 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
             }
         }
         G0 = F0; G1 = F2; G2 = F1;   // normal is v: (mass, hu tangential, hv normal)
+    };
+
+    // face states of the G flux on the face between rows r (lo) and r+1
+    // (hi), corner row r+1 (face_row): lane = column, un = v, ut = u
+    auto y_face_in = [&](const PRow& lo, const PRow& hi, const PRow& face_row, int r, float2 uy_lo, float2 vy_lo,
+                         float2 Ly_lo, float2 uy_hi, float2 vy_hi, float2 Ly_hi) {
+        float2 um = lo.u, up = hi.u;
+        if (EDGE && k.bcS == kWall && r + 1 == 2) um = make_float2(-um.x, -um.y);
+        if (EDGE && k.bcN == kWall && r + 1 == k.ny + 2) up = make_float2(-up.x, -up.y);
+        if (GEN_NORTH) {
+            um = padd(pmul(um, pb(eX)), pmul(lo.v, pb(eY)));
+            up = padd(pmul(up, pb(eX)), pmul(hi.v, pb(eY)));
+        }
+        const float2 half = pb(0.5f);
+        const float2 hp = psub(padd(hi.e, face_row.Hy), by2g(psub(Ly_hi, pmul(pb(k.dy * hi.f), up))));
+        const float2 hm = padd(padd(lo.e, face_row.Hy), by2g(psub(Ly_lo, pmul(pb(k.dy * lo.f), um))));
+        PFace F;
+        F.hm = make_float2(fmaxf(0.0f, hm.x), fmaxf(0.0f, hm.y));
+        F.hp = make_float2(fmaxf(0.0f, hp.x), fmaxf(0.0f, hp.y));
+        F.um = padd(lo.v, pmul(half, vy_lo));
+        F.vm = padd(lo.u, pmul(half, uy_lo));
+        F.up = psub(hi.v, pmul(half, vy_hi));
+        F.vp = psub(hi.u, pmul(half, uy_hi));
+        return F;
+    };
+    // raw y slopes (u_y, v_y, L_y before adjustSlopes_y) of row r = c and the
+    // terms of its adjustment: dyfu = dy f u', the face depths hs, hn
+    auto y_slope_raw = [&](const PRow& lo, const PRow& c, const PRow& up, const PRow& cn, int r, float2& du,
+                           float2& dv, float2& L, float2& dyfu, float2& hs, float2& hn) {
+        du = pslope(lo.u, c.u, up.u, theta2, NZ);
+        dv = pslope(lo.v, c.v, up.v, theta2, NZ);
+        const float2 U2 = pb(k.U);
+        const float2 backward = pmul(thg2, padd(psub(c.e, lo.e), pmul(U2, padd(c.fu, lo.fu))));
+        const float2 central =
+            pmul(hg2, padd(psub(up.e, lo.e), pmul(U2, padd(padd(up.fu, pmul(pb(2.0f), c.fu)), lo.fu))));
+        const float2 forward = pmul(thg2, padd(psub(up.e, c.e), pmul(U2, padd(c.fu, up.fu))));
+        L = pminmod(backward, central, forward);
+        float2 uu = c.u;
+        if (EDGE && flipAdjY(r)) uu = make_float2(-uu.x, -uu.y);
+        dyfu = pmul(pb(k.dy * c.f), uu);
+        const float2 q = by2g(psub(L, dyfu));
+        hs = psub(padd(c.e, c.Hy), q);
+        hn = padd(padd(c.e, cn.Hy), q);
     };
 
     // ---- prime: rows r0-2 .. r0+1 and the G flux on the face (r0-1 | r0) ----
@@ -574,7 +638,7 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
 
     // per-launch constants of the update
     float Xw = 0.0f, Yw = 0.0f;
-    if (!WIND_FIELD) {
+    if (!wind_field) {
         Xw = a.wind_t * a.wxn + (1.0f - a.wind_t) * a.wxc;
         Yw = a.wind_t * a.wyn + (1.0f - a.wind_t) * a.wyc;
     }
@@ -651,8 +715,8 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         const float2 Rv = make_float2(R23.x, R23.y), Rfv = make_float2(R23.z, R23.w);
 
         // ---- x slopes of row j and y slopes of row j+1 -------------------------
-        const float2 du = pslope(Lu, R0.u, Ru, theta2);
-        const float2 dv = pslope(Lv, R0.v, Rv, theta2);
+        const float2 du = pslope(Lu, R0.u, Ru, theta2, NZ);
+        const float2 dv = pslope(Lv, R0.v, Rv, theta2, NZ);
         float2 K;
         {
             const float2 V2 = pb(k.V);
@@ -665,25 +729,33 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         const float2 Hw = pmul(pb(0.5f), padd(R0.Ha, R1.Ha));   // x-face depth west of the cells
         const float2 He = pmul(pb(0.5f), padd(R0.Hb, R1.Hb));   // east
         const float dxf = k.dx * R0.f;
-        {   // adjustSlopes_x (:148-191): K + dx f v, fallbacks 2g(..) - dx f v
-            float2 vv = R0.v;
-            if (EDGE) vv = make_float2(flipAdjX_x ? -vv.x : vv.x, flipAdjX_y ? -vv.y : vv.y);
-            const float2 nw = pmul(pb(dxf), vv);
-            const float2 q = by2g(padd(K, nw));
-            const float2 hw = psub(padd(R0.e, Hw), q);
-            const float2 he = padd(padd(R0.e, He), q);
-            if (!(hw.x > 0.0f && hw.y > 0.0f && he.x > 0.0f && he.y > 0.0f)) {
-                auto fix = [&](float Kv, float nw1, float ce, float Hlo, float Hhi, float hlo, float hhi) {
-                    Kv = (hlo > 0.0f) ? Kv : -nw1 + k.two_g * (ce + Hlo);
-                    Kv = (hhi > 0.0f) ? Kv : -nw1 - k.two_g * (ce + Hhi);
-                    return Kv;
-                };
-                K = make_float2(fix(K.x, nw.x, R0.e.x, Hw.x, He.x, hw.x, he.x),
-                                fix(K.y, nw.y, R0.e.y, Hw.y, He.y, hw.y, he.y));
-            }
+        // adjustSlopes_x (:148-191): K + dx f v, fallbacks 2g(..) - dx f v;
+        // adjustSlopes_y (:198-241) of row j+1: L - dy f u, fallbacks dy f u +- 2g(..)
+        float2 vv = R0.v;
+        if (EDGE) vv = make_float2(flipAdjX_x ? -vv.x : vv.x, flipAdjX_y ? -vv.y : vv.y);
+        const float2 nw = pmul(pb(dxf), vv);
+        const float2 qx = by2g(padd(K, nw));
+        const float2 hw = psub(padd(R0.e, Hw), qx);
+        const float2 he = padd(padd(R0.e, He), qx);
+        float2 uy1, vy1, Ly1, dyfu1, hs1, hn1;
+        y_slope_raw(R0, R1, R2, R2, j + 1, uy1, vy1, Ly1, dyfu1, hs1, hn1);
+        if (!(hw.x > 0.0f && hw.y > 0.0f && he.x > 0.0f && he.y > 0.0f && hs1.x > 0.0f && hs1.y > 0.0f &&
+              hn1.x > 0.0f && hn1.y > 0.0f)) {
+            auto fixx = [&](float Kv, float nw1, float ce, float Hlo, float Hhi, float hlo, float hhi) {
+                Kv = (hlo > 0.0f) ? Kv : -nw1 + k.two_g * (ce + Hlo);
+                Kv = (hhi > 0.0f) ? Kv : -nw1 - k.two_g * (ce + Hhi);
+                return Kv;
+            };
+            K = make_float2(fixx(K.x, nw.x, R0.e.x, Hw.x, He.x, hw.x, he.x),
+                            fixx(K.y, nw.y, R0.e.y, Hw.y, He.y, hw.y, he.y));
+            auto fixy = [&](float Lv, float dyfu, float ce, float Hs, float Hn, float hs, float hn) {
+                Lv = (hs > 0.0f) ? Lv : dyfu + k.two_g * (ce + Hs);
+                Lv = (hn > 0.0f) ? Lv : dyfu - k.two_g * (ce + Hn);
+                return Lv;
+            };
+            Ly1 = make_float2(fixy(Ly1.x, dyfu1.x, R1.e.x, R1.Hy.x, R2.Hy.x, hs1.x, hn1.x),
+                              fixy(Ly1.y, dyfu1.y, R1.e.y, R1.Hy.y, R2.Hy.y, hs1.y, hn1.y));
         }
-        float2 uy1, vy1, Ly1;
-        y_slope(R0, R1, R2, R2, j + 1, uy1, vy1, Ly1);
 
         // ---- publish the x slopes of row j ------------------------------------
         {
@@ -699,7 +771,8 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         const float2 Ldu = make_float2(SL.x, SL.y), Ldv = make_float2(SL.z, SL.w);
 
         // ---- F on the faces west of the two columns (minus: (c-1, c), plus: (c, c+1))
-        float2 F0, F1, F2;
+        //      and G on the face (j | j+1), evaluated side by side
+        float2 F0, F1, F2, G0, G1, G2;
         {
             const float2 half = pb(0.5f);
             float2 vmx = Lv, vpx = R0.v;
@@ -713,22 +786,30 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
             }
             const float2 hp = psub(padd(R0.e, Hw), by2g(padd(K, pmul(pb(dxf), vpx))));
             const float2 hm = padd(padd(Le, Hw), by2g(padd(SK, pmul(pb(dxf), vmx))));
-            const float2 hp0 = make_float2(fmaxf(0.0f, hp.x), fmaxf(0.0f, hp.y));
-            const float2 hm0 = make_float2(fmaxf(0.0f, hm.x), fmaxf(0.0f, hm.y));
-            pflux<RCP>(hm0, padd(Lu, pmul(half, Ldu)), padd(Lv, pmul(half, Ldv)), hp0, psub(R0.u, pmul(half, du)),
-                       psub(R0.v, pmul(half, dv)), k, F0, F1, F2);
-            {   // a land (dry-flag) cell on either side: zero flux (:271-273)
-                const bool dx_ = R0.e.x == kDryFlag || Le.x == kDryFlag;
-                const bool dy_ = R0.e.y == kDryFlag || Le.y == kDryFlag;
-                if (dx_ || dy_) {
-                    const float2 z = pb(0.0f);
-                    F0 = psel(dx_, dy_, z, F0); F1 = psel(dx_, dy_, z, F1); F2 = psel(dx_, dy_, z, F2);
-                }
+            PFace FX;
+            FX.hp = make_float2(fmaxf(0.0f, hp.x), fmaxf(0.0f, hp.y));
+            FX.hm = make_float2(fmaxf(0.0f, hm.x), fmaxf(0.0f, hm.y));
+            FX.um = padd(Lu, pmul(half, Ldu));
+            FX.vm = padd(Lv, pmul(half, Ldv));
+            FX.up = psub(R0.u, pmul(half, du));
+            FX.vp = psub(R0.v, pmul(half, dv));
+            const PFace FY = y_face_in(R0, R1, R1, j, Y.uy, Y.vy, Y.Ly, uy1, vy1, Ly1);
+            float2 Gn, Gt;
+            // one face pair after the other: evaluated side by side the two
+            // keep more values live than 128 registers hold (ptxas spills;
+            // measured 672 against 635 us per 4096^2 step)
+            pflux<RCP>(FX.hm, FX.um, FX.vm, FX.hp, FX.up, FX.vp, k, NZ, F0, F1, F2);
+            pflux<RCP>(FY.hm, FY.um, FY.vm, FY.hp, FY.up, FY.vp, k, NZ, G0, Gn, Gt);
+            G1 = Gt; G2 = Gn;   // G (mass, hu, hv): the normal momentum of a y face is hv
+            // a land (dry-flag) cell on either side: zero flux (:271-273)
+            const bool ax = R0.e.x == kDryFlag || Le.x == kDryFlag, ay = R0.e.y == kDryFlag || Le.y == kDryFlag;
+            const bool bx_ = R1.e.x == kDryFlag || R0.e.x == kDryFlag, by_ = R1.e.y == kDryFlag || R0.e.y == kDryFlag;
+            if (ax || ay || bx_ || by_) {
+                const float2 z = pb(0.0f);
+                F0 = psel(ax, ay, z, F0); F1 = psel(ax, ay, z, F1); F2 = psel(ax, ay, z, F2);
+                G0 = psel(bx_, by_, z, G0); G1 = psel(bx_, by_, z, G1); G2 = psel(bx_, by_, z, G2);
             }
         }
-        // ---- G on the face (j | j+1) ----------------------------------------------
-        float2 G0, G1, G2;
-        y_face(R0, R1, R1, j, Y.uy, Y.vy, Y.Ly, uy1, vy1, Ly1, G0, G1, G2);
 
         // ---- publish F, read the fluxes on the east faces --------------------------
         {
@@ -753,20 +834,15 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
             const float2 ttx = by2g(padd(K, pmul(pb(dxf), R0.v)));
             const float2 tty = by2g(psub(Y.Ly, pmul(pb(k.dy * R0.f), R0.u)));
             const float2 h = padd(R0.e, Hm);
-            float2 hu = pb(0.0f), hv = pb(0.0f);
-            if (h.x > k.cutoff && h.y > k.cutoff) {
-                hu = pmul(R0.u, h);
-                hv = pmul(R0.v, h);
-            } else {
-                if (h.x > k.cutoff) { hu.x = R0.u.x * h.x; hv.x = R0.v.x * h.x; }
-                if (h.y > k.cutoff) { hu.y = R0.u.y * h.y; hv.y = R0.v.y * h.y; }
-            }
-            float2 stx = pb(0.0f), sty = pb(0.0f);
+            // (u h, v h) where the cell is deeper than the cut-off, else zero
+            const float2 hu = psel(h.x > k.cutoff, h.y > k.cutoff, pmul(R0.u, h), pb(0.0f));
+            const float2 hv = psel(h.x > k.cutoff, h.y > k.cutoff, pmul(R0.v, h), pb(0.0f));
+            float2 stx, sty;
             const bool srcx = h.x >= k.cutoff && R0.e.x != kDryFlag;
             const bool srcy = h.y >= k.cutoff && R0.e.y != kDryFlag;
-            if (srcx || srcy) {
+            {
                 float2 Xv = pb(Xw), Yv = pb(Yw);
-                if (WIND_FIELD) {
+                if (wind_field) {
                     const size_t o = (size_t)(j - 2) * a.pw + (cl - 2);
                     auto wl = [&](const float* cur, const float* nxt, size_t oo) {
                         const float xn = __ldg(nxt + oo);
@@ -805,9 +881,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
             const float2 L3 = psub(sty, fd2);
 
             float2 C = pb(0.0f);
-            if (FRIC == kFricLinear) {
-                C = prcp_or_div<RCP>(pb(tr_dt), h);
-            } else if (FRIC == kFricQuad) {
+            if (fric == kFricLinear) {
+                C = prcp_or_div<RCP>(pb(tr_dt), h, NZ);
+            } else if (fric == kFricQuad) {
                 auto slow = [&](float h1, float hu1, float hv1) {
                     const float u = desingularize(h1, hu1, k.desing_eps);
                     const float v = desingularize(h1, hv1, k.desing_eps);
@@ -874,9 +950,13 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
 
             const size_t o = (size_t)j * a.pout + cl;
             if (!EDGE && TMA) {
-                *reinterpret_cast<float2*>(a.eta_out + o) = ne;
-                *reinterpret_cast<float2*>(a.hu_out + o) = nhu;
-                *reinterpret_cast<float2*>(a.hv_out + o) = nhv;
+                if (wr_y) {
+                    *reinterpret_cast<float2*>(a.eta_out + o) = ne;
+                    *reinterpret_cast<float2*>(a.hu_out + o) = nhu;
+                    *reinterpret_cast<float2*>(a.hv_out + o) = nhv;
+                } else {   // the last written column of the grid is this pair's first
+                    a.eta_out[o] = ne.x; a.hu_out[o] = nhu.x; a.hv_out[o] = nhv.x;
+                }
             } else {
                 auto put = [&](int col, float e1, float u1, float v1) {
                     const size_t oo = (size_t)j * a.pout + col;
@@ -921,15 +1001,46 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     // corner row of the row the slot holds next (j+3)
     int j = r0;
     int c = 0;
-    for (; j + 2 < r1; j += 3, ++c) {
-        if (!body(j, A, B, C, 0, c)) return;
-        if (!body(j + 1, B, C, A, 1, c)) return;
-        if (!body(j + 2, C, A, B, 2, c)) return;
-    }
-    if (j < r1) {
-        if (!body(j, A, B, C, 0, c)) return;
-        if (j + 1 < r1) {
+    if (UNR == 3) {
+        for (; j + 2 < r1; j += 3, ++c) {
+            if (!body(j, A, B, C, 0, c)) return;
             if (!body(j + 1, B, C, A, 1, c)) return;
+            if (!body(j + 2, C, A, B, 2, c)) return;
+        }
+        if (j < r1) {
+            if (!body(j, A, B, C, 0, c)) return;
+            if (j + 1 < r1) {
+                if (!body(j + 1, B, C, A, 1, c)) return;
+            }
+        }
+    } else if (UNR == 2) {
+        // two rows per iteration, the window rotated once per iteration
+        int ri = 0;
+#pragma unroll 1
+        for (; j + 1 < r1; j += 2) {
+            if (!body(j, A, B, C, ri, c)) return;
+            if (++ri == kPairRingRows) { ri = 0; ++c; }
+            if (!body(j + 1, B, C, A, ri, c)) return;
+            if (++ri == kPairRingRows) { ri = 0; ++c; }
+            const PRow t0 = A;
+            A = C;
+            C = B;
+            B = t0;
+        }
+        if (j < r1) {
+            if (!body(j, A, B, C, ri, c)) return;
+        }
+    } else {
+        // one row per iteration: a third of the code, the window moved in registers
+        int ri = 0;
+#pragma unroll 1
+        for (; j < r1; ++j) {
+            if (!body(j, A, B, C, ri, c)) return;
+            const PRow t0 = A;
+            A = B;
+            B = C;
+            C = t0;
+            if (++ri == kPairRingRows) { ri = 0; ++c; }
         }
     }
     if (use_ring) chunk_base += (unsigned)nchunks;
@@ -938,22 +1049,6 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
 }  // namespace go
 
 namespace go {
-
-// One block strip: the boundary-free specialisation when the strip touches
-// no ghost cell, wall or periodic image.
-template <int T, int NS, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, bool TMA>
-__device__ __forceinline__ void pair_block(const StageArgs& a, const PairMaps& maps, const float dt, const int bx,
-                                           const int by, PairSmem<T>& sm, float* ring, unsigned& chunk_base) {
-    const int cl0 = bx * (2 * T - 4);
-    const int r0 = 2 + by * a.rows_per_block;
-    const int r1 = min(r0 + a.rows_per_block, a.k.ny + 2);
-    if (pair_interior<T>(a.k, cl0, r0, r1))
-        pair_strip<T, NS, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, false, TMA>(a, maps, dt, bx, by, sm, ring,
-                                                                             chunk_base);
-    else
-        pair_strip<T, NS, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, true, TMA>(a, maps, dt, bx, by, sm, ring,
-                                                                            chunk_base);
-}
 
 // Zeroes the exchange rows (the halves of slots 0 and T that belong to no
 // column stay zero) and initialises the ring's mbarriers.
@@ -974,15 +1069,117 @@ constexpr size_t pair_ring_bytes(int ns, int rk_step) {
     return (size_t)ns * (rk_step ? PairChunk<T>::kFloats1 : PairChunk<T>::kFloats0) * sizeof(float);
 }
 
-template <int T, int MINB, int NS, int FRIC, bool GEN_NORTH, bool WIND_FIELD, bool RCP, bool LAND, bool TMA>
-__global__ void __launch_bounds__(T, MINB) cdklm_pair_kernel(const StageArgs a, const __grid_constant__ PairMapParams mp) {
+// Block grid of one stage launch.  The region, column blocks [bx0, bx1)
+// over rows [4, ny), runs the TMA path in strips of `rows` rows (the last
+// one shorter); it reaches the ghost columns of periodic and open sides,
+// not those of walls.  The frame runs the boundary path in strips of rf
+// rows: the column blocks left of bx0 and right of bx1 (wall sides) over
+// every row, and the two rows next to the north and south ghost rows of the
+// region's column blocks.
+struct PairGrid {
+    int nbx, bx0, bx1;
+    int rows, nby;             // nby: strips of rows [4, ny)
+    int rf;                    // rows per strip of the frame blocks (>= 2)
+    int ny;
+};
+
+__host__ __device__ inline int pair_frame_strips(const PairGrid& g, int& nfull, int& full, int& nband) {
+    full = (g.ny + g.rf - 1) / g.rf;
+    nfull = g.bx0 + (g.nbx - g.bx1);
+    nband = g.bx1 - g.bx0;
+    return nfull * full + nband * 2;
+}
+
+// Frame block idx: its column block and row range.
+__host__ __device__ inline void pair_frame_block(const PairGrid& g, int idx, int& bx, int& r0, int& r1) {
+    int nfull, full, nband;
+    pair_frame_strips(g, nfull, full, nband);
+    if (idx < nfull * full) {
+        const int c = idx / full, s = idx % full;
+        bx = c < g.bx0 ? c : g.bx1 + (c - g.bx0);
+        r0 = 2 + s * g.rf;
+        r1 = min(r0 + g.rf, g.ny + 2);
+        return;
+    }
+    idx -= nfull * full;
+    bx = g.bx0 + (idx >> 1);
+    if ((idx & 1) == 0) { r0 = 2; r1 = 4; }
+    else { r0 = g.ny; r1 = g.ny + 2; }
+}
+
+// The stage over one part of the block grid.  PART 0: the region of TMA
+// strips, column block bx0 + blockIdx.x, strip blockIdx.y; PART 1: the
+// boundary frame (blockIdx.x numbers its strips), per-lane loads with wall
+// mirroring and periodic images.  The parts are separate
+// kernels so that the boundary-free one is compiled, and given registers,
+// without the boundary logic; they write disjoint cells and run
+// concurrently.
+template <int T, int MINB, int NS, int UNR, int FRIC, int WIND, bool GEN_NORTH, bool RCP, bool LAND, int PART>
+__global__ void __launch_bounds__(T, MINB)
+    cdklm_pair_kernel(const StageArgs a, const __grid_constant__ PairMapParams mp, const PairGrid g) {
     __shared__ PairSmem<T> sm;
     extern __shared__ __align__(128) float pair_ring[];
     pair_init<T, NS>(sm);
     const PairMaps maps{{&mp.q[0], &mp.q[1], &mp.q[2]}, {&mp.qn[0], &mp.qn[1], &mp.qn[2]}, &mp.h};
     unsigned chunk_base = 0;
-    pair_block<T, NS, FRIC, GEN_NORTH, WIND_FIELD, RCP, LAND, TMA>(a, maps, a.dt, blockIdx.x, blockIdx.y, sm,
-                                                                   pair_ring, chunk_base);
+    if (PART == 0) {
+        const int r0 = 4 + (int)blockIdx.y * g.rows;
+        const int r1 = min(r0 + g.rows, a.k.ny);
+        pair_strip<T, NS, UNR, FRIC, WIND, GEN_NORTH, RCP, LAND, false, true>(a, maps, a.dt, g.bx0 + blockIdx.x, r0,
+                                                                              r1, sm, pair_ring, chunk_base);
+    } else {
+        int bx, r0, r1;
+        pair_frame_block(g, blockIdx.x, bx, r0, r1);
+        pair_strip<T, NS, UNR, FRIC, WIND, GEN_NORTH, RCP, LAND, true, false>(a, maps, a.dt, bx, r0, r1, sm,
+                                                                              pair_ring, chunk_base);
+    }
+}
+
+// Makes a tensor map that the host copied to global memory visible to the
+// TMA unit before its first use (the maps of a batch live in device memory).
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
+}
+
+// Batched column-pair stage: a packed list of (member, column block, first
+// row, end row) tiles over every member, walked by a persistent grid.  args
+// and maps hold two entries per member (stage 0: h0 -> h1, stage 1: h1 ->
+// h0); dts holds the member's time step, read at launch so a captured graph
+// picks up new values.  PART 0 tiles take the TMA path with the member's
+// maps, PART 1 tiles the boundary path.
+template <int T, int MINB, int NS, int UNR, int FRIC, int WIND, bool GEN_NORTH, bool RCP, bool LAND, int PART>
+__global__ void __launch_bounds__(T, MINB)
+    cdklm_pair_batch_kernel(const StageArgs* __restrict__ args, const float* __restrict__ dts,
+                            const int4* __restrict__ tiles, const int ntiles, const int rk_step,
+                            const PairMapParams* __restrict__ maps) {
+    __shared__ PairSmem<T> sm;
+    extern __shared__ __align__(128) float pair_ring[];
+    pair_init<T, NS>(sm);
+    unsigned chunk_base = 0;
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const int4 tile = tiles[ti];
+        const int e = 2 * tile.x + rk_step;
+        const StageArgs& a = args[e];
+        if (PART == 0) {
+            const PairMapParams& p = maps[e];
+            const PairMaps m{{&p.q[0], &p.q[1], &p.q[2]}, {&p.qn[0], &p.qn[1], &p.qn[2]}, &p.h};
+            if (threadIdx.x == 0) {
+                for (int f = 0; f < 3; ++f) tensormap_acquire(m.q[f]);
+                if (rk_step == 1)
+                    for (int f = 0; f < 3; ++f) tensormap_acquire(m.qn[f]);
+                tensormap_acquire(m.h);
+            }
+            pair_strip<T, NS, UNR, FRIC, WIND, GEN_NORTH, RCP, LAND, false, true>(
+                a, m, __ldg(dts + tile.x), tile.y, tile.z, tile.w, sm, pair_ring, chunk_base);
+        } else {
+            const PairMaps m{};
+            pair_strip<T, NS, UNR, FRIC, WIND, GEN_NORTH, RCP, LAND, true, false>(a, m, __ldg(dts + tile.x), tile.y,
+                                                                                  tile.z, tile.w, sm, pair_ring,
+                                                                                  chunk_base);
+        }
+        __syncthreads();
+        if (sm.x.abort_flag) break;
+    }
 }
 
 }  // namespace go

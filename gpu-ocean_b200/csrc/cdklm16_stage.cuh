@@ -62,6 +62,8 @@ struct StageArgs {
     const float* wy_cur; const float* wy_next; int pw;  // interior-indexed
     int rows_per_block;
     unsigned int* status;
+    float neg_zero;              // -0.0f: the addend of the packed products (column-pair kernel)
+    int fric;                    // friction law kFric* (column-pair kernel; the marching kernel has it as a template)
 };
 
 // Friction law selector.

@@ -81,9 +81,7 @@ cudaError_t dispatch_variant(L& launcher, Variant v) {
 
 inline int shape_block_width(int shape) {
     switch (shape) {
-        case GO_SHAPE_PAIR32: return 64;     // columns per block: two per thread
-        case GO_SHAPE_PAIR64: return 128;
-        case GO_SHAPE_PAIR96: return 192;
+        case GO_SHAPE_PAIR: return 128;     // columns per block: two per thread
         case 2: case 4: case 5: return 128;
         case 3: return 256;
         case 6: return 96;
@@ -114,9 +112,7 @@ inline int ring_shape(long long work5, long long work6) { return work6 * 100 < w
 // Resident blocks per SM the shape is compiled for (its __launch_bounds__).
 inline int shape_blocks_per_sm(int shape) {
     switch (shape) {
-        case GO_SHAPE_PAIR32: return 12;
-        case GO_SHAPE_PAIR64: return 6;
-        case GO_SHAPE_PAIR96: return 4;
+        case GO_SHAPE_PAIR: return 8;
         case 0: case 3: return 2;
         case 1: case 7: return 3;
         case 2: return 4;

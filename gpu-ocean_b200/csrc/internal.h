@@ -28,6 +28,11 @@ struct go_domain {
     int sponge[4];           // open-boundary sponge widths: north, east, south, west
     uint64_t bc_tex[4];      // exterior solution textures: NS cur, NS next, EW cur, EW next
     float bc_t;              // their time weight
+    // column-pair launches: the boundary-frame kernel runs on a second
+    // stream beside the boundary-free one (created on first use)
+    cudaStream_t side;
+    cudaEvent_t ev_fork, ev_join;
+    int own_side;            // go_domain_create's handles may create them (not the allocation-free step)
 };
 
 // Records the message of a failed call (go_last_error) and returns code.
@@ -70,6 +75,14 @@ go::Variant go_variant(const go_domain* d);
 // One single-domain stage launch (stage_launch.cu).
 int go_launch_stage(go_domain* d, cudaStream_t s, const go::StageArgs& a);
 
-// Column-pair shapes (pair_launch.cu).
+// Column-pair shape (pair_launch.cu).
 bool go_pair_shape(int shape);
-int go_pair_threads(int shape);
+namespace go { struct PairMapParams; }
+int go_prepare_pair(const go::StageArgs& a, go::PairMapParams* mp, bool* tma);
+int go_launch_pair(go_domain* d, cudaStream_t s, const go::StageArgs& a, const go::PairMapParams& mp, bool tma);
+
+// A stage launch prepared once (kernel arguments, TMA maps) and launched
+// many times (stage_launch.cu).
+struct PreparedStage;
+int go_prepare_stage(go_domain* d, const go::StageArgs& a, PreparedStage* p);
+int go_launch_prepared(go_domain* d, cudaStream_t s, const PreparedStage& p);

@@ -15,20 +15,31 @@
 //    rows (ny <= 16384) plus the status word: 65,808 bytes per device,
 //    resident for the life of the process.  Larger ny is rejected.
 //  * The device address of the array comes from cudaGetSymbolAddress, looked
-//    up on the first call made with each device current and then cached.
-//    That first lookup can load this library's device code into the context
-//    (lazy module loading), which is not allowed inside stream capture: make
-//    the first call on each device outside any capture (n_steps = 0 is
-//    enough).
+//    up on the first call made with each device current and then cached
+//    together with the device's current context; a call that finds another
+//    context current (after cudaDeviceReset, say) looks it up again.  That
+//    lookup can load this library's device code into the context (lazy
+//    module loading), which is not allowed inside stream capture: make the
+//    first call on each device, and the first after a reset, outside any
+//    capture (n_steps = 0 is enough).
+//  * With a full Coriolis table (n_rows = ny + 4) the table is copied from
+//    the caller's host memory with cudaMemcpyAsync on the call's stream;
+//    from page-locked memory that copy runs after the call returns, so the
+//    caller keeps the table unchanged until the stream has passed the call.
+//  * The input's periodic ghost cells must be current: each stage refreshes
+//    the ghosts of its own output, but nothing refreshes the input's before
+//    the first stage (CDKLM16.step does that once at t = 0).
 //  * Every call on one device shares the one array: calls that overlap in
 //    time (different host threads, or different streams with no ordering
 //    between them) race on the Coriolis table and the status word.  Order
 //    them on one stream or serialise them on the host.
 //  * Each call clears the status word and rewrites the whole table before
 //    its launches, so nothing left by an earlier call is read.
+#include <cudaTypedefs.h>
+
 #include <mutex>
 
-#include "dispatch.cuh"
+#include "pair_dispatch.cuh"
 
 using namespace go;
 
@@ -44,19 +55,39 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
 unsigned char* g_scratch_ptr[kMaxDevices] = {nullptr};
+CUcontext g_scratch_ctx[kMaxDevices] = {nullptr};   // context the cached address belongs to
 
-// Device address of the scratch array on the current device.
+// The calling thread's current context, through the driver entry point the
+// runtime hands out (this library links the runtime only).
+CUcontext current_context() {
+    static PFN_cuCtxGetCurrent_v4000 get = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+    });
+    CUcontext c = nullptr;
+    if (get) get(&c);
+    return c;
+}
+
+// Device address of the scratch array on the current device, looked up
+// again when the device's context changed since the cached lookup.
 int scratch_address(unsigned char** out) {
     int dev = -1;
     GO_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return go_fail(GO_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != current_context()) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);   // makes the context current
         if (e != cudaSuccess)
             return go_fail(GO_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
         g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+        g_scratch_ctx[dev] = current_context();
     }
     *out = g_scratch_ptr[dev];
     return GO_OK;
@@ -154,10 +185,14 @@ extern "C" int go_cdklm_step_static(const go_domain_desc* desc, void* stream, co
                                        Hi_pitch / 4, land_value, 0.0f);
     const StageArgs a1 = go_stage_args(&d, dt, 1, eta1, hu1, hv1, pitch1 / 4, eta0, hu0, hv0, pitch0 / 4, Hi,
                                        Hi_pitch / 4, land_value, 0.0f);
+    PreparedStage p0, p1;
+    rc = go_prepare_stage(&d, a0, &p0);
+    if (!rc) rc = go_prepare_stage(&d, a1, &p1);
+    if (rc) return rc;
     for (int n = 0; n < n_steps; ++n) {
-        rc = go_launch_stage(&d, s, a0);
+        rc = go_launch_prepared(&d, s, p0);
         if (rc) return rc;
-        rc = go_launch_stage(&d, s, a1);
+        rc = go_launch_prepared(&d, s, p1);
         if (rc) return rc;
     }
     if (status_out) {

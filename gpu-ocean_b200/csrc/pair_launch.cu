@@ -1,11 +1,11 @@
-// Launches of the column-pair stage kernel (cdklm16_pair.cuh): TMA tensor
-// maps of the stage's arrays, ring size, kernel variant.
+// Launches of the column-pair stage kernel (cdklm16_pair.cuh): the TMA
+// tensor maps of a stage's arrays and the two-part launch of a stage.
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 
-#include "cdklm16_pair.cuh"
-#include "dispatch.cuh"
+#include "pair_dispatch.cuh"
 
 using namespace go;
 
@@ -41,74 +41,66 @@ bool encode(CUtensorMap* m, const float* base, int cols, int rows, int pitch, in
 
 bool aligned(const void* p, size_t n) { return ((uintptr_t)p % n) == 0; }
 
-int pair_threads(int shape) {
-    switch (shape) {
-        case GO_SHAPE_PAIR32: return 32;
-        case GO_SHAPE_PAIR96: return 96;
-        default: return 64;
-    }
-}
+}  // namespace
 
-struct PairLaunch {
-    const StageArgs* a;
-    const PairMapParams* mp;
-    bool tma;
-    cudaStream_t s;
-    template <int T, int MINB, int NS, int FRIC, bool GN, bool WF, bool RCP, bool LAND>
-    cudaError_t run() {
-        const dim3 grid((a->k.nx + (2 * T - 4) - 1) / (2 * T - 4),
-                        (a->k.ny + a->rows_per_block - 1) / a->rows_per_block);
-        if (tma) {
-            auto kern = cdklm_pair_kernel<T, MINB, NS, FRIC, GN, WF, RCP, LAND, true>;
-            const size_t ring = pair_ring_bytes<T>(NS, a->rk_step);
-            static cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                           (int)pair_ring_bytes<T>(NS, 1));
-            if (attr != cudaSuccess) return attr;
-            kern<<<grid, T, ring, s>>>(*a, *mp);
-        } else {
-            cdklm_pair_kernel<T, MINB, NS, FRIC, GN, WF, RCP, LAND, false><<<grid, T, 0, s>>>(*a, *mp);
-        }
-        return cudaGetLastError();
-    }
-};
+bool go_pair_shape(int shape) { return shape == GO_SHAPE_PAIR; }
 
-template <class L>
-cudaError_t dispatch_pair(L& l, int shape, const Variant& v) {
-    // experimental set: north-up, uniform wind, quadratic friction,
-    // reciprocal quotients, no land
-    if (v.gen_north || v.wind_field || v.fric != kFricQuad || !v.rcp || v.land) return cudaErrorNotSupported;
-    switch (shape) {
-        case GO_SHAPE_PAIR32: return l.template run<32, 12, 2, kFricQuad, false, false, true, false>();
-        case GO_SHAPE_PAIR96: return l.template run<96, 4, 2, kFricQuad, false, false, true, false>();
-        default: return l.template run<64, 6, 2, kFricQuad, false, false, true, false>();
+namespace go {
+namespace {
+// Periodic east/west ghost columns of rows [2, ny+2) of a stage's output
+// (boundary_kernels.cu:76-110 restricted to what the region's strips do
+// not write themselves): columns 0, 1 from nx, nx+1 and nx+2, nx+3 from 2,
+// 3.  blockIdx.y selects the member of a batch (args[2 m + rk_step]).
+__global__ void k_periodic_columns(const StageArgs* __restrict__ args, int rk_step, StageArgs one) {
+    const StageArgs& a = args ? args[2 * blockIdx.y + rk_step] : one;
+    if (a.k.bcE != kPeriodic) return;
+    const int nx = a.k.nx;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 4 * a.k.ny; i += gridDim.x * blockDim.x) {
+        const int j = 2 + (i >> 2), c = i & 3;
+        const int dst = c < 2 ? c : nx + c;
+        const int src = c < 2 ? c + nx : c;
+        const size_t o = (size_t)j * a.pout;
+        a.eta_out[o + dst] = a.eta_out[o + src];
+        a.hu_out[o + dst] = a.hu_out[o + src];
+        a.hv_out[o + dst] = a.hv_out[o + src];
     }
 }
 
 }  // namespace
 
-bool go_pair_shape(int shape) {
-    return shape == GO_SHAPE_PAIR32 || shape == GO_SHAPE_PAIR64 || shape == GO_SHAPE_PAIR96;
+cudaError_t pair_launch_periodic_columns(const StageArgs* args, int n, int max_ny, int rk_step, const StageArgs& one,
+                                         cudaStream_t s) {
+    k_periodic_columns<<<dim3((4 * max_ny + 255) / 256, n), 256, 0, s>>>(args, rk_step, one);
+    return cudaGetLastError();
 }
 
-int go_pair_threads(int shape) { return pair_threads(shape); }
+cudaError_t pair_launch_interior(const PairSingleReq& r, const Variant& v) {
+    if (v.fric == kFricQuad) return pair_launch_interior_f1(r, v);
+    if (v.fric == kFricLinear) return pair_launch_interior_f2(r, v);
+    return pair_launch_interior_f0(r, v);
+}
+cudaError_t pair_batch_launch_interior(const PairBatchReq& r, const Variant& v) {
+    if (v.fric == kFricQuad) return pair_batch_launch_interior_f1(r, v);
+    if (v.fric == kFricLinear) return pair_batch_launch_interior_f2(r, v);
+    return pair_batch_launch_interior_f0(r, v);
+}
+}  // namespace go
 
-int go_prepare_pair(const StageArgs& a, int shape, PairMapParams* mp, bool* tma) {
+int go_prepare_pair(const StageArgs& a, PairMapParams* mp, bool* tma) {
     memset(mp, 0, sizeof(*mp));
-    const int T = pair_threads(shape);
+    constexpr int T = kPairT;
     const int nx = a.k.nx, ny = a.k.ny;
     // TMA needs 16-byte aligned bases and pitches; the vector stores of the
     // boundary-free blocks need 8-byte aligned outputs and an even pitch
-    bool ok = encoder() != nullptr;
+    bool ok = encoder() != nullptr && aligned(a.eta_out, 8) && aligned(a.hu_out, 8) && aligned(a.hv_out, 8) &&
+              (a.pout % 2) == 0 && (a.pin * 4) % 16 == 0;
     const float* q[3] = {a.eta_in, a.hu_in, a.hv_in};
     const float* qn[3] = {a.qn_eta, a.qn_hu, a.qn_hv};
     for (int f = 0; f < 3 && ok; ++f) {
-        ok = aligned(q[f], 16) && (a.pin * 4) % 16 == 0 && aligned(a.eta_out, 8) && aligned(a.hu_out, 8) &&
-             aligned(a.hv_out, 8) && (a.pout % 2) == 0;
-        if (ok) ok = encode(&mp->q[f], q[f], nx + 4, ny + 4, a.pin, 2 * T, kPairRingRows);
-        if (ok && a.rk_step == 1) {
-            ok = aligned(qn[f], 16) && (a.pqn * 4) % 16 == 0;
-            if (ok) ok = encode(&mp->qn[f], qn[f], nx + 4, ny + 4, a.pqn, 2 * T, kPairRingRows);
-        }
+        ok = aligned(q[f], 16) && encode(&mp->q[f], q[f], nx + 4, ny + 4, a.pin, 2 * T, kPairRingRows);
+        if (ok && a.rk_step == 1)
+            ok = aligned(qn[f], 16) && (a.pqn * 4) % 16 == 0 &&
+                 encode(&mp->qn[f], qn[f], nx + 4, ny + 4, a.pqn, 2 * T, kPairRingRows);
     }
     if (ok) ok = aligned(a.Hi, 16) && (a.phi * 4) % 16 == 0 &&
                  encode(&mp->h, a.Hi, nx + 5, ny + 5, a.phi, 2 * T + 4, kPairRingRows);
@@ -116,11 +108,39 @@ int go_prepare_pair(const StageArgs& a, int shape, PairMapParams* mp, bool* tma)
     return GO_OK;
 }
 
+// One stage: the boundary-frame kernel on the domain's high-priority side
+// stream (its short strips are scheduled ahead of the region's blocks),
+// forked from and joined back to the caller's stream, then the periodic
+// east/west ghost columns of the output; without a side stream (the
+// allocation-free step) every part runs on the caller's stream.
 int go_launch_pair(go_domain* d, cudaStream_t s, const StageArgs& a, const PairMapParams& mp, bool tma) {
-    PairLaunch L{&a, &mp, tma, s};
-    const cudaError_t e = dispatch_pair(L, d->shape, go_variant(d));
-    if (e == cudaErrorNotSupported)
-        return go_fail(GO_ERR_UNSUPPORTED, "column-pair launch shape %d has no kernel for this variant", d->shape);
-    if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "pair stage launch failed: %s", cudaGetErrorString(e));
+    const PairGrid g = pair_grid(a.k, a.rows_per_block, tma);
+    const int n_int = (g.bx1 - g.bx0) * g.nby;
+    const int n_frame = pair_frame_count(g);
+    const Variant v = go_variant(d);
+    const bool fork_join = d->side && n_int > 0 && n_frame > 0;
+    PairSingleReq r{&a, &mp, g, s};
+    if (n_frame > 0) {
+        if (fork_join) {
+            GO_CUDA(cudaEventRecord(d->ev_fork, s));
+            GO_CUDA(cudaStreamWaitEvent(d->side, d->ev_fork, 0));
+            r.s = d->side;
+        }
+        const cudaError_t e = pair_launch_frame(r, v);
+        if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "stage launch (boundary frame) failed: %s", cudaGetErrorString(e));
+    }
+    if (n_int > 0) {
+        r.s = s;
+        const cudaError_t e = pair_launch_interior(r, v);
+        if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));
+    }
+    if (fork_join) {
+        GO_CUDA(cudaEventRecord(d->ev_join, d->side));
+        GO_CUDA(cudaStreamWaitEvent(s, d->ev_join, 0));
+    }
+    if (n_int > 0 && a.k.bcE == kPeriodic) {
+        // the region's strips leave the periodic images of their cells to this copy
+        GO_CUDA(pair_launch_periodic_columns(nullptr, 1, a.k.ny, 0, a, s));
+    }
     return GO_OK;
 }

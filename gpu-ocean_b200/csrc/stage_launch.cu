@@ -1,6 +1,6 @@
-// Single-domain stage launches: every kernel variant of the marching stage.
-#include "cdklm16_pair.cuh"
-#include "dispatch.cuh"
+// Single-domain stage launches: the column-pair kernel (pair_launch.cu) or
+// a variant of the marching kernel.
+#include "pair_dispatch.cuh"
 
 using namespace go;
 
@@ -30,19 +30,34 @@ Variant go_variant(const go_domain* d) {
     return v;
 }
 
-int go_prepare_pair(const StageArgs& a, int shape, PairMapParams* mp, bool* tma);
-int go_launch_pair(go_domain* d, cudaStream_t s, const StageArgs& a, const PairMapParams& mp, bool tma);
-
-int go_launch_stage(go_domain* d, cudaStream_t s, const StageArgs& a) {
-    if (go_pair_shape(d->shape)) {
-        PairMapParams mp;
-        bool tma = false;
-        int rc = go_prepare_pair(a, d->shape, &mp, &tma);
-        if (!rc) rc = go_launch_pair(d, s, a, mp, tma);
-        return rc;
+int go_prepare_stage(go_domain* d, const StageArgs& a, PreparedStage* p) {
+    p->a = a;
+    p->pair = go_pair_shape(d->shape);
+    p->tma = false;
+    if (!p->pair) return GO_OK;
+    if (d->own_side && !d->side) {
+        // the boundary-frame kernel's stream and the events that fork it
+        // from, and join it back to, the caller's stream
+        int least = 0, greatest = 0;
+        GO_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        GO_CUDA(cudaStreamCreateWithPriority(&d->side, cudaStreamNonBlocking, greatest));
+        GO_CUDA(cudaEventCreateWithFlags(&d->ev_fork, cudaEventDisableTiming));
+        GO_CUDA(cudaEventCreateWithFlags(&d->ev_join, cudaEventDisableTiming));
     }
-    SingleLaunch L{&a, s};
+    return go_prepare_pair(a, &p->mp, &p->tma);
+}
+
+int go_launch_prepared(go_domain* d, cudaStream_t s, const PreparedStage& p) {
+    if (p.pair) return go_launch_pair(d, s, p.a, p.mp, p.tma);
+    SingleLaunch L{&p.a, s};
     const cudaError_t e = dispatch_variant(L, go_variant(d));
     if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));
     return GO_OK;
+}
+
+int go_launch_stage(go_domain* d, cudaStream_t s, const StageArgs& a) {
+    PreparedStage p;
+    int rc = go_prepare_stage(d, a, &p);
+    if (!rc) rc = go_launch_prepared(d, s, p);
+    return rc;
 }

@@ -50,6 +50,8 @@ extern "C" {
 #define GO_STATUS_NONFINITE 0x1u /* a written cell held NaN or Inf */
 #define GO_STATUS_ADJ_SCOPE 0x2u /* the adjoint met land, a cell shallower than
                                    desing_eps, or a non-north-up grid */
+#define GO_STATUS_TIMEOUT 0x4u   /* a bounded wait in a step kernel gave up
+                                   (a TMA tile that never arrived) */
 
 typedef struct go_domain go_domain;
 
@@ -297,12 +299,13 @@ int go_sample_wind(void* stream, const float* field, int w, int h, int nx, int n
  * recomputed halo rows).  Chosen by the autotuner; every shape computes
  * identical results. */
 int go_domain_set_launch(go_domain* d, int shape, int rows_per_block);
-/* Column-pair shapes: blocks of 32, 64 or 96 threads, each thread two
- * adjacent columns in packed FP32x2 arithmetic, inputs of boundary-free
- * blocks staged by TMA tile loads (16-byte aligned arrays and pitches). */
-#define GO_SHAPE_PAIR32 8
-#define GO_SHAPE_PAIR64 9
-#define GO_SHAPE_PAIR96 10
+/* Shape 8: the column-pair kernel.  Blocks of 64 threads, each thread two
+ * adjacent columns in packed FP32x2 arithmetic (sm_100 FADD2/FFMA2), inputs
+ * of the boundary-free blocks staged through shared memory by TMA tile
+ * loads; the boundary frame runs as a second kernel on a high-priority
+ * stream beside them.  Arrays whose base or pitch is not a multiple of 16
+ * bytes take the boundary path everywhere. */
+#define GO_SHAPE_PAIR 8
 
 /* How quotients are evaluated.  EXACT keeps every '/' of the reference
  * kernel (div.full.f32 under its --prec-div=false).  RCP (the default)
@@ -510,10 +513,17 @@ int go_obs_adjoint(void* stream, const go_state* q, const go_state* lam, int nx,
  * array of 65,808 bytes per device, so ny + 4 <= 16388 (larger ny is
  * rejected with GO_ERR_INVALID).  The status word is cleared at the start
  * of each call; status_out (optional, host) receives it after a stream
- * synchronize.  The first call on each device looks up the array's address
- * and may load the module: make it outside stream capture.  Calls on one
- * device share the array, so overlapping calls race: order them on one
- * stream or one host thread.
+ * synchronize.  The first call on each device (and the first after a
+ * cudaDeviceReset, which gives the device a new context) looks up the
+ * array's address and may load the module: make it outside stream capture.
+ * Calls on one device share the array, so overlapping calls race: order
+ * them on one stream or one host thread.  With n_rows = ny+4 the table is
+ * copied from f_rows_host by cudaMemcpyAsync on the stream: when that host
+ * memory is page-locked the copy runs after the call returns, so keep the
+ * table unchanged until the stream has passed the call.  The input's
+ * periodic ghost cells must be current (the step kernels refresh them for
+ * their outputs; CDKLM16.step refreshes them once at t = 0, this call does
+ * not).
  * --------------------------------------------------------------------- */
 int go_cdklm_step_static(const go_domain_desc* desc, void* stream, const float* f_rows_host,
                          int n_rows, float wind_x, float wind_y, int n_steps, float dt,
@@ -562,6 +572,14 @@ int go_batch_grf_perturb(go_batch* b, void* stream, uint32_t key0, uint32_t even
 /* Device status word (GO_STATUS_* bits) accumulated by the step kernels;
  * synchronous read, optionally clearing it. */
 int go_domain_status(go_domain* d, uint32_t* status, int clear);
+
+/* Status words of every member of a batch (n values to status_host, member
+ * order): each member's step kernels write only its own word, so a member
+ * whose state went non-finite is flagged alone and the others step on
+ * unchanged.  Synchronous; clear != 0 resets the words.  Replaces the
+ * reference's dead-member bookkeeping (BaseOceanStateEnsemble.py:108-110,
+ * EnsembleFromFiles.py:315), which looks for NaN in downloaded states. */
+int go_batch_status(go_batch* b, uint32_t* status_host, int clear);
 
 /* Message of the last failed call on this host thread ("" if none). */
 const char* go_last_error(void);

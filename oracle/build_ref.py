@@ -140,7 +140,17 @@ def up_to_date(cfg, fmad=False):
     return all(os.path.getmtime(d) <= mt for d in deps)
 
 
-def build(ref_root="/root/reference", names=None, force=False):
+def reference_root(argv=None):
+    """The gpu-ocean source tree: the first command-line argument, else the
+    GOCEAN_REFERENCE environment variable; fails clearly when neither is set."""
+    args = [a for a in (sys.argv[1:] if argv is None else argv) if not a.startswith("--")]
+    root = args[0] if args else os.environ.get("GOCEAN_REFERENCE")
+    if not root:
+        raise SystemExit("name the gpu-ocean source tree: build_ref.py <tree> or GOCEAN_REFERENCE=<tree>")
+    return root
+
+
+def build(ref_root, names=None, force=False):
     names = list(CONFIGS) if names is None else names
     todo = []
     for n in names:
@@ -161,6 +171,5 @@ def build(ref_root="/root/reference", names=None, force=False):
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    for p in build(root, force="--force" in sys.argv):
+    for p in build(reference_root(), force="--force" in sys.argv):
         print(p)

@@ -24,7 +24,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GOCEAN_REFERENCE")
+if not REF:
+    raise SystemExit("name the gpu-ocean source tree: make_golden.py <tree> or GOCEAN_REFERENCE=<tree>")
 TESTS = os.path.join(REF, "gpu_ocean", "tests")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cdklm16_timestep50.npz")
 

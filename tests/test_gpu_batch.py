@@ -53,7 +53,8 @@ def test_mixed_batch_equals_member_by_member(ctx):
         assert s.t == a.t
 
 
-@pytest.mark.parametrize("launch", [(5, 16, 0), (5, 3, 148 * 5), (4, 16, 148 * 5), (6, 24, 0), (7, 5, 148 * 3)])
+@pytest.mark.parametrize("launch", [(5, 16, 0), (5, 3, 148 * 5), (4, 16, 148 * 5), (6, 24, 0), (7, 5, 148 * 3),
+                                    (8, 24, 0), (8, 6, 148 * 2)])
 def test_batch_launch_shapes_equal_member_by_member(ctx, launch):
     """The batched kernel under the read-ahead shape (5) and a persistent
     grid that walks several tiles per block gives the member-by-member
@@ -221,3 +222,69 @@ def test_batched_model_error_equals_member_by_member(ctx, lcg):
             assert np.array_equal(x, y)
     e0, e1 = sims[0].download()[0], sims[1].download()[0]
     assert not np.array_equal(e0, e1)
+
+
+def test_nonfinite_member_flagged_isolated_and_dropped(ctx):
+    """A member whose initial eta holds NaN (made on the host) is flagged in
+    its own status word; the other members step bit for bit as a batch
+    without it, and the ensemble drops it and steps on unchanged
+    (BaseOceanStateEnsemble.py:108-110, EnsembleFromFiles.py:315)."""
+    sizes = [128, 96, 160, 128]
+    sims = _members(ctx, sizes, seed0=47000)
+    eta, hu, hv = sims[2].download()
+    eta[40, 50] = np.nan
+    sims[2].upload(eta, hu, hv)
+    keep = [0, 1, 3]
+    ref = [m for k, m in enumerate(_members(ctx, sizes, seed0=47000)) if k in keep]
+    b = BatchedEnsemble.BatchedCDKLM16(sims)
+    b.advance(10)
+    b_ref = BatchedEnsemble.BatchedCDKLM16(ref)
+    b_ref.advance(10)
+    status = b.member_status()
+    assert status[2] & 0x1 and all(status[k] == 0 for k in keep)
+    assert b.failed_members() == [2]
+    for k, r in zip(keep, ref):
+        assert np.array_equal(np.stack(sims[k].download()), np.stack(r.download()))
+    removed = b.drop(b.failed_members())
+    assert removed == [sims[2]] and b.n == 3
+    b.advance(7)
+    b_ref.advance(7)
+    for s, r in zip(b.sims, ref):
+        assert np.array_equal(np.stack(s.download()), np.stack(r.download()))
+    assert b.member_status() == [0, 0, 0]
+
+
+def test_batched_members_vs_reference_kernel(ctx):
+    """Four members of the config-2 physics on a 96 x 80 grid (beta plane,
+    quadratic friction, wind, walls north/south, periodic east/west), each
+    with its own GRF bathymetry, bumps and time step, stepped 200 times by
+    the batched launch; every member against the reference kernel
+    (CDKLM16_kernel.cu:429-1006, rebuilt for this GPU) on the same inputs,
+    bit for bit with ghost cells, so the batch is tied to the reference and
+    not only to the single-domain path."""
+    from oracle import build_ref, ref_kernel
+    from oracle import cdklm16_oracle as O
+    cfg = build_ref.CONFIGS["small_beta"]
+    if not ref_kernel.available(cfg):
+        pytest.skip("reference kernel library not built")
+    nx, ny = cfg["nx"], cfg["ny"]
+    cases = []
+    for m in range(4):
+        c = SC.grf(nx, dx=500.0, steps=200, seed_bathy=20241 + 7 * m, seed_bumps=20242 + 7 * m)
+        c.ny = ny
+        c.Hi = O.fix_bi_ghost_corners(np.ascontiguousarray(c.Hi[: ny + 5]), nx, ny, c.bc)
+        c.eta0 = np.ascontiguousarray(c.eta0[: ny + 4])
+        c.hu0 = np.zeros_like(c.eta0)
+        c.hv0 = np.zeros_like(c.eta0)
+        c.dt = SC.cfl_dt(c)
+        cases.append(c)
+    sims = [CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs()) for c in cases]
+    b = BatchedEnsemble.BatchedCDKLM16(sims)
+    b.advance(200)
+    assert b.member_status() == [0, 0, 0, 0]
+    for c, s in zip(cases, sims):
+        ref = ref_kernel.RefKernelSim(cfg, c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, c.bc, wind=c.wind)
+        for _ in range(200):
+            ref.step(c.dt)
+        for a, r in zip(s.download(), ref.download()):
+            assert np.array_equal(a, r)
