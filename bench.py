@@ -289,16 +289,32 @@ def run_ours(args, world, rank, local):
     h2d = sum(int(a.numel()) * 4 for a in host) * 2      # upload fills h0 and h1
     d2h = sum(int(a.size) * 4 for a in out)
     return dict(c=c, cells=cells, t_ms=t_ms, e_ms=e_ms, clocks=clocks, status=status, h2d=h2d, d2h=d2h,
-                launches=2 * args.steps)
+                launches=2 * args.steps * sim._domain.stage_launches(), stage_launches=sim._domain.stage_launches())
 
 
-def run_ensemble(ctx, n_members=100, n=512, target_steps=300, graph_steps=10):
+def _timed(fn):
+    """(result, ms) of fn() between two device syncs, CUDA events."""
+    import torch
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    out = fn()
+    torch.cuda.synchronize()
+    b.record()
+    b.synchronize()
+    return out, a.elapsed_time(b)
+
+
+def run_ensemble(ctx, n_members=100, n=512, target_steps=3000, graph_steps=50, plain_steps=600):
     """Batched ensemble (100 members of 512^2, config-2 physics at dx = 1 km,
     shared bathymetry seed 20243): per event every member advances 60 s at
     the common dt, gets model error, and the common dt = 0.7 CFL is
-    recomputed.  The same events run batched (one launch per RK stage over
-    all members, graph replays) and member by member from Python (the
-    reference's ensemble loop), from the same initial states."""
+    recomputed.  The batch runs about 3000 steps (one launch per RK stage
+    over all members, CUDA-graph replays of 50 steps); the member-by-member
+    loop of the reference's ensembles runs the same events from the same
+    initial states for about 600 steps, and the states after the events
+    both ran are compared."""
     import torch
     from SWESimulators import BatchedEnsemble, CDKLM16, ModelError, SyntheticCases as SC
 
@@ -313,25 +329,19 @@ def run_ensemble(ctx, n_members=100, n=512, target_steps=300, graph_steps=10):
         torch.cuda.synchronize()
         return sims
 
-    def timed(fn):
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        out = fn()
-        torch.cuda.synchronize()
-        b.record()
-        b.synchronize()
-        return out, a.elapsed_time(b)
-
     # batched
     sims = members()
     batch = BatchedEnsemble.BatchedCDKLM16(sims, graph_steps=graph_steps)
     batch.update_dt(0.7)
     warm = batch.run_events(1, 1)                         # warm-up event (graphs, scratch)
-    n_events = max(1, int(round(target_steps / max(warm, 1))))
-    steps_b, t_b = timed(lambda: batch.run_events(2, n_events))
-    # plain member-by-member loop over the same events
+    per_event = max(warm, 1)
+    n_plain = max(1, int(round(plain_steps / per_event)))
+    steps_b1, t_b1 = _timed(lambda: batch.run_events(2, n_plain))
+    snap = [np.stack(s.download()) for s in sims]         # states after the events both paths run
+    n_rest = max(0, int(round((target_steps - steps_b1) / per_event)))
+    steps_b2, t_b2 = _timed(lambda: batch.run_events(2 + n_plain, n_rest)) if n_rest else (0, 0.0)
+    steps_b, t_b = steps_b1 + steps_b2, t_b1 + t_b2
+    # plain member-by-member loop over the first events
     plain = members()
     lims = []
     for s in plain:
@@ -357,16 +367,69 @@ def run_ensemble(ctx, n_members=100, n=512, target_steps=300, graph_steps=10):
         return steps
 
     plain_events(1, 1)
-    steps_p, t_p = timed(lambda: plain_events(2, n_events))
-    same = all(np.array_equal(np.stack(x.download()), np.stack(y.download())) for x, y in zip(sims, plain))
+    steps_p, t_p = _timed(lambda: plain_events(2, n_plain))
+    same = all(np.array_equal(a, np.stack(y.download())) for a, y in zip(snap, plain))
     cells = n_members * n * n
     vb = cells * steps_b / (t_b * 1e-3) / 1e9
     vp = cells * steps_p / (t_p * 1e-3) / 1e9
-    return {"workload": "ensemble100", "members": n_members, "grid": "%dx%d" % (n, n), "events": n_events,
-            "steps": steps_b, "batched_gcell_steps_s": vb, "plain_loop_gcell_steps_s": vp, "speedup": vb / vp,
+    return {"workload": "ensemble100", "members": n_members, "grid": "%dx%d" % (n, n),
+            "events": n_plain + n_rest, "steps": steps_b, "batched_gcell_steps_s": vb,
+            "plain_loop_gcell_steps_s": vp, "plain_loop_steps": steps_p, "speedup": vb / vp,
             "batched_ms": t_b, "plain_ms": t_p, "identical_states": bool(same), "graph_steps": graph_steps,
+            "launch_shape": batch.batch.launch[0] if hasattr(batch.batch, "launch") else None,
             "note": "per event: 60 s of steps at the common dt, model error (Philox GRF, std 0.05 m, corr 15 "
-                    "cells), dt = 0.7 CFL min over members; both paths from the same perturbed states"}
+                    "cells), dt = 0.7 CFL min over members; both paths from the same perturbed states; the "
+                    "states are compared after the events both ran"}
+
+
+def run_mixed(ctx, n_domains=64, steps=3000, graph_steps=50, plain_steps=300):
+    """Mixed batch: 64 independent domains with nx, ny drawn uniformly from
+    {128, 256, ..., 1024} (default_rng(20244)), config-2 physics at dx = 1 km,
+    each with its own GRF bathymetry (seed 40000 + k) and bumps, stepped at
+    its own CFL time step.  The batch runs 3000 steps; the member-by-member
+    loop (CDKLM16.step of each domain in turn) runs 300, and both states are
+    compared after those."""
+    import torch
+    from SWESimulators import BatchedEnsemble, CDKLM16, SyntheticCases as SC
+
+    rng = np.random.default_rng(20244)
+    sizes = rng.choice(np.arange(128, 1025, 128), size=(n_domains, 2))
+
+    def domains():
+        sims = []
+        for k, (nx, ny) in enumerate(sizes):
+            c = SC.grf(int(nx), ny=int(ny), dx=1000.0, seed_bathy=40000 + k, seed_bumps=41000 + k, steps=1)
+            sims.append(CDKLM16.CDKLM16(ctx, dt=c.dt, **c.kwargs()))
+        torch.cuda.synchronize()
+        return sims
+
+    sims = domains()
+    batch = BatchedEnsemble.BatchedCDKLM16(sims, graph_steps=graph_steps)
+    batch.advance(graph_steps)                              # warm-up (graph, TMA maps)
+    _, t1 = _timed(lambda: batch.advance(plain_steps))
+    snap = [np.stack(s.download()) for s in sims]
+    _, t2 = _timed(lambda: batch.advance(steps - plain_steps))
+    plain = domains()
+    for s in plain:
+        for _ in range(graph_steps):
+            s.step(s.dt)
+
+    def plain_loop(k):
+        for _ in range(k):
+            for s in plain:
+                s.step(s.dt)
+
+    plain_loop(0)
+    _, tp = _timed(lambda: plain_loop(plain_steps))
+    same = all(np.array_equal(a, np.stack(y.download())) for a, y in zip(snap, plain))
+    cells = int(np.sum(sizes[:, 0] * sizes[:, 1]))
+    vb = cells * steps / ((t1 + t2) * 1e-3) / 1e9
+    vp = cells * plain_steps / (tp * 1e-3) / 1e9
+    return {"workload": "mixed64", "domains": n_domains, "cells_per_step": cells,
+            "sizes": "nx, ny in {128, ..., 1024}, default_rng(20244)", "steps": steps,
+            "batched_gcell_steps_s": vb, "plain_loop_gcell_steps_s": vp, "plain_loop_steps": plain_steps,
+            "speedup": vb / vp, "batched_ms": t1 + t2, "plain_ms": tp, "identical_states": bool(same),
+            "graph_steps": graph_steps}
 
 
 def run_drifters(ctx, n_drifters=100000, steps=100):
@@ -785,15 +848,15 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "adjoint512", "adjoint_stage", "drifters", "open_bc",
-                                           "adjoint_batch", "model_error"],
+    ap.add_argument("--workload", choices=["grf4096", "bump256", "ensemble100", "mixed64", "adjoint512", "adjoint_stage",
+                                           "drifters", "open_bc", "adjoint_batch", "model_error"],
                     default="grf4096")
     ap.add_argument("--grid", type=int, default=None,
                     help="grid size of the adjoint_stage (default 2048) and model_error (default 4096) workloads")
     ap.add_argument("--adj-kind", type=int, default=0, help="adjoint launch form (include/gocean.h GO_ADJ_*)")
     ap.add_argument("--adj-rows", type=int, default=0, help="rows per strip of the marching adjoint (0: automatic)")
     ap.add_argument("--rows", type=int, default=0, help="rows per block strip (0: library default)")
-    ap.add_argument("--shape", type=int, default=0, help="launch shape 0..4 (include/gocean.h)")
+    ap.add_argument("--shape", type=int, default=0, help="launch shape 0..8 (include/gocean.h GO_SHAPE_*); with --rows 0 as well, the library default")
     ap.add_argument("--arith", type=int, default=-1,
                     help="quotients: 0 '/' as the reference source, 1 reciprocals (library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -829,8 +892,8 @@ def main():
         print(json.dumps(line))
         return
 
-    if args.workload in ("ensemble100", "adjoint512", "adjoint_stage", "adjoint_batch", "drifters", "open_bc",
-                         "model_error"):
+    if args.workload in ("ensemble100", "mixed64", "adjoint512", "adjoint_stage", "adjoint_batch", "drifters",
+                         "open_bc", "model_error"):
         if rank != 0:
             return
         from SWESimulators import Common
@@ -839,6 +902,8 @@ def main():
         sampler.start()
         if args.workload == "ensemble100":
             r = run_ensemble(ctx)
+        elif args.workload == "mixed64":
+            r = run_mixed(ctx)
         elif args.workload == "adjoint512":
             r = run_adjoint(ctx, kind=args.adj_kind, rows=args.adj_rows)
         elif args.workload == "adjoint_batch":
@@ -862,7 +927,7 @@ def main():
                               "data": "synthetic", "config": {"workload": "adjoint_stage", "grid": r["grid"]},
                               "result": r, "clocks": clocks}))
             return
-        if args.workload == "ensemble100":
+        if args.workload in ("ensemble100", "mixed64"):
             value, ms = r["batched_gcell_steps_s"], r["batched_ms"] / max(r["steps"], 1)
         elif args.workload == "adjoint_batch":
             value, ms = r["forward_adjoint_gcell_steps_s"], r["forward_adjoint_ms"] / r["steps"]
@@ -909,7 +974,7 @@ def main():
         from SWESimulators import Common
         ctx = Common.CUDAContext(local)
         secondary = {}
-        for name, fn in (("ensemble100", run_ensemble), ("adjoint512", run_adjoint),
+        for name, fn in (("ensemble100", run_ensemble), ("mixed64", run_mixed), ("adjoint512", run_adjoint),
                          ("adjoint_batch", run_adjoint_batch), ("drifters", run_drifters),
                          ("open_bc", run_open_bc), ("model_error", run_model_error)):
             try:

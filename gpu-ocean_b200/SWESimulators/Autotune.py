@@ -20,9 +20,9 @@ from . import _native
 
 DOMAIN_CANDIDATES = [(4, 2), (4, 4), (4, 8), (4, 16), (4, 24), (4, 32), (5, 8), (5, 16), (5, 24), (5, 32),
                      (6, 4), (6, 8), (6, 16), (6, 24), (6, 32), (7, 16), (7, 24), (2, 4), (2, 8), (2, 16),
-                     (1, 16), (3, 16), (0, 16)]
+                     (1, 16), (3, 16), (0, 16), (8, 12), (8, 24), (8, 36), (8, 48)]
 BATCH_CANDIDATES = [(4, 16, 0), (4, 32, 0), (5, 16, 0), (5, 24, 0), (5, 32, 0), (6, 16, 0), (6, 24, 0), (6, 32, 0),
-                    (7, 32, 0), (2, 32, 0), (1, 16, 0), (5, 32, 148 * 5)]
+                    (7, 32, 0), (2, 32, 0), (1, 16, 0), (5, 32, 148 * 5), (8, 24, 0), (8, 32, 0), (8, 48, 0)]
 GRAPH_LENGTHS = [10, 50]
 
 

@@ -305,12 +305,23 @@ class BatchedCDKLM16:
         self.set_dt([dt] * self.n)
         return dt
 
-    def run_events(self, first_event, n_events, interval=60.0, std=0.05, corr_cells=15.0, courant=0.7):
+    def run_events(self, first_event, n_events, interval=60.0, std=0.05, corr_cells=15.0, courant=0.7,
+                   device_loop=True):
         """The ensemble workload loop: for each event e, every member advances
         `interval` seconds at the common dt (step(t_end) semantics), then
         gets model error for event e, then the common dt is recomputed from
         the members' CFL limits -- what the reference's ensembles do member
-        by member (OceanNoiseEnsemble.py:506-531).  Returns the steps taken."""
+        by member (OceanNoiseEnsemble.py:506-531).  Returns the steps taken.
+
+        device_loop: the whole loop runs on the device in one graph launch
+        (go_batch_run_events), the host waiting once at the end; the members
+        must share dt (update_dt), carry no OceanStateNoise model error of
+        their own and no time-varying wind.  Otherwise, or with
+        device_loop=False, the host drives each event (one CFL read-back per
+        event); both give the same states, times and steps bit for bit."""
+        dts = {float(np.float32(s.dt)) for s in self.sims}
+        if device_loop and len(dts) == 1 and not self._time_varying_wind() and not self._has_model_error():
+            return self._run_events_device(first_event, n_events, interval, std, corr_cells, courant)
         steps = 0
         self._sync_members()
         self._owned = True
@@ -324,6 +335,33 @@ class BatchedCDKLM16:
         finally:
             self._owned = False
             self._release_members()
+        return steps
+
+    def _run_events_device(self, first_event, n_events, interval, std, corr_cells, courant):
+        from . import ModelError
+        if int(n_events) <= 0:
+            return 0
+        lib = _native.load()
+        n = lib.go_batch_grf_scratch_floats(self.batch.handle, float(corr_cells))
+        if n == 0:
+            raise ValueError("invalid correlation length")
+        self._sync_members()
+        self._first_step_bc()
+        # the captured graph holds the scratch address: keep one buffer
+        buf = getattr(self, "_loop_scratch", None)
+        if buf is None or buf.numel() < n:
+            torch = _native.require_cuda()
+            buf = torch.empty(int(n), dtype=torch.float32, device="cuda")
+            self._loop_scratch = buf
+        t0 = [float(s.t) for s in self.sims]
+        t, steps, dt = self.batch.run_events(self.stream, first_event, n_events, float(interval),
+                                             np.float32(self.sims[0].dt), float(courant),
+                                             ModelError.MODEL_ERROR_SEED, float(std), float(corr_cells), buf, t0)
+        for s, tm in zip(self.sims, t):
+            s.t = float(tm)
+            s.num_iterations += steps
+            s.dt = dt
+        self._release_members()
         return steps
 
     def synchronize(self):

@@ -122,6 +122,9 @@ SIGNATURES = {
     "go_domain_set_open_bc": (_I, [_P, _P, _F]),
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_status": (_I, [_P, _P, _I]),
+    "go_domain_stage_launches": (_I, [_P, _P]),
+    "go_batch_run_events": (_I, [_P, _P, ctypes.c_uint32, _I, ctypes.c_double, _F, ctypes.c_double,
+                                 ctypes.c_uint32, _F, _F, _P, ctypes.c_size_t, _P, _P, _P]),
     "go_noise_lcg": (_I, [_P, _I, _I, _I, _I, _P, _I, _P, _I]),
     "go_noise_xorwow_state_bytes": (ctypes.c_size_t, []),
     "go_noise_xorwow_init": (_I, [_P, ctypes.c_uint64, _I, _P]),
@@ -283,6 +286,12 @@ class Domain:
         check(load().go_domain_status(self.handle, ctypes.byref(v), int(bool(clear))))
         return int(v.value)
 
+    def stage_launches(self):
+        """Kernel launches of the last RK stage (go_domain_stage_launches)."""
+        v = ctypes.c_int()
+        check(load().go_domain_stage_launches(self.handle, ctypes.byref(v)))
+        return int(v.value)
+
 
 class Batch:
     """Owner of one go_batch handle over a list of ``Domain`` objects."""
@@ -350,3 +359,17 @@ class Batch:
         n = ctypes.c_int()
         check(load().go_batch_graph_launch(self.handle, stream_handle(stream), ctypes.byref(n)))
         return n.value
+
+    def run_events(self, stream, first_event, n_events, interval, dt, courant, key0, std, corr_cells, scratch, t):
+        """go_batch_run_events; t: the members' model times (float64, member
+        order).  Returns (t after, steps per member, common dt after)."""
+        tt = np.ascontiguousarray(np.asarray(t, dtype=np.float64).reshape(-1))
+        assert tt.size == self.n
+        steps = ctypes.c_longlong()
+        dt_out = ctypes.c_float()
+        check(load().go_batch_run_events(self.handle, stream_handle(stream), int(first_event) & 0xFFFFFFFF,
+                                         int(n_events), float(interval), float(np.float32(dt)), float(courant),
+                                         int(key0) & 0xFFFFFFFF, float(std), float(corr_cells), ptr(scratch),
+                                         int(scratch.numel()), tt.ctypes.data_as(ctypes.c_void_p),
+                                         ctypes.byref(steps), ctypes.byref(dt_out)))
+        return tt, int(steps.value), np.float32(dt_out.value)

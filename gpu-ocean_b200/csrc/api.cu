@@ -58,12 +58,17 @@ int go_auto_rows(int nx, int ny, int shape) {
     return best;
 }
 
-// Default launch shape: a read-ahead shape (5, or 6 for widths that 96-wide
-// blocks cover with less waste) once the grid needs more than one wave of
-// blocks, where the ring hides the load latency; in a single wave the
-// register prefetch of 128 x 5 blocks (shape 4) is faster (measured on a
-// B200: 2048^2 and up gain 3-5% with the ring, 1024^2 and below lose 6-9%).
+// Default launch shape: the column-pair kernel (shape 8) from about 2400^2
+// cells up (measured on a B200, us per step, shapes 4 / 5 / 8: 2560^2
+// 308 / 291 / 269, 3072^2 429 / 399 / 385, 4096^2 720 / 685 / 627; at
+// 2048^2 the three are within 4% and below it the pair kernel's separate
+// boundary-frame launch does not pay).  Below that a read-ahead shape (5,
+// or 6 for widths that 96-wide blocks cover with less waste) once the grid
+// needs more than one wave of blocks, where the ring hides the load
+// latency; in a single wave the register prefetch of 128 x 5 blocks
+// (shape 4) is faster (1024^2 and below lose 6-9% with the ring).
 int go_auto_shape(int nx, int ny) {
+    if ((long long)nx * ny >= kPairAutoCells) return GO_SHAPE_PAIR;
     const int ring = go::ring_shape(go::shape_columns(5, nx), go::shape_columns(6, nx));
     const int rows = go_auto_rows(nx, ny, ring);
     const long long blocks = go::shape_columns(ring, nx) / go::shape_block_width(ring) * ((ny + rows - 1) / rows);
@@ -450,6 +455,12 @@ int go_domain_status(go_domain* d, uint32_t* status, int clear) {
     GO_CUDA(cudaMemcpy(&v, d->d_status, sizeof(v), cudaMemcpyDeviceToHost));
     *status = v;
     if (clear) GO_CUDA(cudaMemset(d->d_status, 0, sizeof(unsigned int)));
+    return GO_OK;
+}
+
+int go_domain_stage_launches(go_domain* d, int* launches) {
+    if (!d || !launches) return go_fail(GO_ERR_INVALID, "null argument");
+    *launches = d->stage_launches;
     return GO_OK;
 }
 

@@ -14,6 +14,34 @@
 
 using namespace go;
 
+// State of the device-driven ensemble event loop: per event every member
+// advances `interval` seconds of model time at the common dt with the
+// reference's step(t_end) rule (CDKLM16.py:494-598: whole steps while one
+// fits, then one short step), gets the model error of the event, and the
+// common dt = courant x the least CFL limit over the members.
+struct EventLoop {
+    double interval;     // model seconds per event
+    double t_now;        // model time into the current event
+    double courant;
+    float dt;            // common time step
+    int last;            // the short last step of the event is under way
+    uint32_t event;      // model-error event of the current event
+    int events_left;
+    long long steps;
+};
+
+// What a captured event-loop graph depends on besides the loop state.
+struct EventLoopKey {
+    uint32_t key0 = 0;
+    float std_dev = 0.0f, corr_cells = 0.0f;
+    const float* scratch = nullptr;
+    bool valid = false;
+    bool operator==(const EventLoopKey& o) const {
+        return valid && o.valid && key0 == o.key0 && std_dev == o.std_dev && corr_cells == o.corr_cells &&
+               scratch == o.scratch;
+    }
+};
+
 struct go_batch {
     int n = 0;
     std::vector<go_domain*> members;
@@ -43,6 +71,16 @@ struct go_batch {
     int grf_R = -1;
     size_t grf_scratch = 0;
     int grf_max_nx = 0, grf_max_ny = 0;
+    // device-driven event loop (go_batch_run_events): its state, the
+    // members' model times, the CFL limits, the graph and what it captured
+    EventLoop* d_loop = nullptr;
+    double* d_t = nullptr;
+    unsigned int* d_cfl = nullptr;
+    cudaStream_t loop_side = nullptr;
+    cudaGraph_t loop_graph = nullptr;
+    cudaGraphExec_t loop_exec = nullptr;
+    EventLoopKey loop_key;
+    std::vector<double> loop_t;
 };
 
 namespace {
@@ -251,6 +289,230 @@ void drop_graph(go_batch* b) {
     b->graph_exec = nullptr;
     b->graph = nullptr;
     b->graph_steps = 0;
+    if (b->loop_exec) cudaGraphExecDestroy(b->loop_exec);
+    if (b->loop_graph) cudaGraphDestroy(b->loop_graph);
+    b->loop_exec = nullptr;
+    b->loop_graph = nullptr;
+    b->loop_key.valid = false;
+}
+
+// Launches of go_batch_max_dt: every member's CFL limit (float bits) into out.
+int launch_max_dt(go_batch* b, cudaStream_t s, unsigned int* out) {
+    unsigned int init_bits;
+    memcpy(&init_bits, &kRefFltMax, sizeof(init_bits));
+    k_fill_members<<<(b->n + 255) / 256, 256, 0, s>>>(out, init_bits, b->n);
+    long long most = 0;
+    for (const go_domain* d : b->members) most = std::max(most, (long long)d->k.nx * d->k.ny);
+    // about 4 blocks per SM in all, spread over the members
+    const int per_member = (int)std::max(1LL, std::min((most + 255) / 256, (148LL * 4 + b->n - 1) / b->n));
+    k_batch_max_dt<<<dim3(per_member, b->n), 256, 0, s>>>(b->d_args, out);
+    GO_CUDA(cudaGetLastError());
+    return GO_OK;
+}
+
+// Model-error descriptors of the members (their eta buffers, sizes,
+// boundary kinds, member keys, scratch offsets) for filter radius W.R.
+int grf_prepare(go_batch* b, const GrfWeights& W) {
+    if (b->d_grf && b->grf_R == W.R) return GO_OK;
+    std::vector<GrfMember> h(b->n);
+    size_t off = 0;
+    int mx = 0, my = 0;
+    for (int m = 0; m < b->n; ++m) {
+        const Scheme& k = b->members[m]->k;
+        h[m].eta = const_cast<float*>(b->args[2 * m].eta_in);
+        h[m].pitch = b->args[2 * m].pin;
+        h[m].nx = k.nx;
+        h[m].ny = k.ny;
+        h[m].periodic_x = k.bcE == kPeriodic;
+        h[m].periodic_y = k.bcN == kPeriodic;
+        h[m].key1 = (uint32_t)m;
+        h[m].tmp_off = off;
+        off += grf_member_scratch(k.nx, k.ny, W.R);
+        mx = max(mx, k.nx);
+        my = max(my, k.ny);
+    }
+    if (!b->d_grf) GO_CUDA(cudaMalloc(&b->d_grf, sizeof(GrfMember) * b->n));
+    GO_CUDA(cudaMemcpy(b->d_grf, h.data(), sizeof(GrfMember) * b->n, cudaMemcpyHostToDevice));
+    b->grf_R = W.R;
+    b->grf_scratch = off;
+    b->grf_max_nx = mx;
+    b->grf_max_ny = my;
+    return GO_OK;
+}
+
+// ---- device-driven event loop ----------------------------------------------
+// The step of the event that starts at t_now: the common dt, or the model
+// time left in the event rounded to float32 when that is shorter, which
+// makes it the event's last step (CDKLM16.py:508-517: local_dt =
+// float32(min(dt, float32(t_end - t_now))), the whole-step loop stops at the
+// first step shorter than dt).
+__device__ __forceinline__ float event_step_dt(EventLoop* L) {
+    const float rem = __double2float_rn(__dsub_rn(L->interval, L->t_now));
+    const float local = fminf(L->dt, rem);
+    if (local != L->dt) L->last = 1;
+    return local;
+}
+
+// Start of an event: its first step's dt into every member's dt; the step
+// loop's condition set.
+__global__ void k_event_begin(EventLoop* L, float* __restrict__ dts, int n, cudaGraphConditionalHandle steps) {
+    __shared__ float sdt;
+    if (threadIdx.x == 0) {
+        L->t_now = 0.0;
+        L->last = 0;
+        sdt = event_step_dt(L);
+        cudaGraphSetConditional(steps, 1u);
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < n; m += blockDim.x) dts[m] = sdt;
+}
+
+// After a step: the members' model times advance by the dt they stepped
+// with (float64 sums, as CDKLM16.step keeps t), then the next step's dt or
+// the end of the event (the step loop's condition).
+__global__ void k_step_done(EventLoop* L, float* __restrict__ dts, double* __restrict__ t, int n,
+                            cudaGraphConditionalHandle steps) {
+    __shared__ float snext;
+    __shared__ int scont;
+    for (int m = threadIdx.x; m < n; m += blockDim.x) t[m] = __dadd_rn(t[m], (double)dts[m]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        L->steps += 1;
+        int cont = 0;
+        float next = 0.0f;
+        if (!L->last) {
+            L->t_now = __dadd_rn(L->t_now, (double)L->dt);
+            if (L->t_now < L->interval) {
+                next = event_step_dt(L);
+                cont = 1;
+            }
+        }
+        snext = next;
+        scont = cont;
+        cudaGraphSetConditional(steps, (unsigned)cont);
+    }
+    __syncthreads();
+    if (scont)
+        for (int m = threadIdx.x; m < n; m += blockDim.x) dts[m] = snext;
+}
+
+// End of an event, after its model error and the members' CFL limits: the
+// common dt = float32(courant x least limit) (float64 product, as the host
+// computes it), the next event, the event loop's condition.
+__global__ void k_event_end(EventLoop* L, const unsigned int* __restrict__ cfl, float* __restrict__ dts, int n,
+                            cudaGraphConditionalHandle events) {
+    __shared__ float red[256];
+    float mn = kRefFltMax;
+    for (int m = threadIdx.x; m < n; m += blockDim.x) mn = fminf(mn, __uint_as_float(cfl[m]));
+    red[threadIdx.x] = mn;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] = fminf(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float dt = __double2float_rn(__dmul_rn(L->courant, (double)red[0]));
+        L->dt = dt;
+        L->event += 1;
+        L->events_left -= 1;
+        cudaGraphSetConditional(events, L->events_left > 0 ? 1u : 0u);
+        red[0] = dt;
+    }
+    __syncthreads();
+    const float dt = red[0];
+    for (int m = threadIdx.x; m < n; m += blockDim.x) dts[m] = dt;
+}
+
+// The graph of the event loop: WHILE (events left) { event begin; WHILE
+// (steps left) { stage 0; stage 1; step done }; model error; CFL limits;
+// event end }.  s captures the event body, b->loop_side the step body.
+int build_event_graph(go_batch* b, cudaStream_t s, const GrfWeights& W, uint32_t key0, float std_dev,
+                      float* scratch) {
+    cudaGraph_t g = nullptr;
+    GO_CUDA(cudaGraphCreate(&g, 0));
+    int rc = GO_OK;
+    bool capturing_s = false, capturing_side = false;
+    auto fail = [&](cudaError_t e, const char* what) {
+        if (rc == GO_OK) rc = go_fail(GO_ERR_CUDA, "event loop graph: %s: %s", what, cudaGetErrorString(e));
+    };
+    do {
+        cudaGraphConditionalHandle h_events, h_steps;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&h_events, g, 1u, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) { fail(e, "handle"); break; }
+        cudaGraphNodeParams pe = {cudaGraphNodeTypeConditional};
+        pe.conditional.handle = h_events;
+        pe.conditional.type = cudaGraphCondTypeWhile;
+        pe.conditional.size = 1;
+        cudaGraphNode_t n_events;
+        e = cudaGraphAddNode(&n_events, g, nullptr, 0, &pe);
+        if (e != cudaSuccess) { fail(e, "event loop node"); break; }
+        cudaGraph_t body_events = pe.conditional.phGraph_out[0];
+        e = cudaGraphConditionalHandleCreate(&h_steps, body_events, 1u, 0);
+        if (e != cudaSuccess) { fail(e, "step handle"); break; }
+
+        e = cudaStreamBeginCaptureToGraph(s, body_events, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { fail(e, "capture"); break; }
+        capturing_s = true;
+        k_event_begin<<<1, 256, 0, s>>>(b->d_loop, b->d_dt, b->n, h_steps);
+        cudaStreamCaptureStatus st;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        e = cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &ndeps);
+        if (e != cudaSuccess) { fail(e, "capture info"); break; }
+        cudaGraphNodeParams ps = {cudaGraphNodeTypeConditional};
+        ps.conditional.handle = h_steps;
+        ps.conditional.type = cudaGraphCondTypeWhile;
+        ps.conditional.size = 1;
+        cudaGraphNode_t n_steps;
+        e = cudaGraphAddNode(&n_steps, cg, deps, ndeps, &ps);
+        if (e != cudaSuccess) { fail(e, "step loop node"); break; }
+        e = cudaStreamUpdateCaptureDependencies(s, &n_steps, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) { fail(e, "capture dependencies"); break; }
+
+        e = cudaStreamBeginCaptureToGraph(b->loop_side, ps.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { fail(e, "step body capture"); break; }
+        capturing_side = true;
+        rc = batch_launch(b, 0, b->loop_side);
+        if (!rc) rc = batch_launch(b, 1, b->loop_side);
+        if (rc) break;
+        k_step_done<<<1, 256, 0, b->loop_side>>>(b->d_loop, b->d_dt, b->d_t, b->n, h_steps);
+        cudaGraph_t done = nullptr;
+        capturing_side = false;
+        e = cudaStreamEndCapture(b->loop_side, &done);
+        if (e != cudaSuccess) { fail(e, "step body capture end"); break; }
+
+        GrfMember none;
+        memset(&none, 0, sizeof(none));
+        rc = grf_launch(b->d_grf, none, b->n, b->grf_max_nx, b->grf_max_ny, key0, 0u, std_dev, W, scratch, s,
+                        &b->d_loop->event);
+        if (!rc) rc = launch_max_dt(b, s, b->d_cfl);
+        if (rc) break;
+        k_event_end<<<1, 256, 0, s>>>(b->d_loop, b->d_cfl, b->d_dt, b->n, h_events);
+        capturing_s = false;
+        e = cudaStreamEndCapture(s, &done);
+        if (e != cudaSuccess) { fail(e, "event body capture end"); break; }
+        e = cudaGraphInstantiate(&b->loop_exec, g, 0);
+        if (e != cudaSuccess) { fail(e, "instantiate"); break; }
+    } while (false);
+    if (capturing_side) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(b->loop_side, &junk);
+    }
+    if (capturing_s) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(s, &junk);
+    }
+    if (rc) {
+        cudaGetLastError();
+        if (b->loop_exec) cudaGraphExecDestroy(b->loop_exec);
+        b->loop_exec = nullptr;
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    b->loop_graph = g;
+    return GO_OK;
 }
 
 }  // namespace
@@ -292,6 +554,13 @@ int go_batch_create(go_domain* const* members, int n, go_batch** out) {
             tiles += shape_columns(ring, k.nx) / shape_block_width(ring) * ((k.ny + b->rows - 1) / b->rows);
         }
         b->shape = tiles > 148LL * shape_blocks_per_sm(ring) ? ring : 4;
+        // the column-pair kernel once the batch holds a few million cells
+        // (measured on a B200, us per step with the ring shape / the pair
+        // shape: 100 members of 512^2 1424 / 1212; 64 domains of 128..1024
+        // squared cells, 20.5 M cells, 1136 / 946)
+        long long cells = 0;
+        for (int m = 0; m < n; ++m) cells += (long long)members[m]->k.nx * members[m]->k.ny;
+        if (cells >= kPairAutoBatchCells) b->shape = GO_SHAPE_PAIR;
     }
     for (int m = 0; m < n; ++m) {
         const go_domain* d = members[m];
@@ -333,6 +602,10 @@ int go_batch_destroy(go_batch* b) {
     cudaFree(b->d_dt);
     cudaFree(b->d_tiles);
     cudaFree(b->d_grf);
+    cudaFree(b->d_loop);
+    cudaFree(b->d_t);
+    cudaFree(b->d_cfl);
+    if (b->loop_side) cudaStreamDestroy(b->loop_side);
     delete b;
     return GO_OK;
 }
@@ -453,18 +726,7 @@ int go_batch_max_dt(go_batch* b, void* stream, float* dt_dev) {
     if (!b || !dt_dev) return go_fail(GO_ERR_INVALID, "null argument");
     int rc = batch_commit(b);
     if (rc) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
-    unsigned int* out = reinterpret_cast<unsigned int*>(dt_dev);
-    unsigned int init_bits;
-    memcpy(&init_bits, &kRefFltMax, sizeof(init_bits));
-    k_fill_members<<<(b->n + 255) / 256, 256, 0, s>>>(out, init_bits, b->n);
-    long long most = 0;
-    for (const go_domain* d : b->members) most = std::max(most, (long long)d->k.nx * d->k.ny);
-    // about 4 blocks per SM in all, spread over the members
-    const int per_member = (int)std::max(1LL, std::min((most + 255) / 256, (148LL * 4 + b->n - 1) / b->n));
-    k_batch_max_dt<<<dim3(per_member, b->n), 256, 0, s>>>(b->d_args, out);
-    GO_CUDA(cudaGetLastError());
-    return GO_OK;
+    return launch_max_dt(b, (cudaStream_t)stream, reinterpret_cast<unsigned int*>(dt_dev));
 }
 
 int go_batch_status(go_batch* b, uint32_t* status_host, int clear) {
@@ -493,37 +755,81 @@ int go_batch_grf_perturb(go_batch* b, void* stream, uint32_t key0, uint32_t even
     rc = grf_weights(corr_cells, &W);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
-    if (!b->d_grf || b->grf_R != W.R) {
-        std::vector<GrfMember> h(b->n);
-        size_t off = 0;
-        int mx = 0, my = 0;
-        for (int m = 0; m < b->n; ++m) {
-            const Scheme& k = b->members[m]->k;
-            h[m].eta = const_cast<float*>(b->args[2 * m].eta_in);
-            h[m].pitch = b->args[2 * m].pin;
-            h[m].nx = k.nx;
-            h[m].ny = k.ny;
-            h[m].periodic_x = k.bcE == kPeriodic;
-            h[m].periodic_y = k.bcN == kPeriodic;
-            h[m].key1 = (uint32_t)m;
-            h[m].tmp_off = off;
-            off += grf_member_scratch(k.nx, k.ny, W.R);
-            mx = max(mx, k.nx);
-            my = max(my, k.ny);
-        }
-        if (!b->d_grf) GO_CUDA(cudaMalloc(&b->d_grf, sizeof(GrfMember) * b->n));
-        GO_CUDA(cudaMemcpy(b->d_grf, h.data(), sizeof(GrfMember) * b->n, cudaMemcpyHostToDevice));
-        b->grf_R = W.R;
-        b->grf_scratch = off;
-        b->grf_max_nx = mx;
-        b->grf_max_ny = my;
-    }
+    rc = grf_prepare(b, W);
+    if (rc) return rc;
     if (scratch_floats < b->grf_scratch)
         return go_fail(GO_ERR_INVALID, "scratch holds %zu floats, the batch needs %zu", scratch_floats,
                        b->grf_scratch);
     GrfMember none;
     memset(&none, 0, sizeof(none));
     return grf_launch(b->d_grf, none, b->n, b->grf_max_nx, b->grf_max_ny, key0, event, std_dev, W, scratch, s);
+}
+
+int go_batch_run_events(go_batch* b, void* stream, uint32_t first_event, int n_events, double interval, float dt,
+                        double courant, uint32_t key0, float std_dev, float corr_cells, float* scratch,
+                        size_t scratch_floats, double* t_members, long long* steps_out, float* dt_out) {
+    if (!b || !scratch || !t_members) return go_fail(GO_ERR_INVALID, "null argument");
+    if (n_events < 0 || !(interval > 0.0) || !(dt > 0.0f) || !(courant > 0.0))
+        return go_fail(GO_ERR_INVALID, "n_events >= 0, interval > 0, dt > 0 and courant > 0");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (s == nullptr) return go_fail(GO_ERR_INVALID, "the event loop needs a non-default stream");
+    int rc = batch_commit(b);
+    if (rc) return rc;
+    GrfWeights W;
+    rc = grf_weights(corr_cells, &W);
+    if (rc) return rc;
+    rc = grf_prepare(b, W);
+    if (rc) return rc;
+    if (scratch_floats < b->grf_scratch)
+        return go_fail(GO_ERR_INVALID, "scratch holds %zu floats, the batch needs %zu", scratch_floats,
+                       b->grf_scratch);
+    if (steps_out) *steps_out = 0;
+    if (dt_out) *dt_out = dt;
+    if (n_events == 0) return GO_OK;
+    if (!b->d_loop) {
+        GO_CUDA(cudaMalloc(&b->d_loop, sizeof(EventLoop)));
+        GO_CUDA(cudaMalloc(&b->d_t, sizeof(double) * b->n));
+        GO_CUDA(cudaMalloc(&b->d_cfl, sizeof(unsigned int) * b->n));
+        GO_CUDA(cudaStreamCreateWithFlags(&b->loop_side, cudaStreamNonBlocking));
+    }
+    EventLoopKey key;
+    key.key0 = key0;
+    key.std_dev = std_dev;
+    key.corr_cells = corr_cells;
+    key.scratch = scratch;
+    key.valid = true;
+    if (!(b->loop_key == key) || !b->loop_exec) {
+        if (b->loop_exec) cudaGraphExecDestroy(b->loop_exec);
+        if (b->loop_graph) cudaGraphDestroy(b->loop_graph);
+        b->loop_exec = nullptr;
+        b->loop_graph = nullptr;
+        rc = build_event_graph(b, s, W, key0, std_dev, scratch);
+        if (rc) return rc;
+        b->loop_key = key;
+    }
+    EventLoop L;
+    memset(&L, 0, sizeof(L));
+    L.interval = interval;
+    L.courant = courant;
+    L.dt = dt;
+    L.event = first_event;
+    L.events_left = n_events;
+    b->loop_t.assign(t_members, t_members + b->n);
+    GO_CUDA(cudaMemcpyAsync(b->d_loop, &L, sizeof(L), cudaMemcpyHostToDevice, s));
+    GO_CUDA(cudaMemcpyAsync(b->d_t, b->loop_t.data(), sizeof(double) * b->n, cudaMemcpyHostToDevice, s));
+    GO_CUDA(cudaGraphLaunch(b->loop_exec, s));
+    GO_CUDA(cudaMemcpyAsync(&L, b->d_loop, sizeof(L), cudaMemcpyDeviceToHost, s));
+    GO_CUDA(cudaMemcpyAsync(b->loop_t.data(), b->d_t, sizeof(double) * b->n, cudaMemcpyDeviceToHost, s));
+    GO_CUDA(cudaStreamSynchronize(s));
+    std::copy(b->loop_t.begin(), b->loop_t.end(), t_members);
+    for (int m = 0; m < b->n; ++m) {
+        b->dt[m] = L.dt;
+        b->args[2 * m].dt = L.dt;
+        b->args[2 * m + 1].dt = L.dt;
+    }
+    if (steps_out) *steps_out = L.steps;
+    if (dt_out) *dt_out = L.dt;
+    return GO_OK;
 }
 
 }  // extern "C"

@@ -337,13 +337,12 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     int qcx = cl, qcy = cl + 1;
     float husx = 1.0f, husy = 1.0f;
     int hc0 = cl, hc1 = cl + 1, hc2 = cl + 2;
-    // TMA path: the last column block at a periodic or open east side can
-    // reach past the array; its prime loads pairs from a clamped column
-    // (lanes past column nx+3 are never written nor read by a written
-    // cell).  A pair starting at column nx+3 (odd nx) ends in the row's
-    // padding: TMA launches have pitches of whole 16-byte units, so the
-    // padding exists.  (The ring's tile loads fill such columns with zeros.)
-    const int clq = !EDGE ? min(cl, k.nx + 2 + (k.nx & 1)) : cl;   // even, pair within the row's pitch
+    // TMA path: the last column block at a periodic or open east side
+    // reaches past the array.  Its prime reads those columns past the end of
+    // the row, into the next row of the same allocation (the prime reads Q
+    // rows up to ny and corner rows up to ny+1, below the last ones); the
+    // values feed only lanes that are never written nor read by a written
+    // cell.  The ring's tile loads fill such columns with zeros.
     if (EDGE) {
         auto mirror_col = [&](int c, int& qc, float& s) {
             qc = min(c, k.nx + 3);
@@ -386,9 +385,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         const int rr = mirror_row(r, hv_sgn);
         const size_t o = (size_t)rr * a.pin;
         if (!EDGE && TMA) {   // 8-byte aligned pairs
-            e = __ldg(reinterpret_cast<const float2*>(a.eta_in + o + clq));
-            hu = __ldg(reinterpret_cast<const float2*>(a.hu_in + o + clq));
-            hv = __ldg(reinterpret_cast<const float2*>(a.hv_in + o + clq));
+            e = __ldg(reinterpret_cast<const float2*>(a.eta_in + o + cl));
+            hu = __ldg(reinterpret_cast<const float2*>(a.hu_in + o + cl));
+            hv = __ldg(reinterpret_cast<const float2*>(a.hv_in + o + cl));
         } else {
             e = make_float2(__ldg(a.eta_in + o + qcx), __ldg(a.eta_in + o + qcy));
             hu = make_float2(__ldg(a.hu_in + o + qcx), __ldg(a.hu_in + o + qcy));
@@ -407,9 +406,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     auto load_h = [&](int r, float2& Ha, float2& Hb) {
         const float* row = a.Hi + (size_t)r * a.phi;
         float h2;
-        if (!EDGE && TMA) {   // corners 0 .. nx+4 of the row
-            Ha = __ldg(reinterpret_cast<const float2*>(row + clq));
-            h2 = __ldg(row + min(clq + 2, k.nx + 4));
+        if (!EDGE && TMA) {
+            Ha = __ldg(reinterpret_cast<const float2*>(row + cl));
+            h2 = __ldg(row + cl + 2);
         } else {
             Ha = make_float2(__ldg(row + hc0), __ldg(row + hc1));
             h2 = __ldg(row + hc2);

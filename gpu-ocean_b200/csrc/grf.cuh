@@ -32,9 +32,11 @@ int grf_weights(float corr_cells, GrfWeights* W);
 inline size_t grf_member_scratch(int nx, int ny, int R) { return (size_t)(ny + 2 * R) * (size_t)nx; }
 
 // eta += std_dev * field for n members (members == nullptr: the single
-// member passed by value), key (key0, member.key1), counter event.
+// member passed by value), key (key0, member.key1), counter event -- or,
+// when event_dev is given, the event the device holds there when the
+// kernels run (a launch captured into a device-driven event loop).
 int grf_launch(const GrfMember* d_members, const GrfMember& single, int n_members, int max_nx, int max_ny,
                uint32_t key0, uint32_t event, float std_dev, const GrfWeights& W, float* scratch,
-               cudaStream_t s);
+               cudaStream_t s, const uint32_t* event_dev = nullptr);
 
 }  // namespace go

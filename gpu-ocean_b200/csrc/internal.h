@@ -33,6 +33,7 @@ struct go_domain {
     cudaStream_t side;
     cudaEvent_t ev_fork, ev_join;
     int own_side;            // go_domain_create's handles may create them (not the allocation-free step)
+    int stage_launches;      // kernel launches the last RK stage issued
 };
 
 // Records the message of a failed call (go_last_error) and returns code.

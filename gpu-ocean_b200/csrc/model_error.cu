@@ -60,9 +60,11 @@ __device__ __forceinline__ float grf_normal(uint32_t l, uint32_t event, uint2 ke
 // x pass: one block per (noise row, chunk of kChunk columns); the normals of
 // the chunk plus R columns either side (periodic in x) in shared memory.
 __global__ void k_grf_xpass(const GrfMember* __restrict__ members, const GrfMember single, uint32_t key0,
-                            uint32_t event, float* __restrict__ scratch, const GrfWeights W) {
+                            uint32_t event_arg, const uint32_t* __restrict__ event_dev, float* __restrict__ scratch,
+                            const GrfWeights W) {
     __shared__ float row[kChunk + kGrfMaxTaps];
     const GrfMember M = members ? members[blockIdx.z] : single;
+    const uint32_t event = event_dev ? *event_dev : event_arg;
     const int R = W.R;
     const int yext = blockIdx.y;
     const int x0 = blockIdx.x * kChunk;
@@ -142,10 +144,10 @@ int grf_weights(float corr_cells, GrfWeights* W) {
 
 int grf_launch(const GrfMember* d_members, const GrfMember& single, int n_members, int max_nx, int max_ny,
                uint32_t key0, uint32_t event, float std_dev, const GrfWeights& W, float* scratch,
-               cudaStream_t s) {
+               cudaStream_t s, const uint32_t* event_dev) {
     if (n_members < 1) return GO_OK;
     const dim3 gx((max_nx + kChunk - 1) / kChunk, max_ny + 2 * W.R, n_members);
-    k_grf_xpass<<<gx, 256, 0, s>>>(d_members, single, key0, event, scratch, W);
+    k_grf_xpass<<<gx, 256, 0, s>>>(d_members, single, key0, event, event_dev, scratch, W);
     const dim3 b(32, 8), gy((max_nx + 31) / 32, (max_ny + kYTile - 1) / kYTile, n_members);
     k_grf_ypass<<<gy, b, 0, s>>>(d_members, single, std_dev, scratch, W);
     GO_CUDA(cudaGetLastError());

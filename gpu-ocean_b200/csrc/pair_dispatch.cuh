@@ -23,6 +23,10 @@ constexpr int kPairMinBlocksFrame = 6;
 constexpr int kPairSlots = 2;
 constexpr int kPairUnroll = 1;
 constexpr int kPairFrameRows = 8;
+// default-shape thresholds: a grid of at least this many cells, a batch
+// whose members hold at least this many together
+constexpr long long kPairAutoCells = 2400LL * 2400LL;
+constexpr long long kPairAutoBatchCells = 4LL << 20;
 
 // The block grid of an nx x ny domain (see PairGrid): the region of TMA
 // strips of `rows` rows, empty when `tma` is false (every block then takes

@@ -138,9 +138,11 @@ int go_launch_pair(go_domain* d, cudaStream_t s, const StageArgs& a, const PairM
         GO_CUDA(cudaEventRecord(d->ev_join, d->side));
         GO_CUDA(cudaStreamWaitEvent(s, d->ev_join, 0));
     }
+    d->stage_launches = (n_frame > 0) + (n_int > 0);
     if (n_int > 0 && a.k.bcE == kPeriodic) {
         // the region's strips leave the periodic images of their cells to this copy
         GO_CUDA(pair_launch_periodic_columns(nullptr, 1, a.k.ny, 0, a, s));
+        d->stage_launches += 1;
     }
     return GO_OK;
 }

@@ -49,6 +49,7 @@ int go_prepare_stage(go_domain* d, const StageArgs& a, PreparedStage* p) {
 
 int go_launch_prepared(go_domain* d, cudaStream_t s, const PreparedStage& p) {
     if (p.pair) return go_launch_pair(d, s, p.a, p.mp, p.tma);
+    d->stage_launches = 1;
     SingleLaunch L{&p.a, s};
     const cudaError_t e = dispatch_variant(L, go_variant(d));
     if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "stage launch failed: %s", cudaGetErrorString(e));

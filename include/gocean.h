@@ -569,9 +569,40 @@ int go_batch_grf_perturb(go_batch* b, void* stream, uint32_t key0, uint32_t even
                          float std_dev, float corr_cells, float* scratch,
                          size_t scratch_floats);
 
+/* The ensemble event loop on the device, in one launch of a CUDA graph with
+ * two nested WHILE nodes: for events e = first_event .. first_event +
+ * n_events - 1, every member advances `interval` model seconds at the
+ * common dt by the reference's step(t_end) rule (whole steps while one
+ * fits, then one step of float32(t_end - t_now); CDKLM16.py:494-598), gets
+ * go_batch_grf_perturb's model error (key0, e, std_dev, corr_cells), and
+ * the common dt becomes float32(courant x the least go_batch_max_dt limit)
+ * -- what the reference's ensembles do member by member from the host
+ * (OceanNoiseEnsemble.py:506-531), with no host round trip per event.
+ * dt is the members' common dt on entry; t_members (n doubles, member
+ * order) their model times, advanced in place by the float64 sum of the
+ * steps each took; *steps_out the steps per member, *dt_out the common dt
+ * on return (also the members' batch dt).  Every member sees the same
+ * steps and states, bit for bit, as the host loop of go_batch_step,
+ * go_batch_grf_perturb, go_batch_max_dt and go_batch_set_dt.  The graph is
+ * captured on the first call and reused while key0, std_dev, corr_cells,
+ * scratch and the batch's members and launch stay the same; scratch must
+ * stay allocated while it is in use.  Wind stays at the members' bound
+ * wind_stress_t.  Synchronous. */
+int go_batch_run_events(go_batch* b, void* stream, uint32_t first_event, int n_events,
+                        double interval, float dt, double courant, uint32_t key0,
+                        float std_dev, float corr_cells, float* scratch,
+                        size_t scratch_floats, double* t_members, long long* steps_out,
+                        float* dt_out);
+
 /* Device status word (GO_STATUS_* bits) accumulated by the step kernels;
  * synchronous read, optionally clearing it. */
 int go_domain_status(go_domain* d, uint32_t* status, int clear);
+
+/* Kernel launches the domain's last RK stage issued (1 for launch shapes
+ * 0..7; for the column-pair shape the boundary frame, the interior region
+ * and, at periodic east/west sides, the ghost-column copy; 0 before the
+ * first step). */
+int go_domain_stage_launches(go_domain* d, int* launches);
 
 /* Status words of every member of a batch (n values to status_host, member
  * order): each member's step kernels write only its own word, so a member

@@ -116,3 +116,32 @@ def test_event_loop_batched_equals_plain_loop(ctx):
     for x, y in zip(a, p):
         assert np.array_equal(np.stack(x.download()), np.stack(y.download()))
         assert x.t == y.t
+
+
+@pytest.mark.parametrize("launch,interval", [(None, 60.0), ((8, 12, 0), 45.5), ((5, 16, 0), 3.0)])
+def test_device_event_loop_equals_host_loop(ctx, launch, interval):
+    """go_batch_run_events (one graph launch, nested WHILE nodes) == the
+    host-driven event loop: states, model times, step counts and the
+    common dt, bit for bit; the graph is reused across calls.  An interval
+    shorter than dt makes every event one short step."""
+    def members():
+        sims = [flat_sim(ctx, 96, 80) for _ in range(6)]
+        for m, s in enumerate(sims):
+            ModelError.initial_perturbation(s, m)
+        return sims
+    runs = []
+    for device in (True, False):
+        sims = members()
+        b = BatchedEnsemble.BatchedCDKLM16(sims, graph_steps=4, launch=launch)
+        b.update_dt(0.7)
+        steps = b.run_events(1, 2, interval=interval, device_loop=device)
+        steps += b.run_events(3, 3, interval=interval, device_loop=device)
+        torch.cuda.synchronize()
+        runs.append((steps, sims, float(np.float32(sims[0].dt))))
+    (sd, dev, dtd), (sh, host, dth) = runs
+    assert sd == sh and dtd == dth
+    if interval < 10.0:   # dt is above 10 s on this grid: every event is one short step
+        assert sd == 5
+    for x, y in zip(dev, host):
+        assert np.array_equal(np.stack(x.download()), np.stack(y.download()))
+        assert x.t == y.t and x.num_iterations == y.num_iterations
