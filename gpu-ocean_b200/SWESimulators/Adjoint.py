@@ -20,9 +20,10 @@ runs whose full trajectory does not fit.
 the wind) and ``CDKLM16Step`` (one RK2 step) wrap the problem in
 ``torch.autograd.Function`` objects.
 
-Scope: north-up grids, no land, no cell shallower than the
-desingularisation depth (the adjoint kernel flags GO_STATUS_ADJ_SCOPE
-otherwise and ``MisfitProblem`` raises).
+Scope: north-up grids with wall and periodic boundaries; land and cells
+shallower than the desingularisation depth are differentiated through the
+branch the forward takes (land and dry cells are constants, desingularised
+cells use u = hu / D(h)).
 """
 
 import ctypes
@@ -30,6 +31,13 @@ import ctypes
 import numpy as np
 
 from . import _native
+
+
+def _has_land(sim):
+    """Whether any bathymetry corner of the simulator is land (the forward
+    then runs its land-aware kernels, as CDKLM16 does)."""
+    Bi = sim.downloadBathymetry()[0]
+    return bool(np.any(np.abs(Bi.astype(np.float32) - np.float32(sim.bathymetry.mask_value)) < 1e-3))
 
 
 def _round_up(n, m):
@@ -147,9 +155,7 @@ class MisfitProblem:
             raise NotImplementedError("the adjoint is built for north-up grids only")
         if max(d.bc_north, d.bc_east, d.bc_south, d.bc_west) > 2:
             raise NotImplementedError("the adjoint is built for wall and periodic boundaries only")
-        Bm = sim.downloadBathymetry()[1]
-        if np.any(np.abs(Bm - np.float32(sim.bathymetry.mask_value)) < 1e-3):
-            raise NotImplementedError("the adjoint is built for bathymetry without land")
+        has_land = _has_land(sim)
         self.sim = sim
         self.nx, self.ny = int(sim.nx), int(sim.ny)
         self.n_steps = int(n_steps)
@@ -169,7 +175,7 @@ class MisfitProblem:
                                      bc=(d.bc_north, d.bc_east, d.bc_south, d.bc_west),
                                      friction_law=d.friction_law, north=(d.north_x, d.north_y))
         self.domain.set_coriolis(sim.coriolis_rows)
-        self.domain.set_land(False)
+        self.domain.set_land(has_land)
         self.Hi = sim.bathymetry.Bi.tensor
         self.Hi_pitch = int(sim.bathymetry.Bi.pitch)
         self.land = float(sim.bathymetry.mask_value)
@@ -348,8 +354,6 @@ class MisfitProblem:
                 self._obs_adjoint(self.qn, 0, 0)
         self._rstream.synchronize()
         self.stream.synchronize()
-        if self.domain.status() & _native.GO_STATUS_ADJ_SCOPE:
-            raise NotImplementedError("the adjoint met land or a cell shallower than desing_eps")
         g = lam.interior(0).clone()
         return g[0], g[1], g[2], lw[0, :, :self.nx].clone(), lw[1, :, :self.nx].clone()
 
@@ -516,7 +520,7 @@ class BatchedMisfitProblem:
                                  bc=(d.bc_north, d.bc_east, d.bc_south, d.bc_west), friction_law=d.friction_law,
                                  north=(d.north_x, d.north_y))
             dom.set_coriolis(s.coriolis_rows)
-            dom.set_land(False)
+            dom.set_land(_has_land(s))
             dom.set_wind_field(self.wind[m, 0], self.wind[m, 0], self.wind[m, 1], self.wind[m, 1])
             self.domains.append(dom)
         self.batch = _native.Batch(self.domains)
@@ -625,9 +629,6 @@ class BatchedMisfitProblem:
                 self.h0.t.copy_(self.snap[0])
                 self._obs_adjoint(0)
         self.stream.synchronize()
-        for dom in self.domains:
-            if dom.status() & _native.GO_STATUS_ADJ_SCOPE:
-                raise NotImplementedError("the adjoint met land or a cell shallower than desing_eps")
         return (self.J_dev.cpu().numpy(), self.lam.interior().clone(),
                 self.lam_wind[:, :, :, :nx].clone())
 

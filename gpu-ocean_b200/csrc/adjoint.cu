@@ -13,9 +13,14 @@
 // choice of the transverse flux, the dry clamp) are differentiated as the
 // subgradient of the branch the forward recomputation takes.
 //
-// Scope: north-up grids (angle 0), no land and no cell shallower than the
-// desingularisation depth (0.1 m).  A tile that meets a cell outside that
-// scope sets GO_STATUS_ADJ_SCOPE in the domain's status word.
+// Scope: north-up grids (angle 0), with land and shallow cells.  The cell
+// state map has four branches (CDKLM16_kernel.cu:551-602): land (all four
+// corners land: the dry flag, a constant), dry (h <= cutoff: a constant
+// state), desingularised (cutoff < h < desing_eps: u = hu / D(h) with
+// D(h) = h^2 / (2 eps) + eps / 2, common.cu:822-824) and wet (u = hu / h);
+// the constant branches pass no adjoint to their input.  A face with a land
+// cell on either side carries no flux (CDKLM16_kernel.cu:271-273) and passes
+// none either; corners on land read as the dry flag, as the forward's do.
 //
 // Arithmetic: this unit is compiled with FMA contraction (the adjoint is
 // compared with FP64 derivatives, not bit for bit), but every value a branch
@@ -95,6 +100,57 @@ __device__ __forceinline__ float pot_coef(int br, int pos, float theta_g, float 
 }
 
 __device__ __forceinline__ float flip(bool f) { return f ? -1.0f : 1.0f; }
+
+struct Trip3 { float a, b, c; };
+
+// Cell classes of the state map (2 bits).
+enum { kCellWet = 0, kCellDesing = 1, kCellDry = 2, kCellLand = 3 };
+
+// Denominator of desingularize (common.cu:822-824) and its derivative in h:
+// D = max(min(a, eps), |h|) with a = h^2/(2 eps) + eps/2, which is a for
+// |h| <= eps (then a <= eps and a >= |h|), and |h| beyond.
+__device__ __forceinline__ float desing_den(float h, float eps) {
+    const float a = (float)((double)(h * h / (2.0f * eps)) + 0.5 * (double)eps);
+    return fmaxf(fminf(a, eps), fabsf(h));
+}
+__device__ __forceinline__ float desing_den_dh(float h, float eps) {
+    return (fabsf(h) <= eps) ? h / eps : (h < 0.0f ? -1.0f : 1.0f);
+}
+
+// Cell state (e, u, v) and class of one cell from its input (e, hu, hv) and
+// its (dry-flagged) corners, as the forward's to_prim with land: Bm is the
+// mean over the wet corners (initBm).
+__device__ __forceinline__ int adj_prim(float qe, float qu, float qv, float sw, float nw, float se, float ne,
+                                        const Scheme& k, float& e, float& u, float& v) {
+    const float s4 = ((sw + nw) + se) + ne;
+    const float Bm = cell_bm(sw, nw, se, ne, s4, k);
+    if (fabsf(Bm - k.land) <= kDryEps) { e = kDryFlag; u = 0.0f; v = 0.0f; return kCellLand; }
+    const float h = qe + Bm;
+    if (h < k.desing_eps) {
+        if (h <= k.cutoff) { e = -Bm + k.cutoff; u = 0.0f; v = 0.0f; return kCellDry; }
+        e = qe;
+        u = desingularize(h, qu, k.desing_eps);
+        v = desingularize(h, qv, k.desing_eps);
+        return kCellDesing;
+    }
+    e = qe; u = qu / h; v = qv / h;
+    return kCellWet;
+}
+
+// Adjoint of the state map: (lE, lU, lV) of the input (e, hu, hv) from the
+// adjoint (l0, l1, l2) of the state (e, u, v); zero for the constant classes.
+__device__ __forceinline__ Trip3 adj_prim_vjp(int cls, float qe, float u, float v, float sw, float nw, float se,
+                                              float ne, const Scheme& k, float l0, float l1, float l2) {
+    if (cls >= kCellDry) return Trip3{0.0f, 0.0f, 0.0f};
+    const float Bm = cell_bm(sw, nw, se, ne, ((sw + nw) + se) + ne, k);
+    const float h = qe + Bm;
+    float D = h, gD = 1.0f / h;                 // u = hu / D(h): du/dh = -u D'(h) / D
+    if (cls == kCellDesing) {
+        D = desing_den(h, k.desing_eps);
+        gD = desing_den_dh(h, k.desing_eps) / D;
+    }
+    return Trip3{l0 - (l1 * u + l2 * v) * gD, l1 / D, l2 / D};
+}
 
 struct CuGrad { float hm, um, vm, hp, up, vp; };
 
@@ -197,7 +253,6 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
     const int tid = threadIdx.x;
     const bool wallN = k.bcN == kWall, wallS = k.bcS == kWall, wallE = k.bcE == kWall, wallW = k.bcW == kWall;
     const float inv2g = 1.0f / k.two_g;
-    bool scope_bad = false;
     auto RI = [](int ry, int rx) { return ry * RXS + rx; };                 // region
     auto XI = [](int ry, int rx) { return (ry - HALO) * RXS + rx; };        // tile rows
     auto YI = [](int ry, int rx) { return ry * TX + (rx - HALO); };         // tile columns
@@ -206,7 +261,7 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
     for (int c = tid; c < (RY + 1) * (RX + 1); c += NT) {
         const int ry = c / (RX + 1), rx = c % (RX + 1);
         const int j = min(max(oy + ry, 0), ny + 4), i = min(max(ox + rx, 0), nx + 4);
-        S.Hi[c] = a.Hi[(size_t)j * a.phi + i];
+        S.Hi[c] = corner(a.Hi[(size_t)j * a.phi + i], k);
     }
     for (int r = tid; r < RY; r += NT) S.f[r] = a.f_rows[min(max(oy + r, 0), ny + 3)];
     for (int c = tid; c < NXR; c += NT) {
@@ -253,15 +308,9 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
             const int j = oy + ry, i = ox + rx;
             float e = 0.0f, u = 0.0f, v = 0.0f;
             if (j >= 0 && j < ny + 4 && i >= 0 && i < nx + 4) {
-                const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
-                const float h = qe[it] + __fmul_rn(s4, 0.25f);
-                if (fabsf(HI(ry, rx) - k.land) < kDryEps || fabsf(HI(ry + 1, rx) - k.land) < kDryEps ||
-                    fabsf(HI(ry, rx + 1) - k.land) < kDryEps || fabsf(HI(ry + 1, rx + 1) - k.land) < kDryEps ||
-                    h < k.desing_eps)
-                    scope_bad = true;
-                e = qe[it];
-                u = qu[it] / h;
-                v = qv[it] / h;
+                const int cls = adj_prim(qe[it], qu[it], qv[it], HI(ry, rx), HI(ry + 1, rx), HI(ry, rx + 1),
+                                         HI(ry + 1, rx + 1), k, e, u, v);
+                if (ry >= HALO && ry < HALO + TY) S.bx[XI(ry, rx)] = (uint16_t)(cls << 9);
             }
             const int r = RI(ry, rx);
             S.R0[r] = e; S.R1[r] = u; S.R2[r] = v;
@@ -303,7 +352,7 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
         if (!(hw > 0.0f)) { K = -dxfv + __fmul_rn(k.two_g, ec + Hw); ba = kAdjA; }
         if (!(he > 0.0f)) { K = -dxfv - __fmul_rn(k.two_g, ec + He); ba = kAdjB; }
         S.Kx[xi] = K;
-        S.bx[xi] = (uint16_t)(bu | (bv << 2) | (bk << 4) | (ba << 6) | (1 << 8));
+        S.bx[xi] = (uint16_t)((S.bx[xi] & (3 << 9)) | bu | (bv << 2) | (bk << 4) | (ba << 6) | (1 << 8));
     }
     for (int c = tid; c < RY * TX; c += NT) {
         const int ry = c / TX, rx = HALO + c % TX;
@@ -390,11 +439,13 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
             const float h = e + Hm;
             const bool wet = h > k.cutoff;
             const float hu = wet ? u * h : 0.0f, hv = wet ? v * h : 0.0f;
-            float Cf = 0.0f, sq = 0.0f, uw = 0.0f, vw = 0.0f;
+            float Cf = 0.0f, sq = 0.0f, uw = 0.0f, vw = 0.0f, Dn = h;
             if (FRIC == kFricQuad) {
-                uw = hu / h; vw = hv / h;
+                // below desing_eps the speed and C are desingularised (CDKLM16_kernel.cu:884-900)
+                if (h < k.desing_eps) Dn = desing_den(h, k.desing_eps);
+                uw = hu / Dn; vw = hv / Dn;
                 sq = sqrtf(uw * uw + vw * vw);
-                Cf = (a.dt * k.r * sq) / h;
+                Cf = (a.dt * k.r * sq) / Dn;
             } else if (FRIC == kFricLinear) {
                 Cf = (k.two_r * a.dt) / h;
             }
@@ -406,18 +457,19 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
             float lhu = w * lu * iD, lhv = w * lv * iD, leta = w * le, lh = 0.0f;
             const float lCf = -w * (lu * oU[it] + lv * oV[it]) * iD;
             if (FRIC == kFricQuad) {
-                const float ls = lCf * a.dt * k.r / h;
-                lh -= lCf * Cf / h;
+                const float ls = lCf * a.dt * k.r / Dn;
+                float lD = -lCf * Cf / Dn;
                 if (sq > 0.0f) {
                     const float luw = ls * uw / sq, lvw = ls * vw / sq;
-                    lhu += luw / h; lhv += lvw / h;
-                    lh -= (luw * uw + lvw * vw) / h;
+                    lhu += luw / Dn; lhv += lvw / Dn;
+                    lD -= (luw * uw + lvw * vw) / Dn;
                 }
+                lh += (h < k.desing_eps) ? lD * desing_den_dh(h, k.desing_eps) : lD;
             } else if (FRIC == kFricLinear) {
                 lh -= lCf * Cf / h;
             }
             const float fc = S.f[ry];
-            if (h >= k.cutoff) {
+            if (h >= k.cutoff && e != kDryFlag) {
                 const float Hx = 0.5f * (HI(ry, rx + 1) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry + 1, rx));
                 const float Hy = 0.5f * (HI(ry + 1, rx) + HI(ry + 1, rx + 1)) - 0.5f * (HI(ry, rx) + HI(ry, rx + 1));
                 lhv += fc * lL2;
@@ -461,6 +513,7 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
                 const int j = oy + ry, im = ox + rx, ip = im + 1;
                 if (j < 2 || j >= ny + 2 || im < 1 || im > nx + 1) continue;
                 const int m = RI(ry, rx), p = m + 1;
+                if (S.R0[m] == kDryFlag || S.R0[p] == kDryFlag) continue;   // land beside the face: no flux
                 const int xm = XI(ry, rx), xp = xm + 1;
                 const float fJ = S.f[ry];
                 const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Ux[xm]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vx[xm]);
@@ -496,6 +549,7 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
                 const int i = ox + rx, jm = oy + ry, jp = jm + 1;
                 if (i < 2 || i >= nx + 2 || jm < 1 || jm > ny + 1) continue;
                 const int m = RI(ry, rx), p = m + RXS;
+                if (S.R0[m] == kDryFlag || S.R0[p] == kDryFlag) continue;
                 const int ym = YI(ry, rx), yp = ym + TX;
                 const float Rmu = S.R1[m] + __fmul_rn(0.5f, S.Uy[ym]), Rmv = S.R2[m] + __fmul_rn(0.5f, S.Vy[ym]);
                 const float Rpu = S.R1[p] - __fmul_rn(0.5f, S.Uy[yp]), Rpv = S.R2[p] - __fmul_rn(0.5f, S.Vy[yp]);
@@ -590,10 +644,9 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
         }
         l2 += lfv * S.f[ry] * flip((wallW && i < 2) || (wallE && i > nx + 1));
         l1 += lfu * S.f[ry] * flip((wallS && j < 2) || (wallN && j > ny + 1));
-        const float s4 = ((HI(ry, rx) + HI(ry + 1, rx)) + HI(ry, rx + 1)) + HI(ry + 1, rx + 1);
-        const float h = S.R0[q] + __fmul_rn(s4, 0.25f);
-        float lE = l0 - (l1 * S.R1[q] + l2 * S.R2[q]) / h;
-        float lU = l1 / h, lV = l2 / h;
+        const Trip3 lq = adj_prim_vjp((S.bx[xq] >> 9) & 3, S.R0[q], S.R1[q], S.R2[q], HI(ry, rx), HI(ry + 1, rx),
+                                      HI(ry, rx + 1), HI(ry + 1, rx + 1), k, l0, l1, l2);
+        float lE = lq.a, lU = lq.b, lV = lq.c;
         if (!STAGE1 && a.ne && j >= 2 && j < ny + 2 && i >= 2 && i < nx + 2) {
             const size_t no = (size_t)j * a.pn + i;
             lE += a.ne[no]; lU += a.nu[no]; lV += a.nv[no];
@@ -601,7 +654,6 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
         const size_t io = (size_t)j * a.pi + i;
         a.ie[io] = lE; a.iu[io] = lU; a.iv[io] = lV;
     }
-    if (scope_bad && a.status) atomicOr(a.status, GO_STATUS_ADJ_SCOPE);
 }
 
 // ---------------------------------------------------------------------------
@@ -618,7 +670,7 @@ __global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArg
 // ---------------------------------------------------------------------------
 
 struct Cor { float a, b; };                 // corners Hi(r, i), Hi(r, i+1)
-struct PrimC { float e, u, v; };
+struct PrimC { float e, u, v; int cls; };
 struct SlopeC { float u, v, K; uint32_t code; };
 struct Trip { float a, b, c; };
 
@@ -657,12 +709,11 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     if (EDGE && wallE && i > nx + 1) { si = 2 * nx + 3 - i; shu = -1.0f; }
     const float vflip_kx = flip(EDGE && ((wallW && i < 2) || (wallE && i > nx + 1)));
     const float vflip_adj = flip(EDGE && ((wallW && i < 2) || (wallE && i > nx + 2)));
-    bool scope_bad = false;
 
     auto corners = [&](int r) -> Cor {
         if (EDGE && (r < 0 || r > ny + 4 || i < 0 || i > nx + 3)) return Cor{0.0f, 0.0f};
         const float* row = a.Hi + (size_t)r * a.phi;
-        return Cor{row[i], row[i + 1]};
+        return Cor{corner(row[i], k), corner(row[i + 1], k)};
     };
     auto frow = [&](int r) -> float { return a.f_rows[min(max(r, 0), ny + 3)]; };
     // raw (mirrored) state of row r, and its primitive form
@@ -676,13 +727,10 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         return Trip{a.qe[q], a.qu[q] * shu, a.qv[q] * shv};
     };
     auto prim = [&](int r, const Trip& q, const Cor& lo, const Cor& hi) -> PrimC {
-        if (EDGE && (r < 0 || r >= ny + 4 || !col_ok)) return PrimC{0.0f, 0.0f, 0.0f};
-        const float Bm = __fmul_rn(((lo.a + hi.a) + lo.b) + hi.b, 0.25f);
-        const float h = q.a + Bm;
-        if (fabsf(lo.a - k.land) < kDryEps || fabsf(hi.a - k.land) < kDryEps || fabsf(lo.b - k.land) < kDryEps ||
-            fabsf(hi.b - k.land) < kDryEps || h < k.desing_eps)
-            scope_bad = true;
-        return PrimC{q.a, q.b / h, q.c / h};
+        if (EDGE && (r < 0 || r >= ny + 4 || !col_ok)) return PrimC{0.0f, 0.0f, 0.0f, kCellWet};
+        PrimC p;
+        p.cls = adj_prim(q.a, q.b, q.c, lo.a, hi.a, lo.b, hi.b, k, p.e, p.u, p.v);
+        return p;
     };
     // inputs of the own-cell adjoint of row r (output adjoint, stored stage
     // output, and for output cells the wind adjoint accumulated so far)
@@ -752,11 +800,13 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         const float h = p.e + Hm;
         const bool wet = h > k.cutoff;
         const float hu = wet ? p.u * h : 0.0f, hv = wet ? p.v * h : 0.0f;
-        float Cf = 0.0f, sq = 0.0f, uw = 0.0f, vw = 0.0f;
+        float Cf = 0.0f, sq = 0.0f, uw = 0.0f, vw = 0.0f, Dn = h;
         if (FRIC == kFricQuad) {
-            uw = hu / h; vw = hv / h;
+            // below desing_eps the speed and C are desingularised (CDKLM16_kernel.cu:884-900)
+            if (h < k.desing_eps) Dn = desing_den(h, k.desing_eps);
+            uw = hu / Dn; vw = hv / Dn;
             sq = sqrtf(uw * uw + vw * vw);
-            Cf = (a.dt * k.r * sq) / h;
+            Cf = (a.dt * k.r * sq) / Dn;
         } else if (FRIC == kFricLinear) {
             Cf = (k.two_r * a.dt) / h;
         }
@@ -766,18 +816,19 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         float lhu = w * lU * iD, lhv = w * lV * iD, leta = w * lE, lh = 0.0f;
         const float lCf = -w * (lU * in.ou + lV * in.ov) * iD;
         if (FRIC == kFricQuad) {
-            const float ls = lCf * a.dt * k.r / h;
-            lh -= lCf * Cf / h;
+            const float ls = lCf * a.dt * k.r / Dn;
+            float lD = -lCf * Cf / Dn;
             if (sq > 0.0f) {
                 const float luw = ls * uw / sq, lvw = ls * vw / sq;
-                lhu += luw / h; lhv += lvw / h;
-                lh -= (luw * uw + lvw * vw) / h;
+                lhu += luw / Dn; lhv += lvw / Dn;
+                lD -= (luw * uw + lvw * vw) / Dn;
             }
+            lh += (h < k.desing_eps) ? lD * desing_den_dh(h, k.desing_eps) : lD;
         } else if (FRIC == kFricLinear) {
             lh -= lCf * Cf / h;
         }
         const bool out_cell = writer && r >= r0 && r < r1;
-        if (h >= k.cutoff) {
+        if (h >= k.cutoff && p.e != kDryFlag) {
             const float Hx = 0.5f * (clo.b + chi.b) - 0.5f * (clo.a + chi.a);
             const float Hy = 0.5f * (chi.a + chi.b) - 0.5f * (clo.a + clo.b);
             lhv += fc * LL.b;
@@ -846,7 +897,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         // (4) y face (j+1, j+2)
         {
             const int jm = j + 1, jp = j + 2;
-            if (!EDGE || (col_int && jm >= 1 && jm <= ny + 1)) {
+            if ((!EDGE || (col_int && jm >= 1 && jm <= ny + 1)) && P1.e != kDryFlag && P2.e != kDryFlag) {
                 const float Rmu = P1.u + __fmul_rn(0.5f, S1.u), Rmv = P1.v + __fmul_rn(0.5f, S1.v);
                 const float Rpu = P2.u - __fmul_rn(0.5f, S2.u), Rpv = P2.v - __fmul_rn(0.5f, S2.v);
                 const float fm = flip(EDGE && wallS && jp == 2), fp = flip(EDGE && wallN && jp == ny + 2);
@@ -935,7 +986,8 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
             // x face (i, i+1)
             float aK = 0.0f, aux = 0.0f, avx = 0.0f;
             float pe = 0.0f, pu = 0.0f, pv = 0.0f, pK = 0.0f, pux = 0.0f, pvx = 0.0f;
-            if (t >= 1 && t < BW - 2 && (!EDGE || (i >= 1 && i <= nx + 1))) {
+            if (t >= 1 && t < BW - 2 && (!EDGE || (i >= 1 && i <= nx + 1)) && P0.e != kDryFlag &&
+                sb.e[t + 1] != kDryFlag) {
                 const int ip = i + 1;
                 const float Rmu = P0.u + __fmul_rn(0.5f, sx.u), Rmv = P0.v + __fmul_rn(0.5f, sx.v);
                 const float Rpu = sb.u[t + 1] - __fmul_rn(0.5f, sb.su[t + 1]);
@@ -1002,9 +1054,8 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         }
         // (7) write the adjoint of row j
         if (out_row && writer) {
-            const float h = P0.e + __fmul_rn(((C0.a + C1.a) + C0.b) + C1.b, 0.25f);
-            float lE = A0.a - (A0.b * P0.u + A0.c * P0.v) / h;
-            float lU = A0.b / h, lV = A0.c / h;
+            const Trip3 lq = adj_prim_vjp(P0.cls, P0.e, P0.u, P0.v, C0.a, C1.a, C0.b, C1.b, k, A0.a, A0.b, A0.c);
+            float lE = lq.a, lU = lq.b, lV = lq.c;
             lE += qn0.a; lU += qn0.b; lV += qn0.c;       // stage 0: the adjoint of Q^n (zero otherwise)
             const size_t io = (size_t)j * a.pi + i;
             a.ie[io] = lE; a.iu[io] = lU; a.iv[io] = lV;
@@ -1018,7 +1069,6 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         A0 = A1; A1 = A2; A2 = trip0();
         B1 = B2; B2 = trip0();
     }
-    if (scope_bad && a.status) atomicOr(a.status, GO_STATUS_ADJ_SCOPE);
 }
 
 // A block needs no boundary logic when all its columns and the rows it

@@ -48,8 +48,8 @@ extern "C" {
 
 /* Device status word bits (go_domain_status). */
 #define GO_STATUS_NONFINITE 0x1u /* a written cell held NaN or Inf */
-#define GO_STATUS_ADJ_SCOPE 0x2u /* the adjoint met land, a cell shallower than
-                                   desing_eps, or a non-north-up grid */
+#define GO_STATUS_ADJ_SCOPE 0x2u /* reserved: raised by earlier adjoint builds that
+                                   covered no land or shallow cells */
 #define GO_STATUS_TIMEOUT 0x4u   /* a bounded wait in a step kernel gave up
                                    (a TMA tile that never arrived) */
 
@@ -419,8 +419,13 @@ int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done);
 
 /* ---------------------------------------------------------------------
  * Adjoint (reverse mode) of the RK2 step.  No counterpart in the
- * reference, which has no adjoint.  Built for north-up grids without land
- * or cells shallower than desing_eps (GO_STATUS_ADJ_SCOPE otherwise).
+ * reference, which has no adjoint.  Built for north-up grids (other grid
+ * angles are rejected with GO_ERR_UNSUPPORTED); land, dry and
+ * desingularised cells are differentiated through the branch the forward
+ * takes (land and dry cells are constants of the stage, desingularised
+ * cells use u = hu / D(h), D the desingularisation denominator).  The
+ * Hi passed must be the one the forward read, and a domain with land needs
+ * go_domain_set_land(d, 1) for go_traj_step as for the forward.
  * A state is three device arrays of (ny+4) x (nx+4) floats sharing a pitch
  * in bytes; adjoint states hold their values at the interior cells.
  * --------------------------------------------------------------------- */
