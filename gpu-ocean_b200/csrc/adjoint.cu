@@ -44,8 +44,7 @@ using namespace go;
 
 namespace {
 
-constexpr int TX = 32, TY = 16, HALO = 3;
-constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO;   // 38 x 22 region
+constexpr int HALO = 3;
 constexpr int NT = 256;
 
 struct AdjArgs {
@@ -217,12 +216,23 @@ __device__ __forceinline__ CuGrad cu_vjp(float hm, float um, float vm, float hp,
 // that threads walking down rows hit distinct banks), x-slope data on the
 // tile rows only, y-slope data on the tile columns only (74.7 KB per CTA,
 // three CTAs per SM).
-constexpr int RXS = RX + 1;                 // padded row stride of region arrays
-constexpr int NR = RXS * RY;                // region
-constexpr int NXR = TY * RXS;               // tile rows x region columns
-constexpr int NYC = RY * TX;                // region rows x tile columns
+// Tile of TX x TY output cells and its region (the tile with a HALO-cell
+// rim): the region's row stride RXS, and the sizes of the region arrays
+// (NR), the tile-row arrays (NXR) and the tile-column arrays (NYC).
+template <int TX_, int TY_>
+struct TileDims {
+    static constexpr int TX = TX_, TY = TY_;
+    static constexpr int RX = TX + 2 * HALO, RY = TY + 2 * HALO;
+    static constexpr int RXS = RX + 1;       // padded row stride of region arrays
+    static constexpr int NR = RXS * RY;      // region
+    static constexpr int NXR = TY * RXS;     // tile rows x region columns
+    static constexpr int NYC = RY * TX;      // region rows x tile columns
+};
 
+template <int TX_, int TY_>
 struct AdjSmem {
+    using D = TileDims<TX_, TY_>;
+    static constexpr int RX = D::RX, RY = D::RY, NR = D::NR, NXR = D::NXR, NYC = D::NYC;
     float R0[NR], R1[NR], R2[NR];           // primitive state (eta, u, v)
     float LL0[NR], LL1[NR], LL2[NR];        // adjoint of the cell tendencies L
     float Ux[NXR], Vx[NXR], Kx[NXR];        // x slopes (K after adjustment)
@@ -243,10 +253,12 @@ __device__ __forceinline__ int br_k(uint32_t b) { return (b >> 4) & 3; }
 __device__ __forceinline__ int br_a(uint32_t b) { return (b >> 6) & 3; }
 __device__ __forceinline__ bool br_has(uint32_t b) { return (b >> 8) & 1; }
 
-template <int FRIC, bool STAGE1>
-__global__ void __launch_bounds__(NT, 3) cdklm_adjoint_stage_kernel(const AdjArgs a) {
+template <int FRIC, bool STAGE1, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(NT, MINB) cdklm_adjoint_stage_kernel(const AdjArgs a) {
+    using D = TileDims<TX, TY>;
+    constexpr int RX = D::RX, RY = D::RY, RXS = D::RXS, NXR = D::NXR, NYC = D::NYC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    AdjSmem& S = *reinterpret_cast<AdjSmem*>(smem_raw);
+    AdjSmem<TX, TY>& S = *reinterpret_cast<AdjSmem<TX, TY>*>(smem_raw);
     const Scheme& k = a.k;
     const int nx = k.nx, ny = k.ny;
     const int ox = blockIdx.x * TX - HALO, oy = blockIdx.y * TY - HALO;
@@ -1167,23 +1179,32 @@ __device__ __forceinline__ void adj_fold_cell(float* e, float* u, float* v, int 
     e[o] += ae; u[o] += au; v[o] += av;
 }
 
-template <int FRIC, bool STAGE1>
-cudaError_t launch_adj(const AdjArgs& a, cudaStream_t s) {
+template <int FRIC, bool STAGE1, int TX, int TY, int MINB>
+cudaError_t launch_adj_tile(const AdjArgs& a, cudaStream_t s) {
     // the dynamic shared-memory limit is raised once per device
     static unsigned long long attr_set = 0ull;
-    const int bytes = (int)sizeof(AdjSmem);
+    const int bytes = (int)sizeof(AdjSmem<TX, TY>);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 64 || !((attr_set >> dev) & 1ull)) {
-        e = cudaFuncSetAttribute(cdklm_adjoint_stage_kernel<FRIC, STAGE1>,
+        e = cudaFuncSetAttribute(cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_set |= 1ull << dev;
     }
     const dim3 grid((a.k.nx + 4 + TX - 1) / TX, (a.k.ny + 4 + TY - 1) / TY);
-    cdklm_adjoint_stage_kernel<FRIC, STAGE1><<<grid, NT, bytes, s>>>(a);
+    cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB><<<grid, NT, bytes, s>>>(a);
     return cudaGetLastError();
+}
+
+// Tile form: 32-column tiles of a.rows rows (8, 12 or 16; CTAs per SM by
+// shared memory: 5, 3 and 3 of 44.4, 59.6 and 74.7 KB).
+template <int FRIC, bool STAGE1>
+cudaError_t launch_adj(const AdjArgs& a, cudaStream_t s) {
+    if (a.rows <= 8) return launch_adj_tile<FRIC, STAGE1, 32, 8, 4>(a, s);
+    if (a.rows <= 12) return launch_adj_tile<FRIC, STAGE1, 32, 12, 3>(a, s);
+    return launch_adj_tile<FRIC, STAGE1, 32, 16, 3>(a, s);
 }
 
 template <int BW, int FRIC, bool STAGE1>
@@ -1200,8 +1221,8 @@ cudaError_t launch_any(const AdjArgs& a, int kind, cudaStream_t s) {
     return launch_march<128, FRIC, STAGE1>(a, s);
 }
 
-// Launch form and strip height for a grid.  A marching block walks its
-// strip sequentially, so below ~300 k cells (512^2) the grid has too few
+// Launch form and strip (or tile) height for a grid.  A marching block walks
+// its strip sequentially, so below ~300 k cells (512^2) the grid has too few
 // column strips to fill 148 SMs and the tile form is faster (B200: 49.5 vs
 // 58 us per stage at 512^2; 116 vs 170 at 1024^2 the other way).  Marching
 // uses 64-thread blocks up to 1024 columns and 128 above, strips of the power
@@ -1214,7 +1235,13 @@ void adjoint_launch(const go_domain* d, int* kind, int* rows) {
         else kd = (nx <= 1024) ? GO_ADJ_MARCH64 : GO_ADJ_MARCH128;
     }
     int r = d->adj_rows;
-    if (r <= 0) {
+    if (r <= 0 && kd == GO_ADJ_TILE) {
+        // B200, us per stage adjoint at 512^2 with 16 / 12 / 8-row tiles:
+        // 47.3 / 45.2 / 43.2 (the smaller tiles fill the SMs in fewer
+        // partial waves); at 1024^2 the 16-row tiles are fastest (118 / 127 /
+        // 125), but that grid runs the marching form
+        r = 8;
+    } else if (r <= 0) {
         const int bw = (kd == GO_ADJ_MARCH64) ? 64 : 128;
         const long long target = (long long)((nx + bw - 7) / (bw - 6)) * ny / 600;
         r = 8;

@@ -436,8 +436,9 @@ typedef struct go_state {
     int pitch;             /* bytes */
 } go_state;
 
-/* Launch form of the adjoint stage: GO_ADJ_TILE (one block per 32x16 tile,
- * forward recomputed with a 3-cell halo), GO_ADJ_MARCH64 / GO_ADJ_MARCH128
+/* Launch form of the adjoint stage: GO_ADJ_TILE (one block per tile of 32
+ * columns and rows_per_strip = 8, 12 or 16 rows, 0 = 8; the forward is
+ * recomputed with a 3-cell halo), GO_ADJ_MARCH64 / GO_ADJ_MARCH128
  * (one thread per column, blocks of 64 or 128 columns marching up strips of
  * rows_per_strip rows, 0 = automatic), GO_ADJ_AUTO (the default: the tile
  * form below ~300 k cells, where marching strips cannot fill the GPU, else

@@ -512,9 +512,9 @@ def test_autograd_functions(ctx):
                                                   (70, 130, (1, 1, 1, 1), False), (100, 70, (1, 2, 1, 2), True),
                                                   (70, 90, (1, 1, 1, 1), True)])
 def test_adjoint_launch_forms_agree(ctx, nx, ny, bc, coastal):
-    """The tile form and the marching forms (64/128 columns, several strip
-    heights) give the same stage adjoints to FP32 rounding, also with land,
-    dry and desingularised cells."""
+    """The tile form (tiles of 16, 8 and 12 rows) and the marching forms
+    (64/128 columns, several strip heights) give the same stage adjoints to
+    FP32 rounding, also with land, dry and desingularised cells."""
     if coastal:
         c, sim = make_coastal_sim(ctx, nx, ny, bc=bc, seed=63500)
     else:
@@ -532,7 +532,8 @@ def test_adjoint_launch_forms_agree(ctx, nx, ny, bc, coastal):
     lib = _native.load()
     lam_out = torch.randn((3, ny, nx), device="cuda", generator=torch.Generator(device="cuda").manual_seed(14))
     results = {}
-    forms = [(_native.GO_ADJ_TILE, 0), (_native.GO_ADJ_MARCH64, 0), (_native.GO_ADJ_MARCH64, 8),
+    forms = [(_native.GO_ADJ_TILE, 0), (_native.GO_ADJ_TILE, 8), (_native.GO_ADJ_TILE, 12),
+             (_native.GO_ADJ_MARCH64, 0), (_native.GO_ADJ_MARCH64, 8),
              (_native.GO_ADJ_MARCH128, 0), (_native.GO_ADJ_MARCH128, 16), (_native.GO_ADJ_MARCH128, 5)]
     for kind, rows in forms:
         assert lib.go_domain_set_adjoint_launch(prob.domain.handle, kind, rows) == 0
