@@ -20,6 +20,7 @@ GO_FRICTION_LINEAR = 1
 GO_STATUS_NONFINITE = 0x1
 GO_STATUS_ADJ_SCOPE = 0x2
 GO_STATUS_TIMEOUT = 0x4
+GO_DEBUG_SKIP_TMA = 0x1
 GO_ERR_INVALID = -1
 GO_ERR_CUDA = -2
 GO_ERR_UNSUPPORTED = -3
@@ -123,6 +124,7 @@ SIGNATURES = {
     "go_domain_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     "go_batch_status": (_I, [_P, _P, _I]),
     "go_domain_stage_launches": (_I, [_P, _P]),
+    "go_domain_set_debug": (_I, [_P, ctypes.c_uint32]),
     "go_batch_run_events": (_I, [_P, _P, ctypes.c_uint32, _I, ctypes.c_double, _F, ctypes.c_double,
                                  ctypes.c_uint32, _F, _F, _P, ctypes.c_size_t, _P, _P, _P]),
     "go_noise_lcg": (_I, [_P, _I, _I, _I, _I, _P, _I, _P, _I]),
@@ -285,6 +287,10 @@ class Domain:
         v = ctypes.c_uint32()
         check(load().go_domain_status(self.handle, ctypes.byref(v), int(bool(clear))))
         return int(v.value)
+
+    def set_debug(self, flags):
+        """Test hooks (GO_DEBUG_*; 0 in normal runs)."""
+        check(load().go_domain_set_debug(self.handle, int(flags)))
 
     def stage_launches(self):
         """Kernel launches of the last RK stage (go_domain_stage_launches)."""

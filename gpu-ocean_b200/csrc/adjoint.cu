@@ -39,6 +39,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "trace.h"
 
 using namespace go;
 
@@ -1511,6 +1512,7 @@ int go_adjoint_batch_set_member(go_adjoint_batch* b, int m, float dt, const go_s
 }
 
 int go_adjoint_batch_step(go_adjoint_batch* b, void* stream) {
+    GO_TRACE("go_adjoint_batch_step");
     if (!b) return go_fail(GO_ERR_INVALID, "null batch");
     int rc = adjoint_batch_commit(b);
     if (rc) return rc;
@@ -1543,6 +1545,7 @@ int go_adjoint_stage(go_domain* d, void* stream, int rk_step, float dt, const go
                      const go_state* q_out, const go_state* lam_out, const go_state* lam_in,
                      const go_state* lam_qn, float* lam_wx, float* lam_wy, int wind_pitch,
                      const float* Hi, int Hi_pitch) {
+    GO_TRACE("go_adjoint_stage");
     if (!d || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
     if (rk_step != 0 && rk_step != 1) return go_fail(GO_ERR_INVALID, "rk_step %d (RK2 has 0 and 1)", rk_step);
     int rc = check_adjoint_domain(d);
@@ -1568,6 +1571,7 @@ int go_adjoint_step(go_domain* d, void* stream, float dt, const go_state* q_n, c
                     const go_state* q_next, const go_state* lam_next, const go_state* lam_n,
                     const go_state* scratch_star, const go_state* scratch_qn, float* lam_wx, float* lam_wy,
                     int wind_pitch, const float* Hi, int Hi_pitch) {
+    GO_TRACE("go_adjoint_step");
     if (!d || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
     int rc = check_adjoint_domain(d);
     const int w = d->k.nx + 4;
@@ -1598,6 +1602,7 @@ int go_adjoint_step(go_domain* d, void* stream, float dt, const go_state* q_n, c
 int go_traj_step(go_domain* d, void* stream, float dt, float wind_stress_t, const go_state* q_n,
                  const go_state* q_star, const go_state* q_next, const float* Hi, int Hi_pitch,
                  float land_value) {
+    GO_TRACE("go_traj_step");
     if (!d || !Hi) return go_fail(GO_ERR_INVALID, "null argument");
     const int w = d->k.nx + 4;
     int rc = check_state(q_n, w, "q_n");

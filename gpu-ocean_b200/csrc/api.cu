@@ -6,6 +6,7 @@
 #include <string>
 
 #include "pair_dispatch.cuh"
+#include "trace.h"
 
 using namespace go;
 
@@ -103,6 +104,7 @@ StageArgs go_stage_args(const go_domain* d, float dt, int rk_step, const float* 
     a.pw = d->wpitch;
     a.rows_per_block = d->rows_per_block;
     a.status = d->d_status;
+    a.debug = d->debug;
     a.neg_zero = -0.0f;
     a.fric = go_friction_mode(d);
     return a;
@@ -375,6 +377,7 @@ int go_cdklm_swe_2D(go_domain* d, void* stream, float dt, int rk_step,
                     float* hv1, int hv1_pitch,
                     const float* Hi, int Hi_pitch, const float* Hm, int Hm_pitch,
                     float land_value, float wind_stress_t, int boundary_conditions) {
+    GO_TRACE("go_cdklm_swe_2D");
     (void)Hm; (void)Hm_pitch;
     if (!d || !eta0 || !hu0 || !hv0 || !eta1 || !hu1 || !hv1 || !Hi)
         return go_fail(GO_ERR_INVALID, "null argument");
@@ -398,6 +401,7 @@ int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_
                   float* eta0, float* hu0, float* hv0, int pitch0,
                   float* eta1, float* hu1, float* hv1, int pitch1,
                   const float* Hi, int Hi_pitch, float land_value) {
+    GO_TRACE("go_cdklm_step");
     if (!d || !eta0 || !hu0 || !hv0 || !eta1 || !hu1 || !hv1 || !Hi)
         return go_fail(GO_ERR_INVALID, "null argument");
     if (n_steps < 0) return go_fail(GO_ERR_INVALID, "n_steps < 0");
@@ -431,6 +435,7 @@ int go_cdklm_step(go_domain* d, void* stream, int n_steps, float dt, float wind_
 
 int go_max_dt(go_domain* d, void* stream, const float* eta, const float* hu, const float* hv, int pitch,
               const float* Bm, int Bm_pitch, float land_value, float* dt_dev) {
+    GO_TRACE("go_max_dt");
     if (!d || !eta || !hu || !hv || !Bm || !dt_dev) return go_fail(GO_ERR_INVALID, "null argument");
     int rc = go_check_pitch(pitch, d->k.nx + 4, "state");
     if (!rc) rc = go_check_pitch(Bm_pitch, d->k.nx + 4, "Bm");
@@ -455,6 +460,13 @@ int go_domain_status(go_domain* d, uint32_t* status, int clear) {
     GO_CUDA(cudaMemcpy(&v, d->d_status, sizeof(v), cudaMemcpyDeviceToHost));
     *status = v;
     if (clear) GO_CUDA(cudaMemset(d->d_status, 0, sizeof(unsigned int)));
+    return GO_OK;
+}
+
+int go_domain_set_debug(go_domain* d, unsigned flags) {
+    if (!d) return go_fail(GO_ERR_INVALID, "null domain");
+    if (flags & ~GO_DEBUG_SKIP_TMA) return go_fail(GO_ERR_INVALID, "unknown debug flags 0x%x", flags);
+    d->debug = flags;
     return GO_OK;
 }
 

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "grf.cuh"
+#include "trace.h"
 #include "pair_dispatch.cuh"
 
 using namespace go;
@@ -676,6 +677,7 @@ int go_batch_tiles(go_batch* b, int* ntiles) {
 }
 
 int go_batch_step(go_batch* b, void* stream, int n_steps) {
+    GO_TRACE("go_batch_step");
     if (!b || n_steps < 0) return go_fail(GO_ERR_INVALID, "bad arguments");
     int rc = batch_commit(b);
     if (rc) return rc;
@@ -715,6 +717,7 @@ int go_batch_graph_capture(go_batch* b, void* stream, int n_steps) {
 }
 
 int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done) {
+    GO_TRACE("go_batch_graph_launch");
     if (!b) return go_fail(GO_ERR_INVALID, "null batch");
     if (!b->graph_exec) return go_fail(GO_ERR_INVALID, "no captured graph (go_batch_graph_capture)");
     GO_CUDA(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream));
@@ -723,6 +726,7 @@ int go_batch_graph_launch(go_batch* b, void* stream, int* steps_done) {
 }
 
 int go_batch_max_dt(go_batch* b, void* stream, float* dt_dev) {
+    GO_TRACE("go_batch_max_dt");
     if (!b || !dt_dev) return go_fail(GO_ERR_INVALID, "null argument");
     int rc = batch_commit(b);
     if (rc) return rc;
@@ -748,6 +752,7 @@ size_t go_batch_grf_scratch_floats(go_batch* b, float corr_cells) {
 
 int go_batch_grf_perturb(go_batch* b, void* stream, uint32_t key0, uint32_t event, float std_dev,
                          float corr_cells, float* scratch, size_t scratch_floats) {
+    GO_TRACE("go_batch_grf_perturb");
     if (!b || !scratch) return go_fail(GO_ERR_INVALID, "null argument");
     int rc = batch_commit(b);
     if (rc) return rc;
@@ -768,6 +773,7 @@ int go_batch_grf_perturb(go_batch* b, void* stream, uint32_t key0, uint32_t even
 int go_batch_run_events(go_batch* b, void* stream, uint32_t first_event, int n_events, double interval, float dt,
                         double courant, uint32_t key0, float std_dev, float corr_cells, float* scratch,
                         size_t scratch_floats, double* t_members, long long* steps_out, float* dt_out) {
+    GO_TRACE("go_batch_run_events");
     if (!b || !scratch || !t_members) return go_fail(GO_ERR_INVALID, "null argument");
     if (n_events < 0 || !(interval > 0.0) || !(dt > 0.0f) || !(courant > 0.0))
         return go_fail(GO_ERR_INVALID, "n_events >= 0, interval > 0, dt > 0 and courant > 0");

@@ -603,7 +603,11 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     constexpr int Q_ = PairChunk<T>::kQpad, H_ = PairChunk<T>::kHpad;
     auto chunk_ptr = [&](unsigned g) { return ring + (size_t)(g % NS) * (stage1 ? PairChunk<T>::kFloats1 : PairChunk<T>::kFloats0); };
     const int nchunks = (r1 - r0 + kPairRingRows - 1) / kPairRingRows;
+    int n_issued = 0;                 // thread 0: chunks of this strip whose loads are issued
+    const bool skip_tma = (a.debug & GO_DEBUG_SKIP_TMA) != 0u;   // test hook: the waits run out
     auto issue_chunk = [&](int c) {   // thread 0: TMA loads of chunk c of this strip
+        if (skip_tma) return;
+        n_issued = c + 1;
         const unsigned g = chunk_base + (unsigned)c;
         float* base = chunk_ptr(g);
         uint64_t* bar = &sm.bar[g % NS];
@@ -625,6 +629,17 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
                 X.abort_flag = 1;
                 if (a.status) atomicOr(a.status, kStatusTimeout);
                 break;
+            }
+        }
+    };
+    // after a timeout, before the block leaves: thread 0 waits (bounded
+    // again) for the chunks from c on whose loads it issued, so that no copy
+    // lands in the shared memory of a block that has exited
+    auto drain = [&](int c) {
+        if (t != 0) return;
+        for (int cc = c; cc < n_issued; ++cc) {
+            const unsigned g = chunk_base + (unsigned)cc;
+            for (int it = 0; it < kWaitPolls && !mbar_try_wait(&sm.bar[g % NS], (g / NS) & 1u); ++it) {
             }
         }
     };
@@ -703,7 +718,10 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         }
         pair_sync<T>();
         if (use_ring && ri == 0) {
-            if (X.abort_flag) return false;
+            if (X.abort_flag) {
+                drain(c);
+                return false;
+            }
             if (t == 0 && c + NS - 1 < nchunks) issue_chunk(c + NS - 1);
         }
         const float4 L01 = X.st[0][t], L23 = X.st[1][t];          // columns (2t-1, 2t)

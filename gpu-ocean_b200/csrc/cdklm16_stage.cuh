@@ -64,6 +64,7 @@ struct StageArgs {
     unsigned int* status;
     float neg_zero;              // -0.0f: the addend of the packed products (column-pair kernel)
     int fric;                    // friction law kFric* (column-pair kernel; the marching kernel has it as a template)
+    unsigned debug;              // GO_DEBUG_* test hooks (go_domain_set_debug), 0 in normal runs
 };
 
 // Friction law selector.

@@ -34,6 +34,7 @@ struct go_domain {
     cudaEvent_t ev_fork, ev_join;
     int own_side;            // go_domain_create's handles may create them (not the allocation-free step)
     int stage_launches;      // kernel launches the last RK stage issued
+    unsigned debug;          // GO_DEBUG_* test hooks
 };
 
 // Records the message of a failed call (go_last_error) and returns code.

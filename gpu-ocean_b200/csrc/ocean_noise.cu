@@ -35,6 +35,7 @@
 //    generator; its seeds and stream layout are its own, so the XORWOW path
 //    matches the reference in distribution, not draw for draw).
 #include "internal.h"
+#include "trace.h"
 
 #include <curand_kernel.h>
 
@@ -914,6 +915,7 @@ int go_noise_batch_destroy(go_noise_batch* b) {
 
 int go_noise_batch_perturb(go_noise_batch* b, void* stream, double q0_scale, float perturbation_scale,
                            int update_random_field) {
+    GO_TRACE("go_noise_batch_perturb");
     if (!b) return go_fail(GO_ERR_INVALID, "null batch");
     cudaStream_t s = (cudaStream_t)stream;
     if (update_random_field) {

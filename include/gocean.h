@@ -610,6 +610,15 @@ int go_domain_status(go_domain* d, uint32_t* status, int clear);
  * first step). */
 int go_domain_stage_launches(go_domain* d, int* launches);
 
+/* Test hooks of the failure-detection tests (0 in normal runs).
+ * GO_DEBUG_SKIP_TMA: the column-pair kernel issues none of its TMA tile
+ * loads, so its bounded waits on the tiles' mbarriers run out; the stage
+ * then sets GO_STATUS_TIMEOUT, leaves the region's cells unwritten and
+ * returns, and the context stays usable.  Applies to stages prepared
+ * after the call (a batch takes it from its members at go_batch_set_member). */
+#define GO_DEBUG_SKIP_TMA 0x1u
+int go_domain_set_debug(go_domain* d, unsigned flags);
+
 /* Status words of every member of a batch (n values to status_host, member
  * order): each member's step kernels write only its own word, so a member
  * whose state went non-finite is flagged alone and the others step on

@@ -544,6 +544,31 @@ def test_status_word_flags_nonfinite(ctx):
     assert sim.status() == 0
 
 
+def test_tma_wait_runs_out_sets_timeout_and_context_survives(ctx):
+    """Failure detection without a GPU fault: with GO_DEBUG_SKIP_TMA the
+    column-pair kernel issues none of its tile loads, so every block's
+    bounded mbarrier wait runs out (2^20 polls); the stage flags
+    GO_STATUS_TIMEOUT and returns.  The same context then steps a fresh
+    simulator bit-identically to launch shape 5."""
+    c = SC.grf(512, ny=72, dx=1000.0, steps=1)
+    sim = _drop_in(ctx, c)
+    sim._domain.set_launch(8, 6)
+    sim._domain.set_debug(_native.GO_DEBUG_SKIP_TMA)
+    sim.step(c.dt)
+    assert sim.status(clear=True) & _native.GO_STATUS_TIMEOUT
+    sim._domain.set_debug(0)
+    fresh = _drop_in(ctx, c)
+    fresh._domain.set_launch(8, 6)
+    ref = _drop_in(ctx, c)
+    ref._domain.set_launch(5, 8)
+    for _ in range(5):
+        fresh.step(c.dt)
+        ref.step(c.dt)
+    assert fresh.status() == 0
+    for a, b in zip(fresh.download(), ref.download()):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("nx, ny, bc, r", [
     (4, 4, (1, 1, 1, 1), 0.0),
     (5, 11, (2, 2, 2, 2), 3.0e-3),
