@@ -59,11 +59,12 @@ int go_auto_rows(int nx, int ny, int shape) {
     return best;
 }
 
-// Default launch shape: the column-pair kernel (shape 8) from about 2400^2
-// cells up (measured on a B200, us per step, shapes 4 / 5 / 8: 2560^2
-// 308 / 291 / 269, 3072^2 429 / 399 / 385, 4096^2 720 / 685 / 627; at
-// 2048^2 the three are within 4% and below it the pair kernel's separate
-// boundary-frame launch does not pay).  Below that a read-ahead shape (5,
+// Default launch shape: the column-pair kernel (shape 8) from about 1500^2
+// cells up (measured on a B200, us per step, shapes 4 / 5 / 8, walls N/S and
+// periodic E/W: 1536^2 126 / 128 / 118, 2048^2 208 / 203 / 200, 2560^2
+// 308 / 292 / 262, 3072^2 429 / 399 / 373, 4096^2 720 / 686 / 583; at
+// 1024^2 and below the pair kernel's separate boundary-frame launch does not
+// pay: 68 / 72 / 71 and 29 / 32 / 36 at 512^2).  Below that a read-ahead shape (5,
 // or 6 for widths that 96-wide blocks cover with less waste) once the grid
 // needs more than one wave of blocks, where the ring hides the load
 // latency; in a single wave the register prefetch of 128 x 5 blocks

@@ -557,8 +557,8 @@ int go_batch_create(go_domain* const* members, int n, go_batch** out) {
         b->shape = tiles > 148LL * shape_blocks_per_sm(ring) ? ring : 4;
         // the column-pair kernel once the batch holds a few million cells
         // (measured on a B200, us per step with the ring shape / the pair
-        // shape: 100 members of 512^2 1424 / 1212; 64 domains of 128..1024
-        // squared cells, 20.5 M cells, 1136 / 946)
+        // shape: 100 members of 512^2 1524 / 1145; 16 members 307 / 272;
+        // 4 members 123 / 125)
         long long cells = 0;
         for (int m = 0; m < n; ++m) cells += (long long)members[m]->k.nx * members[m]->k.ny;
         if (cells >= kPairAutoBatchCells) b->shape = GO_SHAPE_PAIR;

@@ -25,8 +25,8 @@ constexpr int kPairUnroll = 1;
 constexpr int kPairFrameRows = 8;
 // default-shape thresholds: a grid of at least this many cells, a batch
 // whose members hold at least this many together
-constexpr long long kPairAutoCells = 2400LL * 2400LL;
-constexpr long long kPairAutoBatchCells = 4LL << 20;
+constexpr long long kPairAutoCells = 1500LL * 1500LL;
+constexpr long long kPairAutoBatchCells = 2LL << 20;
 
 // The block grid of an nx x ny domain (see PairGrid): the region of TMA
 // strips of `rows` rows, empty when `tma` is false (every block then takes
