@@ -10,13 +10,13 @@
 namespace go {
 
 // 64 threads (128 columns) per block.  The boundary-free kernel is held to
-// 128 registers (8 blocks, 16 warps per SM) and reads its inputs through a
-// ring of 2 chunks of 3 rows; the boundary-frame kernel gets 168 registers
-// and strips of 8 rows.  Measured on a B200 at 4096^2 (us per RK2 step):
-// 128 registers 635 against 641 with 145 (12 warps); 2 ring slots against 3
-// (3 slots leave room for fewer blocks); one row per loop iteration against
-// 3 (the 3-row unroll keeps the window in place but its code thrashes the
-// instruction cache: 41% issue activity against 59%).
+// 128 registers (8 blocks, 16 warps per SM; it needs no spills there) and
+// reads its inputs through a ring of 2 chunks of 3 rows; the boundary-frame
+// kernel gets 168 registers and strips of 8 rows.  Measured on a B200 at
+// 4096^2 (us per RK2 step): 2 ring slots against 3 (3 slots leave room for
+// fewer blocks); one row per loop iteration 583 against 729 for two (the
+// 2-row loop spills 64 bytes) and against a 3-row unroll whose code thrashes
+// the instruction cache (41% issue activity against 59%).
 constexpr int kPairT = 64;
 constexpr int kPairMinBlocksInterior = 8;
 constexpr int kPairMinBlocksFrame = 6;
