@@ -62,6 +62,7 @@ struct AdjArgs {
     const float* f_rows;
     unsigned int* status;
     int rows;                              // rows per strip (marching form)
+    int land;                              // the bathymetry may hold land (the domain's land flag)
 };
 
 // Branch codes
@@ -120,11 +121,12 @@ __device__ __forceinline__ float desing_den_dh(float h, float eps) {
 // Cell state (e, u, v) and class of one cell from its input (e, hu, hv) and
 // its (dry-flagged) corners, as the forward's to_prim with land: Bm is the
 // mean over the wet corners (initBm).
+template <bool LAND>
 __device__ __forceinline__ int adj_prim(float qe, float qu, float qv, float sw, float nw, float se, float ne,
                                         const Scheme& k, float& e, float& u, float& v) {
     const float s4 = ((sw + nw) + se) + ne;
-    const float Bm = cell_bm(sw, nw, se, ne, s4, k);
-    if (fabsf(Bm - k.land) <= kDryEps) { e = kDryFlag; u = 0.0f; v = 0.0f; return kCellLand; }
+    const float Bm = LAND ? cell_bm(sw, nw, se, ne, s4, k) : __fmul_rn(s4, 0.25f);
+    if (LAND && fabsf(Bm - k.land) <= kDryEps) { e = kDryFlag; u = 0.0f; v = 0.0f; return kCellLand; }
     const float h = qe + Bm;
     if (h < k.desing_eps) {
         if (h <= k.cutoff) { e = -Bm + k.cutoff; u = 0.0f; v = 0.0f; return kCellDry; }
@@ -139,10 +141,12 @@ __device__ __forceinline__ int adj_prim(float qe, float qu, float qv, float sw, 
 
 // Adjoint of the state map: (lE, lU, lV) of the input (e, hu, hv) from the
 // adjoint (l0, l1, l2) of the state (e, u, v); zero for the constant classes.
+template <bool LAND>
 __device__ __forceinline__ Trip3 adj_prim_vjp(int cls, float qe, float u, float v, float sw, float nw, float se,
                                               float ne, const Scheme& k, float l0, float l1, float l2) {
     if (cls >= kCellDry) return Trip3{0.0f, 0.0f, 0.0f};
-    const float Bm = cell_bm(sw, nw, se, ne, ((sw + nw) + se) + ne, k);
+    const float s4 = ((sw + nw) + se) + ne;
+    const float Bm = LAND ? cell_bm(sw, nw, se, ne, s4, k) : __fmul_rn(s4, 0.25f);
     const float h = qe + Bm;
     float D = h, gD = 1.0f / h;                 // u = hu / D(h): du/dh = -u D'(h) / D
     if (cls == kCellDesing) {
@@ -254,7 +258,7 @@ __device__ __forceinline__ int br_k(uint32_t b) { return (b >> 4) & 3; }
 __device__ __forceinline__ int br_a(uint32_t b) { return (b >> 6) & 3; }
 __device__ __forceinline__ bool br_has(uint32_t b) { return (b >> 8) & 1; }
 
-template <int FRIC, bool STAGE1, int TX, int TY, int MINB>
+template <int FRIC, bool STAGE1, int TX, int TY, int MINB, bool LAND>
 __global__ void __launch_bounds__(NT, MINB) cdklm_adjoint_stage_kernel(const AdjArgs a) {
     using D = TileDims<TX, TY>;
     constexpr int RX = D::RX, RY = D::RY, RXS = D::RXS, NXR = D::NXR, NYC = D::NYC;
@@ -274,7 +278,8 @@ __global__ void __launch_bounds__(NT, MINB) cdklm_adjoint_stage_kernel(const Adj
     for (int c = tid; c < (RY + 1) * (RX + 1); c += NT) {
         const int ry = c / (RX + 1), rx = c % (RX + 1);
         const int j = min(max(oy + ry, 0), ny + 4), i = min(max(ox + rx, 0), nx + 4);
-        S.Hi[c] = corner(a.Hi[(size_t)j * a.phi + i], k);
+        const float H = a.Hi[(size_t)j * a.phi + i];
+        S.Hi[c] = LAND ? corner(H, k) : H;
     }
     for (int r = tid; r < RY; r += NT) S.f[r] = a.f_rows[min(max(oy + r, 0), ny + 3)];
     for (int c = tid; c < NXR; c += NT) {
@@ -321,7 +326,7 @@ __global__ void __launch_bounds__(NT, MINB) cdklm_adjoint_stage_kernel(const Adj
             const int j = oy + ry, i = ox + rx;
             float e = 0.0f, u = 0.0f, v = 0.0f;
             if (j >= 0 && j < ny + 4 && i >= 0 && i < nx + 4) {
-                const int cls = adj_prim(qe[it], qu[it], qv[it], HI(ry, rx), HI(ry + 1, rx), HI(ry, rx + 1),
+                const int cls = adj_prim<LAND>(qe[it], qu[it], qv[it], HI(ry, rx), HI(ry + 1, rx), HI(ry, rx + 1),
                                          HI(ry + 1, rx + 1), k, e, u, v);
                 if (ry >= HALO && ry < HALO + TY) S.bx[XI(ry, rx)] = (uint16_t)(cls << 9);
             }
@@ -657,7 +662,7 @@ __global__ void __launch_bounds__(NT, MINB) cdklm_adjoint_stage_kernel(const Adj
         }
         l2 += lfv * S.f[ry] * flip((wallW && i < 2) || (wallE && i > nx + 1));
         l1 += lfu * S.f[ry] * flip((wallS && j < 2) || (wallN && j > ny + 1));
-        const Trip3 lq = adj_prim_vjp((S.bx[xq] >> 9) & 3, S.R0[q], S.R1[q], S.R2[q], HI(ry, rx), HI(ry + 1, rx),
+        const Trip3 lq = adj_prim_vjp<LAND>((S.bx[xq] >> 9) & 3, S.R0[q], S.R1[q], S.R2[q], HI(ry, rx), HI(ry + 1, rx),
                                       HI(ry, rx + 1), HI(ry + 1, rx + 1), k, l0, l1, l2);
         float lE = lq.a, lU = lq.b, lV = lq.c;
         if (!STAGE1 && a.ne && j >= 2 && j < ny + 2 && i >= 2 && i < nx + 2) {
@@ -699,7 +704,7 @@ struct MarchBufs {
     float gu[BW], gv[BW], gK[BW];           // x-slope adjoints after the adjustment
 };
 
-template <int BW, int FRIC, bool STAGE1, bool EDGE>
+template <int BW, int FRIC, bool STAGE1, bool EDGE, bool LAND>
 __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int bx, const int by,
                                                     MarchBufs<BW>& sb) {
     const Scheme& k = a.k;
@@ -726,6 +731,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     auto corners = [&](int r) -> Cor {
         if (EDGE && (r < 0 || r > ny + 4 || i < 0 || i > nx + 3)) return Cor{0.0f, 0.0f};
         const float* row = a.Hi + (size_t)r * a.phi;
+        if (!LAND) return Cor{row[i], row[i + 1]};
         return Cor{corner(row[i], k), corner(row[i + 1], k)};
     };
     auto frow = [&](int r) -> float { return a.f_rows[min(max(r, 0), ny + 3)]; };
@@ -742,7 +748,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
     auto prim = [&](int r, const Trip& q, const Cor& lo, const Cor& hi) -> PrimC {
         if (EDGE && (r < 0 || r >= ny + 4 || !col_ok)) return PrimC{0.0f, 0.0f, 0.0f, kCellWet};
         PrimC p;
-        p.cls = adj_prim(q.a, q.b, q.c, lo.a, hi.a, lo.b, hi.b, k, p.e, p.u, p.v);
+        p.cls = adj_prim<LAND>(q.a, q.b, q.c, lo.a, hi.a, lo.b, hi.b, k, p.e, p.u, p.v);
         return p;
     };
     // inputs of the own-cell adjoint of row r (output adjoint, stored stage
@@ -1067,7 +1073,7 @@ __device__ __forceinline__ void adjoint_march_strip(const AdjArgs& a, const int 
         }
         // (7) write the adjoint of row j
         if (out_row && writer) {
-            const Trip3 lq = adj_prim_vjp(P0.cls, P0.e, P0.u, P0.v, C0.a, C1.a, C0.b, C1.b, k, A0.a, A0.b, A0.c);
+            const Trip3 lq = adj_prim_vjp<LAND>(P0.cls, P0.e, P0.u, P0.v, C0.a, C1.a, C0.b, C1.b, k, A0.a, A0.b, A0.c);
             float lE = lq.a, lU = lq.b, lV = lq.c;
             lE += qn0.a; lU += qn0.b; lV += qn0.c;       // stage 0: the adjoint of Q^n (zero otherwise)
             const size_t io = (size_t)j * a.pi + i;
@@ -1093,28 +1099,28 @@ __device__ __forceinline__ bool march_interior(const AdjArgs& a, int bx, int by)
     return c0 >= 3 && c0 + BW + 1 <= a.k.nx + 1 && r0 - 3 >= 2 && r1 + 4 <= a.k.ny + 1;
 }
 
-template <int BW, int FRIC, bool STAGE1>
+template <int BW, int FRIC, bool STAGE1, bool LAND>
 __device__ __forceinline__ void adjoint_march_block(const AdjArgs& a, int bx, int by, MarchBufs<BW>& sb) {
     if (march_interior<BW>(a, bx, by))
-        adjoint_march_strip<BW, FRIC, STAGE1, false>(a, bx, by, sb);
+        adjoint_march_strip<BW, FRIC, STAGE1, false, LAND>(a, bx, by, sb);
     else
-        adjoint_march_strip<BW, FRIC, STAGE1, true>(a, bx, by, sb);
+        adjoint_march_strip<BW, FRIC, STAGE1, true, LAND>(a, bx, by, sb);
 }
 
-template <int BW, int FRIC, bool STAGE1>
+template <int BW, int FRIC, bool STAGE1, bool LAND>
 __global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_kernel(const AdjArgs a) {
     __shared__ MarchBufs<BW> sb;
-    adjoint_march_block<BW, FRIC, STAGE1>(a, blockIdx.x, blockIdx.y, sb);
+    adjoint_march_block<BW, FRIC, STAGE1, LAND>(a, blockIdx.x, blockIdx.y, sb);
 }
 
 // Batched form: one block per (member, column block, row strip) tile; the
 // member's arguments (2 per member: stage 0 and stage 1) in device memory.
-template <int BW, int FRIC, bool STAGE1>
+template <int BW, int FRIC, bool STAGE1, bool LAND>
 __global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_batch_kernel(
         const AdjArgs* __restrict__ args, const int4* __restrict__ tiles) {
     __shared__ MarchBufs<BW> sb;
     const int4 tile = tiles[blockIdx.x];
-    adjoint_march_block<BW, FRIC, STAGE1>(args[2 * tile.x + (STAGE1 ? 1 : 0)], tile.y, tile.z, sb);
+    adjoint_march_block<BW, FRIC, STAGE1, LAND>(args[2 * tile.x + (STAGE1 ? 1 : 0)], tile.y, tile.z, sb);
 }
 
 // Moves the adjoint held at ghost cells to the interior cells whose values
@@ -1180,7 +1186,7 @@ __device__ __forceinline__ void adj_fold_cell(float* e, float* u, float* v, int 
     e[o] += ae; u[o] += au; v[o] += av;
 }
 
-template <int FRIC, bool STAGE1, int TX, int TY, int MINB>
+template <int FRIC, bool STAGE1, int TX, int TY, int MINB, bool LAND>
 cudaError_t launch_adj_tile(const AdjArgs& a, cudaStream_t s) {
     // the dynamic shared-memory limit is raised once per device
     static unsigned long long attr_set = 0ull;
@@ -1189,37 +1195,45 @@ cudaError_t launch_adj_tile(const AdjArgs& a, cudaStream_t s) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 64 || !((attr_set >> dev) & 1ull)) {
-        e = cudaFuncSetAttribute(cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB>,
+        e = cudaFuncSetAttribute(cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB, LAND>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_set |= 1ull << dev;
     }
     const dim3 grid((a.k.nx + 4 + TX - 1) / TX, (a.k.ny + 4 + TY - 1) / TY);
-    cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB><<<grid, NT, bytes, s>>>(a);
+    cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB, LAND><<<grid, NT, bytes, s>>>(a);
     return cudaGetLastError();
 }
 
 // Tile form: 32-column tiles of a.rows rows (8, 12 or 16; CTAs per SM by
 // shared memory: 5, 3 and 3 of 44.4, 59.6 and 74.7 KB).
-template <int FRIC, bool STAGE1>
+template <int FRIC, bool STAGE1, bool LAND>
 cudaError_t launch_adj(const AdjArgs& a, cudaStream_t s) {
-    if (a.rows <= 8) return launch_adj_tile<FRIC, STAGE1, 32, 8, 4>(a, s);
-    if (a.rows <= 12) return launch_adj_tile<FRIC, STAGE1, 32, 12, 3>(a, s);
-    return launch_adj_tile<FRIC, STAGE1, 32, 16, 3>(a, s);
+    if (a.rows <= 8) return launch_adj_tile<FRIC, STAGE1, 32, 8, 4, LAND>(a, s);
+    if (a.rows <= 12) return launch_adj_tile<FRIC, STAGE1, 32, 12, 3, LAND>(a, s);
+    return launch_adj_tile<FRIC, STAGE1, 32, 16, 3, LAND>(a, s);
 }
 
-template <int BW, int FRIC, bool STAGE1>
+template <int BW, int FRIC, bool STAGE1, bool LAND>
 cudaError_t launch_march(const AdjArgs& a, cudaStream_t s) {
     const dim3 grid((a.k.nx + 4 + BW - 7) / (BW - 6), (a.k.ny + 4 + a.rows - 1) / a.rows);
-    cdklm_adjoint_march_kernel<BW, FRIC, STAGE1><<<grid, BW, 0, s>>>(a);
+    cdklm_adjoint_march_kernel<BW, FRIC, STAGE1, LAND><<<grid, BW, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+// Kernels without the land branches (corners read as they are, the cell
+// depth a plain quarter sum) for domains whose bathymetry holds no land;
+// dry and desingularised cells are handled either way.
+template <int FRIC, bool STAGE1, bool LAND>
+cudaError_t launch_form(const AdjArgs& a, int kind, cudaStream_t s) {
+    if (kind == GO_ADJ_TILE) return launch_adj<FRIC, STAGE1, LAND>(a, s);
+    if (kind == GO_ADJ_MARCH64) return launch_march<64, FRIC, STAGE1, LAND>(a, s);
+    return launch_march<128, FRIC, STAGE1, LAND>(a, s);
 }
 
 template <int FRIC, bool STAGE1>
 cudaError_t launch_any(const AdjArgs& a, int kind, cudaStream_t s) {
-    if (kind == GO_ADJ_TILE) return launch_adj<FRIC, STAGE1>(a, s);
-    if (kind == GO_ADJ_MARCH64) return launch_march<64, FRIC, STAGE1>(a, s);
-    return launch_march<128, FRIC, STAGE1>(a, s);
+    return a.land ? launch_form<FRIC, STAGE1, true>(a, kind, s) : launch_form<FRIC, STAGE1, false>(a, kind, s);
 }
 
 // Launch form and strip (or tile) height for a grid.  A marching block walks
@@ -1282,6 +1296,7 @@ int adjoint_stage(go_domain* d, cudaStream_t s, int rk_step, float dt, const go_
     a.Hi = Hi; a.phi = Hi_pitch / 4;
     a.f_rows = d->d_frows;
     a.status = d->d_status;
+    a.land = d->has_land;
     int kind = GO_ADJ_AUTO;
     adjoint_launch(d, &kind, &a.rows);
     const int fric = go_friction_mode(d);
@@ -1349,6 +1364,7 @@ struct go_adjoint_batch {
     int ntiles = 0;
     int bw = 128, rows = 32;
     int fric = 0;
+    int land = 0;                       // some member's bathymetry may hold land
     int max_fold = 0;
     bool dirty = true;
 };
@@ -1357,7 +1373,10 @@ namespace {
 
 template <int BW, int FRIC, bool STAGE1>
 cudaError_t launch_march_batch(const go_adjoint_batch* b, cudaStream_t s) {
-    cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1><<<b->ntiles, BW, 0, s>>>(b->d_args, b->d_tiles);
+    if (b->land)
+        cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1, true><<<b->ntiles, BW, 0, s>>>(b->d_args, b->d_tiles);
+    else
+        cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1, false><<<b->ntiles, BW, 0, s>>>(b->d_args, b->d_tiles);
     return cudaGetLastError();
 }
 
@@ -1501,12 +1520,15 @@ int go_adjoint_batch_set_member(go_adjoint_batch* b, int m, float dt, const go_s
         a.f_rows = d->d_frows;
         a.status = d->d_status;
         a.rows = b->rows;
+        a.land = d->has_land;
     };
     fill(b->args[2 * m], q_n, q_star, scratch_star, lam);           // stage 0: lam^n = S0^T lam* + lam_qn
     fill(b->args[2 * m + 1], q_star, q_next, lam, scratch_star);    // stage 1: lam* and lam_qn from lam^{n+1}
     b->folds[m] = fold_of(d, scratch_star);
     b->folds[b->n + m] = fold_of(d, lam);
     b->member_set[m] = 1;
+    b->land = 0;
+    for (int i = 0; i < b->n; ++i) b->land = b->land || b->members[i]->has_land;
     b->dirty = true;
     return GO_OK;
 }
