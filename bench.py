@@ -69,6 +69,46 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
+        self.nvml = []          # (sm MHz, max sm MHz, reason names) sampled through NVML
+        self._h = None
+
+    def _handle(self):
+        # NVML handle of the CUDA device (by PCI address; NVML numbers the
+        # GPUs of the machine, CUDA those visible to the process)
+        if self._h is None:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            p = torch.cuda.get_device_properties(self.gpu)
+            try:
+                bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+                self._h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self._h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+        return self._h
+
+    def poll(self, event, period_s=0.0005):
+        """Samples the clocks through NVML until `event` completes: the
+        caller has queued the timed work, so the samples fall inside the
+        timed region however short it is."""
+        try:
+            import pynvml
+            h = self._handle()
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            while True:
+                done = event.query()
+                sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.nvml.append((float(sm), float(smax), [n for n, b in bits.items() if r & b]))
+                if done:
+                    break
+                time.sleep(period_s)
+        except Exception:
+            pass
 
     def start(self):
         try:
@@ -79,15 +119,19 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=5)
-        except Exception:
-            self.proc.kill()
-            out, _ = self.proc.communicate()
+        out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
         sm, smax, reasons = [], [], set()
+        for a, b, r in self.nvml:
+            sm.append(a)
+            smax.append(b)
+            reasons.update(r)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in out.splitlines():
             parts = [x.strip() for x in line.split(",")]
@@ -261,6 +305,7 @@ def run_ours(args, world, rank, local):
     start.record(stream)
     sim._launch_steps(args.steps, np.float32(c.dt), 0.0)
     end.record(stream)
+    sampler.poll(end)
     end.synchronize()
     barrier(world)
     clocks = sampler.stop()
@@ -286,7 +331,7 @@ def run_ours(args, world, rank, local):
     e_end.synchronize()
     barrier(world)
     e_ms = max_over_ranks(e_start.elapsed_time(e_end), world)
-    h2d = sum(int(a.numel()) * 4 for a in host) * 2      # upload fills h0 and h1
+    h2d = sum(int(a.numel()) * 4 for a in host)          # upload fills h0; h1 is a device-side copy
     d2h = sum(int(a.size) * 4 for a in out)
     return dict(c=c, cells=cells, t_ms=t_ms, e_ms=e_ms, clocks=clocks, status=status, h2d=h2d, d2h=d2h,
                 launches=2 * args.steps * sim._domain.stage_launches(), stage_launches=sim._domain.stage_launches())
@@ -843,6 +888,7 @@ def run_reference(args):
     s.record(ref.stream)
     ref.run_steps(args.steps, np.float32(c.dt))
     e.record(ref.stream)
+    sampler.poll(e)
     e.synchronize()
     clocks = sampler.stop()
     return dict(c=c, cells=c.nx * c.ny, t_ms=s.elapsed_time(e), clocks=clocks), None

@@ -124,13 +124,18 @@ class Simulator(object):
             self.drifters.setObservationPosition(otherSim.drifters.getObservationPosition())
 
     def upload(self, eta0, hu0, hv0, eta1=None, hu1=None, hv1=None):
+        """Sets the state (Simulator.py:upload of the reference).  Without a
+        separate second state, the second buffers get a device-side copy of
+        the first instead of a second host-to-device transfer of the same
+        arrays (same contents, half the bus traffic)."""
         self.gpu_data.h0.upload(self.gpu_stream, eta0)
         self.gpu_data.hu0.upload(self.gpu_stream, hu0)
         self.gpu_data.hv0.upload(self.gpu_stream, hv0)
         if eta1 is None:
-            self.gpu_data.h1.upload(self.gpu_stream, eta0)
-            self.gpu_data.hu1.upload(self.gpu_stream, hu0)
-            self.gpu_data.hv1.upload(self.gpu_stream, hv0)
+            for dst, src in ((self.gpu_data.h1, self.gpu_data.h0), (self.gpu_data.hu1, self.gpu_data.hu0),
+                             (self.gpu_data.hv1, self.gpu_data.hv0)):
+                dst.copyBuffer(self.gpu_stream, src)
+                dst.mask = src.mask
         else:
             self.gpu_data.h1.upload(self.gpu_stream, eta1)
             self.gpu_data.hu1.upload(self.gpu_stream, hu1)
