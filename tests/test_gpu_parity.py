@@ -127,6 +127,18 @@ def _drop_in(ctx, case):
     return CDKLM16.CDKLM16(ctx, dt=case.dt, **kw)
 
 
+def _assert_same_under_pair_shape(ctx, dt, kw, steps, expect):
+    """The same run under launch shape 8 (column pairs, 6-row strips, the
+    default of large grids) gives the same bits as `expect`."""
+    sim = CDKLM16.CDKLM16(ctx, dt=dt, **kw)
+    sim._domain.set_launch(8, 6)
+    for _ in range(steps):
+        sim.step(dt)
+    assert sim.status() == 0
+    for a, b in zip(sim.download(), expect):
+        assert np.array_equal(a, b)
+
+
 def test_bump256_1000_steps_vs_reference_kernel_and_fp64(ctx):
     """The parity workload: 256x256 bump, 1000 RK2 steps at CFL 0.7."""
     c = SC.bump256()
@@ -267,7 +279,7 @@ def test_small_beta_friction_wind_periodic_vs_reference_kernel(ctx):
     assert max(e64) <= 2e-2
 
 
-@pytest.mark.parametrize("launch", [(4, 0), (5, 8), (6, 8)])
+@pytest.mark.parametrize("launch", [(4, 0), (5, 8), (6, 8), (8, 6)])
 def test_land_vs_reference_kernel(ctx, launch):
     """Land in the bathymetry (corner depths at the land value 1e20): an
     island and a strip along the south-west coast in the 96x80 config-2
@@ -334,6 +346,7 @@ def test_wind_field_vs_reference_kernel(ctx):
     errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
     print("wind field, 120 steps vs reference kernel:", errs)
     assert max(errs) == 0.0
+    _assert_same_under_pair_shape(ctx, c.dt, kw, c.steps, mine)
 
     # single sub-steps, current != next, wind_t = 0.37
     ref = ref_kernel.RefKernelSim(cfgd, c.eta0, c.hu0, c.hv0, c.Hi, c.dt, c.f, c.beta, c.bc,
@@ -394,6 +407,7 @@ def test_rotated_grid_vs_reference_kernel(ctx, angle):
     errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
     print("angle", angle, "150 steps vs reference kernel:", errs)
     assert max(errs) == 0.0
+    _assert_same_under_pair_shape(ctx, c.dt, kw, c.steps, mine)
 
 
 def test_linear_friction_vs_reference_kernel(ctx):
@@ -422,6 +436,9 @@ def test_linear_friction_vs_reference_kernel(ctx):
     errs = [rel_max(a[2:-2, 2:-2], b[2:-2, 2:-2]) for a, b in zip(mine, theirs)]
     print("linear friction 200 steps vs reference kernel:", errs)
     assert max(errs) == 0.0
+    kw = c.kwargs()
+    kw["linear_friction"] = True
+    _assert_same_under_pair_shape(ctx, c.dt, kw, c.steps, mine)
 
 
 def _open_bc_data(nx, ny, t1, seed):
@@ -603,14 +620,15 @@ def test_small_and_ragged_grids_vs_fp64(ctx, nx, ny, bc, r):
 
 @pytest.mark.parametrize("bc", [(1, 1, 1, 1), (1, 2, 1, 2), (2, 2, 2, 2)])
 def test_every_launch_shape_bit_identical(ctx, bc):
-    """Every launch shape, shape 5 (the read-ahead ring) among them, and
+    """Every launch shape, shapes 5 (the read-ahead ring) and 8 (column
+    pairs with the TMA ring and a separate boundary frame) among them, and
     strip heights that leave a short last strip give bit-identical states.
     The 600 x 520 grid needs several waves of blocks, and strips of 3 rows
     are shorter than the ring, so the ring's refills, empty groups past the
     strip and slot wrap-around all run, at walls and at periodic sides."""
     c = SC.grf(600, ny=520, dx=1000.0, bc=bc, r=3.0e-3, steps=12)
     launches = [(4, 0), (5, 0), (5, 3), (5, 7), (5, 24), (6, 5), (6, 24), (7, 3), (7, 24), (4, 5), (0, 16),
-                (1, 16), (2, 16), (3, 16)]
+                (1, 16), (2, 16), (3, 16), (8, 0), (8, 3), (8, 24)]
     base = None
     for shape, rows in launches:
         sim = _drop_in(ctx, c)
