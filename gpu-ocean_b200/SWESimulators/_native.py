@@ -11,6 +11,11 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libgocean.so")
+# GOCEAN_DEBUG_BOUNDS=1 selects the checked-index build of the stage kernels
+# (lib/libgocean_debug.so: every global access and shared ring read tests its
+# index, flags GO_STATUS_BOUNDS and skips the access when it is outside)
+if os.environ.get("GOCEAN_DEBUG_BOUNDS") == "1":
+    LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libgocean_debug.so")
 
 GO_OK = 0
 GO_BC_WALL = 1
@@ -20,6 +25,7 @@ GO_FRICTION_LINEAR = 1
 GO_STATUS_NONFINITE = 0x1
 GO_STATUS_ADJ_SCOPE = 0x2
 GO_STATUS_TIMEOUT = 0x4
+GO_STATUS_BOUNDS = 0x8
 GO_DEBUG_SKIP_TMA = 0x1
 GO_ERR_INVALID = -1
 GO_ERR_CUDA = -2

@@ -1,4 +1,8 @@
-"""Build the in-tree CUDA library ``lib/libgocean.so`` for sm_100a.
+"""Build the in-tree CUDA library ``lib/libgocean.so`` for sm_100a, and its
+checked-index twin ``lib/libgocean_debug.so`` (the stage-kernel units again
+with -DGO_DEBUG_BOUNDS: every global access and shared ring read of the
+stage kernels tests its index and flags GO_STATUS_BOUNDS instead of going
+outside its array).
 
     python gpu-ocean_b200/build.py [--force]
 
@@ -16,6 +20,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libgocean.so")
+# the checked-index build: the units that instantiate the stage kernels are
+# compiled again with -DGO_DEBUG_BOUNDS and linked with the other objects
+DEBUG_LIB = os.path.join(HERE, "lib", "libgocean_debug.so")
+DEBUG_UNITS = ("batch.cu", "pair_batch_frame.cu", "pair_batch_int_f0.cu", "pair_batch_int_f1.cu",
+               "pair_batch_int_f2.cu", "pair_single_frame.cu", "pair_single_int_f0.cu", "pair_single_int_f1.cu",
+               "pair_single_int_f2.cu", "stage_launch.cu")
 INCLUDE = os.path.join(ROOT, "include")
 
 NVCC_FLAGS = [
@@ -58,9 +68,9 @@ def sources():
 
 
 def up_to_date():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(DEBUG_LIB):
         return False
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(LIB), os.path.getmtime(DEBUG_LIB))
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
@@ -76,18 +86,23 @@ def build(force=False, verbose=False):
     units = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
     work = tempfile.mkdtemp(prefix="gocean_build_")
     try:
-        def compile_one(u):
-            obj = os.path.join(work, u + ".o")
-            cmd = [nvcc] + flags_for(u) + ["-I", INCLUDE, "-c", os.path.join(CSRC, u), "-o", obj]
+        def compile_one(job):
+            u, debug = job
+            obj = os.path.join(work, u + (".debug.o" if debug else ".o"))
+            extra = ["-DGO_DEBUG_BOUNDS"] if debug else []
+            cmd = [nvcc] + flags_for(u) + extra + ["-I", INCLUDE, "-c", os.path.join(CSRC, u), "-o", obj]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
             return obj
-        with ThreadPoolExecutor(max_workers=max(1, min(len(units), os.cpu_count() or 1))) as ex:
-            objs = list(ex.map(compile_one, units))
-        cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + objs + ["-o", LIB + ".tmp"]
-        subprocess.run(cmd, check=True)
-        os.replace(LIB + ".tmp", LIB)
+        jobs = [(u, False) for u in units] + [(u, True) for u in units if u in DEBUG_UNITS]
+        with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+            objs = dict(zip(jobs, ex.map(compile_one, jobs)))
+        for out, pick in ((LIB, lambda u: objs[(u, False)]),
+                          (DEBUG_LIB, lambda u: objs[(u, u in DEBUG_UNITS)])):
+            cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + [pick(u) for u in units]
+            subprocess.run(cmd + ["-o", out + ".tmp"], check=True)
+            os.replace(out + ".tmp", out)
     finally:
         shutil.rmtree(work, ignore_errors=True)
     return LIB

@@ -35,6 +35,7 @@
 #include <cuda.h>
 
 #include "cdklm16_stage.cuh"
+#include "checked.cuh"
 #include "gocean.h"
 
 namespace go {
@@ -327,6 +328,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     const bool wind_field = WIND >= 0 ? (WIND == 1) : (a.wx_cur != nullptr);
 
     const float2 NZ = pb(a.neg_zero);      // -0, opaque to the compiler
+    // array extents of the checked-index build (unused otherwise)
+    const long long xin = ext_in(a), xout = ext_out(a), xqn = ext_qn(a), xhi = ext_hi(a), xf = ext_f(a),
+                    xw = ext_w(a);
     auto pmul = [&](float2 x, float2 y) { return pmul_nz(x, y, NZ); };
     const PDiv<RCP> by2g(k.two_g, NZ);
     const PDiv<RCP> bydx(k.dx, NZ);
@@ -339,10 +343,11 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     int hc0 = cl, hc1 = cl + 1, hc2 = cl + 2;
     // TMA path: the last column block at a periodic or open east side
     // reaches past the array.  Its prime reads those columns past the end of
-    // the row, into the next row of the same allocation (the prime reads Q
-    // rows up to ny and corner rows up to ny+1, below the last ones); the
-    // values feed only lanes that are never written nor read by a written
-    // cell.  The ring's tile loads fill such columns with zeros.
+    // the row, into the following rows of the same allocation (the prime
+    // reads Q rows up to ny and corner rows up to ny+1, and go_prepare_pair
+    // takes the TMA path only when the 4 rows below them hold the overflow);
+    // the values feed only lanes that are never written nor read by a
+    // written cell.  The ring's tile loads fill such columns with zeros.
     if (EDGE) {
         auto mirror_col = [&](int c, int& qc, float& s) {
             qc = min(c, k.nx + 3);
@@ -385,13 +390,13 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         const int rr = mirror_row(r, hv_sgn);
         const size_t o = (size_t)rr * a.pin;
         if (!EDGE && TMA) {   // 8-byte aligned pairs
-            e = __ldg(reinterpret_cast<const float2*>(a.eta_in + o + cl));
-            hu = __ldg(reinterpret_cast<const float2*>(a.hu_in + o + cl));
-            hv = __ldg(reinterpret_cast<const float2*>(a.hv_in + o + cl));
+            e = ldg2(a.eta_in, o + cl, xin, a.status);
+            hu = ldg2(a.hu_in, o + cl, xin, a.status);
+            hv = ldg2(a.hv_in, o + cl, xin, a.status);
         } else {
-            e = make_float2(__ldg(a.eta_in + o + qcx), __ldg(a.eta_in + o + qcy));
-            hu = make_float2(__ldg(a.hu_in + o + qcx), __ldg(a.hu_in + o + qcy));
-            hv = make_float2(__ldg(a.hv_in + o + qcx), __ldg(a.hv_in + o + qcy));
+            e = make_float2(ldg1(a.eta_in, o + qcx, xin, a.status), ldg1(a.eta_in, o + qcy, xin, a.status));
+            hu = make_float2(ldg1(a.hu_in, o + qcx, xin, a.status), ldg1(a.hu_in, o + qcy, xin, a.status));
+            hv = make_float2(ldg1(a.hv_in, o + qcx, xin, a.status), ldg1(a.hv_in, o + qcy, xin, a.status));
         }
         if (EDGE) {
             hu = make_float2(hu.x * husx, hu.y * husy);
@@ -404,14 +409,14 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     };
     // corners of corner row r: Ha = (cl, cl+1), Hb = (cl+1, cl+2)
     auto load_h = [&](int r, float2& Ha, float2& Hb) {
-        const float* row = a.Hi + (size_t)r * a.phi;
+        const long long o = (long long)r * a.phi;
         float h2;
         if (!EDGE && TMA) {
-            Ha = __ldg(reinterpret_cast<const float2*>(row + cl));
-            h2 = __ldg(row + cl + 2);
+            Ha = ldg2(a.Hi, o + cl, xhi, a.status);
+            h2 = ldg1(a.Hi, o + cl + 2, xhi, a.status);
         } else {
-            Ha = make_float2(__ldg(row + hc0), __ldg(row + hc1));
-            h2 = __ldg(row + hc2);
+            Ha = make_float2(ldg1(a.Hi, o + hc0, xhi, a.status), ldg1(a.Hi, o + hc1, xhi, a.status));
+            h2 = ldg1(a.Hi, o + hc2, xhi, a.status);
         }
         Hb = make_float2(Ha.y, h2);
         Ha = land_corner(Ha);
@@ -559,8 +564,8 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
         load_h(r0, A.Ha, A.Hb);
         load_h(r0 + 1, B.Ha, B.Hb);
         load_h(r0 + 2, C.Ha, C.Hb);
-        Pm2.f = __ldg(frow + r0 - 2); Pm1.f = __ldg(frow + r0 - 1);
-        A.f = __ldg(frow + r0); B.f = __ldg(frow + r0 + 1);
+        Pm2.f = ldg1(frow, r0 - 2, xf, a.status); Pm1.f = ldg1(frow, r0 - 1, xf, a.status);
+        A.f = ldg1(frow, r0, xf, a.status); B.f = ldg1(frow, r0 + 1, xf, a.status);
         load_q(r0 - 2, e, hu, hv); to_cell(e, hu, hv, Pm2, Pm1);
         load_q(r0 - 1, e, hu, hv); to_cell(e, hu, hv, Pm1, A);
         load_q(r0, e, hu, hv);     to_cell(e, hu, hv, A, B);
@@ -582,7 +587,7 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
     // ---- inputs of output row j: Q row j+2, corner row j+3, Q^n row j, f(j+2)
     float2 nq_e = pb(0.0f), nq_hu = pb(0.0f), nq_hv = pb(0.0f), nHa = pb(0.0f), nHb = pb(0.0f);
     float2 nqn_e = pb(0.0f), nqn_hu = pb(0.0f), nqn_hv = pb(0.0f);
-    float nf = __ldg(frow + r0 + 2);
+    float nf = ldg1(frow, r0 + 2, xf, a.status);
     const bool use_ring = TMA && !EDGE;
     auto gload_row = [&](int jj) {   // global loads of the inputs of output row jj (one row ahead)
         if (jj < r1) {
@@ -590,9 +595,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
             load_h(jj + 3, nHa, nHb);
             if (stage1 && writer) {
                 const size_t o = (size_t)jj * a.pqn;
-                nqn_e = make_float2(a.qn_eta[o + cl], wr_y ? a.qn_eta[o + cl + 1] : 0.0f);
-                nqn_hu = make_float2(a.qn_hu[o + cl], wr_y ? a.qn_hu[o + cl + 1] : 0.0f);
-                nqn_hv = make_float2(a.qn_hv[o + cl], wr_y ? a.qn_hv[o + cl + 1] : 0.0f);
+                nqn_e = make_float2(ld1(a.qn_eta, o + cl, xqn, a.status), wr_y ? ld1(a.qn_eta, o + cl + 1, xqn, a.status) : 0.0f);
+                nqn_hu = make_float2(ld1(a.qn_hu, o + cl, xqn, a.status), wr_y ? ld1(a.qn_hu, o + cl + 1, xqn, a.status) : 0.0f);
+                nqn_hv = make_float2(ld1(a.qn_hv, o + cl, xqn, a.status), wr_y ? ld1(a.qn_hv, o + cl + 1, xqn, a.status) : 0.0f);
             }
         }
     };
@@ -666,26 +671,31 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
             if (ri == 0) wait_chunk(c);
             const float* base = chunk_ptr(chunk_base + (unsigned)c);
             const int o = ri * 2 * T + 2 * t;
-            q_e = *reinterpret_cast<const float2*>(base + o);
-            q_hu = *reinterpret_cast<const float2*>(base + Q_ + o);
-            q_hv = *reinterpret_cast<const float2*>(base + 2 * Q_ + o);
-            const float* hrow = base + 3 * Q_ + ri * (2 * T + 4) + 2 * t;
-            Ha3 = *reinterpret_cast<const float2*>(hrow);
-            Hb3 = make_float2(Ha3.y, hrow[2]);
+            // shared reads of the chunk: Q rows of Q_ floats, the corner row of H_
+            auto sld2 = [&](const float* p, int i, int extent) {
+                return idx_ok(i, 2, extent, a.status) ? *reinterpret_cast<const float2*>(p + i)
+                                                      : make_float2(0.0f, 0.0f);
+            };
+            q_e = sld2(base, o, Q_);
+            q_hu = sld2(base + Q_, o, Q_);
+            q_hv = sld2(base + 2 * Q_, o, Q_);
+            const int oh = ri * (2 * T + 4) + 2 * t;
+            Ha3 = sld2(base + 3 * Q_, oh, H_);
+            Hb3 = make_float2(Ha3.y, idx_ok(oh + 2, 1, H_, a.status) ? base[3 * Q_ + oh + 2] : 0.0f);
             Ha3 = land_corner(Ha3);
             Hb3 = land_corner(Hb3);
             if (stage1) {
                 const float* nb = base + 3 * Q_ + H_;
-                qn_e = *reinterpret_cast<const float2*>(nb + o);
-                qn_hu = *reinterpret_cast<const float2*>(nb + Q_ + o);
-                qn_hv = *reinterpret_cast<const float2*>(nb + 2 * Q_ + o);
+                qn_e = sld2(nb, o, Q_);
+                qn_hu = sld2(nb + Q_, o, Q_);
+                qn_hv = sld2(nb + 2 * Q_, o, Q_);
             }
-            nf = __ldg(frow + min(j + 3, k.ny + 3));
+            nf = ldg1(frow, min(j + 3, k.ny + 3), xf, a.status);
         } else {
             q_e = nq_e; q_hu = nq_hu; q_hv = nq_hv;
             Ha3 = nHa; Hb3 = nHb;
             qn_e = nqn_e; qn_hu = nqn_hu; qn_hv = nqn_hv;
-            nf = __ldg(frow + min(j + 3, k.ny + 3));
+            nf = ldg1(frow, min(j + 3, k.ny + 3), xf, a.status);
             gload_row(j + 1);
         }
         // corner row j+3 goes into the slot of row j+2's north corners: R2
@@ -856,8 +866,8 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
                 if (wind_field) {
                     const size_t o = (size_t)(j - 2) * a.pw + (cl - 2);
                     auto wl = [&](const float* cur, const float* nxt, size_t oo) {
-                        const float xn = __ldg(nxt + oo);
-                        const float xc = (cur == nxt) ? xn : __ldg(cur + oo);
+                        const float xn = ldg1(nxt, oo, xw, a.status);
+                        const float xc = (cur == nxt) ? xn : ldg1(cur, oo, xw, a.status);
                         return a.wind_t * xn + (1.0f - a.wind_t) * xc;
                     };
                     Xv = make_float2(wl(a.wx_cur, a.wx_next, o), wr_y ? wl(a.wx_cur, a.wx_next, o + 1) : 0.0f);
@@ -958,16 +968,20 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
             const size_t o = (size_t)j * a.pout + cl;
             if (!EDGE && TMA) {
                 if (wr_y) {
-                    *reinterpret_cast<float2*>(a.eta_out + o) = ne;
-                    *reinterpret_cast<float2*>(a.hu_out + o) = nhu;
-                    *reinterpret_cast<float2*>(a.hv_out + o) = nhv;
+                    st2(a.eta_out, o, ne, xout, a.status);
+                    st2(a.hu_out, o, nhu, xout, a.status);
+                    st2(a.hv_out, o, nhv, xout, a.status);
                 } else {   // the last written column of the grid is this pair's first
-                    a.eta_out[o] = ne.x; a.hu_out[o] = nhu.x; a.hv_out[o] = nhv.x;
+                    st1(a.eta_out, o, ne.x, xout, a.status);
+                    st1(a.hu_out, o, nhu.x, xout, a.status);
+                    st1(a.hv_out, o, nhv.x, xout, a.status);
                 }
             } else {
                 auto put = [&](int col, float e1, float u1, float v1) {
                     const size_t oo = (size_t)j * a.pout + col;
-                    a.eta_out[oo] = e1; a.hu_out[oo] = u1; a.hv_out[oo] = v1;
+                    st1(a.eta_out, oo, e1, xout, a.status);
+                    st1(a.hu_out, oo, u1, xout, a.status);
+                    st1(a.hv_out, oo, v1, xout, a.status);
                     if (EDGE) {
                         // periodic ghost images (the reference's BC kernels after the stage)
                         int rows_img[2] = {-1, -1}, cols_img[2] = {-1, -1};
@@ -986,7 +1000,9 @@ __device__ __forceinline__ void pair_strip(const StageArgs& a, const PairMaps& m
                                 for (int ci = 0; ci < 3; ++ci) {
                                     if ((ri2 == 0 && ci == 0) || rr[ri2] < 0 || cc[ci] < 0) continue;
                                     const size_t o2 = (size_t)rr[ri2] * a.pout + cc[ci];
-                                    a.eta_out[o2] = e1; a.hu_out[o2] = u1; a.hv_out[o2] = v1;
+                                    st1(a.eta_out, o2, e1, xout, a.status);
+                                    st1(a.hu_out, o2, u1, xout, a.status);
+                                    st1(a.hv_out, o2, v1, xout, a.status);
                                 }
                             }
                         }

@@ -40,6 +40,7 @@
 #pragma once
 
 #include "cdklm16_device.cuh"
+#include "checked.cuh"
 
 namespace go {
 
@@ -292,6 +293,9 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
     const float* __restrict__ hv_in = a.hv_in;
     const float* __restrict__ Hi = a.Hi;
     const float* __restrict__ frow = a.f_rows;
+    // array extents of the checked-index build (unused otherwise)
+    const long long xin = ext_in(a), xout = ext_out(a), xqn = ext_qn(a), xhi = ext_hi(a), xf = ext_f(a),
+                    xw = ext_w(a);
 
     // wall ghost rows mirror the interior with hv odd
     auto mirror_row = [&](int r, float& hv_sgn) {
@@ -307,15 +311,15 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
         float hv_sgn;
         const int rr = mirror_row(r, hv_sgn);
         const size_t o = (size_t)rr * a.pin + qc;
-        e = __ldg(eta_in + o);
-        hu = __ldg(hu_in + o);
-        hv = __ldg(hv_in + o);
+        e = ldg1(eta_in, o, xin, a.status);
+        hu = ldg1(hu_in, o, xin, a.status);
+        hv = ldg1(hv_in, o, xin, a.status);
         if (EDGE) { hu *= hu_sgn; hv *= hv_sgn; }
     };
     auto load_h = [&](int r, float& ha, float& hb) {
         const size_t o = (size_t)r * a.phi;
-        ha = __ldg(Hi + o + hca);
-        hb = __ldg(Hi + o + hcb);
+        ha = ldg1(Hi, o + hca, xhi, a.status);
+        hb = ldg1(Hi, o + hcb, xhi, a.status);
         if (LAND) { ha = corner(ha, k); hb = corner(hb, k); }
     };
     auto to_cell = [&](float e, float hu, float hv, float ha0, float hb0, float ha1, float hb1) {
@@ -382,8 +386,8 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
         load_q(r0, e, hu, hv);     P0 = to_cell(e, hu, hv, Ha0, Hb0, Ha1, Hb1);
         load_q(r0 + 1, e, hu, hv); P1 = to_cell(e, hu, hv, Ha1, Hb1, Ha2, Hb2);
     }
-    const float f_m2 = __ldg(frow + r0 - 2), f_m1 = __ldg(frow + r0 - 1);
-    float f0 = __ldg(frow + r0), f1 = __ldg(frow + r0 + 1);
+    const float f_m2 = ldg1(frow, r0 - 2, xf, a.status), f_m1 = ldg1(frow, r0 - 1, xf, a.status);
+    float f0 = ldg1(frow, r0, xf, a.status), f1 = ldg1(frow, r0 + 1, xf, a.status);
     const float fu_m2 = fu_of(Pm2, r0 - 2, f_m2);
     const float fu_m1 = fu_of(Pm1, r0 - 1, f_m1);
     float fu0 = fu_of(P0, r0, f0);
@@ -423,18 +427,22 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
         if constexpr (D > 0) {
             if (jj < r1) {
                 float hv_sgn;
+                // checked build: a copy whose source lies outside its array is skipped
+                auto cpa = [&](float* dst, const float* src, size_t i, long long extent) {
+                    if (idx_ok((long long)i, 1, extent, a.status)) cp_async4(dst, src + i);
+                };
                 const size_t o = (size_t)mirror_row(jj + 2, hv_sgn) * a.pin + qc;
-                cp_async4(&sb.ring.q[slot][t].x, eta_in + o);
-                cp_async4(&sb.ring.q[slot][t].y, hu_in + o);
-                cp_async4(&sb.ring.q[slot][t].z, hv_in + o);
+                cpa(&sb.ring.q[slot][t].x, eta_in, o, xin);
+                cpa(&sb.ring.q[slot][t].y, hu_in, o, xin);
+                cpa(&sb.ring.q[slot][t].z, hv_in, o, xin);
                 const size_t oh = (size_t)(jj + 3) * a.phi;
-                cp_async4(&sb.ring.h[slot][t].x, Hi + oh + hca);
-                cp_async4(&sb.ring.h[slot][t].y, Hi + oh + hcb);
+                cpa(&sb.ring.h[slot][t].x, Hi, oh + hca, xhi);
+                cpa(&sb.ring.h[slot][t].y, Hi, oh + hcb, xhi);
                 if (stage1 && writer) {
                     const size_t on = (size_t)jj * a.pqn + cl;
-                    cp_async4(&sb.ring.qn[slot][t].x, a.qn_eta + on);
-                    cp_async4(&sb.ring.qn[slot][t].y, a.qn_hu + on);
-                    cp_async4(&sb.ring.qn[slot][t].z, a.qn_hv + on);
+                    cpa(&sb.ring.qn[slot][t].x, a.qn_eta, on, xqn);
+                    cpa(&sb.ring.qn[slot][t].y, a.qn_hu, on, xqn);
+                    cpa(&sb.ring.qn[slot][t].z, a.qn_hv, on, xqn);
                 }
             }
             cp_async_commit();
@@ -444,7 +452,7 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
     // prefetch row r0+2 (Q), corner row r0+3, f(r0+2) and, for stage 1, Q^n(r0)
     float nq_e = 0.0f, nq_hu = 0.0f, nq_hv = 0.0f, nha = 0.0f, nhb = 0.0f, nf;
     float nqn_e = 0.0f, nqn_hu = 0.0f, nqn_hv = 0.0f;
-    nf = __ldg(frow + r0 + 2);
+    nf = ldg1(frow, r0 + 2, xf, a.status);
     int slot = 0;
     if constexpr (D > 0) {
 #pragma unroll
@@ -454,7 +462,9 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
         load_h(r0 + 3, nha, nhb);
         if (stage1 && writer) {
             const size_t o = (size_t)r0 * a.pqn + cl;
-            nqn_e = a.qn_eta[o]; nqn_hu = a.qn_hu[o]; nqn_hv = a.qn_hv[o];
+            nqn_e = ld1(a.qn_eta, o, xqn, a.status);
+            nqn_hu = ld1(a.qn_hu, o, xqn, a.status);
+            nqn_hv = ld1(a.qn_hv, o, xqn, a.status);
         }
     }
     const bool col_img = EDGE && (k.bcE == kPeriodic) && (cl < 4 || cl >= k.nx);
@@ -492,17 +502,19 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
                 qn_e = qn.x; qn_hu = qn.y; qn_hv = qn.z;
             }
             slot = (slot == D) ? 0 : slot + 1;
-            nf = __ldg(frow + min(j + 3, k.ny + 3));
+            nf = ldg1(frow, min(j + 3, k.ny + 3), xf, a.status);
         } else {
             Ha3 = nha; Hb3 = nhb;
             q_e = nq_e; q_hu = nq_hu; q_hv = nq_hv;
             qn_e = nqn_e; qn_hu = nqn_hu; qn_hv = nqn_hv;
             load_q(min(j + 3, r1 + 1), nq_e, nq_hu, nq_hv);
             load_h(min(j + 4, r1 + 2), nha, nhb);
-            nf = __ldg(frow + min(j + 3, k.ny + 3));
+            nf = ldg1(frow, min(j + 3, k.ny + 3), xf, a.status);
             if (stage1 && writer && j + 1 < r1) {
                 const size_t o = (size_t)(j + 1) * a.pqn + cl;
-                nqn_e = a.qn_eta[o]; nqn_hu = a.qn_hu[o]; nqn_hv = a.qn_hv[o];
+                nqn_e = ld1(a.qn_eta, o, xqn, a.status);
+                nqn_hu = ld1(a.qn_hu, o, xqn, a.status);
+                nqn_hv = ld1(a.qn_hv, o, xqn, a.status);
             }
         }
         const Cell P2 = to_cell(q_e, q_hu, q_hv, Ha2, Hb2, Ha3, Hb3);
@@ -629,9 +641,9 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
                 if (WIND_FIELD) {
                     // one load when the current and next fields are one array
                     const size_t o = (size_t)(j - 2) * a.pw + (cl - 2);
-                    const float xn = __ldg(a.wx_next + o), yn = __ldg(a.wy_next + o);
-                    const float xc = (a.wx_cur == a.wx_next) ? xn : __ldg(a.wx_cur + o);
-                    const float yc = (a.wy_cur == a.wy_next) ? yn : __ldg(a.wy_cur + o);
+                    const float xn = ldg1(a.wx_next, o, xw, a.status), yn = ldg1(a.wy_next, o, xw, a.status);
+                    const float xc = (a.wx_cur == a.wx_next) ? xn : ldg1(a.wx_cur, o, xw, a.status);
+                    const float yc = (a.wy_cur == a.wy_next) ? yn : ldg1(a.wy_cur, o, xw, a.status);
                     X = a.wind_t * xn + (1.0f - a.wind_t) * xc;
                     Y = a.wind_t * yn + (1.0f - a.wind_t) * yc;
                 } else {
@@ -693,7 +705,9 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
             if (!isfinite(ne + nhu + nhv) && a.status) atomicOr(a.status, 1u);
 
             const size_t o = (size_t)j * a.pout + cl;
-            a.eta_out[o] = ne; a.hu_out[o] = nhu; a.hv_out[o] = nhv;
+            st1(a.eta_out, o, ne, xout, a.status);
+            st1(a.hu_out, o, nhu, xout, a.status);
+            st1(a.hv_out, o, nhv, xout, a.status);
             if (EDGE) {
                 // periodic ghost images (the reference's BC kernels after the stage)
                 const bool row_img = (k.bcN == kPeriodic) && (j < 4 || j >= k.ny);
@@ -713,7 +727,9 @@ __device__ __forceinline__ void stage_strip(const StageArgs& a, const float dt, 
                         for (int ci = 0; ci < 3; ++ci) {
                             if ((ri == 0 && ci == 0) || rr[ri] < 0 || cc[ci] < 0) continue;
                             const size_t oo = (size_t)rr[ri] * a.pout + cc[ci];
-                            a.eta_out[oo] = ne; a.hu_out[oo] = nhu; a.hv_out[oo] = nhv;
+                            st1(a.eta_out, oo, ne, xout, a.status);
+                            st1(a.hu_out, oo, nhu, xout, a.status);
+                            st1(a.hv_out, oo, nhv, xout, a.status);
                         }
                     }
                 }

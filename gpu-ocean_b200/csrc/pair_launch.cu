@@ -104,6 +104,14 @@ int go_prepare_pair(const StageArgs& a, PairMapParams* mp, bool* tma) {
     }
     if (ok) ok = aligned(a.Hi, 16) && (a.phi * 4) % 16 == 0 &&
                  encode(&mp->h, a.Hi, nx + 5, ny + 5, a.phi, 2 * T + 4, kPairRingRows);
+    // The region's prime reads each block's 2T (+2 corner) columns straight
+    // from global memory, past the end of a row into the following rows for
+    // the last column block; its last Q row is ny and its last corner row
+    // ny + 1, so the arrays' 4 rows below them must hold that overflow.  On
+    // grids narrower than that (nx below about 37 columns) every block takes
+    // the boundary path, whose loads are clamped per lane.
+    const int last_cl0 = ((nx + (2 * T - 4) - 1) / (2 * T - 4) - 1) * (2 * T - 4);
+    if (ok) ok = last_cl0 + 2 * T <= 4 * a.pin && last_cl0 + 2 * T + 1 <= 4 * a.phi;
     *tma = ok;
     return GO_OK;
 }

@@ -52,6 +52,9 @@ extern "C" {
                                    covered no land or shallow cells */
 #define GO_STATUS_TIMEOUT 0x4u   /* a bounded wait in a step kernel gave up
                                    (a TMA tile that never arrived) */
+#define GO_STATUS_BOUNDS 0x8u    /* the checked-index build (lib/libgocean_debug.so,
+                                   built with -DGO_DEBUG_BOUNDS) met a global or
+                                   shared index outside its array and skipped it */
 
 typedef struct go_domain go_domain;
 

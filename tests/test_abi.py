@@ -38,6 +38,19 @@ def test_library_exports_every_declared_symbol(lib):
         assert hasattr(lib, name), name
 
 
+def test_checked_index_library_exports_every_declared_symbol(lib):
+    """lib/libgocean_debug.so (the stage kernels built with
+    -DGO_DEBUG_BOUNDS) is a drop-in for lib/libgocean.so."""
+    path = os.path.join(ROOT, "gpu-ocean_b200", "lib", "libgocean_debug.so")
+    if not os.path.exists(path):
+        import subprocess
+        import sys
+        subprocess.run([sys.executable, os.path.join(ROOT, "gpu-ocean_b200", "build.py")], check=True)
+    dbg = ctypes.CDLL(path)
+    for name in declared_functions():
+        assert hasattr(dbg, name), name
+
+
 def test_version_and_empty_error(lib):
     assert b"sm_100a" in lib.go_version()
     assert isinstance(lib.go_last_error(), bytes)
