@@ -50,17 +50,26 @@ UNIT_FLAGS["open_boundaries.cu"] = UNIT_FLAGS["drifters.cu"]
 # flush to zero, approximate division and square root (already set), FMA
 # contraction and the fast intrinsics for logf, expf, sinf, cosf
 UNIT_FLAGS["ocean_noise.cu"] = {"--fmad=false": "--use_fast_math"}
+# Flags added for some units.  The single-domain column-pair region kernel is
+# allocated at ptxas register-usage level 10 (the same arithmetic, so the same
+# bits): measured on a B200 at 4096^2, 579-584 us per RK2 step against 588-589
+# at the default level, and 623-629 at levels 0 and 2; the batched kernel was
+# 0.2% slower at level 10 and stays at the default.
+UNIT_EXTRA = {u: ["-Xptxas", "--register-usage-level=10"]
+              for u in ("pair_single_int_f0.cu", "pair_single_int_f1.cu", "pair_single_int_f2.cu")}
 
 
 def flags_for(unit):
     """nvcc flags of one source unit; GOCEAN_NVCC_FLAGS appends more (e.g.
     -DGO_PACKED_PAIRS for the packed-sum build of the stage kernel)."""
     sub = UNIT_FLAGS.get(unit, {})
-    return [sub.get(f, f) for f in NVCC_FLAGS] + os.environ.get("GOCEAN_NVCC_FLAGS", "").split()
+    return ([sub.get(f, f) for f in NVCC_FLAGS] + UNIT_EXTRA.get(unit, [])
+            + os.environ.get("GOCEAN_NVCC_FLAGS", "").split())
 
 
 def sources():
-    out = [os.path.join(INCLUDE, "gocean.h")]
+    # this file too: its flags are part of what the libraries are built from
+    out = [os.path.join(INCLUDE, "gocean.h"), os.path.abspath(__file__)]
     for f in sorted(os.listdir(CSRC)):
         if f.endswith((".cu", ".cuh", ".h")):
             out.append(os.path.join(CSRC, f))
