@@ -48,6 +48,33 @@ namespace {
 constexpr int HALO = 3;
 constexpr int NT = 256;
 
+// Programmatic dependent launch of the stage-adjoint and fold kernels
+// (launch_pdl): the blocks of such a grid may be scheduled while the kernel
+// before it on the stream is still running.  pdl_enter is the first statement
+// of each of these kernels: griddepcontrol.wait holds the block until the
+// previous grid has completed and its writes are visible (it returns at once
+// for a launch without the attribute); launch_dependents then lets the next
+// launch on the stream be scheduled once every block of this grid has started.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 struct AdjArgs {
     Scheme k;
     float dt;
@@ -260,6 +287,7 @@ __device__ __forceinline__ bool br_has(uint32_t b) { return (b >> 8) & 1; }
 
 template <int FRIC, bool STAGE1, int TX, int TY, int MINB, bool LAND>
 __global__ void __launch_bounds__(NT, MINB) cdklm_adjoint_stage_kernel(const AdjArgs a) {
+    pdl_enter();
     using D = TileDims<TX, TY>;
     constexpr int RX = D::RX, RY = D::RY, RXS = D::RXS, NXR = D::NXR, NYC = D::NYC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1110,6 +1138,7 @@ __device__ __forceinline__ void adjoint_march_block(const AdjArgs& a, int bx, in
 template <int BW, int FRIC, bool STAGE1, bool LAND>
 __global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_kernel(const AdjArgs a) {
     __shared__ MarchBufs<BW> sb;
+    pdl_enter();
     adjoint_march_block<BW, FRIC, STAGE1, LAND>(a, blockIdx.x, blockIdx.y, sb);
 }
 
@@ -1119,6 +1148,7 @@ template <int BW, int FRIC, bool STAGE1, bool LAND>
 __global__ void __launch_bounds__(BW, 512 / BW) cdklm_adjoint_march_batch_kernel(
         const AdjArgs* __restrict__ args, const int4* __restrict__ tiles) {
     __shared__ MarchBufs<BW> sb;
+    pdl_enter();
     const int4 tile = tiles[blockIdx.x];
     adjoint_march_block<BW, FRIC, STAGE1, LAND>(args[2 * tile.x + (STAGE1 ? 1 : 0)], tile.y, tile.z, sb);
 }
@@ -1137,10 +1167,12 @@ __device__ __forceinline__ void adj_fold_cell(float* e, float* u, float* v, int 
 
 __global__ void k_adj_fold(float* e, float* u, float* v, int p, int nx, int ny, int bcN, int bcE, int bcS,
                            int bcW) {
+    pdl_enter();
     adj_fold_cell(e, u, v, p, nx, ny, bcN, bcE, bcS, bcW, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __global__ void k_adj_fold_batch(const FoldMember* __restrict__ members) {
+    pdl_enter();
     const FoldMember M = members[blockIdx.y];
     adj_fold_cell(M.e, M.u, M.v, M.p, M.nx, M.ny, M.bcN, M.bcE, M.bcS, M.bcW, blockIdx.x * blockDim.x + threadIdx.x);
 }
@@ -1201,8 +1233,7 @@ cudaError_t launch_adj_tile(const AdjArgs& a, cudaStream_t s) {
         if (dev < 64) attr_set |= 1ull << dev;
     }
     const dim3 grid((a.k.nx + 4 + TX - 1) / TX, (a.k.ny + 4 + TY - 1) / TY);
-    cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB, LAND><<<grid, NT, bytes, s>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(cdklm_adjoint_stage_kernel<FRIC, STAGE1, TX, TY, MINB, LAND>, grid, dim3(NT), (size_t)bytes, s, a);
 }
 
 // Tile form: 32-column tiles of a.rows rows (8, 12 or 16; CTAs per SM by
@@ -1217,8 +1248,7 @@ cudaError_t launch_adj(const AdjArgs& a, cudaStream_t s) {
 template <int BW, int FRIC, bool STAGE1, bool LAND>
 cudaError_t launch_march(const AdjArgs& a, cudaStream_t s) {
     const dim3 grid((a.k.nx + 4 + BW - 7) / (BW - 6), (a.k.ny + 4 + a.rows - 1) / a.rows);
-    cdklm_adjoint_march_kernel<BW, FRIC, STAGE1, LAND><<<grid, BW, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(cdklm_adjoint_march_kernel<BW, FRIC, STAGE1, LAND>, grid, dim3(BW), 0, s, a);
 }
 
 // Kernels without the land branches (corners read as they are, the cell
@@ -1269,9 +1299,8 @@ void adjoint_launch(const go_domain* d, int* kind, int* rows) {
 cudaError_t launch_fold(const go_domain* d, const go_state* l, cudaStream_t s) {
     const int nx = d->k.nx, ny = d->k.ny;
     const int n = 4 * nx + 4 * (ny - 4 > 0 ? ny - 4 : 0);
-    k_adj_fold<<<(n + 255) / 256, 256, 0, s>>>(l->eta, l->hu, l->hv, l->pitch / 4, nx, ny, d->k.bcN, d->k.bcE,
-                                               d->k.bcS, d->k.bcW);
-    return cudaGetLastError();
+    return launch_pdl(k_adj_fold, dim3((n + 255) / 256), dim3(256), 0, s, l->eta, l->hu, l->hv, (int)(l->pitch / 4), nx,
+                      ny, d->k.bcN, d->k.bcE, d->k.bcS, d->k.bcW);
 }
 
 int check_state(const go_state* s, int min_floats, const char* what) {
@@ -1374,10 +1403,10 @@ namespace {
 template <int BW, int FRIC, bool STAGE1>
 cudaError_t launch_march_batch(const go_adjoint_batch* b, cudaStream_t s) {
     if (b->land)
-        cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1, true><<<b->ntiles, BW, 0, s>>>(b->d_args, b->d_tiles);
-    else
-        cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1, false><<<b->ntiles, BW, 0, s>>>(b->d_args, b->d_tiles);
-    return cudaGetLastError();
+        return launch_pdl(cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1, true>, dim3(b->ntiles), dim3(BW), 0, s,
+                          (const AdjArgs*)b->d_args, (const int4*)b->d_tiles);
+    return launch_pdl(cdklm_adjoint_march_batch_kernel<BW, FRIC, STAGE1, false>, dim3(b->ntiles), dim3(BW), 0, s,
+                      (const AdjArgs*)b->d_args, (const int4*)b->d_tiles);
 }
 
 template <bool STAGE1>
@@ -1542,13 +1571,11 @@ int go_adjoint_batch_step(go_adjoint_batch* b, void* stream) {
     const dim3 fg((b->max_fold + 255) / 256, b->n);
     cudaError_t e = batch_stage<true>(b, s);
     if (e == cudaSuccess) {
-        k_adj_fold_batch<<<fg, 256, 0, s>>>(b->d_folds);
-        e = cudaGetLastError();
+        e = launch_pdl(k_adj_fold_batch, fg, dim3(256), 0, s, (const FoldMember*)b->d_folds);
     }
     if (e == cudaSuccess) e = batch_stage<false>(b, s);
     if (e == cudaSuccess) {
-        k_adj_fold_batch<<<fg, 256, 0, s>>>(b->d_folds + b->n);
-        e = cudaGetLastError();
+        e = launch_pdl(k_adj_fold_batch, fg, dim3(256), 0, s, (const FoldMember*)(b->d_folds + b->n));
     }
     if (e != cudaSuccess) return go_fail(GO_ERR_CUDA, "adjoint batch launch failed: %s", cudaGetErrorString(e));
     return GO_OK;
