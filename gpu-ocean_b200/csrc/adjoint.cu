@@ -1275,17 +1275,20 @@ cudaError_t launch_any(const AdjArgs& a, int kind, cudaStream_t s) {
 void adjoint_launch(const go_domain* d, int* kind, int* rows) {
     int kd = d->adj_kind;
     const int nx = d->k.nx + 4, ny = d->k.ny + 4;
+    // B200, us per stage adjoint with dependent launches, tiles of 8 / 16 rows
+    // against the 64-column marching form: 512^2 37.5 / 43.4 / 58.0, 640^2
+    // 52.5 / 50.0 / 67.0, 768^2 71.1 / 69.3 / 100.8, 1024^2 (16 rows) 115.0
+    // against 114.4.  The tile form runs up to about 1000^2 cells, with 8-row
+    // tiles (more, smaller CTAs: fewer partial waves) up to about 590^2.
+    // Marching blocks of 64 columns up to 1024 interior columns (1024^2:
+    // 114.4 us against 124 with 128-column blocks).
     if (kd == GO_ADJ_AUTO) {
-        if ((long long)nx * ny < 300000LL) kd = GO_ADJ_TILE;
-        else kd = (nx <= 1024) ? GO_ADJ_MARCH64 : GO_ADJ_MARCH128;
+        if ((long long)nx * ny < 1000000LL) kd = GO_ADJ_TILE;
+        else kd = (d->k.nx <= 1024) ? GO_ADJ_MARCH64 : GO_ADJ_MARCH128;
     }
     int r = d->adj_rows;
     if (r <= 0 && kd == GO_ADJ_TILE) {
-        // B200, us per stage adjoint at 512^2 with 16 / 12 / 8-row tiles:
-        // 47.3 / 45.2 / 43.2 (the smaller tiles fill the SMs in fewer
-        // partial waves); at 1024^2 the 16-row tiles are fastest (118 / 127 /
-        // 125), but that grid runs the marching form
-        r = 8;
+        r = ((long long)nx * ny < 350000LL) ? 8 : 16;
     } else if (r <= 0) {
         const int bw = (kd == GO_ADJ_MARCH64) ? 64 : 128;
         const long long target = (long long)((nx + bw - 7) / (bw - 6)) * ny / 600;

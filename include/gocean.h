@@ -440,12 +440,12 @@ typedef struct go_state {
 } go_state;
 
 /* Launch form of the adjoint stage: GO_ADJ_TILE (one block per tile of 32
- * columns and rows_per_strip = 8, 12 or 16 rows, 0 = 8; the forward is
- * recomputed with a 3-cell halo), GO_ADJ_MARCH64 / GO_ADJ_MARCH128
- * (one thread per column, blocks of 64 or 128 columns marching up strips of
- * rows_per_strip rows, 0 = automatic), GO_ADJ_AUTO (the default: the tile
- * form below ~300 k cells, where marching strips cannot fill the GPU, else
- * marching, 64 up to 1024 columns).  The forms agree to FP32 rounding. */
+ * columns and rows_per_strip = 8, 12 or 16 rows, 0 = automatic: 8 below
+ * ~350 k cells, else 16; the forward is recomputed with a 3-cell halo),
+ * GO_ADJ_MARCH64 / GO_ADJ_MARCH128 (one thread per column, blocks of 64 or
+ * 128 columns marching up strips of rows_per_strip rows, 0 = automatic),
+ * GO_ADJ_AUTO (the default: the tile form below ~1 M cells, else marching,
+ * 64 up to 1024 columns).  The forms agree to FP32 rounding. */
 #define GO_ADJ_AUTO 0
 #define GO_ADJ_TILE 1
 #define GO_ADJ_MARCH64 2
